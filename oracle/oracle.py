@@ -1,0 +1,223 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle.so): TEST INFRASTRUCTURE ONLY.
+
+The oracle restates the reference engine's spectral-centrality path in C++
+(see oracle.hpp). Tests, the smoke check and the benchmark's CPU-baseline leg
+use it as the checker; the product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+ERR_LEN = 1024
+
+_lib = None
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def build(force: bool = False) -> Path:
+    """Compiles the oracle with its Makefile (g++)."""
+    if force or not LIB_PATH.exists():
+        subprocess.run(["make", "-C", str(HERE)] + (["-B"] if force else []), check=True,
+                       capture_output=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    build()
+    L = ctypes.CDLL(str(LIB_PATH))
+    i32, i64, u64, f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+    vp, cp, sz = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t
+    L.orc_philox4x32_10.argtypes = [vp, vp, vp]
+    L.orc_stream_u32.argtypes = [u64, u64, i64, vp]
+    L.orc_stream_below.argtypes = [u64, u64, u64, i64, vp]
+    L.orc_gnm.argtypes = [i64, i64, i32, i32, u64, u64, vp, vp, cp, sz]
+    L.orc_gnm.restype = i32
+    L.orc_rmat.argtypes = [i32, i64, f64, f64, f64, u64, vp, vp]
+    L.orc_graph_new.argtypes = [i64, vp, vp, vp, i64, i32, ctypes.POINTER(vp), cp, sz]
+    L.orc_graph_new.restype = i32
+    L.orc_graph_free.argtypes = [vp]
+    L.orc_graph_node_count.argtypes = [vp]
+    L.orc_graph_node_count.restype = i64
+    L.orc_graph_edge_count.argtypes = [vp]
+    L.orc_graph_edge_count.restype = i64
+    L.orc_graph_arc_count.argtypes = [vp, i32]
+    L.orc_graph_arc_count.restype = i64
+    L.orc_graph_csr.argtypes = [vp, i32, vp, vp, vp]
+    L.orc_degree.argtypes = [vp, i32, i32, i32, vp, cp, sz]
+    L.orc_degree.restype = i32
+    L.orc_components.argtypes = [vp, i32, vp, ctypes.POINTER(i64)]
+    L.orc_components.restype = i32
+    L.orc_pagerank_ex.argtypes = [vp, f64, i32, i32, vp, i32, i32, f64, i64, i32, i64, vp,
+                                  ctypes.POINTER(i64), cp, sz]
+    L.orc_pagerank_ex.restype = i32
+    L.orc_pagerank_time_op.argtypes = [i64, vp, vp, vp, vp, f64, i64, i32, vp]
+    L.orc_pagerank_time_op.restype = f64
+    L.orc_threads_for.argtypes = [i32, i64, i64]
+    L.orc_threads_for.restype = i64
+    L.orc_eigenvector_ex.argtypes = [vp, i32, i32, i32, i32, f64, i64, i32, vp,
+                                     ctypes.POINTER(f64), ctypes.POINTER(i32),
+                                     ctypes.POINTER(i64), cp, sz]
+    L.orc_eigenvector_ex.restype = i32
+    L.orc_symmetric_eigen.argtypes = [i64, vp, vp, vp]
+    L.orc_symmetric_eigen.restype = i32
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def philox(ctr, key):
+    c = np.asarray(ctr, dtype=np.uint32)
+    k = np.asarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().orc_philox4x32_10(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+def stream_u32(seed: int, index: int, count: int) -> np.ndarray:
+    out = np.zeros(count, dtype=np.uint32)
+    lib().orc_stream_u32(seed, index, count, _ptr(out))
+    return out
+
+
+def stream_below(seed: int, index: int, bound: int, count: int) -> np.ndarray:
+    out = np.zeros(count, dtype=np.uint64)
+    lib().orc_stream_below(seed, index, bound, count, _ptr(out))
+    return out
+
+
+def gnm(n: int, m: int, directed: bool = False, loops: bool = False, seed: int = 1,
+        rep: int = 0):
+    f = np.zeros(m, dtype=np.uint32)
+    t = np.zeros(m, dtype=np.uint32)
+    err = ctypes.create_string_buffer(ERR_LEN)
+    if lib().orc_gnm(n, m, int(directed), int(loops), seed, rep, _ptr(f), _ptr(t), err, ERR_LEN):
+        raise OracleError(err.value.decode())
+    return f, t
+
+
+def rmat_raw(scale: int, m: int, a: float, b: float, c: float, seed: int):
+    s = np.zeros(m, dtype=np.uint32)
+    t = np.zeros(m, dtype=np.uint32)
+    lib().orc_rmat(scale, m, a, b, c, seed, _ptr(s), _ptr(t))
+    return s, t
+
+
+class Graph:
+    """An oracle graph handle (mirror of net_graph_new / net_graph_free)."""
+
+    def __init__(self, n, src, tgt, weights=None, directed=True):
+        self.n = int(n)
+        s = np.ascontiguousarray(src, dtype=np.int64)
+        t = np.ascontiguousarray(tgt, dtype=np.int64)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        self.m = len(s)
+        self.directed = bool(directed)
+        self.weighted = w is not None
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_graph_new(self.n, _ptr(s), _ptr(t), _ptr(w), self.m, int(directed),
+                               ctypes.byref(h), err, ERR_LEN):
+            raise OracleError(err.value.decode())
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.orc_graph_free(self.h)
+            self.h = None
+
+    def csr(self, which: int = 0):
+        arcs = lib().orc_graph_arc_count(self.h, which)
+        off = np.zeros(self.n + 1, dtype=np.uint64)
+        tgt = np.zeros(max(arcs, 1), dtype=np.uint32)
+        w = np.zeros(max(arcs, 1), dtype=np.float64) if self.weighted else None
+        lib().orc_graph_csr(self.h, which, _ptr(off), _ptr(tgt), _ptr(w))
+        return off, tgt[:arcs], (None if w is None else w[:arcs])
+
+    def degree(self, mode=3, loops=True, weighted=False):
+        out = np.zeros(max(self.n, 1))
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_degree(self.h, mode, int(loops), int(weighted), _ptr(out), err, ERR_LEN):
+            raise OracleError(err.value.decode())
+        return out[: self.n]
+
+    def components(self, strong=False):
+        memb = np.zeros(max(self.n, 1), dtype=np.uint32)
+        cnt = ctypes.c_int64()
+        lib().orc_components(self.h, int(strong), _ptr(memb), ctypes.byref(cnt))
+        return memb[: self.n], cnt.value
+
+    def pagerank(self, damping=0.85, directed=True, weighted=False, personalization=None,
+                 dangling=0, loops=0, tol=0.0, max_iter=0, threads=0, fixed_iters=0):
+        out = np.zeros(max(self.n, 1))
+        p = None if personalization is None else np.ascontiguousarray(personalization,
+                                                                       dtype=np.float64)
+        it = ctypes.c_int64()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_pagerank_ex(self.h, damping, int(directed), int(weighted), _ptr(p),
+                                 dangling, loops, tol, max_iter, threads, fixed_iters, _ptr(out),
+                                 ctypes.byref(it), err, ERR_LEN):
+            raise OracleError(err.value.decode())
+        self.last_iters = it.value
+        return out[: self.n]
+
+    def eigenvector(self, mode=2, weighted=False, scale=0, loops=0, tol=0.0, max_iter=0,
+                    threads=0):
+        out = np.zeros(max(self.n, 1))
+        val = ctypes.c_double()
+        conn = ctypes.c_int32()
+        it = ctypes.c_int64()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_eigenvector_ex(self.h, mode, int(weighted), scale, loops, tol, max_iter,
+                                    threads, _ptr(out), ctypes.byref(val), ctypes.byref(conn),
+                                    ctypes.byref(it), err, ERR_LEN):
+            raise OracleError(err.value.decode())
+        self.last_iters = it.value
+        return out[: self.n], val.value, bool(conn.value)
+
+
+def symmetric_eigen(a: np.ndarray):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    vals = np.zeros(n)
+    vecs = np.zeros((n, n))
+    if lib().orc_symmetric_eigen(n, _ptr(a), _ptr(vals), _ptr(vecs)):
+        raise OracleError("symmetric eigenvalue iteration did not converge")
+    return vals, vecs
+
+
+def pagerank_time_op(off, cols, vals, out_strength, damping, iters, threads):
+    """Seconds for `iters` reference-style PageRank iterations on a prebuilt
+    pull operator (CPU baseline)."""
+    n = len(off) - 1
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    vals = None if vals is None else np.ascontiguousarray(vals, dtype=np.float64)
+    os_ = np.ascontiguousarray(out_strength, dtype=np.float64)
+    out = np.zeros(n)
+    secs = lib().orc_pagerank_time_op(n, _ptr(off), _ptr(cols), _ptr(vals), _ptr(os_), damping,
+                                      iters, threads, _ptr(out))
+    return secs, out
+
+
+def threads_for(requested: int, items: int, work: int) -> int:
+    return int(lib().orc_threads_for(requested, items, work))
+
+
+if os.environ.get("KNAPPNET_ORACLE_REBUILD"):
+    build(force=True)

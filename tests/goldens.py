@@ -1,0 +1,101 @@
+"""Reads the packed golden file and runs a manifest variant on an engine.
+
+An "engine" is any object with the reference's graph and measure calls
+(oracle.oracle.Graph, or knappnet_b200.Graph over the CUDA library), so the
+same variant code checks the oracle and the product.
+"""
+from __future__ import annotations
+
+import json
+import math
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "spectral_golden.json"
+
+MODES = {"out": 1, "in": 2, "all": 3}
+LOOPS = {"twice": 0, "once": 1, "ignore": 2}
+DANGLING = {"personalized": 0, "uniform": 1}
+SCALES = {"max": 0, "unit": 1}
+
+
+@lru_cache(maxsize=1)
+def load():
+    return json.loads(GOLDEN.read_text())
+
+
+def node_rule(rule: str, n: int):
+    """validation/bindings/spectral.py:84-96 (the rules on this path)."""
+    if rule == "mod3plus1":
+        return [float(v % 3 + 1) for v in range(n)]
+    raise ValueError(rule)
+
+
+def applies(spec: dict, fx: dict) -> bool:
+    kind = spec.get("applies_to", "any")
+    if kind == "directed" and not fx["directed"]:
+        return False
+    if kind == "undirected" and fx["directed"]:
+        return False
+    if spec.get("requires_weights") and not fx["weighted"]:
+        return False
+    return True
+
+
+def cases():
+    """(fixture, variant, oracle) triples that have a golden vector."""
+    doc = load()
+    out = []
+    for fx_name, per in doc["golden"].items():
+        fx = doc["fixtures"][fx_name]
+        for variant, oracles in per.items():
+            if not applies(doc["manifest"][variant], fx):
+                continue
+            for oracle in oracles:
+                out.append((fx_name, variant, oracle))
+    return out
+
+
+def make_graph(graph_cls, fx: dict):
+    w = None if fx["w"] is None else np.asarray(fx["w"], dtype=np.float64)
+    return graph_cls(fx["n"], np.asarray(fx["src"], dtype=np.int64),
+                     np.asarray(fx["tgt"], dtype=np.int64), w, fx["directed"])
+
+
+def run_variant(g, fx: dict, variant: str):
+    """Runs the manifest's engine options for `variant` on graph `g`."""
+    e = load()["manifest"][variant]["engine"]
+    n = fx["n"]
+    if e["fn"] == "pagerank":
+        p = e.get("personalization")
+        pers = np.asarray(node_rule(p, n)) if p else None
+        return g.pagerank(damping=float(e.get("damping", 0.85)),
+                          directed=bool(e.get("directed", True)),
+                          weighted=bool(e.get("weighted", False)), personalization=pers,
+                          dangling=DANGLING[e.get("dangling", "personalized")],
+                          loops=LOOPS[e.get("loops", "twice")])
+    if e["fn"] == "eigenvector":
+        vals, _, _ = g.eigenvector(mode=MODES[e.get("mode", "in")],
+                                   weighted=bool(e.get("weighted", False)),
+                                   scale=SCALES[e.get("scale", "max")],
+                                   loops=LOOPS[e.get("loops", "twice")])
+        return vals
+    raise ValueError(e["fn"])
+
+
+def agree(ours, theirs, tol: dict):
+    """validation/compare.py:38-39: |a - b| <= abs + rel * max(|a|, |b|);
+    an undefined golden value matches only NaN."""
+    rel, abs_ = float(tol["rel"]), float(tol["abs"])
+    if len(ours) != len(theirs):
+        return False, f"length {len(ours)} != {len(theirs)}"
+    for i, (a, b) in enumerate(zip(ours, theirs)):
+        if b is None:
+            if not math.isnan(a):
+                return False, f"[{i}] {a} but golden undefined"
+            continue
+        if not abs(a - b) <= abs_ + rel * max(abs(a), abs(b)):
+            return False, f"[{i}] {a!r} vs {b!r}"
+    return True, ""
