@@ -1,0 +1,411 @@
+"""Benchmark: PageRank GTEPS per iteration on R-MAT scale 24 (directed,
+weighted), mixed FP32 + FP64-refined path versus the all-FP64 GPU path, both
+to the reference's stopping rule at L1 change <= 1e-9.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: R-MAT scale 24, edge factor 16 (2^28 draws), a/b/c/d =
+0.57/0.19/0.19/0.05, self-loops and duplicate arcs removed, lognormal(0, 1)
+arc strengths rounded to FP32; PageRank with damping 0.85, uniform teleport,
+dangling nodes jumping by the teleport vector, weights as strengths, tol 1e-9.
+The graph is generated on the device from seeded Philox streams (synthetic;
+no dataset). A step is one PageRank solve.
+
+Metric: GTEPS per iteration = arcs / (solve time / sweeps) / 1e9.
+- `value`: the mixed path with the graph resident in HBM (device time of the
+  solve, CUDA events on the library's stream).
+- `e2e`: the same call through the C ABI with host buffers: the teleport
+  vector is copied from pinned host memory and the scores back to pinned
+  host memory inside the timed region.
+- `roofline`: the dominant kernel (the merge-path sweep; FP32 and FP64 sweeps
+  reported separately), its algorithmic bytes per launch over its average
+  CUDA-event duration, against the measured HBM copy bandwidth.
+- `cpu_baseline`: the oracle's restatement of the reference's multithreaded
+  CPU PageRank iteration (oracle/), timed on this host's cores on a bounded
+  sample of the same workload.
+With --impl reference the reference arm runs instead: the CPU restatement
+(the Rust reference cannot be built here) times the reference's
+net_pagerank call on the same graph, one bounded sample per step.
+
+Multi-GPU (torchrun, one process per GPU): independent replicas of the same
+solve (PageRank on one graph does not shard without an exchange per
+iteration); value is the arcs all ranks processed per
+iteration-second, timed as the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PageRank GTEPS/iter & % HBM peak, R-MAT 24: mixed vs FP64 at L1≤1e-9"
+UNIT = "GTEPS/iter"
+SCALE, EDGE_FACTOR, A, B, C = 24, 16, 0.57, 0.19, 0.19
+SEED, WSEED = 20240601, 20240602
+DAMPING, TOL = 0.85, 1e-9
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    if n_gpus <= 1 and "WORLD_SIZE" not in os.environ:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    return rank, world, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_graph():
+    import knappnet_b200 as K
+    g = K.generate_rmat(SCALE, EDGE_FACTOR, A, B, C, seed=SEED, clean=True, symmetrize=False,
+                        lognormal=True, wseed=WSEED)
+    K.device_sync()
+    return g
+
+
+def pinned(n: int):
+    """A pinned host float64 array of n values (torch pinned memory)."""
+    import torch
+    t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    return t, t.numpy()
+
+
+def cpu_sample(g, budget_s: float, full_iters: int):
+    """The oracle's PageRank iteration on this host (all cores), on the same
+    pull operator, for about `budget_s` seconds: returns (GTEPS/iter, cores,
+    iterations, seconds)."""
+    from oracle import oracle as O
+    off, cols, w = g.csr(1)
+    # out-strength = column sums of the pull operator (the graph has no loops)
+    outs = g.degree(mode=1, loops=True, weighted=True)
+    cores = O.threads_for(0, g.n, len(cols) // 2)
+    secs1, _ = O.pagerank_time_op(off, cols, w, outs, DAMPING, 1, 0)
+    iters = int(max(1, min(full_iters, budget_s / max(secs1, 1e-3))))
+    secs, _ = O.pagerank_time_op(off, cols, w, outs, DAMPING, iters, 0)
+    return len(cols) * iters / secs / 1e9, cores, iters, secs
+
+
+def run_ours(args):
+    import knappnet_b200 as K
+    rank, world, local, dist = dist_setup(args.gpus)
+    hbm, peak_kind = peaks()
+    g = make_graph()
+    n, m = g.n, g.m
+
+    import torch
+    # scores stay in device memory for the device-resident measurements
+    d_out = torch.empty(n, dtype=torch.float64, device="cuda")
+
+    def solve(precision):
+        return g.pagerank_device(d_out.data_ptr(), DAMPING, True, True, None, 0, 0, TOL, 0,
+                                 precision)
+
+    # FP64 solve on the GPU (the all-FP64 path) and its timing
+    K.set_sweep_timing(True)
+    for _ in range(max(1, args.warmup // 2)):
+        info64 = solve(K.PREC_FP64)
+    t64 = []
+    for _ in range(max(2, args.steps // 2)):
+        info64 = solve(K.PREC_FP64)
+        t64.append(info64.seconds)
+    x64 = d_out.cpu().numpy()
+    sw64 = K.sweep_timing(1)
+
+    # warm-up of the measured (mixed) path
+    for _ in range(args.warmup):
+        infom = solve(K.PREC_MIXED)
+
+    # timed region: K mixed solves, device-resident graph and scores
+    with ClockSampler(local) as clocks:
+        barrier(dist)
+        torch.cuda.synchronize()
+        wall0 = time.perf_counter()
+        dev_s, sweeps, launches = 0.0, 0, 0
+        sw32_ms = sw32_n = sw64m_ms = sw64m_n = 0.0
+        for _ in range(args.steps):
+            infom = solve(K.PREC_MIXED)
+            dev_s += infom.seconds
+            sweeps += infom.iterations
+            launches += infom.kernel_launches
+            a = K.sweep_timing(0)
+            b = K.sweep_timing(1)
+            sw32_n += a[0]
+            sw32_ms += a[1]
+            sw64m_n += b[0]
+            sw64m_ms += b[1]
+            bytes32, bytes64 = a[2], b[2]
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        barrier(dist)
+    xm = d_out.cpu().numpy()
+    dev_s = max_over_ranks(dist, dev_s)
+    total_arcs_iters = sum_over_ranks(dist, float(m) * sweeps)
+    value = total_arcs_iters / dev_s / 1e9
+
+    # end to end through the C ABI with host buffers (pinned)
+    tp, p_host = pinned(n)
+    p_host[:] = 1.0 / n
+    to, out_host = pinned(n)
+    for _ in range(max(1, args.warmup // 2)):
+        g.pagerank_ex(DAMPING, True, True, p_host, 0, 0, TOL, 0, K.PREC_MIXED, out=out_host)
+    barrier(dist)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    e_sweeps = 0
+    for _ in range(args.steps):
+        xe, infoe = g.pagerank_ex(DAMPING, True, True, p_host, 0, 0, TOL, 0, K.PREC_MIXED,
+                                  out=out_host)
+        e_sweeps += infoe.iterations
+    torch.cuda.synchronize()
+    e_wall = max_over_ranks(dist, time.perf_counter() - e0)
+    e2e_value = sum_over_ranks(dist, float(m) * e_sweeps) / e_wall / 1e9
+
+    # accuracy of the mixed path against the all-FP64 path (which matches
+    # the CPU oracle to 1e-12 L1 in the tests)
+    l1 = float(np.abs(xm - x64).sum())
+    linf = float(np.abs(xm - x64).max())
+    top64 = np.argsort(-x64, kind="stable")[:100]
+    topm = np.argsort(-xm, kind="stable")[:100]
+    fp64_time = statistics.median(t64)
+    mixed_time = dev_s / args.steps
+
+    def roof(ms, cnt, nbytes):
+        if cnt <= 0:
+            return None
+        dur = ms / cnt * 1e-3
+        ach = nbytes / dur / 1e9
+        return {"achieved": round(ach, 1), "duration_ms": round(dur * 1e3, 4),
+                "launches": int(cnt), "bytes_per_launch": nbytes, "frac": round(ach / hbm, 4)}
+
+    r32 = roof(sw32_ms, sw32_n, bytes32)
+    r64m = roof(sw64m_ms, sw64m_n, bytes64)
+    r64 = roof(sw64[1], sw64[0], sw64[2])
+    # dominant kernel of the measured path: the sweep kind with most time
+    dom, dom_name = (r32, "tile_spmv<fp32>") if sw32_ms >= sw64m_ms else (r64m, "tile_spmv<fp64>")
+    traffic = None
+    tfile = ROOT / "profiles" / "sweep_traffic.json"
+    if tfile.exists():
+        tdoc = json.loads(tfile.read_text())
+        key = "fp32" if dom_name.endswith("fp32>") else "fp64"
+        if key in tdoc:
+            traffic = tdoc[key].get("bytes_per_launch_full_scale")
+
+    clock = clocks.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dev_s / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
+        "data": "synthetic (R-MAT generated on the device from seeded Philox streams)",
+        "config": {"workload": "R-MAT scale 24, edge factor 16, a/b/c/d=.57/.19/.19/.05, "
+                               "directed, loops and duplicates removed, lognormal(0,1) FP32 "
+                               "strengths; PageRank d=0.85, uniform teleport, tol 1e-9 (L1)",
+                   "nodes": n, "arcs": m, "precision": "mixed (FP32 sweeps, FP64 sweeps)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (arc arrays 2.1 GB per sweep)"},
+        "gpu_launches": launches,
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                "ms_per_step": round(e_wall / args.steps * 1e3, 3)},
+        "roofline": {"bound": "hbm", "kernel": dom_name,
+                     "achieved": dom["achieved"] if dom else None, "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": dom["frac"] if dom else None, "traffic": traffic,
+                     "fp32_sweep": r32, "fp64_sweep_in_mixed": r64m, "fp64_path_sweep": r64},
+        "clocks": clock,
+        "fp64_path": {"value": round(float(m) * info64.iterations / fp64_time / 1e9, 3),
+                      "time_to_solution_ms": round(fp64_time * 1e3, 3),
+                      "sweeps": info64.iterations},
+        "mixed_path": {"time_to_solution_ms": round(mixed_time * 1e3, 3),
+                       "sweeps": infom.iterations, "fp32_sweeps": infom.iterations_fp32,
+                       "speedup_vs_fp64": round(fp64_time / mixed_time, 3),
+                       "l1_vs_fp64": l1, "linf_vs_fp64": linf,
+                       "top100_identical": bool(np.array_equal(top64, topm))},
+        "wall_s_timed": round(wall, 3),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        gteps, cores, iters, secs = cpu_sample(g, args.cpu_budget, info64.iterations)
+        line["cpu_baseline"] = {"value": round(gteps, 4), "unit": UNIT, "cores": cores,
+                                "kind": "port",
+                                "sample": f"{iters} reference PageRank iterations (FP64, "
+                                          f"serial scalar passes, threaded row-block SpMV) on "
+                                          f"the same operator, {secs:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference arm: the CPU restatement of net_pagerank on this host's
+    cores, one bounded sample of the same workload per step."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    import knappnet_b200 as K
+    g = make_graph()
+    n, m = g.n, g.m
+    s, t, w = g.edges()
+    K.lib()
+    t0 = time.perf_counter()
+    og = O.Graph(n, s, t, w, True)
+    build_s = time.perf_counter() - t0
+    del s, t, w
+    cores = O.threads_for(0, n, m // 2)
+    # one iteration to size the sample
+    t1 = time.perf_counter()
+    og.pagerank(DAMPING, True, True, None, 0, 0, TOL, 0, 0, 1)
+    one = time.perf_counter() - t1
+    iters = int(max(1, min(28, args.ref_budget / max(one, 1e-3))))
+    for _ in range(args.warmup if iters <= 2 else 1):
+        og.pagerank(DAMPING, True, True, None, 0, 0, TOL, 0, 0, 1)
+    times = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        og.pagerank(DAMPING, True, True, None, 0, 0, TOL, 0, 0, iters)
+        times.append(time.perf_counter() - t1)
+    total = sum(times)
+    value = m * iters * args.steps / total / 1e9
+    sample = (f"{iters} iterations of the reference net_pagerank call per step (operator "
+              f"setup included, as in the reference), graph build {build_s:.1f} s excluded")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic (same R-MAT graph)",
+            "config": {"workload": "R-MAT scale 24, edge factor 16, directed, lognormal FP32 "
+                                   "strengths; PageRank d=0.85, tol 1e-9", "nodes": n,
+                       "arcs": m, "parallelism": f"{cores} CPU threads"},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of CPU work for the cpu_baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=8.0,
+                    help="seconds per reference-arm step")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

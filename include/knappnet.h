@@ -1,0 +1,184 @@
+/*
+ * C interface of the knappnet B200 library: the spectral-centrality path
+ * (graph build, degree, PageRank, eigenvector centrality) of the reference
+ * engine's C ABI, computed on an NVIDIA B200 (sm_100a), plus additive
+ * extensions.
+ *
+ * Conventions (as the reference's crates/capi/include/netcapi.h:1-25):
+ * - Functions that take `err` return 0 on success and non-zero on failure,
+ *   after writing a NUL-terminated message into `err` (at most `err_len`
+ *   bytes). Accessors that return a count give -1 for a NULL handle.
+ * - Node indices are 0-based. Output buffers are allocated by the caller; a
+ *   node-aligned result holds n doubles.
+ * - A handle belongs to the caller until released with net_graph_free,
+ *   which accepts NULL. Handles are immutable: concurrent calls on one
+ *   handle are safe.
+ * - Codes: mode 1 = out, 2 = in, 3 = all; loops 0 = an undirected self-loop
+ *   counts twice (igraph), 1 = once (NetworkX), 2 = not at all; dangling
+ *   0 = jump by the personalization vector, 1 = jump uniformly; scale 0 =
+ *   largest score 1, 1 = unit Euclidean norm. tol <= 0 and max_iter <= 0
+ *   select the defaults (1e-12 and 10000). `threads` is accepted for
+ *   compatibility; results never depend on it.
+ * - The graph lives in GPU memory (the current CUDA device when it is
+ *   built). Functions with `_device` in their name take device pointers.
+ */
+#ifndef KNAPPNET_H
+#define KNAPPNET_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NET_API __attribute__((visibility("default")))
+#else
+#define NET_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct GraphHandle GraphHandle;
+
+/* ---- Reference entry points ------------------------------------------- */
+
+/* Builds a graph from m edges on n nodes; weights may be NULL; directed != 0
+ * keeps arc directions. Replaces netcapi.h:46-48 (crates/capi/src/lib.rs:139-164). */
+NET_API int32_t net_graph_new(int64_t n, const int64_t *src, const int64_t *tgt,
+                      const double *weights, int64_t m, int32_t directed,
+                      GraphHandle **out, char *err, size_t err_len);
+
+/* Releases a graph (NULL is allowed). Replaces netcapi.h:51 (lib.rs:171-175). */
+NET_API void net_graph_free(GraphHandle *h);
+
+/* Number of nodes, or -1 for NULL. Replaces netcapi.h:54 (lib.rs:182-184). */
+NET_API int64_t net_graph_node_count(const GraphHandle *h);
+
+/* Edges as supplied, or -1 for NULL. Replaces netcapi.h:57. */
+NET_API int64_t net_graph_edge_count(const GraphHandle *h);
+
+/* Degree (weighted == 0) or strength; out holds n doubles. Replaces
+ * netcapi.h:383-384 (lib.rs:192-212). */
+NET_API int32_t net_degree(const GraphHandle *h, int32_t mode, int32_t loops,
+                   int32_t weighted, double *out, char *err, size_t err_len);
+
+/* PageRank; out holds n doubles summing to 1. personalization is NULL
+ * (uniform) or n nonnegative values. directed == 0 ignores directions.
+ * Replaces netcapi.h:463-467 (crates/capi/src/spectral.rs:59-97). */
+NET_API int32_t net_pagerank(const GraphHandle *h, double damping, int32_t directed,
+                     int32_t weighted, const double *personalization,
+                     int32_t dangling, int32_t loops, double tol,
+                     int64_t max_iter, int32_t threads, double *out,
+                     char *err, size_t err_len);
+
+/* Eigenvector centrality; out holds n doubles; *eigenvalue receives the
+ * principal eigenvalue and *connected 1 if the graph is (strongly)
+ * connected. Replaces netcapi.h:455-459 (crates/capi/src/topography.rs:208-249). */
+NET_API int32_t net_eigenvector(const GraphHandle *h, int32_t mode, int32_t weighted,
+                        int32_t scale, int32_t loops, double tol,
+                        int64_t max_iter, int32_t threads, double *out,
+                        double *eigenvalue, int32_t *connected, char *err,
+                        size_t err_len);
+
+/* ---- Extensions (no counterpart in the reference) ---------------------- */
+
+/* What a solve did. */
+typedef struct NetSolveInfo {
+  int64_t iterations;      /* sweeps (PageRank) or matrix-vector products */
+  int64_t iterations_fp32; /* of which in FP32 */
+  double change;           /* last L1 change (PageRank) / residual (eigen) */
+  double seconds;          /* device time of the solve */
+  int32_t converged;
+  int32_t kernel_launches; /* CUDA kernels the solve launched */
+  double eigenvalue;
+  int32_t connected;
+  int32_t reserved;
+} NetSolveInfo;
+
+/* Precision codes: 0 = FP64, 1 = mixed (FP32 sweeps, then FP64 sweeps on
+ * the same trajectory until the reference's stopping rule holds in FP64),
+ * 2 = FP32 only. */
+NET_API int32_t net_pagerank_ex(const GraphHandle *h, double damping, int32_t directed,
+                        int32_t weighted, const double *personalization,
+                        int32_t dangling, int32_t loops, double tol,
+                        int64_t max_iter, int32_t precision, double *out,
+                        NetSolveInfo *info, char *err, size_t err_len);
+
+/* As net_pagerank_ex with device pointers for personalization and out. */
+NET_API int32_t net_pagerank_device(const GraphHandle *h, double damping,
+                            int32_t directed, int32_t weighted,
+                            const double *d_personalization, int32_t dangling,
+                            int32_t loops, double tol, int64_t max_iter,
+                            int32_t precision, double *d_out,
+                            NetSolveInfo *info, char *err, size_t err_len);
+
+/* As net_eigenvector, with a precision code (0 = FP64, 1 = FP32
+ * matrix-vector products with FP64 basis, dots and reorthogonalisation)
+ * and the solve information. */
+NET_API int32_t net_eigenvector_ex(const GraphHandle *h, int32_t mode, int32_t weighted,
+                           int32_t scale, int32_t loops, double tol,
+                           int64_t max_iter, int32_t precision, double *out,
+                           double *eigenvalue, int32_t *connected,
+                           NetSolveInfo *info, char *err, size_t err_len);
+
+/* Builds a graph from device arrays: 32-bit endpoints and FP32 (d_w32) or
+ * FP64 (d_w64) weights, either may be NULL. */
+NET_API int32_t net_graph_new_device(int64_t n, const uint32_t *d_src,
+                             const uint32_t *d_tgt, const float *d_w32,
+                             const double *d_w64, int64_t m, int32_t directed,
+                             GraphHandle **out, char *err, size_t err_len);
+
+/* Number of arcs of the out (which = 0), in (1) or undirected (2) CSR. */
+NET_API int64_t net_graph_arc_count(const GraphHandle *h, int32_t which);
+
+/* Copies a CSR to the host: off (n + 1), tgt and edge (the input edge of
+ * each arc) and w (weighted graphs) hold one value per arc; any of tgt,
+ * edge, w may be NULL. which: 0 out, 1 in, 2 directions ignored. */
+NET_API int32_t net_graph_csr(const GraphHandle *h, int32_t which, uint32_t *off,
+                      uint32_t *tgt, uint32_t *edge, double *w, char *err,
+                      size_t err_len);
+
+/* Copies the edge list (input order) to the host; w may be NULL. */
+NET_API int32_t net_graph_edges(const GraphHandle *h, int64_t *src, int64_t *tgt,
+                        double *w, char *err, size_t err_len);
+
+/* Synthetic R-MAT graph (Chakrabarti, Zhan and Faloutsos 2004) built on the
+ * device: m = edge_factor << scale draws; edge k takes `scale` 32-bit words
+ * of Philox stream (seed, k), most significant level first, quadrant
+ * a / b / c / d by comparing with floor(a 2^32), floor((a+b) 2^32),
+ * floor((a+b+c) 2^32). clean != 0 removes self-loops and duplicates
+ * (sorted); symmetrize != 0 also merges (u, v) and (v, u) and builds an
+ * undirected graph. lognormal != 0 draws weights exp(N(0, 1)) rounded to
+ * FP32 (Box-Muller on stream (wseed, e) of cleaned edge e). *m_out
+ * receives the edge count. */
+NET_API int32_t net_generate_rmat(int32_t scale, int64_t edge_factor, double a,
+                          double b, double c, uint64_t seed, int32_t clean,
+                          int32_t symmetrize, int32_t lognormal, uint64_t wseed,
+                          GraphHandle **out, int64_t *m_out, char *err,
+                          size_t err_len);
+
+/* Timing of the merge-path sweep kernel in the last PageRank solve of the
+ * calling thread, when enabled with net_set_sweep_timing(1), for the FP32
+ * (phase 0) or FP64 (phase 1) sweeps: launches, their total device
+ * milliseconds (CUDA events) and the algorithmic bytes one sweep moves. */
+NET_API int32_t net_sweep_timing(int32_t phase, int64_t *launches, double *total_ms,
+                         double *bytes_per_launch);
+NET_API void net_set_sweep_timing(int32_t on);
+
+/* Process-wide tuning of the PageRank sweeps (results stay within the
+ * documented tolerances whatever the setting): key 0 = merge-path items per
+ * thread (0 automatic, 4, 8, 16); 1 = renumber nodes by gather frequency
+ * (1, default) or not (0); 2 = mixed precision: leave FP32 once the change is
+ * below tol times this factor (default 8192); 3 = ... or below this floor
+ * (default 2e-6); 4 = sweep kernel (0 automatic, 1 one merge-path tile per
+ * CTA, 2 one tile per warp). Returns 1 for an unknown key or value. */
+NET_API int32_t net_set_tuning(int32_t key, double value);
+
+/* Waits for the device; reports an asynchronous CUDA error if one occurred. */
+NET_API int32_t net_device_sync(char *err, size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KNAPPNET_H */

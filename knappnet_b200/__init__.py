@@ -1,0 +1,294 @@
+"""knappnet B200: the reference engine's spectral-centrality path on an NVIDIA
+B200 (sm_100a), behind the reference's C ABI.
+
+The compute lives in the CUDA library libknappnet_b200.so (C ABI declared in
+include/knappnet.h). This module is a thin ctypes binding with the same
+calls and argument meaning as the reference's ctypes bindings
+(validation/bindings/spectral.py, topography.py): a graph handle, then
+degree, PageRank and eigenvector centrality on it.
+
+There is no CPU fallback: if the library is missing or cannot be loaded,
+importing `lib()` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libknappnet_b200.so"
+ERR_LEN = 1024
+
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    """A call of the C ABI returned a failure status."""
+
+
+class NetSolveInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int64), ("iterations_fp32", ctypes.c_int64),
+                ("change", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("converged", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
+                ("eigenvalue", ctypes.c_double), ("connected", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library (built in-tree by knappnet_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("KNAPPNET_LIB", LIB_PATH))
+    if not path.exists():
+        raise EngineError(f"{path} is missing: build it with `python -m knappnet_b200.build`")
+    L = ctypes.CDLL(str(path))
+    i32, i64, u64, f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+    vp, cp, sz = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t
+    h = ctypes.c_void_p
+    info_p = ctypes.POINTER(NetSolveInfo)
+    L.net_graph_new.argtypes = [i64, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
+    L.net_graph_new.restype = i32
+    L.net_graph_free.argtypes = [h]
+    L.net_graph_free.restype = None
+    L.net_graph_node_count.argtypes = [h]
+    L.net_graph_node_count.restype = i64
+    L.net_graph_edge_count.argtypes = [h]
+    L.net_graph_edge_count.restype = i64
+    L.net_degree.argtypes = [h, i32, i32, i32, vp, cp, sz]
+    L.net_degree.restype = i32
+    L.net_pagerank.argtypes = [h, f64, i32, i32, vp, i32, i32, f64, i64, i32, vp, cp, sz]
+    L.net_pagerank.restype = i32
+    L.net_eigenvector.argtypes = [h, i32, i32, i32, i32, f64, i64, i32, vp,
+                                  ctypes.POINTER(f64), ctypes.POINTER(i32), cp, sz]
+    L.net_eigenvector.restype = i32
+    L.net_pagerank_ex.argtypes = [h, f64, i32, i32, vp, i32, i32, f64, i64, i32, vp, info_p,
+                                  cp, sz]
+    L.net_pagerank_ex.restype = i32
+    L.net_pagerank_device.argtypes = [h, f64, i32, i32, vp, i32, i32, f64, i64, i32, vp, info_p,
+                                      cp, sz]
+    L.net_pagerank_device.restype = i32
+    L.net_eigenvector_ex.argtypes = [h, i32, i32, i32, i32, f64, i64, i32, vp,
+                                     ctypes.POINTER(f64), ctypes.POINTER(i32), info_p, cp, sz]
+    L.net_eigenvector_ex.restype = i32
+    L.net_graph_new_device.argtypes = [i64, vp, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
+    L.net_graph_new_device.restype = i32
+    L.net_graph_arc_count.argtypes = [h, i32]
+    L.net_graph_arc_count.restype = i64
+    L.net_graph_csr.argtypes = [h, i32, vp, vp, vp, vp, cp, sz]
+    L.net_graph_csr.restype = i32
+    L.net_graph_edges.argtypes = [h, vp, vp, vp, cp, sz]
+    L.net_graph_edges.restype = i32
+    L.net_generate_rmat.argtypes = [i32, i64, f64, f64, f64, u64, i32, i32, i32, u64,
+                                    ctypes.POINTER(h), ctypes.POINTER(i64), cp, sz]
+    L.net_generate_rmat.restype = i32
+    L.net_sweep_timing.argtypes = [i32, ctypes.POINTER(i64), ctypes.POINTER(f64),
+                                   ctypes.POINTER(f64)]
+    L.net_sweep_timing.restype = i32
+    L.net_set_sweep_timing.argtypes = [i32]
+    L.net_set_sweep_timing.restype = None
+    L.net_set_tuning.argtypes = [i32, f64]
+    L.net_set_tuning.restype = i32
+    L.net_device_sync.argtypes = [cp, sz]
+    L.net_device_sync.restype = i32
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(status: int, err) -> None:
+    if status:
+        raise EngineError(err.value.decode(errors="replace"))
+
+
+class Graph:
+    """A graph handle in GPU memory (net_graph_new / net_graph_free)."""
+
+    def __init__(self, n, src=None, tgt=None, weights=None, directed=True, _handle=None,
+                 _m=None, _weighted=None):
+        self.n = int(n)
+        self.directed = bool(directed)
+        if _handle is not None:
+            self.h = _handle
+            self.m = int(_m)
+            self.weighted = bool(_weighted)
+            return
+        s = np.ascontiguousarray(src, dtype=np.int64)
+        t = np.ascontiguousarray(tgt, dtype=np.int64)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        self.m = len(s)
+        self.weighted = w is not None
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_graph_new(self.n, _ptr(s), _ptr(t), _ptr(w), self.m, int(directed),
+                                   ctypes.byref(h), err, ERR_LEN), err)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.net_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def node_count(self) -> int:
+        return int(lib().net_graph_node_count(self.h))
+
+    def edge_count(self) -> int:
+        return int(lib().net_graph_edge_count(self.h))
+
+    def csr(self, which: int = 0, edges: bool = False):
+        """(off, tgt, w) of the out (0), in (1) or undirected (2) CSR, and the
+        input edge of each arc when edges=True."""
+        arcs = int(lib().net_graph_arc_count(self.h, which if which != 2 else 0))
+        if which == 2:
+            arcs = -1
+        off = np.zeros(self.n + 1, dtype=np.uint32)
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if arcs < 0:  # undirected rows: size known after the offsets
+            _check(lib().net_graph_csr(self.h, which, _ptr(off), None, None, None, err, ERR_LEN),
+                   err)
+            arcs = int(off[-1])
+        tgt = np.zeros(max(arcs, 1), dtype=np.uint32)
+        eid = np.zeros(max(arcs, 1), dtype=np.uint32) if edges else None
+        w = np.zeros(max(arcs, 1), dtype=np.float64) if self.weighted else None
+        _check(lib().net_graph_csr(self.h, which, _ptr(off), _ptr(tgt), _ptr(eid), _ptr(w), err,
+                                   ERR_LEN), err)
+        out = (off.astype(np.uint64), tgt[:arcs], None if w is None else w[:arcs])
+        if edges:
+            return out + (eid[:arcs],)
+        return out
+
+    def edges(self):
+        s = np.zeros(max(self.m, 1), dtype=np.int64)
+        t = np.zeros(max(self.m, 1), dtype=np.int64)
+        w = np.zeros(max(self.m, 1)) if self.weighted else None
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_graph_edges(self.h, _ptr(s), _ptr(t), _ptr(w), err, ERR_LEN), err)
+        return s[: self.m], t[: self.m], (None if w is None else w[: self.m])
+
+    def degree(self, mode=3, loops=True, weighted=False):
+        out = np.zeros(max(self.n, 1))
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_degree(self.h, mode, int(loops), int(weighted), _ptr(out), err,
+                                ERR_LEN), err)
+        return out[: self.n]
+
+    def pagerank(self, damping=0.85, directed=True, weighted=False, personalization=None,
+                 dangling=0, loops=0, tol=0.0, max_iter=0, threads=0, precision=PREC_FP64):
+        vals, _ = self.pagerank_ex(damping, directed, weighted, personalization, dangling, loops,
+                                   tol, max_iter, precision)
+        return vals
+
+    def pagerank_ex(self, damping=0.85, directed=True, weighted=False, personalization=None,
+                    dangling=0, loops=0, tol=0.0, max_iter=0, precision=PREC_FP64, out=None):
+        if out is None:
+            out = np.zeros(max(self.n, 1))
+        p = None if personalization is None else np.ascontiguousarray(personalization,
+                                                                       dtype=np.float64)
+        info = NetSolveInfo()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_pagerank_ex(self.h, damping, int(directed), int(weighted), _ptr(p),
+                                     dangling, loops, tol, max_iter, precision, _ptr(out),
+                                     ctypes.byref(info), err, ERR_LEN), err)
+        return out[: self.n], info
+
+    def pagerank_device(self, out_ptr: int, damping=0.85, directed=True, weighted=False,
+                        personalization_ptr=None, dangling=0, loops=0, tol=0.0, max_iter=0,
+                        precision=PREC_FP64):
+        """net_pagerank_device: scores written to device memory at out_ptr (n
+        doubles, e.g. a torch CUDA tensor's data_ptr()); the optional teleport
+        vector is read from device memory."""
+        info = NetSolveInfo()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_pagerank_device(self.h, damping, int(directed), int(weighted),
+                                         personalization_ptr, dangling, loops, tol, max_iter,
+                                         precision, ctypes.c_void_p(out_ptr), ctypes.byref(info),
+                                         err, ERR_LEN), err)
+        return info
+
+    def pagerank_reference_call(self, damping=0.85, directed=True, weighted=False,
+                                personalization=None, dangling=0, loops=0, tol=0.0, max_iter=0,
+                                threads=0):
+        """net_pagerank with the reference's exact signature."""
+        out = np.zeros(max(self.n, 1))
+        p = None if personalization is None else np.ascontiguousarray(personalization,
+                                                                       dtype=np.float64)
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_pagerank(self.h, damping, int(directed), int(weighted), _ptr(p),
+                                  dangling, loops, tol, max_iter, threads, _ptr(out), err,
+                                  ERR_LEN), err)
+        return out[: self.n]
+
+    def eigenvector(self, mode=2, weighted=False, scale=0, loops=0, tol=0.0, max_iter=0,
+                    threads=0, precision=0):
+        vals, info = self.eigenvector_ex(mode, weighted, scale, loops, tol, max_iter, precision)
+        return vals, info.eigenvalue, bool(info.connected)
+
+    def eigenvector_ex(self, mode=2, weighted=False, scale=0, loops=0, tol=0.0, max_iter=0,
+                       precision=0):
+        out = np.zeros(max(self.n, 1))
+        val = ctypes.c_double()
+        conn = ctypes.c_int32()
+        info = NetSolveInfo()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_eigenvector_ex(self.h, mode, int(weighted), scale, loops, tol, max_iter,
+                                        precision, _ptr(out), ctypes.byref(val),
+                                        ctypes.byref(conn), ctypes.byref(info), err, ERR_LEN),
+               err)
+        info.eigenvalue = val.value
+        info.connected = conn.value
+        return out[: self.n], info
+
+
+def generate_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, clean=True,
+                  symmetrize=False, lognormal=False, wseed=2) -> Graph:
+    """An R-MAT graph generated and built on the device (net_generate_rmat)."""
+    h = ctypes.c_void_p()
+    m = ctypes.c_int64()
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_generate_rmat(scale, edge_factor, a, b, c, seed, int(clean), int(symmetrize),
+                                   int(lognormal), wseed, ctypes.byref(h), ctypes.byref(m), err,
+                                   ERR_LEN), err)
+    return Graph(1 << scale, directed=not symmetrize, _handle=h, _m=m.value, _weighted=lognormal)
+
+
+def sweep_timing(phase: int = 1):
+    """(launches, total ms, algorithmic bytes per launch) of the merge-path
+    sweep kernel in the last PageRank solve of this thread: FP32 sweeps
+    (phase 0) or FP64 sweeps (phase 1)."""
+    n = ctypes.c_int64()
+    ms = ctypes.c_double()
+    b = ctypes.c_double()
+    lib().net_sweep_timing(phase, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(b))
+    return n.value, ms.value, b.value
+
+
+def set_sweep_timing(on: bool) -> None:
+    lib().net_set_sweep_timing(int(on))
+
+
+TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT = 0, 1, 2, 3, 4
+
+
+def set_tuning(key: int, value: float) -> None:
+    """Process-wide PageRank tuning (net_set_tuning)."""
+    if lib().net_set_tuning(key, float(value)):
+        raise EngineError(f"invalid tuning key {key} or value {value}")
+
+
+def device_sync() -> None:
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_device_sync(err, ERR_LEN), err)

@@ -1,0 +1,561 @@
+// The C ABI of the B200 library: the reference's netcapi.h entry points for
+// the spectral-centrality path, with its argument meaning, defaults and error
+// behaviour (crates/capi/src/lib.rs:57-212, crates/capi/src/spectral.rs:35-97,
+// crates/capi/src/topography.rs:208-249), plus additive extensions declared
+// in include/knappnet.h.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/knappnet.h"
+#include "eigen.cuh"
+#include "generate.cuh"
+#include "graph.cuh"
+#include "pagerank.cuh"
+
+using knb::Error;
+
+struct GraphHandle {
+  knb::GraphHandleImpl g;
+};
+
+namespace {
+
+void write_err(char* err, size_t len, const std::string& msg) {
+  if (!err || len == 0) return;
+  size_t k = std::min(msg.size(), len - 1);
+  memcpy(err, msg.data(), k);
+  err[k] = 0;
+}
+
+template <class F>
+int32_t guard(char* err, size_t len, F f) {
+  try {
+    f();
+    return 0;
+  } catch (const Error& e) {
+    write_err(err, len, e.what());
+  } catch (const std::bad_alloc&) {
+    write_err(err, len, "out of host memory in the network engine");
+  } catch (const std::exception& e) {
+    write_err(err, len, std::string("internal error in the network engine: ") + e.what());
+  } catch (...) {
+    write_err(err, len, "internal error in the network engine");
+  }
+  return 1;
+}
+
+knb::GraphHandleImpl& handle(const GraphHandle* h) {
+  if (!h) throw Error("graph handle is null");
+  return const_cast<GraphHandle*>(h)->g;
+}
+
+std::string fmt_g(double v) {
+  char b[64];
+  snprintf(b, sizeof b, "%g", v);
+  return b;
+}
+
+// ---------------------------------------------------------------- device checks
+// First invalid endpoint, as 2 * edge + (0 for source, 1 for target), so the
+// smallest value names the edge and endpoint the reference reports first
+// (crates/engine/src/graph.rs:182-194).
+__global__ void convert_edges(const int64_t* __restrict__ s64, const int64_t* __restrict__ t64,
+                              uint64_t m, uint64_t n, uint32_t* __restrict__ s32,
+                              uint32_t* __restrict__ t32, unsigned long long* __restrict__ bad) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    int64_t a = s64[e], b = t64[e];
+    bool ba = a < 0 || (uint64_t)a >= n, bb = b < 0 || (uint64_t)b >= n;
+    if (ba) atomicMin(bad, (unsigned long long)(2 * e));
+    else if (bb) atomicMin(bad, (unsigned long long)(2 * e + 1));
+    s32[e] = (uint32_t)a;
+    t32[e] = (uint32_t)b;
+  }
+}
+
+__global__ void check_u32_edges(const uint32_t* __restrict__ s, const uint32_t* __restrict__ t,
+                                uint64_t m, uint64_t n, unsigned long long* __restrict__ bad) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    if (s[e] >= n) atomicMin(bad, (unsigned long long)(2 * e));
+    else if (t[e] >= n) atomicMin(bad, (unsigned long long)(2 * e + 1));
+  }
+}
+
+// First weight that is not finite (mode 0) or negative (mode 1).
+__global__ void first_bad_weight(const double* __restrict__ w, uint64_t m, int mode,
+                                 unsigned long long* __restrict__ bad) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    double x = w[e];
+    bool b = mode == 0 ? !isfinite(x) : x < 0.0;
+    if (b) atomicMin(bad, (unsigned long long)e);
+  }
+}
+
+__global__ void widen_weights(const float* __restrict__ w32, uint64_t m, double* __restrict__ w) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    w[e] = (double)w32[e];
+}
+
+// Degree or strength per node from CSR rows (metrics/degree.rs:41-73): an
+// undirected loop counts twice, a directed loop once in each direction;
+// loops == 0 skips loops. Integer counts are exact in any order.
+__global__ void degree_rows(const uint32_t* __restrict__ off1, const uint32_t* __restrict__ tgt1,
+                            const double* __restrict__ w1, const uint32_t* __restrict__ off2,
+                            const uint32_t* __restrict__ tgt2, const double* __restrict__ w2,
+                            uint32_t n, int undirected, int loops, double* __restrict__ out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (uint32_t k = off1[v]; k < off1[v + 1]; ++k) {
+      double x = w1 ? w1[k] : 1.0;
+      if (tgt1[k] == v) {
+        if (!loops) continue;
+        if (undirected) x += x;
+      }
+      s += x;
+    }
+    if (off2) {
+      for (uint32_t k = off2[v]; k < off2[v + 1]; ++k) {
+        double x = w2 ? w2[k] : 1.0;
+        if (tgt2[k] == v && !loops) continue;
+        s += x;
+      }
+    }
+    out[v] = s;
+  }
+}
+
+unsigned long long read_u64(const unsigned long long* d, cudaStream_t s) {
+  unsigned long long h = 0;
+  KNB_CUDA(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+const uint64_t NONE = ~0ull;
+
+// Finishes a handle whose device edge arrays (src, tgt, optional w) are set.
+void finish_build(knb::GraphHandleImpl& g, cudaStream_t s) {
+  if (g.directed) {
+    knb::build_csr(g.n, g.m, g.src.get(), g.tgt.get(), nullptr, g.weighted ? g.w.get() : nullptr,
+                   &g.out, s);
+    knb::build_csr(g.n, g.m, g.tgt.get(), g.src.get(), nullptr, g.weighted ? g.w.get() : nullptr,
+                   &g.inc, s);
+  } else {
+    knb::build_undirected(g.n, g.m, g.src.get(), g.tgt.get(), g.weighted ? g.w.get() : nullptr,
+                          &g.out, s);
+  }
+}
+
+void check_nonnegative(knb::GraphHandleImpl& g, const char* what, cudaStream_t s) {
+  if (!g.weighted) throw Error("the graph has no edge weights");
+  knb::DevBuf<unsigned long long> bad(1);
+  KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+  if (g.m) {
+    first_bad_weight<<<knb::grid_for(g.m, 256), 256, 0, s>>>(g.w.get(), g.m, 1, bad.get());
+    KNB_LAUNCH("first_bad_weight");
+  }
+  uint64_t e = read_u64(bad.get(), s);
+  if (e != NONE) {
+    double w = 0;
+    KNB_CUDA(cudaMemcpy(&w, g.w.get() + e, 8, cudaMemcpyDeviceToHost));
+    throw Error("edge " + std::to_string(e) + " has negative weight " + fmt_g(w) + "; " + what +
+                " requires non-negative weights");
+  }
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+int32_t net_graph_new(int64_t n, const int64_t* src, const int64_t* tgt, const double* weights,
+                      int64_t m, int32_t directed, GraphHandle** out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (n < 0 || m < 0) throw Error("negative node or edge count");
+    if ((uint64_t)n > 0xFFFFFFFFull)
+      throw Error("node count (" + std::to_string(n) + ") exceeds the supported maximum");
+    if (!out) throw Error("output handle pointer is null");
+    cudaStream_t s = knb::thread_stream();
+    auto h = std::make_unique<GraphHandle>();
+    knb::GraphHandleImpl& g = h->g;
+    g.n = (uint32_t)n;
+    g.m = (uint64_t)m;
+    g.directed = directed != 0;
+    g.weighted = weights != nullptr;
+    KNB_CUDA(cudaGetDevice(&g.device));
+    knb::DevBuf<unsigned long long> bad(1);
+    if (g.weighted) {
+      if ((uint64_t)m > 0xFFFFFFFFull / 2)
+        throw Error("edge count (" + std::to_string(m) + ") exceeds the supported maximum");
+      g.w.alloc(std::max<uint64_t>(g.m, 1));
+      if (m) KNB_CUDA(cudaMemcpyAsync(g.w.get(), weights, m * 8, cudaMemcpyHostToDevice, s));
+      KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+      if (m) {
+        first_bad_weight<<<knb::grid_for(m, 256), 256, 0, s>>>(g.w.get(), m, 0, bad.get());
+        KNB_LAUNCH("first_bad_weight");
+      }
+      uint64_t e = read_u64(bad.get(), s);
+      if (e != NONE)
+        throw Error("edge " + std::to_string(e) + " has a missing, NaN, or infinite weight");
+    }
+    if ((uint64_t)m > 0xFFFFFFFFull / 2)
+      throw Error("edge count (" + std::to_string(m) + ") exceeds the supported maximum");
+    g.src.alloc(std::max<uint64_t>(g.m, 1));
+    g.tgt.alloc(std::max<uint64_t>(g.m, 1));
+    if (m) {
+      knb::DevBuf<int64_t> s64(m), t64(m);
+      KNB_CUDA(cudaMemcpyAsync(s64.get(), src, m * 8, cudaMemcpyHostToDevice, s));
+      KNB_CUDA(cudaMemcpyAsync(t64.get(), tgt, m * 8, cudaMemcpyHostToDevice, s));
+      KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+      convert_edges<<<knb::grid_for(m, 256), 256, 0, s>>>(s64.get(), t64.get(), m, (uint64_t)n,
+                                                          g.src.get(), g.tgt.get(), bad.get());
+      KNB_LAUNCH("convert_edges");
+      uint64_t b = read_u64(bad.get(), s);
+      if (b != NONE) {
+        uint64_t e = b / 2;
+        int64_t node = (b & 1) ? tgt[e] : src[e];
+        throw Error("edge " + std::to_string(e) + " refers to node index " + std::to_string(node) +
+                    ", but valid indices are 0.." + std::to_string(n));
+      }
+    }
+    finish_build(g, s);
+    *out = h.release();
+  });
+}
+
+void net_graph_free(GraphHandle* h) { delete h; }
+
+int64_t net_graph_node_count(const GraphHandle* h) { return h ? (int64_t)h->g.n : -1; }
+
+int64_t net_graph_edge_count(const GraphHandle* h) { return h ? (int64_t)h->g.m : -1; }
+
+int32_t net_degree(const GraphHandle* h, int32_t mode, int32_t loops, int32_t weighted,
+                   double* out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (mode < 1 || mode > 3) throw Error("unknown degree mode code " + std::to_string(mode));
+    if (weighted && !g.weighted) throw Error("the graph has no edge weights");
+    if (g.n == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    knb::DevBuf<double> d(g.n);
+    const knb::DevCsr* a = &g.out;
+    const knb::DevCsr* b = nullptr;
+    if (g.directed) {
+      if (mode == 2) a = &g.inc;
+      if (mode == 3) b = &g.inc;
+    }
+    degree_rows<<<knb::grid_for(g.n, 128), 128, 0, s>>>(
+        a->off.get(), a->tgt.get(), weighted ? a->w.get() : nullptr, b ? b->off.get() : nullptr,
+        b ? b->tgt.get() : nullptr, (b && weighted) ? b->w.get() : nullptr, g.n, g.directed ? 0 : 1,
+        loops != 0, d.get());
+    KNB_LAUNCH("degree_rows");
+    KNB_CUDA(cudaMemcpyAsync(out, d.get(), (size_t)g.n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t directed,
+                             int32_t weighted, const double* personalization, int pers_dev,
+                             int32_t dangling, int32_t loops, double tol, int64_t max_iter,
+                             int32_t precision, double* out, int out_dev, NetSolveInfo* info,
+                             char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (dangling != 0 && dangling != 1)
+      throw Error("unknown dangling-node code " + std::to_string(dangling));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (precision < 0 || precision > 2)
+      throw Error("unknown precision code " + std::to_string(precision));
+    knb::PagerankParams p;
+    p.damping = damping;
+    p.directed = directed != 0;
+    p.weighted = weighted != 0;
+    p.dangling = dangling;
+    p.loops = loops;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    p.precision = precision;
+    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    if (!(damping >= 0.0 && damping <= 1.0))
+      throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
+    if (g.n == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    if (p.weighted) check_nonnegative(g, "PageRank", s);
+    if (personalization) {
+      // checked and rescaled on the device (pagerank.cu, normalize_personalization)
+      p.personalization = personalization;
+      p.pers_on_device = pers_dev != 0;
+    }
+    knb::PagerankInfo pi;
+    knb::pagerank(g, p, out, out_dev != 0, &pi, s);
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->iterations = pi.iterations;
+      info->iterations_fp32 = pi.iterations_fp32;
+      info->change = pi.change;
+      info->seconds = pi.seconds;
+      info->converged = pi.converged;
+      info->kernel_launches = pi.kernel_launches;
+    }
+  });
+}
+
+int32_t net_pagerank(const GraphHandle* h, double damping, int32_t directed, int32_t weighted,
+                     const double* personalization, int32_t dangling, int32_t loops, double tol,
+                     int64_t max_iter, int32_t threads, double* out, char* err, size_t err_len) {
+  (void)threads;  // results never depend on it; the device decides the parallelism
+  return pagerank_impl(h, damping, directed, weighted, personalization, 0, dangling, loops, tol,
+                       max_iter, 0, out, 0, nullptr, err, err_len);
+}
+
+int32_t net_pagerank_ex(const GraphHandle* h, double damping, int32_t directed, int32_t weighted,
+                        const double* personalization, int32_t dangling, int32_t loops, double tol,
+                        int64_t max_iter, int32_t precision, double* out, NetSolveInfo* info,
+                        char* err, size_t err_len) {
+  return pagerank_impl(h, damping, directed, weighted, personalization, 0, dangling, loops, tol,
+                       max_iter, precision, out, 0, info, err, err_len);
+}
+
+int32_t net_pagerank_device(const GraphHandle* h, double damping, int32_t directed,
+                            int32_t weighted, const double* d_personalization, int32_t dangling,
+                            int32_t loops, double tol, int64_t max_iter, int32_t precision,
+                            double* d_out, NetSolveInfo* info, char* err, size_t err_len) {
+  return pagerank_impl(h, damping, directed, weighted, d_personalization, 1, dangling, loops, tol,
+                       max_iter, precision, d_out, 1, info, err, err_len);
+}
+
+static int32_t eigen_impl(const GraphHandle* h, int32_t mode, int32_t weighted, int32_t scale,
+                          int32_t loops, double tol, int64_t max_iter, int32_t precision,
+                          double* out, double* eigenvalue, int32_t* connected, NetSolveInfo* info,
+                          char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    // Codes decoded first, as the reference's C wrapper does
+    // (crates/capi/src/topography.rs:225-240).
+    if (mode < 1 || mode > 3) throw Error("unknown degree mode code " + std::to_string(mode));
+    if (scale != 0 && scale != 1)
+      throw Error("unknown eigenvector scale code " + std::to_string(scale));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (precision != 0 && precision != 1)
+      throw Error("unknown precision code " + std::to_string(precision));
+    knb::EigenParams p;
+    p.mode = mode;
+    p.weighted = weighted != 0;
+    p.scale = scale;
+    p.loops = loops;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    p.precision = precision;
+    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    cudaStream_t s = knb::thread_stream();
+    if (g.n > 0 && p.weighted) check_nonnegative(g, "eigenvector centrality", s);
+    knb::EigenResult r;
+    knb::eigenvector(g, p, out, &r, s);
+    if (eigenvalue) *eigenvalue = r.eigenvalue;
+    if (connected) *connected = r.connected ? 1 : 0;
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->iterations = r.matvecs;
+      info->iterations_fp32 = r.matvecs_fp32;
+      info->seconds = r.seconds;
+      info->converged = 1;
+      info->kernel_launches = r.kernel_launches;
+      info->eigenvalue = r.eigenvalue;
+      info->connected = r.connected ? 1 : 0;
+    }
+  });
+}
+
+int32_t net_eigenvector(const GraphHandle* h, int32_t mode, int32_t weighted, int32_t scale,
+                        int32_t loops, double tol, int64_t max_iter, int32_t threads, double* out,
+                        double* eigenvalue, int32_t* connected, char* err, size_t err_len) {
+  (void)threads;
+  return eigen_impl(h, mode, weighted, scale, loops, tol, max_iter, 0, out, eigenvalue, connected,
+                    nullptr, err, err_len);
+}
+
+int32_t net_eigenvector_ex(const GraphHandle* h, int32_t mode, int32_t weighted, int32_t scale,
+                           int32_t loops, double tol, int64_t max_iter, int32_t precision,
+                           double* out, double* eigenvalue, int32_t* connected,
+                           NetSolveInfo* info, char* err, size_t err_len) {
+  return eigen_impl(h, mode, weighted, scale, loops, tol, max_iter, precision, out, eigenvalue,
+                    connected, info, err, err_len);
+}
+
+int32_t net_generate_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                          uint64_t seed, int32_t clean, int32_t symmetrize, int32_t lognormal,
+                          uint64_t wseed, GraphHandle** out, int64_t* m_out, char* err,
+                          size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (edge_factor < 0) throw Error("edge factor must be non-negative");
+    cudaStream_t s = knb::thread_stream();
+    knb::RmatEdges e = knb::generate_rmat(scale, (uint64_t)edge_factor, a, b, c, seed, clean != 0,
+                                          symmetrize != 0, lognormal != 0, wseed, s);
+    auto h = std::make_unique<GraphHandle>();
+    knb::GraphHandleImpl& g = h->g;
+    g.n = e.n;
+    g.m = e.m;
+    g.directed = symmetrize == 0;
+    g.weighted = lognormal != 0;
+    KNB_CUDA(cudaGetDevice(&g.device));
+    g.src = std::move(e.src);
+    g.tgt = std::move(e.tgt);
+    if (g.weighted) {
+      g.w.alloc(std::max<uint64_t>(g.m, 1));
+      if (g.m) {
+        widen_weights<<<knb::grid_for(g.m, 256), 256, 0, s>>>(e.w32.get(), g.m, g.w.get());
+        KNB_LAUNCH("widen_weights");
+      }
+    }
+    finish_build(g, s);
+    if (m_out) *m_out = (int64_t)g.m;
+    *out = h.release();
+  });
+}
+
+int64_t net_graph_arc_count(const GraphHandle* h, int32_t which) {
+  if (!h) return -1;
+  const knb::GraphHandleImpl& g = h->g;
+  if (which == 1) return (int64_t)g.in_rows().arcs;
+  return (int64_t)g.out.arcs;
+}
+
+int32_t net_graph_csr(const GraphHandle* h, int32_t which, uint32_t* off, uint32_t* tgt,
+                      uint32_t* edge, double* w, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    cudaStream_t s = knb::thread_stream();
+    const knb::DevCsr* c = which == 1 ? &g.in_rows() : which == 2 ? &g.undirected_rows(s) : &g.out;
+    KNB_CUDA(cudaMemcpyAsync(off, c->off.get(), ((size_t)g.n + 1) * 4, cudaMemcpyDeviceToHost, s));
+    if (c->arcs) {
+      if (tgt) KNB_CUDA(cudaMemcpyAsync(tgt, c->tgt.get(), c->arcs * 4, cudaMemcpyDeviceToHost, s));
+      if (edge) KNB_CUDA(cudaMemcpyAsync(edge, c->edge.get(), c->arcs * 4, cudaMemcpyDeviceToHost, s));
+      if (w && g.weighted)
+        KNB_CUDA(cudaMemcpyAsync(w, c->w.get(), c->arcs * 8, cudaMemcpyDeviceToHost, s));
+    }
+    KNB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int32_t net_graph_new_device(int64_t n, const uint32_t* d_src, const uint32_t* d_tgt,
+                             const float* d_w32, const double* d_w64, int64_t m, int32_t directed,
+                             GraphHandle** out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (n < 0 || m < 0) throw Error("negative node or edge count");
+    if ((uint64_t)n > 0xFFFFFFFFull)
+      throw Error("node count (" + std::to_string(n) + ") exceeds the supported maximum");
+    if ((uint64_t)m > 0xFFFFFFFFull / 2)
+      throw Error("edge count (" + std::to_string(m) + ") exceeds the supported maximum");
+    cudaStream_t s = knb::thread_stream();
+    auto h = std::make_unique<GraphHandle>();
+    knb::GraphHandleImpl& g = h->g;
+    g.n = (uint32_t)n;
+    g.m = (uint64_t)m;
+    g.directed = directed != 0;
+    g.weighted = d_w32 != nullptr || d_w64 != nullptr;
+    KNB_CUDA(cudaGetDevice(&g.device));
+    g.src.alloc(std::max<uint64_t>(g.m, 1));
+    g.tgt.alloc(std::max<uint64_t>(g.m, 1));
+    knb::DevBuf<unsigned long long> bad(1);
+    if (m) {
+      KNB_CUDA(cudaMemcpyAsync(g.src.get(), d_src, m * 4, cudaMemcpyDeviceToDevice, s));
+      KNB_CUDA(cudaMemcpyAsync(g.tgt.get(), d_tgt, m * 4, cudaMemcpyDeviceToDevice, s));
+      KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+      check_u32_edges<<<knb::grid_for(m, 256), 256, 0, s>>>(g.src.get(), g.tgt.get(), m,
+                                                            (uint64_t)n, bad.get());
+      KNB_LAUNCH("check_u32_edges");
+      uint64_t b = read_u64(bad.get(), s);
+      if (b != NONE) throw Error("edge " + std::to_string(b / 2) + " refers to a node index out of range");
+    }
+    if (g.weighted) {
+      g.w.alloc(std::max<uint64_t>(g.m, 1));
+      if (m) {
+        if (d_w64) {
+          KNB_CUDA(cudaMemcpyAsync(g.w.get(), d_w64, m * 8, cudaMemcpyDeviceToDevice, s));
+        } else {
+          widen_weights<<<knb::grid_for(m, 256), 256, 0, s>>>(d_w32, m, g.w.get());
+          KNB_LAUNCH("widen_weights");
+        }
+        KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+        first_bad_weight<<<knb::grid_for(m, 256), 256, 0, s>>>(g.w.get(), m, 0, bad.get());
+        KNB_LAUNCH("first_bad_weight");
+        uint64_t e = read_u64(bad.get(), s);
+        if (e != NONE)
+          throw Error("edge " + std::to_string(e) + " has a missing, NaN, or infinite weight");
+      }
+    }
+    finish_build(g, s);
+    *out = h.release();
+  });
+}
+
+int32_t net_graph_edges(const GraphHandle* h, int64_t* src, int64_t* tgt, double* w, char* err,
+                        size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    cudaStream_t s = knb::thread_stream();
+    std::vector<uint32_t> a(g.m), b(g.m);
+    if (g.m) {
+      KNB_CUDA(cudaMemcpyAsync(a.data(), g.src.get(), g.m * 4, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaMemcpyAsync(b.data(), g.tgt.get(), g.m * 4, cudaMemcpyDeviceToHost, s));
+      if (w && g.weighted) KNB_CUDA(cudaMemcpyAsync(w, g.w.get(), g.m * 8, cudaMemcpyDeviceToHost, s));
+    }
+    KNB_CUDA(cudaStreamSynchronize(s));
+    for (uint64_t e = 0; e < g.m; ++e) {
+      if (src) src[e] = a[e];
+      if (tgt) tgt[e] = b[e];
+    }
+  });
+}
+
+int32_t net_sweep_timing(int32_t phase, int64_t* launches, double* total_ms,
+                         double* bytes_per_launch) {
+  knb::SweepTiming t = knb::last_sweep_timing(phase);
+  if (launches) *launches = t.launches;
+  if (total_ms) *total_ms = t.ms;
+  if (bytes_per_launch) *bytes_per_launch = t.bytes_per_launch;
+  return 0;
+}
+
+void net_set_sweep_timing(int32_t on) { knb::set_sweep_timing(on != 0); }
+
+int32_t net_set_tuning(int32_t key, double value) {
+  knb::Tuning& t = knb::tuning();
+  switch (key) {
+    case 0:
+      if (value != 0 && value != 4 && value != 8 && value != 16) return 1;
+      t.ipt = (int)value;
+      return 0;
+    case 1:
+      t.relabel = value != 0 ? 1 : 0;
+      return 0;
+    case 2:
+      if (!(value >= 1)) return 1;
+      t.switch_factor = value;
+      return 0;
+    case 3:
+      if (!(value >= 0)) return 1;
+      t.switch_floor = value;
+      return 0;
+    case 4:
+      if (value != 0 && value != 1 && value != 2) return 1;
+      t.variant = (int)value;
+      return 0;
+    default:
+      return 1;
+  }
+}
+
+int32_t net_device_sync(char* err, size_t err_len) {
+  return guard(err, err_len, [&] { KNB_CUDA(cudaDeviceSynchronize()); });
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// Shared device and host helpers of the knappnet B200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+
+namespace knb {
+
+// ---------------------------------------------------------------- errors
+// Every failure below the C ABI is a C++ exception carrying the message the
+// ABI writes into the caller's err buffer.
+struct Error : std::runtime_error {
+  explicit Error(const std::string& m) : std::runtime_error(m) {}
+};
+
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw Error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+#define KNB_CUDA(x) ::knb::cuda_check((x), #x)
+#define KNB_LAUNCH(what) ::knb::cuda_check(cudaGetLastError(), what)
+
+constexpr int WARP = 32;
+
+// ---------------------------------------------------------------- L2 cache policy
+// Streamed arrays (column indices, arc values) are read once per sweep and
+// should not push the gathered iterate out of the 126 MB L2; the iterate
+// should stay. createpolicy builds the 64-bit L2 cache-policy operands.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// Read-only loads with an L2 policy (ld.global.nc.L2::cache_hint). They are
+// not `volatile`, so the compiler may batch independent loads ahead of their
+// uses (a volatile asm would keep every gather in program order).
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p, uint64_t pol) {
+  uint32_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+               : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
+               : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
+               : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_keep(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+// ---------------------------------------------------------------- reductions
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide sum in a fixed order (warp butterflies, then warp 0 over the
+// warp totals), so the result is the same on every run. `scratch` holds at
+// least blockDim.x / 32 values. The total is returned to every thread.
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* scratch) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) scratch[w] = v;
+  __syncthreads();
+  T t = lane < nw ? scratch[lane] : T(0);
+  t = warp_sum(t);
+  return t;
+}
+template <class T>
+__device__ __forceinline__ T block_max(T v, T* scratch) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) scratch[w] = v;
+  __syncthreads();
+  T t = lane < nw ? scratch[lane] : T(-1e308);
+  t = warp_max(t);
+  return t;
+}
+
+// ---------------------------------------------------------------- launch helpers
+inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap = 148u * 32u) {
+  uint64_t g = (work + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+// Device memory owned by RAII (freed with cudaFree on destruction).
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) {
+      cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+      if (e != cudaSuccess) {
+        p = nullptr;
+        n = 0;
+        throw Error("out of device memory allocating " + std::to_string(count * sizeof(T)) +
+                    " bytes");
+      }
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  T* get() const { return p; }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace knb

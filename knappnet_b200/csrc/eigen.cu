@@ -1,0 +1,1357 @@
+// Eigenvector centrality on the device (reference:
+// crates/engine/src/metrics/eigenvector.rs:229-1137).
+//
+// - Directed matrices: power iteration on A' + I, rescaled to a largest
+//   entry of 1 after every product, stopped when no entry changes by more
+//   than tol (eigenvector.rs:330-374). One step is the merge-path product
+//   with the shift fused into its epilogue (y = A'x + x and the block
+//   maximum), the split-row kernel, and a vertex kernel that divides by the
+//   maximum and reduces the infinity-norm change.
+// - Symmetric matrices: per weak component, thick-restart Lanczos with full
+//   reorthogonalisation (classical Gram-Schmidt with the DGKS test) and the
+//   reference's constants (basis <= 20, keep 8, a convergence check every 4
+//   steps, a true-residual check of every candidate; eigenvector.rs:729-878).
+//   The basis, the products, the projections and the norms live on the
+//   device; the DGKS decision is taken on the device, and the host only runs
+//   the <= 20 x 20 projected eigenproblem at each check. Sums over vectors
+//   use fixed 4096-row blocks added in a fixed order (eigenvector.rs:913-971),
+//   so the results do not change from run to run.
+// - Components: weak components by a concurrent union-find on the device
+//   whose roots are the smallest node of each component, relabelled in order
+//   of their smallest node (topography.rs:183-246); strong components (for
+//   directed matrices) by Tarjan's algorithm on the host (topography.rs:248-305).
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "eigen.cuh"
+
+namespace knb {
+
+// ======================================================================= dense eigensolver
+// Householder tridiagonalisation with accumulated transformations and the
+// implicit QL method (EISPACK tred2 / tql2; Martin, Reinsch and Wilkinson),
+// in EISPACK's order of operations. V is row-major n x n.
+bool symmetric_eigen(const double* a, int n, double* d, double* V) {
+  if (n == 0) return true;
+  std::vector<double> e(n, 0.0);
+  std::memcpy(V, a, sizeof(double) * n * n);
+  auto at = [&](int r, int c) -> double& { return V[r * n + c]; };
+  // tred2
+  for (int j = 0; j < n; ++j) d[j] = at(n - 1, j);
+  for (int i = n - 1; i > 0; --i) {
+    double scale = 0.0, h = 0.0;
+    for (int k = 0; k < i; ++k) scale += std::fabs(d[k]);
+    if (scale == 0.0) {
+      e[i] = d[i - 1];
+      for (int j = 0; j < i; ++j) {
+        d[j] = at(i - 1, j);
+        at(i, j) = 0.0;
+        at(j, i) = 0.0;
+      }
+    } else {
+      for (int k = 0; k < i; ++k) {
+        d[k] /= scale;
+        h += d[k] * d[k];
+      }
+      double f = d[i - 1], g = std::sqrt(h);
+      if (f > 0) g = -g;
+      e[i] = scale * g;
+      h -= f * g;
+      d[i - 1] = f - g;
+      for (int j = 0; j < i; ++j) e[j] = 0.0;
+      for (int j = 0; j < i; ++j) {
+        f = d[j];
+        at(j, i) = f;
+        g = e[j] + at(j, j) * f;
+        for (int k = j + 1; k < i; ++k) {
+          g += at(k, j) * d[k];
+          e[k] += at(k, j) * f;
+        }
+        e[j] = g;
+      }
+      f = 0.0;
+      for (int j = 0; j < i; ++j) {
+        e[j] /= h;
+        f += e[j] * d[j];
+      }
+      const double hh = f / (h + h);
+      for (int j = 0; j < i; ++j) e[j] -= hh * d[j];
+      for (int j = 0; j < i; ++j) {
+        f = d[j];
+        g = e[j];
+        for (int k = j; k < i; ++k) at(k, j) -= (f * e[k] + g * d[k]);
+        d[j] = at(i - 1, j);
+        at(i, j) = 0.0;
+      }
+    }
+    d[i] = h;
+  }
+  for (int i = 0; i < n - 1; ++i) {
+    at(n - 1, i) = at(i, i);
+    at(i, i) = 1.0;
+    const double h = d[i + 1];
+    if (h != 0.0) {
+      for (int k = 0; k <= i; ++k) d[k] = at(k, i + 1) / h;
+      for (int j = 0; j <= i; ++j) {
+        double g = 0.0;
+        for (int k = 0; k <= i; ++k) g += at(k, i + 1) * at(k, j);
+        for (int k = 0; k <= i; ++k) at(k, j) -= g * d[k];
+      }
+    }
+    for (int k = 0; k <= i; ++k) at(k, i + 1) = 0.0;
+  }
+  for (int j = 0; j < n; ++j) {
+    d[j] = at(n - 1, j);
+    at(n - 1, j) = 0.0;
+  }
+  at(n - 1, n - 1) = 1.0;
+  e[0] = 0.0;
+  // tql2
+  for (int i = 1; i < n; ++i) e[i - 1] = e[i];
+  e[n - 1] = 0.0;
+  double f = 0.0, tst1 = 0.0;
+  const double eps = DBL_EPSILON;
+  for (int l = 0; l < n; ++l) {
+    tst1 = std::max(tst1, std::fabs(d[l]) + std::fabs(e[l]));
+    int m = l;
+    while (m < n && !(std::fabs(e[m]) <= eps * tst1)) ++m;
+    if (m > l) {
+      int iter = 0;
+      do {
+        if (++iter > 60) return false;
+        double g = d[l];
+        double p = (d[l + 1] - g) / (2.0 * e[l]);
+        double r = std::hypot(p, 1.0);
+        if (p < 0) r = -r;
+        d[l] = e[l] / (p + r);
+        d[l + 1] = e[l] * (p + r);
+        const double dl1 = d[l + 1];
+        double h = g - d[l];
+        for (int i = l + 2; i < n; ++i) d[i] -= h;
+        f += h;
+        p = d[m];
+        double c = 1.0, c2 = c, c3 = c, s = 0.0, s2 = 0.0;
+        const double el1 = e[l + 1];
+        for (int i = m - 1; i >= l; --i) {
+          c3 = c2;
+          c2 = c;
+          s2 = s;
+          g = c * e[i];
+          h = c * p;
+          r = std::hypot(p, e[i]);
+          e[i + 1] = s * r;
+          s = e[i] / r;
+          c = p / r;
+          p = c * d[i] - s * g;
+          d[i + 1] = h + s * (c * g + s * d[i]);
+          for (int k = 0; k < n; ++k) {
+            h = at(k, i + 1);
+            at(k, i + 1) = s * at(k, i) + c * h;
+            at(k, i) = c * at(k, i) - s * h;
+          }
+        }
+        p = -s * s2 * c3 * el1 * e[l] / dl1;
+        e[l] = s * p;
+        d[l] = c * p;
+      } while (std::fabs(e[l]) > eps * tst1);
+    }
+    d[l] += f;
+    e[l] = 0.0;
+  }
+  for (int i = 0; i < n - 1; ++i) {
+    int k = i;
+    double p = d[i];
+    for (int j = i + 1; j < n; ++j)
+      if (d[j] < p) {
+        k = j;
+        p = d[j];
+      }
+    if (k != i) {
+      d[k] = d[i];
+      d[i] = p;
+      for (int r = 0; r < n; ++r) std::swap(at(r, i), at(r, k));
+    }
+  }
+  return true;
+}
+
+// ======================================================================= components
+constexpr int ET = 256;
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t v) {
+  uint32_t p = parent[v];
+  while (p != v) {
+    uint32_t gp = parent[p];
+    if (gp != p) parent[v] = gp;  // path halving; races only shorten paths
+    v = p;
+    p = gp;
+  }
+  return v;
+}
+
+__global__ void uf_init(uint32_t* parent, uint32_t n) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    parent[v] = v;
+}
+
+// Union by smaller root with compare-and-swap: a root only ever hooks under
+// a smaller root, so every final root is its component's smallest node.
+__global__ void uf_union(uint32_t* parent, const uint32_t* __restrict__ src,
+                         const uint32_t* __restrict__ tgt, uint64_t m) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = uf_find(parent, src[e]), b = uf_find(parent, tgt[e]);
+    while (a != b) {
+      uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+      uint32_t old = atomicCAS(&parent[hi], hi, lo);
+      if (old == hi) break;
+      a = uf_find(parent, old);
+      b = uf_find(parent, lo);
+    }
+  }
+}
+
+__global__ void uf_roots(uint32_t* parent, uint32_t n, uint32_t* root, uint32_t* is_root) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    uint32_t r = uf_find(parent, v);
+    root[v] = r;
+    is_root[v] = r == v;
+  }
+}
+
+__global__ void uf_label(const uint32_t* __restrict__ root, const uint32_t* __restrict__ rank,
+                         uint32_t n, uint32_t* __restrict__ label, uint32_t* __restrict__ sizes) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    uint32_t c = rank[root[v]];
+    label[v] = c;
+    atomicAdd(&sizes[c], 1u);
+  }
+}
+
+struct Comps {
+  std::vector<uint32_t> membership;
+  std::vector<uint32_t> sizes;
+  size_t count() const { return sizes.size(); }
+};
+
+static Comps weak_components(GraphHandleImpl& g, cudaStream_t s) {
+  const uint32_t n = g.n;
+  DevBuf<uint32_t> parent(n), root(n), flag(n + 1), label(n);
+  uf_init<<<grid_for(n, ET), ET, 0, s>>>(parent.get(), n);
+  if (g.m) uf_union<<<grid_for(g.m, ET), ET, 0, s>>>(parent.get(), g.src.get(), g.tgt.get(), g.m);
+  uf_roots<<<grid_for(n, ET), ET, 0, s>>>(parent.get(), n, root.get(), flag.get());
+  KNB_LAUNCH("weak components");
+  uint32_t k = exclusive_scan<uint32_t>(flag.get(), flag.get(), n, s);
+  DevBuf<uint32_t> sizes(std::max<uint32_t>(k, 1));
+  KNB_CUDA(cudaMemsetAsync(sizes.get(), 0, (size_t)std::max<uint32_t>(k, 1) * 4, s));
+  uf_label<<<grid_for(n, ET), ET, 0, s>>>(root.get(), flag.get(), n, label.get(), sizes.get());
+  KNB_LAUNCH("uf_label");
+  Comps c;
+  c.membership.resize(n);
+  c.sizes.resize(k);
+  KNB_CUDA(cudaMemcpyAsync(c.membership.data(), label.get(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  if (k) KNB_CUDA(cudaMemcpyAsync(c.sizes.data(), sizes.get(), (size_t)k * 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  return c;
+}
+
+// Tarjan's algorithm with an explicit stack over the out-CSR (host).
+static Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint32_t>& tgt,
+                               uint32_t n) {
+  const uint32_t UNSEEN = 0xFFFFFFFFu;
+  std::vector<uint32_t> index(n, UNSEEN), low(n, 0), comp(n, UNSEEN), stack;
+  std::vector<uint8_t> on(n, 0);
+  std::vector<std::pair<uint32_t, uint32_t>> frames;
+  uint32_t counter = 0, ncomp = 0;
+  for (uint32_t root = 0; root < n; ++root) {
+    if (index[root] != UNSEEN) continue;
+    frames.push_back({root, 0});
+    index[root] = low[root] = counter++;
+    stack.push_back(root);
+    on[root] = 1;
+    while (!frames.empty()) {
+      uint32_t v = frames.back().first;
+      uint32_t& pos = frames.back().second;
+      if (pos < off[v + 1] - off[v]) {
+        uint32_t w = tgt[off[v] + pos];
+        ++pos;
+        if (index[w] == UNSEEN) {
+          index[w] = low[w] = counter++;
+          stack.push_back(w);
+          on[w] = 1;
+          frames.push_back({w, 0});
+        } else if (on[w]) {
+          low[v] = std::min(low[v], index[w]);
+        }
+        continue;
+      }
+      frames.pop_back();
+      if (!frames.empty()) low[frames.back().first] = std::min(low[frames.back().first], low[v]);
+      if (low[v] == index[v]) {
+        for (;;) {
+          uint32_t w = stack.back();
+          stack.pop_back();
+          on[w] = 0;
+          comp[w] = ncomp;
+          if (w == v) break;
+        }
+        ++ncomp;
+      }
+    }
+  }
+  Comps c;
+  std::vector<uint32_t> relabel(n, UNSEEN);
+  c.membership.resize(n);
+  for (uint32_t v = 0; v < n; ++v) {
+    uint32_t r = comp[v];
+    if (relabel[r] == UNSEEN) {
+      relabel[r] = (uint32_t)c.sizes.size();
+      c.sizes.push_back(0);
+    }
+    c.membership[v] = relabel[r];
+    c.sizes[relabel[r]]++;
+  }
+  return c;
+}
+
+// ======================================================================= small kernels
+// Any arc (v, j) inside one component with a positive value (a cycle of
+// positive weight; eigenvector.rs:283-287).
+__global__ void cyclic_arcs(OpView<double> op, const uint32_t* __restrict__ comp,
+                            unsigned int* __restrict__ flag) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < op.n; v += gridDim.x * blockDim.x) {
+    for (uint32_t k = op.off[v]; k < op.off[v + 1]; ++k) {
+      double w = op.vals ? op.vals[k] : 1.0;
+      if (w > 0.0 && comp[op.cols[k]] == comp[v]) {
+        *flag = 1u;
+        return;
+      }
+    }
+  }
+}
+
+// Nodes whose column has no positive entry score 1 (eigenvector.rs:288-298).
+__global__ void sink_scores(OpView<double> op, double* __restrict__ x) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < op.n; v += gridDim.x * blockDim.x)
+    for (uint32_t k = op.off[v]; k < op.off[v + 1]; ++k) {
+      double w = op.vals ? op.vals[k] : 1.0;
+      if (w > 0.0) x[op.cols[k]] = 0.0;
+    }
+}
+
+__global__ void fill_value(double* x, uint32_t n, double v) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+// Row sum and the sum of squares with parallel entries merged
+// (eigenvector.rs:566-584).
+__global__ void op_row_sums(OpView<double> op, double* __restrict__ s_out,
+                            double* __restrict__ q_out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < op.n; v += gridDim.x * blockDim.x) {
+    double s = 0, q = 0, acc = 0;
+    uint32_t c = 0xFFFFFFFFu;
+    for (uint32_t k = op.off[v]; k < op.off[v + 1]; ++k) {
+      uint32_t j = op.cols[k];
+      double w = op.vals ? op.vals[k] : 1.0;
+      s += w;
+      if (j == c) {
+        acc += w;
+      } else {
+        if (c != 0xFFFFFFFFu) q += acc * acc;
+        c = j;
+        acc = w;
+      }
+    }
+    if (c != 0xFFFFFFFFu) q += acc * acc;
+    s_out[v] = s;
+    q_out[v] = q;
+  }
+}
+
+// Submatrix rows of `nodes` with columns renumbered by `local`
+// (eigenvector.rs:589-624): lengths, then copies.
+__global__ void sub_lengths(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nodes,
+                            uint32_t k, uint32_t* __restrict__ len) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    uint32_t v = nodes[i];
+    len[i] = off[v + 1] - off[v];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) len[k] = 0;
+}
+
+__global__ void sub_copy(OpView<double> op, const uint32_t* __restrict__ nodes, uint32_t k,
+                         const uint32_t* __restrict__ local, const uint32_t* __restrict__ soff,
+                         uint32_t* __restrict__ scols, double* __restrict__ s64,
+                         float* __restrict__ s32) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    uint32_t v = nodes[i];
+    uint32_t o = soff[i];
+    for (uint32_t q = op.off[v]; q < op.off[v + 1]; ++q, ++o) {
+      scols[o] = local[op.cols[q]];
+      if (op.vals) {
+        s64[o] = op.vals[q];
+        s32[o] = (float)op.vals[q];
+      }
+    }
+  }
+}
+
+__global__ void scatter_local(const uint32_t* __restrict__ nodes, uint32_t k,
+                              uint32_t* __restrict__ local) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
+    local[nodes[i]] = i;
+}
+
+__global__ void scatter_scaled(const uint32_t* __restrict__ nodes, uint32_t k,
+                               const double* __restrict__ u, double factor, double* __restrict__ x) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
+    x[nodes[i]] = u[i] * factor;
+}
+
+// ======================================================================= vector kernels
+// Fixed 4096-row blocks (eigenvector.rs:913-971): one CTA per block writes
+// its partial sums; the last CTA adds the partials in block order (lane l
+// takes blocks l, l + 32, ...; then a fixed butterfly), so sums are
+// reproducible.
+constexpr int VB = 4096;
+constexpr int VB_T = 256;
+constexpr int MAXB = 20;  // largest basis (eigenvector.rs:730)
+
+struct LzState {
+  double coef[MAXB];   // Gram-Schmidt coefficients of the current step
+  double tmp[MAXB];    // coefficients of the current pass
+  double before, mid, after, beta;
+  double xx, xy, value, rinf, xinf, sum;
+  int32_t need2;       // second full DGKS pass needed
+  int32_t breakdown;   // set at the step where beta <= 1e-12 * before
+  int32_t bd_step;     // that step's j
+  int32_t pad;
+  uint32_t ticket;
+};
+
+__device__ __forceinline__ double fixed_block_sum(const double* part, uint32_t nb, int stride,
+                                                  int slot) {
+  // called by one full warp
+  const volatile double* p = part;
+  int lane = threadIdx.x & 31;
+  double a = 0;
+  for (uint32_t b = lane; b < nb; b += 32) a += p[(size_t)b * stride + slot];
+  return warp_sum(a);
+}
+
+__device__ __forceinline__ bool lz_last(unsigned int* ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Block-level sums of K values per thread; writes part[blockIdx * stride + s].
+template <int K>
+__device__ __forceinline__ void block_partials(double (&a)[K], double* part, int stride, int count) {
+  __shared__ double sh[VB_T / 32][MAXB + 2];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int s = 0; s < count; ++s) {
+    double v = warp_sum(a[s]);
+    if (lane == 0) sh[w][s] = v;
+  }
+  __syncthreads();
+  if (w == 0) {
+    for (int s = 0; s < count; ++s) {
+      double v = lane < VB_T / 32 ? sh[lane][s] : 0.0;
+      v = warp_sum(v);
+      if (lane == 0) part[(size_t)blockIdx.x * stride + s] = v;
+    }
+  }
+}
+
+// mode 0: local pass (also computes ||w||^2 -> before); 1: full pass; 2: full
+// pass 2 (skipped unless need2). Projects w on V[lo..hi).
+__global__ void __launch_bounds__(VB_T)
+lz_project(const double* __restrict__ V, size_t dim, int lo, int hi, const double* __restrict__ w,
+           int mode, double* __restrict__ part, LzState* st, const IterState* ist) {
+  if (ist && iteration_done(ist)) return;
+  if (mode == 2 && !st->need2) return;
+  const int K = hi - lo;
+  double a[MAXB + 1];
+#pragma unroll
+  for (int s = 0; s <= MAXB; ++s) a[s] = 0.0;
+  size_t r0 = (size_t)blockIdx.x * VB, r1 = min(dim, r0 + VB);
+  for (size_t i = r0 + threadIdx.x; i < r1; i += VB_T) {
+    double wi = w[i];
+#pragma unroll
+    for (int s = 0; s < MAXB; ++s)
+      if (s < K) a[s] += V[(size_t)(lo + s) * dim + i] * wi;
+    a[MAXB] += wi * wi;
+  }
+  // pack the norm after the K coefficients
+  a[K] = a[MAXB];
+  block_partials<MAXB + 1>(a, part, MAXB + 1, K + 1);
+  if (!lz_last(&st->ticket)) return;
+  if (threadIdx.x < 32) {
+    for (int s = 0; s <= K; ++s) {
+      double v = fixed_block_sum(part, gridDim.x, MAXB + 1, s);
+      if (threadIdx.x == 0) {
+        if (s < K) st->tmp[s] = v;
+        else if (mode == 0) st->before = sqrt(v);
+      }
+    }
+  }
+  if (threadIdx.x == 0) st->ticket = 0;
+}
+
+// w -= V[lo..hi) tmp, ||w|| into mid (mode 0) or after; coefficients added
+// into coef; the DGKS decision after full passes (eigenvector.rs:997-1021).
+__global__ void __launch_bounds__(VB_T)
+lz_subtract(const double* __restrict__ V, size_t dim, int lo, int hi, double* __restrict__ w,
+            int mode, double* __restrict__ part, LzState* st, const IterState* ist) {
+  if (ist && iteration_done(ist)) return;
+  if (mode == 2 && !st->need2) return;
+  const int K = hi - lo;
+  __shared__ double c[MAXB];
+  if (threadIdx.x < K) c[threadIdx.x] = st->tmp[threadIdx.x];
+  __syncthreads();
+  double a[1] = {0.0};
+  size_t r0 = (size_t)blockIdx.x * VB, r1 = min(dim, r0 + VB);
+  for (size_t i = r0 + threadIdx.x; i < r1; i += VB_T) {
+    double x = w[i];
+    for (int s = 0; s < K; ++s) x -= c[s] * V[(size_t)(lo + s) * dim + i];
+    w[i] = x;
+    a[0] += x * x;
+  }
+  block_partials<1>(a, part, 1, 1);
+  if (!lz_last(&st->ticket)) return;
+  if (threadIdx.x < 32) {
+    double v = sqrt(fixed_block_sum(part, gridDim.x, 1, 0));
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < K; ++s) st->coef[lo + s] += st->tmp[s];
+      if (mode == 0) {
+        st->mid = v;
+      } else if (mode == 1) {
+        st->after = v;
+        bool done = v >= M_SQRT1_2 * st->mid || v == 0.0 || st->mid == st->before;
+        st->need2 = done ? 0 : 1;
+        if (!done) st->mid = st->before;
+      } else {
+        st->after = v;
+      }
+      st->ticket = 0;
+    }
+  }
+}
+
+// Start of a step: zero the coefficients.
+__global__ void lz_begin(LzState* st, const IterState* ist) {
+  if (ist && iteration_done(ist)) return;
+  if (threadIdx.x < MAXB) st->coef[threadIdx.x] = 0.0;
+  if (threadIdx.x == 0) st->need2 = 0;
+}
+
+// End of a step: coefficients into the projected matrix, beta, breakdown
+// (eigenvector.rs:786-796).
+__global__ void lz_end(LzState* st, IterState* ist, double* hm, int m, int j) {
+  if (iteration_done(ist)) return;
+  if (threadIdx.x < j + 1) {
+    hm[threadIdx.x * m + j] = st->coef[threadIdx.x];
+    hm[j * m + threadIdx.x] = st->coef[threadIdx.x];
+  }
+  if (threadIdx.x == 0) {
+    double beta = st->after;
+    st->beta = beta;
+    bool bd = beta <= 1e-12 * st->before || isnan(beta);
+    if (bd) {
+      st->breakdown = 1;
+      st->bd_step = j;
+      ist->stopped = 1;  // later enqueued steps do nothing
+    }
+  }
+}
+
+// v = w / beta into basis column `col` (and its FP32 copy); hm(col, col-1).
+__global__ void lz_next(double* __restrict__ V, size_t dim, int col, const double* __restrict__ w,
+                        float* __restrict__ v32, double* hm, int m, const LzState* st,
+                        const IterState* ist, int set_hm) {
+  if (ist && iteration_done(ist)) return;
+  const double beta = st->beta;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double v = w[i] / beta;
+    V[(size_t)col * dim + i] = v;
+    if (v32) v32[i] = (float)v;
+  }
+  if (set_hm && blockIdx.x == 0 && threadIdx.x == 0) {
+    hm[col * m + col - 1] = beta;
+    hm[(col - 1) * m + col] = beta;
+  }
+}
+
+// x = V[0..cols) s (eigenvector.rs:1080-1092).
+__global__ void lz_combine(const double* __restrict__ V, size_t dim, int cols,
+                           const double* __restrict__ s, double* __restrict__ x) {
+  __shared__ double c[MAXB];
+  if (threadIdx.x < cols) c[threadIdx.x] = s[threadIdx.x];
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double o = 0.0;
+    for (int l = 0; l < cols; ++l) o += c[l] * V[(size_t)l * dim + i];
+    x[i] = o;
+  }
+}
+
+// V[:, 0..p) = V[:, 0..cols) S (S row-major cols x p) via `out` (p vectors).
+__global__ void lz_rotate(const double* __restrict__ V, size_t dim, int cols,
+                          const double* __restrict__ S, int p, double* __restrict__ out) {
+  __shared__ double c[MAXB * MAXB];
+  for (int k = threadIdx.x; k < cols * p; k += blockDim.x) c[k] = S[k];
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double o[MAXB];
+    for (int q = 0; q < p; ++q) o[q] = 0.0;
+    for (int l = 0; l < cols; ++l) {
+      double x = V[(size_t)l * dim + i];
+      for (int q = 0; q < p; ++q) o[q] += c[l * p + q] * x;
+    }
+    for (int q = 0; q < p; ++q) out[(size_t)q * dim + i] = o[q];
+  }
+}
+
+// xx = x.x, xy = x.y, sum = sum(x); the last CTA sets value = xy / xx.
+__global__ void __launch_bounds__(VB_T)
+lz_dots(const double* __restrict__ x, const double* __restrict__ y, size_t dim,
+        double* __restrict__ part, LzState* st) {
+  double a[3] = {0, 0, 0};
+  size_t r0 = (size_t)blockIdx.x * VB, r1 = min(dim, r0 + VB);
+  for (size_t i = r0 + threadIdx.x; i < r1; i += VB_T) {
+    double xi = x[i];
+    a[0] += xi * xi;
+    a[1] += xi * (y ? y[i] : 0.0);
+    a[2] += xi;
+  }
+  block_partials<3>(a, part, 3, 3);
+  if (!lz_last(&st->ticket)) return;
+  if (threadIdx.x < 32) {
+    double xx = fixed_block_sum(part, gridDim.x, 3, 0);
+    double xy = fixed_block_sum(part, gridDim.x, 3, 1);
+    double sm = fixed_block_sum(part, gridDim.x, 3, 2);
+    if (threadIdx.x == 0) {
+      st->xx = xx;
+      st->xy = xy;
+      st->sum = sm;
+      st->value = xy / xx;
+      st->ticket = 0;
+    }
+  }
+}
+
+// rinf = max |y - value x|, xinf = max |x| (eigenvector.rs:811-818).
+__global__ void __launch_bounds__(VB_T)
+lz_resid(const double* __restrict__ x, const double* __restrict__ y, size_t dim,
+         double* __restrict__ part, LzState* st) {
+  const double value = st->value;
+  double r = 0, xm = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x) {
+    r = fmax(r, fabs(y[i] - value * x[i]));
+    xm = fmax(xm, fabs(x[i]));
+  }
+  __shared__ double sh[2][VB_T / 32];
+  r = warp_max(r);
+  xm = warp_max(xm);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[0][w] = r;
+    sh[1][w] = xm;
+  }
+  __syncthreads();
+  if (w == 0) {
+    r = warp_max(lane < VB_T / 32 ? sh[0][lane] : 0.0);
+    xm = warp_max(lane < VB_T / 32 ? sh[1][lane] : 0.0);
+    if (lane == 0) {
+      part[blockIdx.x * 2] = r;
+      part[blockIdx.x * 2 + 1] = xm;
+    }
+  }
+  if (!lz_last(&st->ticket)) return;
+  if (threadIdx.x < 32) {
+    const volatile double* p = part;
+    double a = 0, b = 0;
+    for (uint32_t q = threadIdx.x; q < gridDim.x; q += 32) {
+      a = fmax(a, p[q * 2]);
+      b = fmax(b, p[q * 2 + 1]);
+    }
+    a = warp_max(a);
+    b = warp_max(b);
+    if (threadIdx.x == 0) {
+      st->rinf = a;
+      st->xinf = b;
+      st->ticket = 0;
+    }
+  }
+}
+
+// finish_vector (eigenvector.rs:880-899): sign by the sum, clamp negatives.
+__global__ void lz_sign_clamp(double* x, size_t dim, const LzState* st) {
+  const double sgn = st->sum < 0.0 ? -1.0 : 1.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double v = x[i] * sgn;
+    x[i] = v < 0.0 ? 0.0 : v;
+  }
+}
+
+__global__ void scale_by(double* x, size_t dim, double f, int divide) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = divide ? x[i] / f : x[i] * f;
+}
+
+__global__ void to_float(const double* __restrict__ x, size_t dim, float* __restrict__ y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
+// ======================================================================= epilogues
+// y_i = (A x)_i in FP64.
+template <class VT>
+struct PlainEpi {
+  static constexpr int NACC = 0;
+  double* y;
+  __device__ __forceinline__ void prepare(const IterState*) {}
+  static __device__ __forceinline__ void init(double*) {}
+  static __device__ __forceinline__ double identity(int) { return 0.0; }
+  static __device__ __forceinline__ double combine(int, double a, double b) { return a + b; }
+  static __device__ __forceinline__ double warp_combine(int, double v) { return v; }
+  __device__ __forceinline__ void row(uint32_t g, VT s, double*) const { y[g] = (double)s; }
+  __device__ void finish(IterState*, const double*) const {}
+};
+
+// Power iteration on A' + I: y_i = (A' x)_i + x_i and the largest y.
+struct PowerEpi {
+  static constexpr int NACC = 1;
+  const double* x;
+  double* y;
+  __device__ __forceinline__ void prepare(const IterState*) {}
+  static __device__ __forceinline__ void init(double* a) { a[0] = 0.0; }
+  static __device__ __forceinline__ double identity(int) { return 0.0; }
+  static __device__ __forceinline__ double combine(int, double a, double b) { return fmax(a, b); }
+  static __device__ __forceinline__ double warp_combine(int, double v) { return warp_max(v); }
+  __device__ __forceinline__ void row(uint32_t g, double s, double* a) const {
+    double v = s + x[g];
+    y[g] = v;
+    a[0] = fmax(a[0], v);
+  }
+  __device__ void finish(IterState* st, const double* tot) const { st->top = tot[0]; }
+};
+
+// x_new = y / top; change = max |x_new - x_old| (eigenvector.rs:341-347).
+__global__ void power_vertex(const double* __restrict__ x_old, const double* __restrict__ y,
+                             double* __restrict__ x_new, uint32_t n, double* __restrict__ part,
+                             IterState* st) {
+  if (iteration_done(st)) return;
+  const double top = st->top;
+  double ch = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = y[i] / top;
+    x_new[i] = v;
+    ch = fmax(ch, fabs(v - x_old[i]));
+  }
+  __shared__ double sh[VB_T / 32];
+  ch = block_max(ch, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = ch;
+  if (!lz_last(&st->ticket2)) return;
+  if (threadIdx.x < 32) {
+    const volatile double* p = part;
+    double a = 0;
+    for (uint32_t q = threadIdx.x; q < gridDim.x; q += 32) a = fmax(a, p[q]);
+    a = warp_max(a);
+    if (threadIdx.x == 0) {
+      st->change = a;
+      st->iter += 1;
+      if (a <= st->tol) st->converged = 1;
+      else if (st->iter >= st->max_iter) st->stopped = 1;
+      st->ticket2 = 0;
+    }
+  }
+}
+
+// ======================================================================= products
+// A device operator (a whole operator or a component's submatrix).
+struct DevOp {
+  uint32_t n = 0;
+  uint64_t nnz = 0;
+  const uint32_t* off = nullptr;
+  const uint32_t* cols = nullptr;
+  const double* v64 = nullptr;
+  const float* v32 = nullptr;
+  const Partition* part = nullptr;
+  // owned storage for submatrices
+  DevBuf<uint32_t> own_off, own_cols;
+  DevBuf<double> own_v64;
+  DevBuf<float> own_v32;
+  std::unique_ptr<Partition> own_part;
+  OpView<double> view64() const { return {n, nnz, off, cols, v64}; }
+  OpView<float> view32() const { return {n, nnz, off, cols, v32}; }
+};
+
+struct SpmvScratch {
+  DevBuf<double> carry64, head64, part1, part2;
+  DevBuf<float> carry32, head32;
+  void ensure(uint32_t ntiles) {
+    if (carry64.n < ntiles + 1) {
+      carry64.alloc(ntiles + 1);
+      head64.alloc(ntiles + 1);
+      carry32.alloc(ntiles + 1);
+      head32.alloc(ntiles + 1);
+      part1.alloc((size_t)ntiles * 2 + 2);
+      part2.alloc(SPLIT_CTAS * 2 + 2);
+    }
+  }
+};
+
+constexpr int EIG_IPT = 8;
+// Relative residual below which FP32 products stop helping the Lanczos
+// process (FP32 rounding of the products is about 1e-7 relative).
+constexpr double FP32_FLOOR = 1e-5;
+
+// y = A x (FP64 or, with x32 given, FP32 products accumulated in FP32).
+static int spmv(const DevOp& A, const double* x, const float* x32, double* y, SpmvScratch& sc,
+                const IterState* ist, cudaStream_t s) {
+  const Partition& P = *A.part;
+  sc.ensure(P.ntiles);
+  const unsigned g2 = SPLIT_CTAS;
+  if (x32) {
+    PlainEpi<float> e{y};
+    constexpr size_t sm = tile_smem_bytes<float, EIG_IPT>();
+    tile_spmv<float, float, PlainEpi<float>, EIG_IPT><<<P.ntiles, SPMV_THREADS, sm, s>>>(
+        A.view32(), x32, e, P.coords.get(), sc.carry32.get(), sc.head32.get(), sc.part1.get(), ist);
+    split_rows<float, PlainEpi<float>><<<g2, SPMV_THREADS, 0, s>>>(
+        P.split.get(), P.nsplit, P.nshort, sc.carry32.get(), sc.head32.get(), e, sc.part1.get(), P.ntiles,
+        sc.part2.get(), const_cast<IterState*>(ist));
+  } else {
+    PlainEpi<double> e{y};
+    constexpr size_t sm = tile_smem_bytes<double, EIG_IPT>();
+    tile_spmv<double, double, PlainEpi<double>, EIG_IPT><<<P.ntiles, SPMV_THREADS, sm, s>>>(
+        A.view64(), x, e, P.coords.get(), sc.carry64.get(), sc.head64.get(), sc.part1.get(), ist);
+    split_rows<double, PlainEpi<double>><<<g2, SPMV_THREADS, 0, s>>>(
+        P.split.get(), P.nsplit, P.nshort, sc.carry64.get(), sc.head64.get(), e, sc.part1.get(), P.ntiles,
+        sc.part2.get(), const_cast<IterState*>(ist));
+  }
+  KNB_LAUNCH("spmv");
+  return 2;
+}
+
+// ======================================================================= Lanczos
+struct Leading {
+  double value = 0;
+  int64_t matvecs = 0;
+  int64_t matvecs32 = 0;
+};
+
+// Thick-restart Lanczos (eigenvector.rs:746-878) on device operator A from
+// the all-ones vector; the unit eigenvector is left in `xout` (device).
+static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t max_matvecs,
+                              bool mixed, double* xout, Leading* res, int* launches,
+                              cudaStream_t s) {
+  const size_t dim = A.n;
+  const int m = (int)std::max<size_t>(
+      1, std::min<size_t>(std::min<size_t>(dim, MAXB), std::max<size_t>((1ull << 27) / dim, 8)));
+  const int keep = std::max(1, std::min(8, m >= 2 ? m - 2 : 0));
+  const unsigned nb = (unsigned)((dim + VB - 1) / VB);
+  const unsigned gv = grid_for(dim, 256, 148 * 16);
+  DevBuf<double> V((size_t)m * dim), w(dim), y(dim), x(dim), rot((size_t)m * dim);
+  DevBuf<float> v32(mixed ? dim : 0);
+  DevBuf<double> hm_d((size_t)m * m), svec(MAXB * MAXB);
+  DevBuf<double> part(std::max<size_t>((size_t)nb * (MAXB + 1), (size_t)gv * 2) + 64);
+  DevBuf<LzState> st(1);
+  DevBuf<IterState> ist(1);
+  SpmvScratch sc;
+  LzState* hst = nullptr;
+  KNB_CUDA(cudaMallocHost(&hst, sizeof(LzState)));
+  struct F {
+    LzState* p;
+    ~F() { cudaFreeHost(p); }
+  } fh{hst};
+  auto read_state = [&] {
+    KNB_CUDA(cudaMemcpyAsync(hst, st.get(), sizeof(LzState), cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+  };
+  KNB_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(LzState), s));
+  KNB_CUDA(cudaMemsetAsync(ist.get(), 0, sizeof(IterState), s));
+  KNB_CUDA(cudaMemsetAsync(hm_d.get(), 0, (size_t)m * m * 8, s));
+  // v0 = ones / ||ones|| (blocked norm as the reference's Blocks::dot)
+  fill_value<<<gv, 256, 0, s>>>(x.get(), (uint32_t)dim, 1.0);
+  lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
+  read_state();
+  const double norm0 = std::sqrt(hst->xx);
+  if (norm0 == 0.0 || !std::isfinite(norm0)) return false;
+  scale_by<<<gv, 256, 0, s>>>(x.get(), dim, norm0, 1);
+  KNB_CUDA(cudaMemcpyAsync(V.get(), x.get(), dim * 8, cudaMemcpyDeviceToDevice, s));
+  if (mixed) to_float<<<gv, 256, 0, s>>>(x.get(), dim, v32.get());
+  *launches += 4;
+
+  std::vector<double> hm((size_t)m * m, 0.0), theta, S;
+  int64_t matvecs = 0, matvecs32 = 0;
+  int j0 = 0;
+  bool use32 = mixed;
+  double threshold = std::numeric_limits<double>::infinity();
+  for (;;) {
+    int j = j0;
+    bool restart = false;
+    while (!restart) {
+      // Enqueue steps j .. jc, where jc is the next check step.
+      int jc = j;
+      while (!((jc + 1) == m || ((jc + 1) - j0) % 4 == 0)) ++jc;
+      KNB_CUDA(cudaMemsetAsync(&ist.get()->stopped, 0, 4, s));
+      int enq_from = j;
+      for (int jj = j; jj <= jc; ++jj) {
+        if (matvecs + (jj - enq_from) >= max_matvecs) {
+          jc = jj - 1;
+          break;
+        }
+        const double* vj = V.get() + (size_t)jj * dim;
+        lz_begin<<<1, 32, 0, s>>>(st.get(), ist.get());
+        *launches += 1 + spmv(A, vj, use32 ? v32.get() : nullptr, w.get(), sc, ist.get(), s);
+        const int cols = jj + 1, lo = cols >= 2 ? cols - 2 : 0;
+        lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
+        lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
+        lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 1, part.get(), st.get(), ist.get());
+        lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 1, part.get(), st.get(), ist.get());
+        lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 2, part.get(), st.get(), ist.get());
+        lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 2, part.get(), st.get(), ist.get());
+        lz_end<<<1, 32, 0, s>>>(st.get(), ist.get(), hm_d.get(), m, jj);
+        *launches += 7;
+        if (jj < jc) {
+          lz_next<<<gv, 256, 0, s>>>(V.get(), dim, jj + 1, w.get(), use32 ? v32.get() : nullptr,
+                                     hm_d.get(), m, st.get(), ist.get(), 1);
+          ++*launches;
+        }
+      }
+      KNB_LAUNCH("lanczos step");
+      if (jc < j) return false;  // matvec cap
+      read_state();
+      int jdone = hst->breakdown ? hst->bd_step : jc;
+      int64_t done_now = jdone - j + 1;
+      matvecs += done_now;
+      if (use32) matvecs32 += done_now;
+      j = jdone;
+      const int size = j + 1;
+      const bool breakdown = hst->breakdown != 0;
+      const double beta = hst->beta;
+      const bool end = breakdown || size == m;
+      const bool check = end || (size - j0) % 4 == 0;
+      KNB_CUDA(cudaMemcpyAsync(hm.data(), hm_d.get(), (size_t)m * m * 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      if (!check) {
+        if (matvecs >= max_matvecs) return false;
+        continue;  // cap reached mid-cycle; loop will return at next enqueue
+      }
+      // projected eigenproblem (eigenvector.rs:1128-1137)
+      std::vector<double> b((size_t)size * size);
+      for (int r = 0; r < size; ++r)
+        for (int c = 0; c < size; ++c) b[r * size + c] = 0.5 * (hm[r * m + c] + hm[c * m + r]);
+      theta.assign(size, 0.0);
+      S.assign((size_t)size * size, 0.0);
+      if (!symmetric_eigen(b.data(), size, theta.data(), S.data())) return false;
+      int top = 0;
+      for (int i = 0; i < size; ++i)
+        if (theta[i] > theta[top]) top = i;
+      const double estimate = breakdown ? 0.0 : beta * std::fabs(S[(size - 1) * size + top]);
+      const double limit = tol * (std::max(theta[top], 0.0) + shift);
+      if (use32 && estimate <= std::max(limit, FP32_FLOOR * (std::max(theta[top], 0.0) + shift))) {
+        // FP32 products cannot resolve the residual further: restart the
+        // Lanczos process with FP64 products from the current Ritz vector.
+        std::vector<double> cf(size);
+        for (int l = 0; l < size; ++l) cf[l] = S[l * size + top];
+        KNB_CUDA(cudaMemcpyAsync(svec.get(), cf.data(), size * 8, cudaMemcpyHostToDevice, s));
+        lz_combine<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), x.get());
+        lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
+        read_state();
+        KNB_CUDA(cudaMemcpyAsync(V.get(), x.get(), dim * 8, cudaMemcpyDeviceToDevice, s));
+        scale_by<<<gv, 256, 0, s>>>(V.get(), dim, std::sqrt(hst->xx), 1);
+        KNB_CUDA(cudaMemsetAsync(hm_d.get(), 0, (size_t)m * m * 8, s));
+        KNB_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(LzState), s));
+        *launches += 3;
+        use32 = false;
+        threshold = std::numeric_limits<double>::infinity();
+        j0 = 0;
+        restart = true;
+        continue;
+      }
+      if (estimate <= std::min(limit, threshold)) {
+        std::vector<double> cf(size);
+        for (int l = 0; l < size; ++l) cf[l] = S[l * size + top];
+        KNB_CUDA(cudaMemcpyAsync(svec.get(), cf.data(), size * 8, cudaMemcpyHostToDevice, s));
+        lz_combine<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), x.get());
+        if (matvecs >= max_matvecs) return false;
+        *launches += 1 + spmv(A, x.get(), nullptr, y.get(), sc, nullptr, s);
+        ++matvecs;
+        lz_dots<<<nb, VB_T, 0, s>>>(x.get(), y.get(), dim, part.get(), st.get());
+        lz_resid<<<gv, VB_T, 0, s>>>(x.get(), y.get(), dim, part.get(), st.get());
+        *launches += 2;
+        read_state();
+        const double xx = hst->xx, value = hst->value, rinf = hst->rinf, xinf = hst->xinf;
+        const double need = tol * (std::max(value, 0.0) + shift) * xinf;
+        if (rinf <= need) {
+          // finish_vector: sign, clamp, unit norm
+          lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
+          lz_sign_clamp<<<gv, 256, 0, s>>>(x.get(), dim, st.get());
+          lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
+          read_state();
+          const double nrm = std::sqrt(hst->xx);
+          if (nrm > 0.0) scale_by<<<gv, 256, 0, s>>>(x.get(), dim, nrm, 1);
+          KNB_CUDA(cudaMemcpyAsync(xout, x.get(), dim * 8, cudaMemcpyDeviceToDevice, s));
+          KNB_CUDA(cudaStreamSynchronize(s));
+          *launches += 4;
+          res->value = value;
+          res->matvecs = matvecs;
+          res->matvecs32 = matvecs32;
+          return true;
+        }
+        // A failed true-residual check means FP32 products limit the
+        // attainable accuracy: continue with FP64 products.
+        if (use32) use32 = false;
+        threshold = rinf > 0.0 ? std::min(estimate, limit) * (need / rinf) * 0.5
+                               : std::min(estimate, limit) * 0.5;
+        if (breakdown) {
+          const double nx = std::sqrt(xx);
+          KNB_CUDA(cudaMemcpyAsync(V.get(), x.get(), dim * 8, cudaMemcpyDeviceToDevice, s));
+          scale_by<<<gv, 256, 0, s>>>(V.get(), dim, nx, 1);
+          if (mixed) to_float<<<gv, 256, 0, s>>>(V.get(), dim, v32.get());
+          KNB_CUDA(cudaMemsetAsync(hm_d.get(), 0, (size_t)m * m * 8, s));
+          KNB_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(LzState), s));
+          *launches += 2;
+          j0 = 0;
+          restart = true;
+          continue;
+        }
+      }
+      if (end) {
+        if (breakdown) return false;
+        std::vector<int> idx(size);
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b2) { return theta[a] > theta[b2]; });
+        const int p = std::min(keep, size - 1);
+        std::vector<double> sv((size_t)size * p);
+        for (int q = 0; q < p; ++q)
+          for (int l = 0; l < size; ++l) sv[l * p + q] = S[l * size + idx[q]];
+        KNB_CUDA(cudaMemcpyAsync(svec.get(), sv.data(), sv.size() * 8, cudaMemcpyHostToDevice, s));
+        lz_rotate<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), p, rot.get());
+        KNB_CUDA(cudaMemcpyAsync(V.get(), rot.get(), (size_t)p * dim * 8, cudaMemcpyDeviceToDevice, s));
+        std::fill(hm.begin(), hm.end(), 0.0);
+        for (int q = 0; q < p; ++q) {
+          hm[q * m + q] = theta[idx[q]];
+          double c = beta * S[(size - 1) * size + idx[q]];
+          hm[q * m + p] = c;
+          hm[p * m + q] = c;
+        }
+        KNB_CUDA(cudaMemcpyAsync(hm_d.get(), hm.data(), hm.size() * 8, cudaMemcpyHostToDevice, s));
+        KNB_CUDA(cudaMemsetAsync(&ist.get()->stopped, 0, 4, s));
+        lz_next<<<gv, 256, 0, s>>>(V.get(), dim, p, w.get(), use32 ? v32.get() : nullptr,
+                                   hm_d.get(), m, st.get(), ist.get(), 0);
+        KNB_CUDA(cudaStreamSynchronize(s));
+        *launches += 2;
+        j0 = p;
+        restart = true;
+        continue;
+      }
+      // continue the cycle: v = w / beta as column j + 1
+      KNB_CUDA(cudaMemsetAsync(&ist.get()->stopped, 0, 4, s));
+      lz_next<<<gv, 256, 0, s>>>(V.get(), dim, j + 1, w.get(), use32 ? v32.get() : nullptr,
+                                 hm_d.get(), m, st.get(), ist.get(), 1);
+      ++*launches;
+      ++j;
+    }
+  }
+}
+
+// ======================================================================= driver
+static std::string fmt_g(double v) {
+  char b[64];
+  snprintf(b, sizeof b, "%g", v);
+  return b;
+}
+
+static void scale_host(std::vector<double>& x, int how) {
+  double d = 0.0;
+  if (how == 0) {
+    for (double v : x) d = std::max(d, v);
+  } else {
+    for (double v : x) d += v * v;
+    d = std::sqrt(d);
+  }
+  if (d > 0.0)
+    for (double& v : x) v /= d;
+}
+
+void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenResult* r,
+                 cudaStream_t s) {
+  const uint32_t n = g.n;
+  if (n == 0) {
+    r->eigenvalue = std::numeric_limits<double>::quiet_NaN();
+    r->connected = true;
+    return;
+  }
+  cudaEvent_t t0, t1;
+  KNB_CUDA(cudaEventCreate(&t0));
+  KNB_CUDA(cudaEventCreate(&t1));
+  KNB_CUDA(cudaEventRecord(t0, s));
+  int launches = 0;
+  const int mode = g.directed ? p.mode : 3;
+  const bool hdir = g.directed && mode != 3;
+  const int which = !g.directed ? 0 : (mode == 3 ? 2 : (mode == 2 ? 1 : 0));
+  const double lf = p.loops == 2 ? 0.0 : (!hdir && p.loops == 0 ? 2.0 : 1.0);
+  Operator& op = g.op(which, p.weighted, lf, s);
+  const unsigned gv = grid_for(n, 256, 148 * 16);
+
+  // components: strong (directed h) or weak
+  Comps strong;
+  if (hdir) {
+    std::vector<uint32_t> off(n + 1), tgt(g.out.arcs);
+    KNB_CUDA(cudaMemcpyAsync(off.data(), g.out.off.get(), ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
+    if (g.out.arcs)
+      KNB_CUDA(cudaMemcpyAsync(tgt.data(), g.out.tgt.get(), g.out.arcs * 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    strong = strong_components(off, tgt, n);
+  } else {
+    strong = weak_components(g, s);
+    launches += 5;
+  }
+  r->connected = strong.count() == 1;
+
+  // cyclic?
+  OpView<double> v64 = op.view64();
+  DevBuf<uint32_t> comp(n);
+  DevBuf<unsigned int> flag(1);
+  KNB_CUDA(cudaMemcpyAsync(comp.get(), strong.membership.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
+  KNB_CUDA(cudaMemsetAsync(flag.get(), 0, 4, s));
+  cyclic_arcs<<<grid_for(n, 256), 256, 0, s>>>(v64, comp.get(), flag.get());
+  ++launches;
+  unsigned int cyc = 0;
+  KNB_CUDA(cudaMemcpyAsync(&cyc, flag.get(), 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  DevBuf<double> xd(n);
+  std::vector<double> x(n);
+  if (!cyc) {
+    fill_value<<<gv, 256, 0, s>>>(xd.get(), n, 1.0);
+    sink_scores<<<grid_for(n, 256), 256, 0, s>>>(v64, xd.get());
+    launches += 2;
+    KNB_CUDA(cudaMemcpyAsync(x.data(), xd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    scale_host(x, p.scale);
+    memcpy(out, x.data(), (size_t)n * 8);
+    r->eigenvalue = 0.0;
+    r->matvecs = 0;
+  } else if (hdir) {
+    // power iteration on A' + I (eigenvector.rs:330-374)
+    const Partition& P = op.partition(SPMV_THREADS * EIG_IPT, s);
+    DevBuf<double> xb[2] = {DevBuf<double>(n), DevBuf<double>(n)}, y(n);
+    DevBuf<double> carry(P.ntiles + 1), head(P.ntiles + 1), part1((size_t)P.ntiles + 2),
+        part2(SPLIT_CTAS + 2), part3(gv + 2);
+    DevBuf<IterState> st(1);
+    IterState is{};
+    is.tol = p.tol;
+    is.max_iter = (int32_t)std::min<int64_t>(p.max_iter, INT32_MAX);
+    KNB_CUDA(cudaMemcpyAsync(st.get(), &is, sizeof(is), cudaMemcpyHostToDevice, s));
+    fill_value<<<gv, 256, 0, s>>>(xb[0].get(), n, 1.0);
+    ++launches;
+    const unsigned g2 = SPLIT_CTAS;
+    constexpr size_t sm = tile_smem_bytes<double, EIG_IPT>();
+    IterState hs{};
+    int batch = 0;
+    for (;;) {
+      for (int k = 0; k < 8; ++k) {
+        int b = k & 1;
+        PowerEpi e{xb[b].get(), y.get()};
+        tile_spmv<double, double, PowerEpi, EIG_IPT><<<P.ntiles, SPMV_THREADS, sm, s>>>(
+            v64, xb[b].get(), e, P.coords.get(), carry.get(), head.get(), part1.get(), st.get());
+        split_rows<double, PowerEpi><<<g2, SPMV_THREADS, 0, s>>>(
+            P.split.get(), P.nsplit, P.nshort, carry.get(), head.get(), e, part1.get(), P.ntiles,
+            part2.get(), st.get());
+        power_vertex<<<gv, 256, 0, s>>>(xb[b].get(), y.get(), xb[1 - b].get(), n, part3.get(), st.get());
+        launches += 3;
+      }
+      KNB_LAUNCH("power iteration");
+      KNB_CUDA(cudaMemcpyAsync(&hs, st.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      ++batch;
+      if (hs.converged || hs.stopped) break;
+    }
+    if (!hs.converged)
+      throw Error("eigenvector centrality did not converge to tolerance " + fmt_g(p.tol) +
+                  " within " + std::to_string(p.max_iter) +
+                  " iterations. Power iteration converges slowly when the largest eigenvalue is "
+                  "close to the next one, and not at all to a single answer when several "
+                  "strongly connected components share it; a larger iteration cap may help in "
+                  "the first case");
+    double* xf = xb[hs.iter & 1].get();
+    // eigenvalue sum(A'x) / sum(x), scores times sum(x) / sum(x^2)
+    DevOp A;
+    A.n = n;
+    A.nnz = op.nnz;
+    A.off = op.rows->off.get();
+    A.cols = op.rows->tgt.get();
+    A.v64 = op.has_vals ? op.vals64.get() : nullptr;
+    A.part = &P;
+    SpmvScratch sc;
+    launches += spmv(A, xf, nullptr, y.get(), sc, nullptr, s);
+    std::vector<double> hx(n), hy(n);
+    KNB_CUDA(cudaMemcpyAsync(hx.data(), xf, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(hy.data(), y.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (uint32_t v = 0; v < n; ++v) {
+      s0 += hy[v];
+      s1 += hx[v];
+      s2 += hx[v] * hx[v];
+    }
+    r->eigenvalue = s1 > 0.0 ? s0 / s1 : 0.0;
+    if (s2 > 0.0) {
+      double wgt = s1 / s2;
+      for (double& xv : hx) xv *= wgt;
+    }
+    r->matvecs = hs.iter;
+    scale_host(hx, p.scale);
+    memcpy(out, hx.data(), (size_t)n * 8);
+  } else {
+    // symmetric: Lanczos per weak component (eigenvector.rs:383-479)
+    const Comps& comps = strong;  // weak components of h
+    const size_t k = comps.count();
+    DevBuf<double> sdev(n), qdev(n);
+    op_row_sums<<<grid_for(n, 256), 256, 0, s>>>(v64, sdev.get(), qdev.get());
+    ++launches;
+    std::vector<double> rs(n), rq(n);
+    KNB_CUDA(cudaMemcpyAsync(rs.data(), sdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(rq.data(), qdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> upper(k, 0.0), sum(k, 0.0), square(k, 0.0), lower(k);
+    for (uint32_t v = 0; v < n; ++v) {
+      uint32_t c = comps.membership[v];
+      upper[c] = std::max(upper[c], rs[v]);
+      sum[c] += rs[v];
+      square[c] = std::max(square[c], rq[v]);
+    }
+    for (size_t c = 0; c < k; ++c)
+      lower[c] = std::max(sum[c] / (double)comps.sizes[c], std::sqrt(square[c]));
+    std::vector<size_t> order(k);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return lower[b] < lower[a]; });
+    std::vector<size_t> start(k + 1, 0);
+    for (uint32_t c : comps.membership) start[c + 1]++;
+    for (size_t c = 0; c < k; ++c) start[c + 1] += start[c];
+    std::vector<uint32_t> members(n);
+    {
+      std::vector<size_t> cur(start.begin(), start.end() - 1);
+      for (uint32_t v = 0; v < n; ++v) members[cur[comps.membership[v]]++] = v;
+    }
+    double best = 0.0;
+    int64_t matvecs = 0, matvecs32 = 0;
+    struct Solved {
+      size_t c;
+      double value;
+      DevBuf<double> u;
+    };
+    std::vector<Solved> solved;
+    DevBuf<uint32_t> local(n), nodes_d(n);
+    const double TIE = 1e-9;
+    for (size_t c : order) {
+      if (upper[c] <= 0.0 || upper[c] < best * (1.0 - TIE)) continue;
+      const uint32_t kn = (uint32_t)(start[c + 1] - start[c]);
+      DevOp A;
+      if (k == 1) {
+        A.n = n;
+        A.nnz = op.nnz;
+        A.off = op.rows->off.get();
+        A.cols = op.rows->tgt.get();
+        A.v64 = op.has_vals ? op.vals64.get() : nullptr;
+        A.v32 = op.has_vals ? op.vals32.get() : nullptr;
+        A.part = &op.partition(SPMV_THREADS * EIG_IPT, s);
+      } else {
+        KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), members.data() + start[c], (size_t)kn * 4,
+                                 cudaMemcpyHostToDevice, s));
+        scatter_local<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d.get(), kn, local.get());
+        A.own_off.alloc((size_t)kn + 1);
+        sub_lengths<<<grid_for(kn + 1, 256), 256, 0, s>>>(op.rows->off.get(), nodes_d.get(), kn,
+                                                          A.own_off.get());
+        uint64_t nnz = exclusive_scan<uint32_t>(A.own_off.get(), A.own_off.get(), (size_t)kn + 1, s);
+        A.n = kn;
+        A.nnz = nnz;
+        A.own_cols.alloc(std::max<uint64_t>(nnz, 1));
+        if (op.has_vals) {
+          A.own_v64.alloc(std::max<uint64_t>(nnz, 1));
+          A.own_v32.alloc(std::max<uint64_t>(nnz, 1));
+        }
+        sub_copy<<<grid_for(kn, 128), 128, 0, s>>>(v64, nodes_d.get(), kn, local.get(),
+                                                   A.own_off.get(), A.own_cols.get(),
+                                                   op.has_vals ? A.own_v64.get() : nullptr,
+                                                   op.has_vals ? A.own_v32.get() : nullptr);
+        KNB_LAUNCH("submatrix");
+        launches += 4;
+        A.off = A.own_off.get();
+        A.cols = A.own_cols.get();
+        A.v64 = op.has_vals ? A.own_v64.get() : nullptr;
+        A.v32 = op.has_vals ? A.own_v32.get() : nullptr;
+        A.own_part = build_partition(kn, nnz, A.off, SPMV_THREADS * EIG_IPT, s);
+        A.part = A.own_part.get();
+      }
+      Solved sv;
+      sv.c = c;
+      sv.u.alloc(kn);
+      Leading res;
+      if (!symmetric_leading(A, p.tol, 1.0, p.max_iter, p.precision == 1, sv.u.get(), &res,
+                             &launches, s))
+        throw Error("eigenvector centrality did not converge to tolerance " + fmt_g(p.tol) +
+                    " within " + std::to_string(p.max_iter) +
+                    " matrix-vector products; a larger iteration cap may help");
+      matvecs += res.matvecs;
+      matvecs32 += res.matvecs32;
+      best = std::max(best, res.value);
+      sv.value = res.value;
+      solved.push_back(std::move(sv));
+    }
+    fill_value<<<gv, 256, 0, s>>>(xd.get(), n, 0.0);
+    ++launches;
+    for (auto& sv : solved) {
+      if (sv.value < best * (1.0 - TIE)) continue;
+      const uint32_t kn = (uint32_t)(start[sv.c + 1] - start[sv.c]);
+      std::vector<double> u(kn);
+      KNB_CUDA(cudaMemcpyAsync(u.data(), sv.u.get(), (size_t)kn * 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      double total = 0.0;
+      for (double v : u) total += v;
+      KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), members.data() + start[sv.c], (size_t)kn * 4,
+                               cudaMemcpyHostToDevice, s));
+      scatter_scaled<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d.get(), kn, sv.u.get(), total, xd.get());
+      ++launches;
+    }
+    KNB_CUDA(cudaMemcpyAsync(x.data(), xd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    scale_host(x, p.scale);
+    memcpy(out, x.data(), (size_t)n * 8);
+    r->eigenvalue = best;
+    r->matvecs = matvecs;
+    r->matvecs_fp32 = matvecs32;
+  }
+  KNB_CUDA(cudaEventRecord(t1, s));
+  KNB_CUDA(cudaEventSynchronize(t1));
+  float ms = 0;
+  KNB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  r->seconds = ms * 1e-3;
+  r->kernel_launches = launches;
+}
+
+}  // namespace knb

@@ -1,0 +1,38 @@
+// Eigenvector centrality on the device: power iteration for directed
+// matrices and thick-restart Lanczos for symmetric ones.
+#pragma once
+
+#include "graph.cuh"
+
+namespace knb {
+
+struct EigenParams {
+  int mode = 2;       // 1 out, 2 in, 3 all
+  bool weighted = false;
+  int scale = 0;      // 0 max, 1 unit
+  int loops = 0;      // 0 twice, 1 once, 2 ignore
+  double tol = 1e-12;
+  int64_t max_iter = 10000;
+  int precision = 0;  // 0 FP64, 1 FP32 products with FP64 basis
+};
+
+struct EigenResult {
+  double eigenvalue = 0;
+  int64_t matvecs = 0;
+  int64_t matvecs_fp32 = 0;
+  bool connected = true;
+  double seconds = 0;
+  int kernel_launches = 0;
+};
+
+// Writes n scores to `out` (host). Throws knb::Error on failure.
+void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenResult* r,
+                 cudaStream_t s);
+
+// Dense symmetric eigensolver for the projected Lanczos problems: EISPACK
+// tred2 + tql2 order (reference: crates/engine/src/linalg.rs:478-720).
+// a is row-major n x n; eigenvalues ascending, eigenvectors in the columns of
+// vecs. Returns false if the QL iteration does not converge.
+bool symmetric_eigen(const double* a, int n, double* vals, double* vecs);
+
+}  // namespace knb

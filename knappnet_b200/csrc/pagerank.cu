@@ -1,0 +1,683 @@
+// PageRank power iteration on the device (reference: the loop of
+// crates/engine/src/metrics/spectral.rs:211-281).
+//
+// One sweep is two kernels: the merge-path SpMV with the PageRank update
+// fused into its epilogue (tile_spmv + PagerankEpi) and the split-row /
+// reduction kernel (split_rows). A third, normally idle, kernel computes the
+// exact L1 change when the fused estimate is too close to the tolerance.
+//
+// Normalisation is folded into the next sweep. The device stores the
+// unnormalised iterate y_k and z_k = y_k / out (0 for dangling nodes); with
+// T_k = sum(y_k) the normalised iterate is x_k = y_k / T_k, and one sweep
+// computes, for every row i,
+//     u_i = d ((A z_k)_i / T_k + (D_k / T_k) jump_i) + (1 - d) p_i
+// which is the reference's y_i before its division by `total` (D_k is the
+// dangling mass of y_k). The L1 change sum |u_i / T_{k+1} - x_k,i| needs
+// T_{k+1}, known only after the sweep; the sweep accumulates
+// sum |u_i - x_k,i| instead, which differs from it by at most |1 - T_{k+1}|
+// (T is 1 up to rounding since the transition matrix is column
+// stochastic). When the estimate is within that bound of the tolerance, the
+// exact change is computed by pr_exact_change before deciding.
+//
+// Mixed precision runs the same trajectory: FP32 sweeps (FP32 arc values,
+// iterate and row sums; FP64 reductions) from the uniform start, then FP64
+// sweeps from the FP32 iterate until the reference's stopping rule holds in
+// FP64. The FP32 phase ends when its change falls below
+// max(tol * switch_factor, switch_floor): the FP32 perturbation of the
+// trajectory (about 1e-7 in L1) then decays over the remaining FP64 sweeps by
+// the same factor as the change, to well below the tolerance.
+#include <cfloat>
+#include <mutex>
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pagerank.cuh"
+
+namespace knb {
+
+// ======================================================================= epilogue
+template <class VT, bool PV, bool JU, bool EXACT>
+struct PagerankEpi {
+  static constexpr int NACC = 3;
+  const VT* y_old;
+  VT* y_new;
+  VT* z_new;
+  const VT* inv_out;
+  const double* p;  // personalization (rescaled), when PV
+  double d;
+  double pu;        // 1 / n
+  VT c_it = 0, c_dt = 0;
+
+  __device__ __forceinline__ void prepare(const IterState* st) {
+    c_it = (VT)st->inv_total;
+    c_dt = (VT)st->dterm;
+  }
+  static __device__ __forceinline__ void init(double* a) { a[0] = a[1] = a[2] = 0.0; }
+  static __device__ __forceinline__ double identity(int) { return 0.0; }
+  static __device__ __forceinline__ double combine(int, double a, double b) { return a + b; }
+  static __device__ __forceinline__ double warp_combine(int, double v) { return warp_sum(v); }
+
+  __device__ __forceinline__ void row(uint32_t g, VT s, double* a) const {
+    const VT pg = PV ? (VT)p[g] : (VT)pu;
+    const VT jg = JU ? (VT)pu : pg;
+    const VT u = (VT)d * (s * c_it + c_dt * jg) + (VT)(1.0 - d) * pg;
+    const VT xo = y_old[g] * c_it;
+    const VT io = inv_out[g];
+    y_new[g] = u;
+    z_new[g] = u * io;
+    a[0] += (double)u;
+    if (io == VT(0)) a[1] += (double)u;
+    a[2] += fabs((double)u - (double)xo);
+  }
+
+  __device__ void finish(IterState* st, const double* tot) const {
+    const double T = tot[0], D = tot[1], ch = tot[2];
+    st->prev_inv_total = st->inv_total;
+    st->total = T;
+    st->dang = D;
+    st->change = ch;
+    st->inv_total = 1.0 / T;
+    st->dterm = D / T;
+    st->iter += 1;
+    bool amb = false;
+    if (EXACT) {
+      double slack = 2.0 * fabs(1.0 - T) + 64.0 * DBL_EPSILON * fmax(ch, st->tol);
+      st->slack = slack;
+      amb = fabs(ch - st->tol) <= slack;
+    }
+    if (amb) st->ambiguous = 1;
+    else if (ch <= st->tol) st->converged = 1;
+    else if (st->iter >= st->max_iter) st->stopped = 1;
+  }
+};
+
+// ======================================================================= vertex kernels
+constexpr int VT_THREADS = 256;
+
+// Last-CTA fixed-order sum of `k` partial arrays of `nb` blocks each.
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+template <int K>
+__device__ __forceinline__ void reduce_parts(const double* part, uint32_t nb, double* out,
+                                             double* scratch) {
+  const volatile double* p = part;
+  for (int s = 0; s < K; ++s) {
+    double a = 0;
+    for (uint32_t q = threadIdx.x; q < nb; q += blockDim.x) a += p[(size_t)q * K + s];
+    a = block_sum(a, scratch);
+    out[s] = a;
+  }
+}
+
+// x0 = 1/n, z0 = x0 / out, D0 = dangling mass (spectral.rs:248-259).
+template <class VT>
+__global__ void pr_init(VT* __restrict__ y, VT* __restrict__ z, const VT* __restrict__ inv_out,
+                        uint32_t n, double* __restrict__ part, IterState* st) {
+  __shared__ double sh[VT_THREADS / 32];
+  const VT x0 = (VT)(1.0 / (double)n);
+  double dang = 0, tot = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    VT io = inv_out[i];
+    y[i] = x0;
+    z[i] = x0 * io;
+    tot += (double)x0;
+    if (io == VT(0)) dang += (double)x0;
+  }
+  dang = block_sum(dang, sh);
+  tot = block_sum(tot, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x * 2] = tot;
+    part[blockIdx.x * 2 + 1] = dang;
+  }
+  if (!last_block(&st->ticket)) return;
+  double r[2];
+  reduce_parts<2>(part, gridDim.x, r, sh);
+  if (threadIdx.x == 0) {
+    st->inv_total = 1.0;
+    st->dterm = r[1];
+    st->total = r[0];
+    st->prev_inv_total = 1.0;
+    st->ticket = 0;
+  }
+}
+
+// Exact L1 change sum |y_new / T - y_old * prev_inv_total| when the fused
+// estimate cannot decide (see the file comment).
+__global__ void pr_exact_change(const double* __restrict__ y_old, const double* __restrict__ y_new,
+                                uint32_t n, double* __restrict__ part, IterState* st) {
+  if (!st->ambiguous || st->converged || st->stopped) return;
+  __shared__ double sh[VT_THREADS / 32];
+  const double T = st->total, ip = st->prev_inv_total;
+  double a = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    a += fabs(y_new[i] / T - y_old[i] * ip);
+  a = block_sum(a, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = a;
+  if (!last_block(&st->ticket2)) return;
+  double r[1];
+  reduce_parts<1>(part, gridDim.x, r, sh);
+  if (threadIdx.x == 0) {
+    st->change = r[0];
+    st->ambiguous = 0;
+    if (r[0] <= st->tol) st->converged = 1;
+    else if (st->iter >= st->max_iter) st->stopped = 1;
+    st->ticket2 = 0;
+  }
+}
+
+// FP32 -> FP64 hand-over: y64 = y32 / T32, z64 = y64 / out, new scalars.
+__global__ void pr_switch(const float* __restrict__ y32, const IterState* __restrict__ st32,
+                          double* __restrict__ y64, double* __restrict__ z64,
+                          const double* __restrict__ inv_out, uint32_t n,
+                          double* __restrict__ part, IterState* st) {
+  __shared__ double sh[VT_THREADS / 32];
+  const double it = st32->inv_total;
+  double tot = 0, dang = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double y = (double)y32[i] * it;
+    double io = inv_out[i];
+    y64[i] = y;
+    z64[i] = y * io;
+    tot += y;
+    if (io == 0.0) dang += y;
+  }
+  tot = block_sum(tot, sh);
+  dang = block_sum(dang, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x * 2] = tot;
+    part[blockIdx.x * 2 + 1] = dang;
+  }
+  if (!last_block(&st->ticket)) return;
+  double r[2];
+  reduce_parts<2>(part, gridDim.x, r, sh);
+  if (threadIdx.x == 0) {
+    st->total = r[0];
+    st->inv_total = 1.0 / r[0];
+    st->prev_inv_total = st->inv_total;
+    st->dterm = r[1] / r[0];
+    st->ticket = 0;
+  }
+}
+
+// out = y / T (spectral.rs:268-270), in FP64, in the caller's node order
+// (iperm maps a node to its number in a relabelled operator, or is null).
+template <class VT>
+__global__ void pr_output(const VT* __restrict__ y, const IterState* __restrict__ st, uint32_t n,
+                          const uint32_t* __restrict__ iperm, double* __restrict__ out) {
+  const double T = st->total;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = (double)y[iperm ? iperm[i] : i] / T;
+}
+
+__global__ void permute_in(const double* __restrict__ in, const uint32_t* __restrict__ perm,
+                           uint32_t n, double* __restrict__ out) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    out[k] = in[perm[k]];
+}
+
+// Personalization checks and rescaling to sum 1 (spectral.rs:284-304): the
+// first pass finds any value that is not finite or negative and sums the
+// rest in a fixed order; the second divides by the sum.
+__global__ void pers_check(const double* __restrict__ p, uint32_t n, double* __restrict__ part,
+                           IterState* st) {
+  __shared__ double sh[VT_THREADS / 32];
+  double a = 0, bad = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = p[i];
+    if (!isfinite(v) || v < 0.0) bad = 1;
+    else a += v;
+  }
+  a = block_sum(a, sh);
+  bad = block_sum(bad, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x * 2] = a;
+    part[blockIdx.x * 2 + 1] = bad;
+  }
+  if (!last_block(&st->ticket)) return;
+  double r[2];
+  reduce_parts<2>(part, gridDim.x, r, sh);
+  if (threadIdx.x == 0) {
+    st->total = r[0];
+    st->stopped = r[1] > 0 ? 1 : 0;
+    st->ticket = 0;
+  }
+}
+
+__global__ void pers_scale(double* __restrict__ p, uint32_t n, const IterState* __restrict__ st) {
+  const double sum = st->total;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = p[i] / sum;
+}
+
+static void normalize_personalization(double* p, uint32_t n, double* part, IterState* st,
+                                      IterState* hst, cudaStream_t s) {
+  const unsigned gv = grid_for(n, VT_THREADS, 1184);
+  KNB_CUDA(cudaMemsetAsync(st, 0, sizeof(IterState), s));
+  pers_check<<<gv, VT_THREADS, 0, s>>>(p, n, part, st);
+  KNB_LAUNCH("pers_check");
+  KNB_CUDA(cudaMemcpyAsync(hst, st, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  if (hst->stopped) throw Error("the personalization vector must hold finite, nonnegative values");
+  if (!(hst->total > 0.0)) throw Error("the personalization vector must have a positive sum");
+  pers_scale<<<gv, VT_THREADS, 0, s>>>(p, n, st);
+  KNB_LAUNCH("pers_scale");
+}
+
+// Scratch of PageRank solves on one operator, kept between calls: iterates,
+// per-tile partials, carries, states, pinned host state slots and events.
+// A solve holds `mu` while it runs, so concurrent calls on one operator take
+// turns instead of sharing buffers.
+struct PrWorkspace : Workspace {
+  std::mutex mu;
+  uint32_t n = 0, nt = 0;
+  DevBuf<double> y64[2], z64[2], carry64, head64, pvec, ptmp, dout, part1, part2, part3;
+  DevBuf<float> y32[2], z32[2], carry32, head32;
+  DevBuf<IterState> st;        // 0: FP32 phase, 1: FP64 phase, 2: personalization
+  IterState* hstate = nullptr;  // pinned, 3 slots
+  cudaEvent_t t0 = nullptr, t1 = nullptr, done[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> pool;  // sweep-timing events
+
+  ~PrWorkspace() override {
+    if (hstate) cudaFreeHost(hstate);
+    for (cudaEvent_t e : {t0, t1, done[0], done[1]})
+      if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+  void ensure(uint32_t nn, uint32_t ntiles, bool need32, bool need64, bool need_p) {
+    if (!hstate) {
+      KNB_CUDA(cudaMallocHost(&hstate, 3 * sizeof(IterState)));
+      KNB_CUDA(cudaEventCreate(&t0));
+      KNB_CUDA(cudaEventCreate(&t1));
+      KNB_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+      KNB_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+      st.alloc(3);
+    }
+    const unsigned gv = grid_for(nn, VT_THREADS, 1184);
+    if (n != nn) {
+      n = nn;
+      for (int k = 0; k < 2; ++k) {
+        y32[k].release(); z32[k].release(); y64[k].release(); z64[k].release();
+      }
+      pvec.release(); ptmp.release(); dout.release();
+      part3.alloc((size_t)gv * 2 + 8);
+      part2.alloc((size_t)SPLIT_CTAS * 3 + 8);
+    }
+    if (nt < ntiles) {
+      nt = ntiles;
+      part1.alloc((size_t)nt * 3 + 8);
+      carry32.release(); head32.release(); carry64.release(); head64.release();
+    }
+    if (need32 && !y32[0].p) {
+      for (int k = 0; k < 2; ++k) { y32[k].alloc(n); z32[k].alloc(n); }
+    }
+    if (need32 && !carry32.p) { carry32.alloc(nt + 1); head32.alloc(nt + 1); }
+    if (need64 && !y64[0].p) {
+      for (int k = 0; k < 2; ++k) { y64[k].alloc(n); z64[k].alloc(n); }
+    }
+    if (need64 && !carry64.p) { carry64.alloc(nt + 1); head64.alloc(nt + 1); }
+    if (need_p && !pvec.p) { pvec.alloc(n); ptmp.alloc(n); }
+  }
+  cudaEvent_t timing_event(size_t k) {
+    while (pool.size() <= k) {
+      cudaEvent_t e;
+      KNB_CUDA(cudaEventCreate(&e));
+      pool.push_back(e);
+    }
+    return pool[k];
+  }
+};
+
+// ======================================================================= sweeps
+struct SweepBuffers {
+  OpView<double> v64;
+  OpView<float> v32;
+  void* y[2];
+  void* z[2];
+  const void* inv_out;
+  const double* p;
+  void* carry;
+  void* head;
+  double* part1;
+  double* part2;
+  double* part3;
+  IterState* st;
+};
+
+enum SweepVariant : int { VAR_CTA = 1, VAR_WARP = 2 };
+constexpr int WPB = 8;  // warps per CTA of the warp-tile sweep
+
+template <class VT, class MT, bool PV, bool JU, bool EXACT, int VAR, int IPT>
+static void launch_sweep(const Operator& op, const Partition& P, const SweepBuffers& B, int buf,
+                         double d, cudaStream_t s, unsigned g2, cudaEvent_t ev0, cudaEvent_t ev1) {
+  using Epi = PagerankEpi<VT, PV, JU, EXACT>;
+  Epi e;
+  e.y_old = (const VT*)B.y[buf];
+  e.y_new = (VT*)B.y[1 - buf];
+  e.z_new = (VT*)B.z[1 - buf];
+  e.inv_out = (const VT*)B.inv_out;
+  e.p = B.p;
+  e.d = d;
+  e.pu = 1.0 / (double)op.n;
+  OpView<MT> v;
+  if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
+  if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
+  if constexpr (VAR == VAR_CTA) {
+    constexpr size_t smem = tile_smem_bytes<VT, IPT>();
+    static bool attr_set = false;
+    if (!attr_set) {
+      KNB_CUDA(cudaFuncSetAttribute(tile_spmv<VT, MT, Epi, IPT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_set = true;
+    }
+    tile_spmv<VT, MT, Epi, IPT><<<P.ntiles, SPMV_THREADS, smem, s>>>(
+        v, (const VT*)B.z[buf], e, P.coords.get(), (VT*)B.carry, (VT*)B.head, B.part1, B.st);
+  } else {
+    constexpr size_t smem = warp_smem_bytes<VT, IPT, WPB>();
+    static bool attr_set = false;
+    if (!attr_set) {
+      KNB_CUDA(cudaFuncSetAttribute(warp_spmv<VT, MT, Epi, IPT, WPB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_set = true;
+    }
+    const unsigned grid = (P.ntiles + WPB - 1) / WPB;
+    warp_spmv<VT, MT, Epi, IPT, WPB><<<grid, WPB * 32, smem, s>>>(
+        v, (const VT*)B.z[buf], e, P.coords.get(), P.ntiles, (VT*)B.carry, (VT*)B.head,
+        B.part1, B.st);
+  }
+  KNB_LAUNCH("sweep");
+  if (ev1) KNB_CUDA(cudaEventRecord(ev1, s));
+  split_rows<VT, Epi><<<g2, SPMV_THREADS, 0, s>>>(P.split.get(), P.nsplit, P.nshort,
+                                                   (const VT*)B.carry, (const VT*)B.head, e,
+                                                   B.part1, P.ntiles, B.part2, B.st);
+  KNB_LAUNCH("split_rows");
+  if (EXACT) {
+    pr_exact_change<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
+        (const double*)B.y[buf], (const double*)B.y[1 - buf], op.n, B.part3, B.st);
+    KNB_LAUNCH("pr_exact_change");
+  }
+}
+
+using SweepFn = void (*)(const Operator&, const Partition&, const SweepBuffers&, int, double,
+                         cudaStream_t, unsigned, cudaEvent_t, cudaEvent_t);
+
+template <class VT, class MT, bool EXACT, int VAR, int IPT>
+static SweepFn pick_pv(bool pv, bool ju) {
+  if (!pv) return launch_sweep<VT, MT, false, true, EXACT, VAR, IPT>;
+  if (ju) return launch_sweep<VT, MT, true, true, EXACT, VAR, IPT>;
+  return launch_sweep<VT, MT, true, false, EXACT, VAR, IPT>;
+}
+
+template <class VT, class MT, bool EXACT>
+static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
+  if (var == VAR_CTA) {
+    switch (ipt) {
+      case 4: return pick_pv<VT, MT, EXACT, VAR_CTA, 4>(pv, ju);
+      default: return pick_pv<VT, MT, EXACT, VAR_CTA, 8>(pv, ju);
+    }
+  }
+  switch (ipt) {
+    case 4: return pick_pv<VT, MT, EXACT, VAR_WARP, 4>(pv, ju);
+    case 16: return pick_pv<VT, MT, EXACT, VAR_WARP, 16>(pv, ju);
+    default: return pick_pv<VT, MT, EXACT, VAR_WARP, 8>(pv, ju);
+  }
+}
+
+static uint32_t tile_items(int var, int ipt) {
+  return (uint32_t)((var == VAR_CTA ? SPMV_THREADS : 32) * ipt);
+}
+
+// ======================================================================= timing
+static thread_local SweepTiming g_timing[2];
+static thread_local bool g_timing_on = false;
+SweepTiming last_sweep_timing(int phase) { return g_timing[phase & 1]; }
+void set_sweep_timing(bool on) { g_timing_on = on; }
+
+// Algorithmic bytes of one sweep (counted once each): row offsets 4(n+1),
+// column indices 4 nnz, values sizeof(MT) nnz, the gathered z once
+// (sizeof(VT) n), own y_old and inv_out read, y_new and z_new written
+// (4 sizeof(VT) n), plus p when personalised.
+static double sweep_bytes(const Operator& op, size_t vt, size_t mt, bool pv) {
+  double n = op.n, nnz = (double)op.nnz;
+  double b = 4.0 * (n + 1) + 4.0 * nnz + (op.has_vals ? mt * nnz : 0.0) + 5.0 * vt * n;
+  if (pv) b += 8.0 * n;
+  return b;
+}
+
+// ======================================================================= phases
+struct PhaseResult {
+  int32_t iter = 0;
+  int32_t converged = 0;
+  int32_t stopped = 0;
+  double change = 0;
+  int launches = 0;
+};
+
+// Runs sweeps until the phase's state converges or stops. The host keeps
+// one batch of `U` sweeps in flight ahead of the state it inspects, so the
+// GPU never waits for the host; sweeps after convergence exit at once.
+static PhaseResult run_phase(SweepFn fn, const Operator& op, const Partition& P,
+                             const SweepBuffers& B, double d, bool exact, cudaStream_t s,
+                             PrWorkspace& ws, IterState* h_state /* pinned, 2 slots */,
+                             double* timing_ms, int64_t* timing_n) {
+  const int U = 8;
+  const unsigned g2 = SPLIT_CTAS;
+  PhaseResult r;
+  int batch = 0;
+  size_t nev = 0;
+  bool finished = false;
+  auto enqueue = [&](int b) {
+    for (int k = 0; k < U; ++k) {
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (g_timing_on) {
+        e0 = ws.timing_event(nev++);
+        e1 = ws.timing_event(nev++);
+      }
+      fn(op, P, B, k & 1, d, s, g2, e0, e1);
+      r.launches += exact ? 3 : 2;
+    }
+    KNB_CUDA(cudaMemcpyAsync(&h_state[b & 1], B.st, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaEventRecord(ws.done[b & 1], s));
+  };
+  enqueue(batch);
+  while (!finished) {
+    enqueue(batch + 1);
+    KNB_CUDA(cudaEventSynchronize(ws.done[batch & 1]));
+    const IterState& hs = h_state[batch & 1];
+    if (hs.converged || hs.stopped) finished = true;
+    ++batch;
+  }
+  KNB_CUDA(cudaMemcpyAsync(&h_state[0], B.st, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  const IterState fin = h_state[0];
+  r.iter = fin.iter;
+  r.converged = fin.converged;
+  r.stopped = fin.stopped;
+  r.change = fin.change;
+  // Only sweeps that did work count for the timing (later ones exit at once).
+  if (g_timing_on) {
+    for (size_t k = 0; k + 1 < nev; k += 2) {
+      if ((int64_t)(k / 2) < fin.iter) {
+        float ms = 0;
+        KNB_CUDA(cudaEventElapsedTime(&ms, ws.pool[k], ws.pool[k + 1]));
+        *timing_ms += ms;
+        *timing_n += 1;
+      }
+    }
+  }
+  return r;
+}
+
+static int default_ipt(const Operator& op, int var) {
+  (void)op;
+  return var == VAR_CTA ? 4 : 8;
+}
+
+// ======================================================================= driver
+Tuning& tuning() {
+  static Tuning t;
+  return t;
+}
+
+void pagerank(GraphHandleImpl& g, const PagerankParams& prm_in, double* out, bool out_on_device,
+              PagerankInfo* info, cudaStream_t s) {
+  PagerankParams prm = prm_in;
+  const Tuning& tu = tuning();
+  if (tu.ipt) prm.ipt = tu.ipt;
+  if (tu.variant) prm.variant = tu.variant;
+  prm.relabel = tu.relabel != 0;
+  prm.switch_factor = tu.switch_factor;
+  prm.switch_floor = tu.switch_floor;
+  const uint32_t n = g.n;
+  if (n == 0) return;
+  int which = (g.directed && prm.directed) ? 1 : (g.directed ? 2 : 0);
+  // Loop factor follows the orientation of the rows (eigenvector.rs:163-169):
+  // rows of a directed graph count a loop once unless ignored.
+  double lfac = prm.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (prm.loops == 0 ? 2.0 : 1.0));
+  Operator& op = g.op(which, prm.weighted, lfac, s);
+  const int var = prm.variant ? prm.variant : VAR_WARP;
+  const int ipt = prm.ipt ? prm.ipt : default_ipt(op, var);
+  const bool rl = prm.relabel;
+  const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
+  const uint32_t tile = tile_items(var, ipt);
+  const Partition& P = rl ? op.relabeled_partition(tile, s) : op.partition(tile, s);
+  const OpView<double> v64 = rl ? op.rview64() : op.view64();
+  const OpView<float> v32 = rl ? op.rview32() : op.view32();
+  const double* inv64 = rl ? R->inv_out64.get() : op.inv_out64.get();
+  const float* inv32 = rl ? R->inv_out32.get() : op.inv_out32.get();
+  const uint32_t* perm = rl ? R->perm.get() : nullptr;
+  const uint32_t* iperm = rl ? R->iperm.get() : nullptr;
+
+  const bool pv = prm.personalization != nullptr;
+  const bool ju = !pv || prm.dangling == 1;
+  const bool mixed = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
+  const uint32_t nt = P.ntiles;
+  const unsigned gv = grid_for(n, VT_THREADS, 1184);
+
+  PrWorkspace* wsp = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(op.mu);
+    if (!op.pr_ws) op.pr_ws = std::make_unique<PrWorkspace>();
+    wsp = static_cast<PrWorkspace*>(op.pr_ws.get());
+  }
+  PrWorkspace& ws = *wsp;
+  std::lock_guard<std::mutex> ws_lock(ws.mu);
+  ws.ensure(n, nt, mixed, prm.precision != PREC_FP32, pv || !out_on_device);
+  IterState* st = ws.st.get();
+  IterState* hstate = ws.hstate;
+
+  KNB_CUDA(cudaEventRecord(ws.t0, s));
+  if (pv) {
+    KNB_CUDA(cudaMemcpyAsync(ws.ptmp.get(), prm.personalization, (size_t)n * 8,
+                             prm.pers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                             s));
+    normalize_personalization(ws.ptmp.get(), n, ws.part3.get(), st + 2, hstate + 2, s);
+    if (perm) {
+      permute_in<<<grid_for(n, 256), 256, 0, s>>>(ws.ptmp.get(), perm, n, ws.pvec.get());
+      KNB_LAUNCH("permute_in");
+    } else {
+      KNB_CUDA(cudaMemcpyAsync(ws.pvec.get(), ws.ptmp.get(), (size_t)n * 8,
+                               cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  const double* pdev = pv ? ws.pvec.get() : nullptr;
+
+  IterState init{};
+  int launches = pv ? 3 : 0;
+  double tms32 = 0, tms64 = 0;
+  int64_t tn32 = 0, tn64 = 0;
+  PhaseResult r32, r64;
+  const int64_t cap = prm.max_iter;
+  double tol32 = std::max(prm.tol * prm.switch_factor, prm.switch_floor);
+  if (prm.precision == PREC_FP32) tol32 = prm.tol;
+
+  if (mixed) {
+    init.tol = tol32;
+    init.max_iter = (int32_t)std::min<int64_t>(cap, INT32_MAX);
+    KNB_CUDA(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    pr_init<float><<<gv, VT_THREADS, 0, s>>>(ws.y32[0].get(), ws.z32[0].get(), inv32, n,
+                                              ws.part3.get(), st);
+    KNB_LAUNCH("pr_init");
+    ++launches;
+    SweepBuffers B{v64, v32, {ws.y32[0].get(), ws.y32[1].get()},
+                   {ws.z32[0].get(), ws.z32[1].get()}, inv32, pdev, ws.carry32.get(),
+                   ws.head32.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st};
+    SweepFn fn = pick_kernel<float, float, false>(var, ipt, pv, ju);
+    r32 = run_phase(fn, op, P, B, prm.damping, false, s, ws, hstate, &tms32, &tn32);
+    launches += r32.launches;
+    if (r32.stopped && !r32.converged)
+      throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +
+                  " within " + std::to_string(prm.max_iter) + " iterations");
+  }
+  const float* y32_last = mixed ? ws.y32[r32.iter & 1].get() : nullptr;
+  if (prm.precision != PREC_FP32) {
+    IterState i64{};
+    i64.tol = prm.tol;
+    i64.max_iter = (int32_t)std::min<int64_t>(cap - r32.iter, INT32_MAX);
+    if (i64.max_iter <= 0) i64.max_iter = 1;
+    KNB_CUDA(cudaMemcpyAsync(st + 1, &i64, sizeof(i64), cudaMemcpyHostToDevice, s));
+    if (mixed) {
+      pr_switch<<<gv, VT_THREADS, 0, s>>>(y32_last, st, ws.y64[0].get(), ws.z64[0].get(), inv64,
+                                          n, ws.part3.get(), st + 1);
+      KNB_LAUNCH("pr_switch");
+    } else {
+      pr_init<double><<<gv, VT_THREADS, 0, s>>>(ws.y64[0].get(), ws.z64[0].get(), inv64, n,
+                                                 ws.part3.get(), st + 1);
+      KNB_LAUNCH("pr_init");
+    }
+    ++launches;
+    SweepBuffers B{v64, v32, {ws.y64[0].get(), ws.y64[1].get()},
+                   {ws.z64[0].get(), ws.z64[1].get()}, inv64, pdev, ws.carry64.get(),
+                   ws.head64.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1};
+    bool use32 = op.has_vals && op.vals32_exact && !prm.fp64_values;
+    SweepFn fn = use32 ? pick_kernel<double, float, true>(var, ipt, pv, ju)
+                       : pick_kernel<double, double, true>(var, ipt, pv, ju);
+    r64 = run_phase(fn, op, P, B, prm.damping, true, s, ws, hstate, &tms64, &tn64);
+    launches += r64.launches;
+    if (!r64.converged)
+      throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +
+                  " within " + std::to_string(prm.max_iter) + " iterations");
+  }
+  // output, in the caller's node order
+  double* outp = out_on_device ? out : ws.dout.get();
+  if (!out_on_device && !outp) {
+    ws.dout.alloc(n);
+    outp = ws.dout.get();
+  }
+  if (prm.precision == PREC_FP32) {
+    pr_output<float><<<gv, VT_THREADS, 0, s>>>(y32_last, st, n, iperm, outp);
+  } else {
+    pr_output<double><<<gv, VT_THREADS, 0, s>>>(ws.y64[r64.iter & 1].get(), st + 1, n, iperm,
+                                                 outp);
+  }
+  KNB_LAUNCH("pr_output");
+  ++launches;
+  if (!out_on_device)
+    KNB_CUDA(cudaMemcpyAsync(out, outp, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaEventRecord(ws.t1, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  KNB_CUDA(cudaEventElapsedTime(&ms, ws.t0, ws.t1));
+  if (info) {
+    info->iterations = r32.iter + r64.iter;
+    info->iterations_fp32 = r32.iter;
+    info->change = prm.precision == PREC_FP32 ? r32.change : r64.change;
+    info->seconds = ms * 1e-3;
+    info->converged = 1;
+    info->kernel_launches = launches;
+  }
+  const bool use32v = op.has_vals && op.vals32_exact && !prm.fp64_values;
+  g_timing[0] = {tn32, tms32, sweep_bytes(op, 4, 4, pv)};
+  g_timing[1] = {tn64, tms64, sweep_bytes(op, 8, use32v ? 4 : 8, pv)};
+}
+
+}  // namespace knb

@@ -1,0 +1,390 @@
+"""Parity of the CUDA library with the CPU oracle and the reference's golden
+files, through the C ABI.
+
+Bars: integer CSR structure (offsets, targets, arc order) and degree counts
+bit-exact; FP64 PageRank within 1e-12 L1 of the oracle; mixed-precision
+PageRank within 1e-9 L1 with the same top-100 order; eigenvector centrality
+within the golden tolerance (rel 1e-8 / abs 1e-9) and within 1e-9 (max
+norm) of the oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import goldens
+import knappnet_b200 as K
+from oracle import oracle as O
+from test_oracle import SplitMix64, dense, random_case
+
+pytestmark = pytest.mark.gpu
+
+DOC = goldens.load()
+
+
+def both(fx):
+    return goldens.make_graph(K.Graph, fx), goldens.make_graph(O.Graph, fx)
+
+
+# ------------------------------------------------------------------ golden files
+@pytest.mark.parametrize("fx_name,variant,orc", goldens.cases())
+def test_golden(fx_name, variant, orc):
+    fx = DOC["fixtures"][fx_name]
+    g = goldens.make_graph(K.Graph, fx)
+    got = goldens.run_variant(g, fx, variant)
+    ok, msg = goldens.agree(list(got), DOC["golden"][fx_name][variant][orc],
+                            DOC["manifest"][variant]["tolerance"])
+    assert ok, msg
+
+
+# ------------------------------------------------------------------ CSR and degree
+def random_graphs(seed, count, max_n):
+    rng = SplitMix64(seed)
+    for _ in range(count):
+        n, src, tgt, w, directed = random_case(rng, max_n)
+        yield n, src, tgt, w, directed
+
+
+def assert_same_csr(kg, og, which):
+    ko, kt, kw = kg.csr(which)
+    oo, ot, ow = og.csr(which)
+    assert np.array_equal(ko.astype(np.uint64), oo)
+    assert np.array_equal(kt, ot)
+    if ow is not None:
+        assert np.array_equal(kw, ow)
+
+
+@pytest.mark.parametrize("fx_name", sorted(DOC["fixtures"]))
+def test_csr_bit_exact_fixtures(fx_name):
+    kg, og = both(DOC["fixtures"][fx_name])
+    assert_same_csr(kg, og, 0)
+    if kg.directed:
+        assert_same_csr(kg, og, 1)
+
+
+def test_csr_bit_exact_random_multigraphs():
+    for n, src, tgt, w, directed in random_graphs(7, 60, 60):
+        kg = K.Graph(n, src, tgt, w, directed)
+        og = O.Graph(n, src, tgt, w, directed)
+        assert_same_csr(kg, og, 0)
+        if directed:
+            assert_same_csr(kg, og, 1)
+            # directions ignored: the reference rebuilds an undirected graph
+            ug = O.Graph(n, src, tgt, w, False)
+            ko, kt, kw = kg.csr(2)
+            oo, ot, ow = ug.csr(0)
+            assert np.array_equal(ko.astype(np.uint64), oo) and np.array_equal(kt, ot)
+            assert np.array_equal(kw, ow)
+
+
+def test_csr_bit_exact_large_with_parallel_arcs():
+    rng = np.random.default_rng(5)
+    n, m = 20_000, 400_000
+    src = rng.integers(0, n // 10, m)  # many parallel arcs and loops
+    tgt = rng.integers(0, n // 10, m)
+    w = rng.random(m)
+    for directed in (True, False):
+        kg = K.Graph(n, src, tgt, w, directed)
+        og = O.Graph(n, src, tgt, w, directed)
+        assert_same_csr(kg, og, 0)
+        if directed:
+            assert_same_csr(kg, og, 1)
+
+
+@pytest.mark.parametrize("fx_name", sorted(DOC["fixtures"]))
+def test_degree_bit_exact(fx_name):
+    fx = DOC["fixtures"][fx_name]
+    kg, og = both(fx)
+    for mode in (1, 2, 3):
+        for loops in (False, True):
+            for weighted in ((False, True) if fx["weighted"] else (False,)):
+                a = kg.degree(mode, loops, weighted)
+                b = og.degree(mode, loops, weighted)
+                if weighted:
+                    assert np.allclose(a, b, rtol=1e-15, atol=0)
+                else:
+                    assert np.array_equal(a, b)
+
+
+# ------------------------------------------------------------------ PageRank
+PR_OPTIONS = [
+    dict(),
+    dict(loops=1),
+    dict(loops=2),
+    dict(directed=False),
+    dict(dangling=1, pers="mod3plus1"),
+    dict(pers="mod3plus1"),
+    dict(damping=0.6),
+]
+
+
+@pytest.mark.parametrize("fx_name", sorted(DOC["fixtures"]))
+def test_pagerank_fp64_within_1e12_of_oracle(fx_name):
+    fx = DOC["fixtures"][fx_name]
+    kg, og = both(fx)
+    n = fx["n"]
+    for opt in PR_OPTIONS + ([dict(weighted=True)] if fx["weighted"] else []):
+        o = dict(opt)
+        pers = o.pop("pers", None)
+        p = np.asarray(goldens.node_rule(pers, n)) if pers else None
+        a = kg.pagerank(personalization=p, **o)
+        b = og.pagerank(personalization=p, **o)
+        assert np.abs(a - b).sum() <= 1e-12, (opt, np.abs(a - b).sum())
+
+
+def test_pagerank_reference_signature_call():
+    g = K.Graph(5, [0, 0, 1, 2, 3, 2], [1, 2, 2, 0, 2, 4], None, True)
+    a = g.pagerank_reference_call(0.85, 1, 0, None, 0, 0, 0.0, 0, 4)
+    want = [0.2142011097, 0.1574496602, 0.3477339318, 0.0664141886, 0.2142011097]
+    assert np.allclose(a, want, atol=1e-9, rtol=0)
+
+
+def test_pagerank_hand_values():
+    g = K.Graph(5, [0, 0, 1, 2, 3, 2], [1, 2, 2, 0, 2, 4], None, True)
+    p = [1.0, 0.0, 0.0, 0.0, 0.0]
+    assert np.allclose(g.pagerank(personalization=p),
+                       [0.3928645968, 0.1669674536, 0.3088897892, 0.0, 0.1312781604],
+                       atol=1e-9, rtol=0)
+    assert np.allclose(g.pagerank(personalization=p, dangling=1),
+                       [0.3166510816, 0.1629073936, 0.3254597594, 0.0283306839, 0.1666510816],
+                       atol=1e-9, rtol=0)
+
+
+def test_pagerank_stationary_random_cases():
+    rng = SplitMix64(21)
+    for _ in range(60):
+        n, src, tgt, w, directed = random_case(rng, 30)
+        weighted = rng.below(2) == 0
+        g = K.Graph(n, src, tgt, w if weighted else None, directed)
+        x = g.pagerank(weighted=weighted)
+        assert abs(x.sum() - 1.0) < 1e-12
+        a = dense(n, src, tgt, w, directed, weighted, False, 2.0)
+        out = a.sum(axis=1)
+        stuck = x[out == 0].sum()
+        flow = np.array([sum(a[j, i] / out[j] * x[j] for j in range(n) if out[j] > 0)
+                         for i in range(n)])
+        rhs = 0.85 * (flow + stuck / n) + 0.15 / n
+        assert np.abs(x - rhs).max() < 1e-10
+
+
+def rmat_pair(scale, weighted, symmetrize=False, seed=3):
+    kg = K.generate_rmat(scale, 16, seed=seed, clean=True, symmetrize=symmetrize,
+                         lognormal=weighted, wseed=seed + 100)
+    s, t, w = kg.edges()
+    og = O.Graph(kg.n, s, t, w, not symmetrize)
+    return kg, og
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_pagerank_rmat_fp64_and_mixed(weighted):
+    kg, og = rmat_pair(14, weighted)
+    ref = og.pagerank(weighted=weighted, tol=1e-9)
+    x64, i64 = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_FP64)
+    assert np.abs(x64 - ref).sum() <= 1e-12
+    assert i64.iterations == og.last_iters
+    xm, im = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_MIXED)
+    assert np.abs(xm - ref).sum() <= 1e-9, np.abs(xm - ref).sum()
+    assert im.iterations_fp32 > 0
+    top = np.argsort(-ref, kind="stable")[:100]
+    assert np.array_equal(np.argsort(-xm, kind="stable")[:100], top)
+
+
+def test_pagerank_personalized_and_undirected_rmat():
+    kg, og = rmat_pair(12, True)
+    n = kg.n
+    p = np.zeros(n)
+    p[[3, 17, 400]] = [1.0, 2.0, 0.5]
+    for opts in (dict(personalization=p), dict(personalization=p, dangling=1),
+                 dict(directed=False), dict(directed=False, loops=1)):
+        a = kg.pagerank(weighted=True, **opts)
+        b = og.pagerank(weighted=True, **opts)
+        assert np.abs(a - b).sum() <= 1e-12, opts
+
+
+def test_pagerank_repeat_runs_are_bit_identical():
+    kg, _ = rmat_pair(13, True)
+    a = kg.pagerank(weighted=True)
+    b = kg.pagerank(weighted=True)
+    assert np.array_equal(a, b)
+
+
+def test_pagerank_errors():
+    g = K.Graph(5, [0, 0, 1, 2, 3, 2], [1, 2, 2, 0, 2, 4], None, True)
+    with pytest.raises(K.EngineError, match="damping is 1.5"):
+        g.pagerank(damping=1.5)
+    with pytest.raises(K.EngineError, match="dangling-node code 7"):
+        g.pagerank(dangling=7)
+    with pytest.raises(K.EngineError, match="self-loop weight code 5"):
+        g.pagerank(loops=5)
+    with pytest.raises(K.EngineError, match="no edge weights"):
+        g.pagerank(weighted=True)
+    with pytest.raises(K.EngineError, match="finite, nonnegative"):
+        g.pagerank(personalization=[1.0, -1.0, 0, 0, 0])
+    with pytest.raises(K.EngineError, match="positive sum"):
+        g.pagerank(personalization=[0.0] * 5)
+    with pytest.raises(K.EngineError, match="did not converge"):
+        g.pagerank(tol=1e-15, max_iter=2)
+    neg = K.Graph(3, [0, 1], [1, 2], [1.0, -2.0], True)
+    with pytest.raises(K.EngineError, match="edge 1 has negative weight -2"):
+        neg.pagerank(weighted=True)
+    with pytest.raises(K.EngineError, match="edge 1 refers to node index 9"):
+        K.Graph(3, [0, 1], [1, 9], None, True)
+    with pytest.raises(K.EngineError, match="edge 0 refers to node index -1"):
+        K.Graph(3, [-1, 1], [1, 9], None, True)
+    with pytest.raises(K.EngineError, match="NaN"):
+        K.Graph(3, [0, 1], [1, 2], [1.0, float("nan")], True)
+
+
+def test_empty_and_single_node():
+    e = K.Graph(0, [], [], None, True)
+    assert e.pagerank().size == 0
+    s = K.Graph(1, [], [], None, True)
+    assert np.allclose(s.pagerank(), [1.0])
+
+
+# ------------------------------------------------------------------ eigenvector
+def test_eigen_closed_forms():
+    star = K.Graph(5, [0, 0, 0, 0], [1, 2, 3, 4], None, False)
+    v, lam, conn = star.eigenvector()
+    assert abs(lam - 2.0) < 1e-10 and conn
+    assert np.allclose(v, [1.0, 0.5, 0.5, 0.5, 0.5], atol=1e-10, rtol=0)
+    path = K.Graph(4, [0, 1, 2], [1, 2, 3], None, False)
+    v, lam, _ = path.eigenvector()
+    phi = (1 + 5 ** 0.5) / 2
+    assert abs(lam - phi) < 1e-10
+    assert np.allclose(v, [1 / phi, 1, 1, 1 / phi], atol=1e-10, rtol=0)
+    lw = K.Graph(2, [0, 0], [0, 1], [1.0, 3.0], False)
+    assert abs(lw.eigenvector()[1] - (1 + 2 ** 0.5)) < 1e-10
+    assert abs(lw.eigenvector(loops=1, weighted=True)[1] - (1 + 37 ** 0.5) / 2) < 1e-10
+    empty = K.Graph(3, [], [], None, False)
+    v, lam, conn = empty.eigenvector()
+    assert v.tolist() == [1.0, 1.0, 1.0] and lam == 0.0 and not conn
+    dag = K.Graph(3, [0, 1], [1, 2], None, True)
+    assert dag.eigenvector(mode=2)[0].tolist() == [0.0, 0.0, 1.0]
+    assert dag.eigenvector(mode=1)[0].tolist() == [1.0, 0.0, 0.0]
+    tri = K.Graph(5, [0, 1, 2, 3], [1, 2, 0, 4], None, False)
+    v, lam, conn = tri.eigenvector()
+    assert not conn and abs(lam - 2.0) < 1e-10
+    assert np.allclose(v, [1, 1, 1, 0, 0], atol=1e-9, rtol=0)
+
+
+def test_eigen_directed_modes():
+    g = K.Graph(3, [0, 1, 2, 2], [1, 2, 0, 1], None, True)
+    ins, li, _ = g.eigenvector(mode=2)
+    outs, lo, _ = g.eigenvector(mode=1)
+    a = np.array([[0.0, 1, 0], [0, 0, 1], [1, 1, 0]])
+    assert np.allclose(a.T @ ins, li * ins, atol=1e-10)
+    assert np.allclose(a @ outs, lo * outs, atol=1e-10)
+
+
+@pytest.mark.parametrize("fx_name", sorted(DOC["fixtures"]))
+def test_eigen_matches_oracle_on_fixtures(fx_name):
+    fx = DOC["fixtures"][fx_name]
+    kg, og = both(fx)
+    for opts in (dict(), dict(mode=1), dict(mode=3), dict(scale=1, loops=1)):
+        try:
+            b = og.eigenvector(**opts)
+        except O.OracleError:
+            with pytest.raises(K.EngineError):
+                kg.eigenvector(**opts)
+            continue
+        a = kg.eigenvector(**opts)
+        assert np.abs(a[0] - b[0]).max() <= 1e-9, opts
+        assert abs(a[1] - b[1]) <= 1e-9 * max(1.0, abs(b[1])), opts
+        assert a[2] == b[2]
+
+
+def test_lanczos_eigen_equation_random():
+    rng = SplitMix64(11)
+    for _ in range(40):
+        n, src, tgt, w, _ = random_case(rng, 40)
+        weighted = rng.below(2) == 0
+        g = K.Graph(n, src, tgt, w if weighted else None, False)
+        x, lam, _ = g.eigenvector(weighted=weighted, scale=1)
+        if lam == 0.0:
+            continue
+        a = dense(n, src, tgt, w, False, weighted, True, 2.0)
+        assert (x >= 0).all()
+        assert np.all(np.abs(a @ x - lam * x) <= 1e-9 * (1 + lam))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_lanczos_symmetric_rmat_matches_oracle(precision):
+    kg, og = rmat_pair(13, False, symmetrize=True)
+    b, lb, cb = og.eigenvector(mode=3, tol=1e-10)
+    a, info = kg.eigenvector_ex(mode=3, tol=1e-10, precision=precision)
+    assert abs(info.eigenvalue - lb) <= 1e-9 * lb
+    assert np.abs(a - b).max() <= 1e-8
+    assert bool(info.connected) == cb
+
+
+def test_power_iteration_directed_rmat_matches_oracle():
+    kg, og = rmat_pair(11, True, seed=9)
+    for mode in (1, 2):
+        try:
+            b = og.eigenvector(mode=mode, weighted=True, tol=1e-10)
+        except O.OracleError:
+            continue
+        a = kg.eigenvector(mode=mode, weighted=True, tol=1e-10)
+        assert np.abs(a[0] - b[0]).max() <= 1e-9
+        assert abs(a[1] - b[1]) <= 1e-9 * max(1.0, b[1])
+
+
+# ------------------------------------------------------------------ generator
+def test_rmat_generator_matches_oracle():
+    scale, ef, seed = 10, 16, 77
+    raw = K.generate_rmat(scale, ef, seed=seed, clean=False)
+    s, t, _ = raw.edges()
+    os_, ot = O.rmat_raw(scale, ef << scale, 0.57, 0.19, 0.19, seed)
+    assert np.array_equal(s, os_) and np.array_equal(t, ot)
+    clean = K.generate_rmat(scale, ef, seed=seed, clean=True)
+    cs, ct, _ = clean.edges()
+    keep = os_ != ot
+    key = np.unique(os_[keep].astype(np.int64) << scale | ot[keep].astype(np.int64))
+    assert np.array_equal(cs, key >> scale) and np.array_equal(ct, key & ((1 << scale) - 1))
+    sym = K.generate_rmat(scale, ef, seed=seed, symmetrize=True)
+    ss, st, _ = sym.edges()
+    lo, hi = np.minimum(os_, ot)[keep], np.maximum(os_, ot)[keep]
+    key = np.unique(lo.astype(np.int64) << scale | hi.astype(np.int64))
+    assert np.array_equal(ss, key >> scale) and np.array_equal(st, key & ((1 << scale) - 1))
+    assert not sym.directed
+
+
+def test_lognormal_weights_match_box_muller():
+    g = K.generate_rmat(8, 8, seed=1, lognormal=True, wseed=5)
+    _, _, w = g.edges()
+    u = np.array([O.stream_u32(5, e, 4) for e in range(len(w))], dtype=np.uint64)
+    a = (u[:, 0] << np.uint64(32) | u[:, 1]) >> np.uint64(11)
+    b = (u[:, 2] << np.uint64(32) | u[:, 3]) >> np.uint64(11)
+    u1 = a.astype(np.float64) / 2.0 ** 53
+    u2 = b.astype(np.float64) / 2.0 ** 53
+    z = np.sqrt(-2 * np.log(1 - u1)) * np.cos(2 * np.pi * u2)
+    want = np.exp(z).astype(np.float32).astype(np.float64)
+    assert np.abs(w / want - 1).max() <= 2 ** -23
+    assert abs(np.log(w).mean()) < 0.1 and abs(np.log(w).std() - 1) < 0.1
+
+
+@pytest.mark.parametrize("variant,ipt,relabel", [(1, 4, 0), (1, 8, 1), (2, 4, 1), (2, 8, 0),
+                                                 (2, 8, 1), (2, 16, 1)])
+def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel):
+    kg, og = rmat_pair(12, True, seed=21)
+    n = kg.n
+    p = np.zeros(n)
+    p[[1, 50, 600]] = 1.0
+    try:
+        K.set_tuning(K.TUNE_VARIANT, variant)
+        K.set_tuning(K.TUNE_IPT, ipt)
+        K.set_tuning(K.TUNE_RELABEL, relabel)
+        for opts in (dict(), dict(personalization=p), dict(directed=False)):
+            b = og.pagerank(weighted=True, **opts)
+            a = kg.pagerank(weighted=True, **opts)
+            assert np.abs(a - b).sum() <= 1e-12, opts
+            am, _ = kg.pagerank_ex(weighted=True, precision=K.PREC_MIXED, tol=1e-10,
+                                   personalization=opts.get("personalization"),
+                                   directed=opts.get("directed", True))
+            bm = og.pagerank(weighted=True, tol=1e-10, **opts)
+            assert np.abs(am - bm).sum() <= 1e-9, opts
+    finally:
+        K.set_tuning(K.TUNE_VARIANT, 0)
+        K.set_tuning(K.TUNE_IPT, 0)
+        K.set_tuning(K.TUNE_RELABEL, 1)
