@@ -121,6 +121,38 @@ NET_API int32_t net_eigenvector_ex(const GraphHandle *h, int32_t mode, int32_t w
                            double *eigenvalue, int32_t *connected,
                            NetSolveInfo *info, char *err, size_t err_len);
 
+/* What a batched solve did. */
+typedef struct NetBatchInfo {
+  double seconds;                /* device time of the solve */
+  int64_t sweeps;                /* batch sweeps (one SpMM each) */
+  int64_t sweeps_fp32;           /* of which in FP32 */
+  int64_t column_iterations;     /* sum over vectors of their own iteration counts */
+  int64_t max_column_iterations;
+  int32_t kernel_launches;
+  int32_t reserved;
+} NetBatchInfo;
+
+/* Personalised PageRank for `batch` teleport vectors at once (one sparse
+ * matrix times dense matrix product per sweep). personalization and out are
+ * column-major n x batch: vector c at offset c * n. Each vector gets exactly
+ * the result of net_pagerank with that personalization (own rescaling,
+ * dangling mass and stopping sweep). precision 0 = FP64, 1 = mixed. */
+NET_API int32_t net_pagerank_batch(const GraphHandle *h, double damping,
+                           int32_t directed, int32_t weighted,
+                           const double *personalization, int64_t batch,
+                           int32_t dangling, int32_t loops, double tol,
+                           int64_t max_iter, int32_t precision, double *out,
+                           NetBatchInfo *info, char *err, size_t err_len);
+
+/* As net_pagerank_batch with device pointers. */
+NET_API int32_t net_pagerank_batch_device(const GraphHandle *h, double damping,
+                                  int32_t directed, int32_t weighted,
+                                  const double *d_personalization, int64_t batch,
+                                  int32_t dangling, int32_t loops, double tol,
+                                  int64_t max_iter, int32_t precision,
+                                  double *d_out, NetBatchInfo *info, char *err,
+                                  size_t err_len);
+
 /* Builds a graph from device arrays: 32-bit endpoints and FP32 (d_w32) or
  * FP64 (d_w64) weights, either may be NULL. */
 NET_API int32_t net_graph_new_device(int64_t n, const uint32_t *d_src,

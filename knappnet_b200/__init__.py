@@ -31,6 +31,16 @@ class EngineError(RuntimeError):
     """A call of the C ABI returned a failure status."""
 
 
+class NetBatchInfo(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("sweeps", ctypes.c_int64),
+                ("sweeps_fp32", ctypes.c_int64), ("column_iterations", ctypes.c_int64),
+                ("max_column_iterations", ctypes.c_int64), ("kernel_launches", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class NetSolveInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int64), ("iterations_fp32", ctypes.c_int64),
                 ("change", ctypes.c_double), ("seconds", ctypes.c_double),
@@ -79,6 +89,13 @@ def lib() -> ctypes.CDLL:
     L.net_eigenvector_ex.argtypes = [h, i32, i32, i32, i32, f64, i64, i32, vp,
                                      ctypes.POINTER(f64), ctypes.POINTER(i32), info_p, cp, sz]
     L.net_eigenvector_ex.restype = i32
+    binfo_p = ctypes.POINTER(NetBatchInfo)
+    L.net_pagerank_batch.argtypes = [h, f64, i32, i32, vp, i64, i32, i32, f64, i64, i32, vp,
+                                     binfo_p, cp, sz]
+    L.net_pagerank_batch.restype = i32
+    L.net_pagerank_batch_device.argtypes = [h, f64, i32, i32, vp, i64, i32, i32, f64, i64, i32,
+                                            vp, binfo_p, cp, sz]
+    L.net_pagerank_batch_device.restype = i32
     L.net_graph_new_device.argtypes = [i64, vp, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
     L.net_graph_new_device.restype = i32
     L.net_graph_arc_count.argtypes = [h, i32]
@@ -219,6 +236,21 @@ class Graph:
                                          err, ERR_LEN), err)
         return info
 
+    def pagerank_batch(self, personalization, damping=0.85, directed=True, weighted=False,
+                       dangling=0, loops=0, tol=0.0, max_iter=0, precision=PREC_FP64):
+        """Personalised PageRank for every row of `personalization` (shape
+        (batch, n)); returns scores of the same shape and the NetBatchInfo."""
+        P = np.ascontiguousarray(personalization, dtype=np.float64)
+        if P.ndim != 2 or P.shape[1] != self.n:
+            raise ValueError("personalization must have shape (batch, n)")
+        out = np.zeros_like(P)
+        info = NetBatchInfo()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_pagerank_batch(self.h, damping, int(directed), int(weighted), _ptr(P),
+                                        P.shape[0], dangling, loops, tol, max_iter, precision,
+                                        _ptr(out), ctypes.byref(info), err, ERR_LEN), err)
+        return out, info
+
     def pagerank_reference_call(self, damping=0.85, directed=True, weighted=False,
                                 personalization=None, dangling=0, loops=0, tol=0.0, max_iter=0,
                                 threads=0):
@@ -280,7 +312,8 @@ def set_sweep_timing(on: bool) -> None:
     lib().net_set_sweep_timing(int(on))
 
 
-TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT = 0, 1, 2, 3, 4
+TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT = \
+    0, 1, 2, 3, 4, 5
 
 
 def set_tuning(key: int, value: float) -> None:

@@ -1,0 +1,676 @@
+// Batched personalised PageRank: B teleport vectors solved together as a
+// sparse matrix times dense matrix iteration (SpMM). Each column is the
+// reference's PageRank with that personalization vector
+// (crates/engine/src/metrics/spectral.rs:211-281): it has its own
+// normalisation, dangling mass and L1 change, and it stops at its own first
+// sweep with change <= tol, keeping that iterate while the others go on.
+//
+// Layout: the iterate is node-major, Y[i * B + c], so the gather of a source
+// node's B values is one contiguous run (coalesced across the warp: lane l
+// holds columns l, l + 32, ...). Rows are split over warps in ranges of
+// about equal arc counts; rows with more than LONG_ROW arcs are cut into
+// chunks whose partial sums a second kernel adds in chunk order. Per-column
+// sums are kept per lane, joined per CTA in warp order and per sweep in CTA
+// order, so the results do not change from run to run.
+//
+// Precision: FP64, or mixed (FP32 sweeps until every column's change is below
+// max(tol * switch_factor, switch_floor), then FP64 sweeps on the same
+// trajectories until each column meets tol).
+#include <algorithm>
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+#include "batch.cuh"
+#include "pagerank.cuh"
+
+namespace knb {
+
+constexpr int BT = 256;          // threads per CTA
+constexpr int BW = BT / 32;      // warps per CTA
+constexpr int MAXVW = 8;         // columns per lane (B <= 256 per launch)
+constexpr uint32_t LONG_ROW = 512;
+constexpr uint32_t RANGE_ARCS = 1024;
+
+struct RowRange {
+  uint32_t lo, hi;
+};
+struct Chunk {
+  uint32_t row, a0, a1;
+};
+
+// Per-column state of a batch phase.
+struct ColState {
+  double inv_total;       // 1 / sum of the column's current iterate
+  double dterm;           // its dangling mass, normalised
+  double prev_inv_total;
+  double total, change;
+  int32_t frozen;         // converged (or finished) columns keep their iterate
+  int32_t iter;           // sweeps this column took
+  int32_t converged;
+  int32_t pad;
+};
+
+struct BatchScalars {
+  double d;
+  double pu;    // 1 / n
+  uint32_t n, B;
+  int jump_uniform;
+  double tol;
+  int32_t max_iter;
+  int32_t exact;
+};
+
+// Row sum of one row of A times Z for this lane's columns.
+template <class VT, class MT, int VW>
+__device__ __forceinline__ void row_product(const OpView<MT>& op, const VT* __restrict__ Z,
+                                            uint32_t B, uint32_t a0, uint32_t a1, int lane,
+                                            VT (&acc)[VW]) {
+#pragma unroll
+  for (int v = 0; v < VW; ++v) acc[v] = VT(0);
+  for (uint32_t k = a0; k < a1; ++k) {
+    const uint32_t j = __ldg(op.cols + k);
+    const VT w = op.vals ? (VT)__ldg(op.vals + k) : VT(1);
+    const VT* zr = Z + (size_t)j * B;
+#pragma unroll
+    for (int v = 0; v < VW; ++v) {
+      const uint32_t c = lane + 32 * v;
+      if (c < B) acc[v] += w * __ldg(zr + c);
+    }
+  }
+}
+
+// The PageRank update of row i for this lane's columns, and its per-column
+// sums (mass, dangling mass, L1 change) into red.
+template <class VT, int VW>
+__device__ __forceinline__ void row_update(uint32_t i, const VT (&s)[VW], int lane,
+                                           const BatchScalars& bs, const ColState* cs,
+                                           const VT* __restrict__ Yold, VT* __restrict__ Ynew,
+                                           VT* __restrict__ Znew, const VT* __restrict__ inv_out,
+                                           const double* __restrict__ P,
+                                           double (&red)[3][VW]) {
+  const VT io = inv_out[i];
+#pragma unroll
+  for (int v = 0; v < VW; ++v) {
+    const uint32_t c = lane + 32 * v;
+    if (c >= bs.B || cs[c].frozen) continue;
+    const VT it = (VT)cs[c].inv_total, dt = (VT)cs[c].dterm;
+    const size_t q = (size_t)i * bs.B + c;
+    const VT pg = (VT)P[q];
+    const VT jg = bs.jump_uniform ? (VT)bs.pu : pg;
+    const VT u = (VT)bs.d * (s[v] * it + dt * jg) + (VT)(1.0 - bs.d) * pg;
+    const VT xo = Yold[q] * it;
+    Ynew[q] = u;
+    Znew[q] = u * io;
+    red[0][v] += (double)u;
+    if (io == VT(0)) red[1][v] += (double)u;
+    red[2][v] += fabs((double)u - (double)xo);
+  }
+}
+
+// Joins the lanes' per-column sums of a CTA in warp order into part[cta][3][B].
+template <int VW>
+__device__ __forceinline__ void cta_column_sums(double (&red)[3][VW], uint32_t B,
+                                                double* __restrict__ part, double* smem) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  // smem: [BW][3][B]
+  for (int s = 0; s < 3; ++s)
+#pragma unroll
+    for (int v = 0; v < VW; ++v) {
+      const uint32_t c = lane + 32 * v;
+      if (c < B) smem[((size_t)w * 3 + s) * B + c] = red[s][v];
+    }
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < 3 * B; q += BT) {
+    double a = 0;
+    for (int ww = 0; ww < BW; ++ww) a += smem[(size_t)ww * 3 * B + q];
+    part[(size_t)blockIdx.x * 3 * B + q] = a;
+  }
+}
+
+template <class VT, class MT, int VW>
+__global__ void __launch_bounds__(BT)
+spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ ranges,
+          uint32_t nranges, BatchScalars bs, const ColState* __restrict__ cs,
+          const VT* __restrict__ Yold, VT* __restrict__ Ynew, VT* __restrict__ Znew,
+          const VT* __restrict__ inv_out, const double* __restrict__ P,
+          double* __restrict__ part, const int32_t* __restrict__ all_frozen) {
+  if (*all_frozen) return;
+  extern __shared__ double smem_b[];
+  const int lane = threadIdx.x & 31;
+  double red[3][VW];
+#pragma unroll
+  for (int s = 0; s < 3; ++s)
+#pragma unroll
+    for (int v = 0; v < VW; ++v) red[s][v] = 0.0;
+  const uint32_t gw = blockIdx.x * BW + (threadIdx.x >> 5), nw = gridDim.x * BW;
+  for (uint32_t r = gw; r < nranges; r += nw) {
+    const RowRange rr = ranges[r];
+    for (uint32_t i = rr.lo; i < rr.hi; ++i) {
+      const uint32_t a0 = op.off[i], a1 = op.off[i + 1];
+      if (a1 - a0 > LONG_ROW) continue;  // long rows: spmm_chunks / spmm_long
+      VT acc[VW];
+      row_product<VT, MT, VW>(op, Z, bs.B, a0, a1, lane, acc);
+      row_update<VT, VW>(i, acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
+    }
+  }
+  cta_column_sums<VW>(red, bs.B, part, smem_b);
+}
+
+// Partial products of the chunks of long rows.
+template <class VT, class MT, int VW>
+__global__ void __launch_bounds__(BT)
+spmm_chunks(OpView<MT> op, const VT* __restrict__ Z, const Chunk* __restrict__ chunks,
+            uint32_t nchunks, uint32_t B, VT* __restrict__ scratch,
+            const int32_t* __restrict__ all_frozen) {
+  if (*all_frozen) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = blockIdx.x * BW + (threadIdx.x >> 5), nw = gridDim.x * BW;
+  for (uint32_t q = gw; q < nchunks; q += nw) {
+    const Chunk ch = chunks[q];
+    VT acc[VW];
+    row_product<VT, MT, VW>(op, Z, B, ch.a0, ch.a1, lane, acc);
+#pragma unroll
+    for (int v = 0; v < VW; ++v) {
+      const uint32_t c = lane + 32 * v;
+      if (c < B) scratch[(size_t)q * B + c] = acc[v];
+    }
+  }
+}
+
+// Long rows: chunk partials added in chunk order, then the update.
+template <class VT, int VW>
+__global__ void __launch_bounds__(BT)
+spmm_long(const uint32_t* __restrict__ lrow, const uint32_t* __restrict__ lfirst, uint32_t nlong,
+          const VT* __restrict__ scratch, BatchScalars bs, const ColState* __restrict__ cs,
+          const VT* __restrict__ Yold, VT* __restrict__ Ynew, VT* __restrict__ Znew,
+          const VT* __restrict__ inv_out, const double* __restrict__ P,
+          double* __restrict__ part, const int32_t* __restrict__ all_frozen) {
+  if (*all_frozen) return;
+  extern __shared__ double smem_b[];
+  const int lane = threadIdx.x & 31;
+  double red[3][VW];
+#pragma unroll
+  for (int s = 0; s < 3; ++s)
+#pragma unroll
+    for (int v = 0; v < VW; ++v) red[s][v] = 0.0;
+  const uint32_t gw = blockIdx.x * BW + (threadIdx.x >> 5), nw = gridDim.x * BW;
+  for (uint32_t q = gw; q < nlong; q += nw) {
+    VT acc[VW];
+#pragma unroll
+    for (int v = 0; v < VW; ++v) acc[v] = VT(0);
+    for (uint32_t k = lfirst[q]; k < lfirst[q + 1]; ++k)
+#pragma unroll
+      for (int v = 0; v < VW; ++v) {
+        const uint32_t c = lane + 32 * v;
+        if (c < bs.B) acc[v] += scratch[(size_t)k * bs.B + c];
+      }
+    row_update<VT, VW>(lrow[q], acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
+  }
+  cta_column_sums<VW>(red, bs.B, part, smem_b);
+}
+
+// Per column: sums over the CTAs in order, the stopping rule, the scalars of
+// the next sweep; then whether every column is frozen.
+__global__ void spmm_finish(const double* __restrict__ part, uint32_t nparts, BatchScalars bs,
+                            ColState* cs, int32_t* all_frozen, int32_t count_sweep) {
+  __shared__ int any_active;
+  if (threadIdx.x == 0) any_active = 0;
+  __syncthreads();
+  if (*all_frozen) return;
+  for (uint32_t c = threadIdx.x; c < bs.B; c += blockDim.x) {
+    ColState s = cs[c];
+    if (!s.frozen) {
+      double T = 0, D = 0, ch = 0;
+      for (uint32_t q = 0; q < nparts; ++q) {
+        const double* p = part + (size_t)q * 3 * bs.B;
+        T += p[c];
+        D += p[bs.B + c];
+        ch += p[2 * bs.B + c];
+      }
+      s.prev_inv_total = s.inv_total;
+      s.total = T;
+      s.inv_total = 1.0 / T;
+      s.dterm = D / T;
+      s.change = ch;
+      s.iter += count_sweep;
+      if (ch <= bs.tol) {
+        s.converged = 1;
+        s.frozen = 1;
+      } else if (s.iter >= bs.max_iter) {
+        s.frozen = 1;
+      }
+      cs[c] = s;
+    }
+    if (!s.frozen) atomicOr(&any_active, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !any_active) *all_frozen = 1;
+}
+
+// Start: Y = 1/n, Z = Y / out, per-column dangling mass (fixed-order sums).
+template <class VT>
+__global__ void spmm_init(VT* __restrict__ Y, VT* __restrict__ Zb, const VT* __restrict__ inv_out,
+                          uint32_t n, uint32_t B, double* __restrict__ colD) {
+  // one CTA per column group of 256 threads: thread c sums column c's dangling mass
+  const VT x0 = (VT)(1.0 / (double)n);
+  const uint64_t total = (uint64_t)n * B;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(q / B);
+    Y[q] = x0;
+    Zb[q] = x0 * inv_out[i];
+  }
+  (void)colD;
+}
+
+// Dangling count (same for every column at the start): D0 = n_dangling / n.
+__global__ void spmm_set_state(ColState* cs, uint32_t B, double dterm0, int32_t max_iter) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < B; c += gridDim.x * blockDim.x) {
+    ColState s{};
+    s.inv_total = 1.0;
+    s.prev_inv_total = 1.0;
+    s.dterm = dterm0;
+    s.total = 1.0;
+    cs[c] = s;
+  }
+  (void)max_iter;
+}
+
+// FP32 -> FP64 hand-over: Y64 = Y32 / T per column, read from the buffer the
+// column's FP32 phase stopped in; Z64 = Y64 / out.
+__global__ void spmm_switch(const float* __restrict__ Y0, const float* __restrict__ Y1,
+                            const ColState* __restrict__ cs32, double* __restrict__ Y64,
+                            double* __restrict__ Z64, const double* __restrict__ inv_out,
+                            uint32_t n, uint32_t B) {
+  const uint64_t total = (uint64_t)n * B;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(q / B), c = (uint32_t)(q % B);
+    const ColState s = cs32[c];
+    const float* Y = (s.iter & 1) ? Y1 : Y0;
+    const double y = (double)Y[q] * s.inv_total;
+    Y64[q] = y;
+    Z64[q] = y * inv_out[i];
+  }
+}
+
+// Column sums (and dangling sums) of a node-major n x B matrix: CTA b adds
+// rows b, b + G, ... per column (thread c owns column c), then one CTA adds
+// the CTA partials in order and writes the column states.
+__global__ void column_sums_part(const double* __restrict__ Y, const double* __restrict__ inv_out,
+                                 uint32_t n, uint32_t B, double* __restrict__ part) {
+  const uint32_t c = threadIdx.x;
+  if (c >= B) return;
+  double T = 0, D = 0;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const double y = Y[(size_t)i * B + c];
+    T += y;
+    if (inv_out[i] == 0.0) D += y;
+  }
+  part[(size_t)blockIdx.x * 2 * B + c] = T;
+  part[(size_t)blockIdx.x * 2 * B + B + c] = D;
+}
+
+__global__ void column_sums_finish(const double* __restrict__ part, uint32_t nparts, uint32_t B,
+                                   ColState* cs) {
+  const uint32_t c = threadIdx.x;
+  if (c >= B) return;
+  double T = 0, D = 0;
+  for (uint32_t q = 0; q < nparts; ++q) {
+    T += part[(size_t)q * 2 * B + c];
+    D += part[(size_t)q * 2 * B + B + c];
+  }
+  ColState s{};
+  s.total = T;
+  s.inv_total = 1.0 / T;
+  s.prev_inv_total = s.inv_total;
+  s.dterm = D / T;
+  cs[c] = s;
+}
+
+// Personalization: column-major input (p[c * n + i]) checked and rescaled per
+// column, stored node-major.
+__global__ void pers_columns(const double* __restrict__ pin, uint32_t n, uint32_t B,
+                             double* __restrict__ pnm, int32_t* __restrict__ bad,
+                             double* __restrict__ sums) {
+  // one warp per column: fixed-order sum
+  const int lane = threadIdx.x & 31;
+  for (uint32_t c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); c < B;
+       c += gridDim.x * (blockDim.x / 32)) {
+    double a = 0;
+    int b = 0;
+    for (uint32_t i = lane; i < n; i += 32) {
+      double v = pin[(size_t)c * n + i];
+      if (!isfinite(v) || v < 0.0) b = 1;
+      else a += v;
+    }
+    a = warp_sum(a);
+    b = __any_sync(0xffffffffu, b);
+    if (lane == 0) {
+      sums[c] = a;
+      if (b || !(a > 0.0)) atomicOr(bad, b ? 1 : 2);
+    }
+  }
+}
+
+__global__ void pers_scatter(const double* __restrict__ pin, const double* __restrict__ sums,
+                             uint32_t n, uint32_t B, double* __restrict__ pnm) {
+  const uint64_t total = (uint64_t)n * B;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(q / B), c = (uint32_t)(q % B);
+    pnm[q] = pin[(size_t)c * n + i] / sums[c];
+  }
+}
+
+// Output: column-major out[c * n + i] = Y_c[i] / T_c from the buffer the
+// column stopped in.
+template <class VT>
+__global__ void spmm_output(const VT* __restrict__ Y0, const VT* __restrict__ Y1,
+                            const ColState* __restrict__ cs, uint32_t n, uint32_t B,
+                            double* __restrict__ out) {
+  const uint64_t total = (uint64_t)n * B;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(q % n), c = (uint32_t)(q / n);
+    const ColState s = cs[c];
+    const VT* Y = (s.iter & 1) ? Y1 : Y0;
+    out[q] = (double)Y[(size_t)i * B + c] / s.total;
+  }
+}
+
+// ----------------------------------------------------------------------- host
+struct BatchPlan {
+  std::vector<RowRange> ranges;
+  std::vector<Chunk> chunks;
+  std::vector<uint32_t> lrow, lfirst;
+};
+
+static BatchPlan make_plan(const std::vector<uint32_t>& off, uint32_t n) {
+  BatchPlan p;
+  uint32_t lo = 0;
+  uint64_t acc = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t deg = off[i + 1] - off[i];
+    if (deg > LONG_ROW) {
+      p.lrow.push_back(i);
+      p.lfirst.push_back((uint32_t)p.chunks.size());
+      for (uint32_t a = off[i]; a < off[i + 1]; a += LONG_ROW)
+        p.chunks.push_back({i, a, std::min(off[i + 1], a + LONG_ROW)});
+    } else {
+      acc += deg + 1;
+    }
+    if (acc >= RANGE_ARCS) {
+      p.ranges.push_back({lo, i + 1});
+      lo = i + 1;
+      acc = 0;
+    }
+  }
+  if (lo < n) p.ranges.push_back({lo, n});
+  p.lfirst.push_back((uint32_t)p.chunks.size());
+  return p;
+}
+
+template <class T>
+static void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
+  d.alloc(std::max<size_t>(h.size(), 1));
+  if (!h.empty()) KNB_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+template <class VT, class MT, int VW>
+static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uint32_t nranges,
+                       const DevBuf<Chunk>& chunks, uint32_t nchunks, const DevBuf<uint32_t>& lrow,
+                       const DevBuf<uint32_t>& lfirst, uint32_t nlong, const BatchScalars& bs,
+                       ColState* cs, const VT* Yold, VT* Ynew, const VT* Zold, VT* Znew,
+                       const VT* inv_out, const double* P, VT* scratch, double* part,
+                       int32_t* all_frozen, unsigned grid, cudaStream_t s) {
+  const size_t smem = (size_t)BW * 3 * bs.B * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    KNB_CUDA(cudaFuncSetAttribute(spmm_rows<VT, MT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(BW * 3 * 256 * sizeof(double))));
+    KNB_CUDA(cudaFuncSetAttribute(spmm_long<VT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(BW * 3 * 256 * sizeof(double))));
+    attr = true;
+  }
+  int launches = 0;
+  if (nchunks) {
+    spmm_chunks<VT, MT, VW><<<grid, BT, 0, s>>>(op, Zold, chunks.get(), nchunks, bs.B, scratch,
+                                                 all_frozen);
+    ++launches;
+  }
+  spmm_rows<VT, MT, VW><<<grid, BT, smem, s>>>(op, Zold, ranges.get(), nranges, bs, cs, Yold, Ynew,
+                                               Znew, inv_out, P, part, all_frozen);
+  spmm_long<VT, VW><<<grid, BT, smem, s>>>(lrow.get(), lfirst.get(), nlong, scratch, bs, cs, Yold,
+                                           Ynew, Znew, inv_out, P, part + (size_t)grid * 3 * bs.B,
+                                           all_frozen);
+  spmm_finish<<<1, 256, 0, s>>>(part, 2 * grid, bs, cs, all_frozen, 1);
+  KNB_LAUNCH("batch sweep");
+  return launches + 3;
+}
+
+template <class VT, class MT>
+static int batch_sweep_vw(int vw, const OpView<MT>& op, const DevBuf<RowRange>& ranges,
+                          uint32_t nranges, const DevBuf<Chunk>& chunks, uint32_t nchunks,
+                          const DevBuf<uint32_t>& lrow, const DevBuf<uint32_t>& lfirst,
+                          uint32_t nlong, const BatchScalars& bs, ColState* cs, const VT* Yold,
+                          VT* Ynew, const VT* Zold, VT* Znew, const VT* inv_out, const double* P,
+                          VT* scratch, double* part, int32_t* all_frozen, unsigned grid,
+                          cudaStream_t s) {
+#define KNB_SW(V)                                                                                 \
+  return batch_sweep<VT, MT, V>(op, ranges, nranges, chunks, nchunks, lrow, lfirst, nlong, bs, cs, \
+                                Yold, Ynew, Zold, Znew, inv_out, P, scratch, part, all_frozen,     \
+                                grid, s)
+  switch (vw) {
+    case 1: KNB_SW(1);
+    case 2: KNB_SW(2);
+    case 4: KNB_SW(4);
+    default: KNB_SW(8);
+  }
+#undef KNB_SW
+}
+
+static int vw_for(uint32_t B) {
+  if (B <= 32) return 1;
+  if (B <= 64) return 2;
+  if (B <= 128) return 4;
+  return 8;
+}
+
+void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pers_colmajor,
+                    double* out_colmajor, BatchInfo* info, cudaStream_t s) {
+  const uint32_t n = g.n;
+  if (n == 0 || prm.B == 0) return;
+  const int which = (g.directed && prm.directed) ? 1 : (g.directed ? 2 : 0);
+  const double lfac = prm.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (prm.loops == 0 ? 2.0 : 1.0));
+  Operator& op = g.op(which, prm.weighted, lfac, s);
+  std::vector<uint32_t> hoff(n + 1);
+  KNB_CUDA(cudaMemcpyAsync(hoff.data(), op.rows->off.get(), ((size_t)n + 1) * 4,
+                           cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  BatchPlan plan = make_plan(hoff, n);
+  DevBuf<RowRange> d_ranges;
+  DevBuf<Chunk> d_chunks;
+  DevBuf<uint32_t> d_lrow, d_lfirst;
+  upload(d_ranges, plan.ranges, s);
+  upload(d_chunks, plan.chunks, s);
+  upload(d_lrow, plan.lrow, s);
+  upload(d_lfirst, plan.lfirst, s);
+  const uint32_t nranges = (uint32_t)plan.ranges.size(), nchunks = (uint32_t)plan.chunks.size(),
+                 nlong = (uint32_t)plan.lrow.size();
+  const unsigned grid = 148 * 4;
+
+  cudaEvent_t t0, t1;
+  KNB_CUDA(cudaEventCreate(&t0));
+  KNB_CUDA(cudaEventCreate(&t1));
+  KNB_CUDA(cudaEventRecord(t0, s));
+  int launches = 0;
+  int64_t sweeps32 = 0, sweeps64 = 0;
+  const bool mixed = prm.precision == PREC_MIXED;
+  const uint32_t Btot = prm.B;
+  DevBuf<double> pin((size_t)n * Btot);
+  KNB_CUDA(cudaMemcpyAsync(pin.get(), pers_colmajor, (size_t)n * Btot * 8,
+                           prm.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  DevBuf<double> dout;
+  double* outp = out_colmajor;
+  if (!prm.on_device) {
+    dout.alloc((size_t)n * Btot);
+    outp = dout.get();
+  }
+  std::vector<int32_t> col_iters(Btot, 0);
+  std::vector<uint8_t> col_conv(Btot, 0);
+  // column groups of at most 256
+  for (uint32_t c0 = 0; c0 < Btot; c0 += 256) {
+    const uint32_t B = std::min<uint32_t>(256, Btot - c0);
+    const int vw = vw_for(B);
+    DevBuf<double> P((size_t)n * B), sums(B);
+    DevBuf<int32_t> flags(2);
+    KNB_CUDA(cudaMemsetAsync(flags.get(), 0, 8, s));
+    pers_columns<<<grid_for(B, BW, 1184), BT, 0, s>>>(pin.get() + (size_t)c0 * n, n, B, P.get(),
+                                                      flags.get(), sums.get());
+    int32_t hf[2];
+    KNB_CUDA(cudaMemcpyAsync(hf, flags.get(), 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    if (hf[0] & 1) throw Error("the personalization vector must hold finite, nonnegative values");
+    if (hf[0] & 2) throw Error("the personalization vector must have a positive sum");
+    pers_scatter<<<grid_for((uint64_t)n * B, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n,
+                                                                 sums.get(), n, B, P.get());
+    launches += 2;
+    BatchScalars bs{prm.damping, 1.0 / n, n, B, prm.dangling == 1 ? 1 : 0, 0.0, 0, 0};
+    DevBuf<ColState> cs(B);
+    DevBuf<int32_t> all_frozen(1);
+    DevBuf<double> part(std::max<size_t>((size_t)2 * grid * 3 * B, (size_t)1184 * 2 * B));
+    const double dterm0 = (double)op.n_dangling / (double)n;
+    int64_t done32 = 0;
+    const size_t nb = (size_t)n * B;
+    DevBuf<float> Y32[2], Z32[2], sc32;
+    DevBuf<double> Y64[2], Z64[2], sc64;
+    if (mixed) {
+      for (int k = 0; k < 2; ++k) {
+        Y32[k].alloc(nb);
+        Z32[k].alloc(nb);
+      }
+      sc32.alloc(std::max<size_t>((size_t)nchunks * B, 1));
+      spmm_init<float><<<grid_for(nb, 256), 256, 0, s>>>(Y32[0].get(), Z32[0].get(),
+                                                          op.inv_out32.get(), n, B, nullptr);
+      spmm_set_state<<<1, 256, 0, s>>>(cs.get(), B, dterm0, 0);
+      KNB_CUDA(cudaMemsetAsync(all_frozen.get(), 0, 4, s));
+      bs.tol = std::max(prm.tol * prm.switch_factor, prm.switch_floor);
+      bs.max_iter = (int32_t)prm.max_iter;
+      launches += 2;
+      int k = 0;
+      for (;;) {
+        const int b = k & 1;
+        launches += batch_sweep_vw<float, float>(
+            vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
+            cs.get(), Y32[b].get(), Y32[1 - b].get(), Z32[b].get(), Z32[1 - b].get(),
+            op.inv_out32.get(), P.get(), sc32.get(), part.get(), all_frozen.get(), grid, s);
+        ++k;
+        if (k % 4 == 0) {
+          int32_t af = 0;
+          KNB_CUDA(cudaMemcpyAsync(&af, all_frozen.get(), 4, cudaMemcpyDeviceToHost, s));
+          KNB_CUDA(cudaStreamSynchronize(s));
+          if (af) break;
+        }
+      }
+      // every column's FP32 phase ended; hand over from its own buffer
+      std::vector<ColState> h(B);
+      KNB_CUDA(cudaMemcpyAsync(h.data(), cs.get(), B * sizeof(ColState), cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      for (uint32_t c = 0; c < B; ++c) {
+        if (!h[c].converged)
+          throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +
+                      " within " + std::to_string(prm.max_iter) + " iterations");
+        done32 = std::max<int64_t>(done32, h[c].iter);
+      }
+      sweeps32 += k;
+      // columns stopped at different sweeps: each is read from its own buffer
+      for (int kk = 0; kk < 2; ++kk) {
+        Y64[kk].alloc(nb);
+        Z64[kk].alloc(nb);
+      }
+      spmm_switch<<<grid_for(nb, 256), 256, 0, s>>>(Y32[0].get(), Y32[1].get(), cs.get(),
+                                                    Y64[0].get(), Z64[0].get(),
+                                                    op.inv_out64.get(), n, B);
+      column_sums_part<<<1184, 256, 0, s>>>(Y64[0].get(), op.inv_out64.get(), n, B, part.get());
+      column_sums_finish<<<1, 256, 0, s>>>(part.get(), 1184, B, cs.get());
+      KNB_LAUNCH("batch hand-over");
+      launches += 3;
+      for (uint32_t c = 0; c < B; ++c) col_iters[c0 + c] = h[c].iter;
+    } else {
+      for (int kk = 0; kk < 2; ++kk) {
+        Y64[kk].alloc(nb);
+        Z64[kk].alloc(nb);
+      }
+      spmm_init<double><<<grid_for(nb, 256), 256, 0, s>>>(Y64[0].get(), Z64[0].get(),
+                                                           op.inv_out64.get(), n, B, nullptr);
+      spmm_set_state<<<1, 256, 0, s>>>(cs.get(), B, dterm0, 0);
+      launches += 2;
+    }
+    // FP64 phase
+    KNB_CUDA(cudaMemsetAsync(all_frozen.get(), 0, 4, s));
+    bs.tol = prm.tol;
+    bs.max_iter = (int32_t)(prm.max_iter - (mixed ? 0 : 0));
+    sc64.alloc(std::max<size_t>((size_t)nchunks * B, 1));
+    const bool use32v = op.has_vals && op.vals32_exact;
+    int k = 0;
+    for (;;) {
+      const int b = k & 1;
+      if (use32v)
+        launches += batch_sweep_vw<double, float>(
+            vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
+            cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
+            op.inv_out64.get(), P.get(), sc64.get(), part.get(), all_frozen.get(), grid, s);
+      else
+        launches += batch_sweep_vw<double, double>(
+            vw, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
+            cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
+            op.inv_out64.get(), P.get(), sc64.get(), part.get(), all_frozen.get(), grid, s);
+      ++k;
+      if (k % 4 == 0) {
+        int32_t af = 0;
+        KNB_CUDA(cudaMemcpyAsync(&af, all_frozen.get(), 4, cudaMemcpyDeviceToHost, s));
+        KNB_CUDA(cudaStreamSynchronize(s));
+        if (af) break;
+      }
+    }
+    sweeps64 += k;
+    std::vector<ColState> h(B);
+    KNB_CUDA(cudaMemcpyAsync(h.data(), cs.get(), B * sizeof(ColState), cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t c = 0; c < B; ++c) {
+      if (!h[c].converged)
+        throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +
+                    " within " + std::to_string(prm.max_iter) + " iterations");
+      col_iters[c0 + c] += h[c].iter;
+      col_conv[c0 + c] = 1;
+    }
+    spmm_output<double><<<grid_for(nb, 256), 256, 0, s>>>(Y64[0].get(), Y64[1].get(), cs.get(), n,
+                                                          B, outp + (size_t)c0 * n);
+    ++launches;
+  }
+  if (!prm.on_device)
+    KNB_CUDA(cudaMemcpyAsync(out_colmajor, outp, (size_t)n * Btot * 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaEventRecord(t1, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  KNB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (info) {
+    info->seconds = ms * 1e-3;
+    info->sweeps = sweeps32 + sweeps64;
+    info->sweeps_fp32 = sweeps32;
+    int64_t tot = 0, mx = 0;
+    for (uint32_t c = 0; c < Btot; ++c) {
+      tot += col_iters[c];
+      mx = std::max<int64_t>(mx, col_iters[c]);
+    }
+    info->column_iterations = tot;
+    info->max_column_iterations = mx;
+    info->kernel_launches = launches;
+  }
+}
+
+}  // namespace knb

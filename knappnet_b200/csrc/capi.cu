@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/knappnet.h"
+#include "batch.cuh"
 #include "eigen.cuh"
 #include "generate.cuh"
 #include "graph.cuh"
@@ -421,6 +422,73 @@ int32_t net_generate_rmat(int32_t scale, int64_t edge_factor, double a, double b
   });
 }
 
+static int32_t batch_impl(const GraphHandle* h, double damping, int32_t directed, int32_t weighted,
+                          const double* personalization, int64_t batch, int32_t dangling,
+                          int32_t loops, double tol, int64_t max_iter, int32_t precision,
+                          int on_device, double* out, NetBatchInfo* info, char* err,
+                          size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (dangling != 0 && dangling != 1)
+      throw Error("unknown dangling-node code " + std::to_string(dangling));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (precision != 0 && precision != 1)
+      throw Error("unknown precision code " + std::to_string(precision));
+    if (batch < 0 || batch > 0xFFFFFFFFll) throw Error("batch size out of range");
+    if (!personalization && batch > 0)
+      throw Error("a batch needs one personalization vector per column");
+    knb::BatchParams p;
+    p.damping = damping;
+    p.directed = directed != 0;
+    p.weighted = weighted != 0;
+    p.dangling = dangling;
+    p.loops = loops;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    p.precision = precision;
+    p.B = (uint32_t)batch;
+    p.on_device = on_device != 0;
+    const knb::Tuning& tu = knb::tuning();
+    p.switch_factor = tu.switch_factor;
+    p.switch_floor = tu.switch_floor;
+    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    if (!(damping >= 0.0 && damping <= 1.0))
+      throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
+    if (g.n == 0 || batch == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    if (p.weighted) check_nonnegative(g, "PageRank", s);
+    knb::BatchInfo bi;
+    knb::pagerank_batch(g, p, personalization, out, &bi, s);
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->seconds = bi.seconds;
+      info->sweeps = bi.sweeps;
+      info->sweeps_fp32 = bi.sweeps_fp32;
+      info->column_iterations = bi.column_iterations;
+      info->max_column_iterations = bi.max_column_iterations;
+      info->kernel_launches = bi.kernel_launches;
+    }
+  });
+}
+
+int32_t net_pagerank_batch(const GraphHandle* h, double damping, int32_t directed,
+                           int32_t weighted, const double* personalization, int64_t batch,
+                           int32_t dangling, int32_t loops, double tol, int64_t max_iter,
+                           int32_t precision, double* out, NetBatchInfo* info, char* err,
+                           size_t err_len) {
+  return batch_impl(h, damping, directed, weighted, personalization, batch, dangling, loops, tol,
+                    max_iter, precision, 0, out, info, err, err_len);
+}
+
+int32_t net_pagerank_batch_device(const GraphHandle* h, double damping, int32_t directed,
+                                  int32_t weighted, const double* d_personalization,
+                                  int64_t batch, int32_t dangling, int32_t loops, double tol,
+                                  int64_t max_iter, int32_t precision, double* d_out,
+                                  NetBatchInfo* info, char* err, size_t err_len) {
+  return batch_impl(h, damping, directed, weighted, d_personalization, batch, dangling, loops, tol,
+                    max_iter, precision, 1, d_out, info, err, err_len);
+}
+
 int64_t net_graph_arc_count(const GraphHandle* h, int32_t which) {
   if (!h) return -1;
   const knb::GraphHandleImpl& g = h->g;
@@ -546,8 +614,12 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (value != 0 && value != 1 && value != 2) return 1;
+      if (!(value >= 0 && value <= 5) || value != (int)value) return 1;
       t.variant = (int)value;
+      return 0;
+    case 5:
+      if (!(value >= -1 && value <= 100)) return 1;
+      t.carveout = (int)value;
       return 0;
     default:
       return 1;

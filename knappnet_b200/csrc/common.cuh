@@ -72,6 +72,18 @@ __device__ __forceinline__ double ld_keep(const double* p, uint64_t pol) {
   return v;
 }
 
+// Gathers that skip L1 allocation (the L2 policy still applies).
+__device__ __forceinline__ float ld_keep_na(const float* p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_keep_na(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // ---------------------------------------------------------------- reductions
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {

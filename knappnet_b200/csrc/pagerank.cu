@@ -353,8 +353,7 @@ struct SweepBuffers {
   IterState* st;
 };
 
-enum SweepVariant : int { VAR_CTA = 1, VAR_WARP = 2 };
-constexpr int WPB = 8;  // warps per CTA of the warp-tile sweep
+enum SweepVariant : int { VAR_CTA = 1, VAR_WARP = 2, VAR_WARP4 = 3, VAR_WARP16 = 4, VAR_WARPNA = 5 };
 
 template <class VT, class MT, bool PV, bool JU, bool EXACT, int VAR, int IPT>
 static void launch_sweep(const Operator& op, const Partition& P, const SweepBuffers& B, int buf,
@@ -382,15 +381,23 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
     tile_spmv<VT, MT, Epi, IPT><<<P.ntiles, SPMV_THREADS, smem, s>>>(
         v, (const VT*)B.z[buf], e, P.coords.get(), (VT*)B.carry, (VT*)B.head, B.part1, B.st);
   } else {
+    constexpr int WPB = VAR == VAR_WARP4 ? 4 : VAR == VAR_WARP16 ? 16 : 8;
+    constexpr int GNA = VAR == VAR_WARPNA ? 1 : 0;
     constexpr size_t smem = warp_smem_bytes<VT, IPT, WPB>();
     static bool attr_set = false;
+    static int carve = -2;
+    auto fnp = warp_spmv<VT, MT, Epi, IPT, WPB, GNA>;
     if (!attr_set) {
-      KNB_CUDA(cudaFuncSetAttribute(warp_spmv<VT, MT, Epi, IPT, WPB>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      KNB_CUDA(cudaFuncSetAttribute(fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       attr_set = true;
     }
+    if (tuning().carveout != carve) {
+      carve = tuning().carveout;
+      KNB_CUDA(cudaFuncSetAttribute(fnp, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    carve >= 0 ? carve : -1));
+    }
     const unsigned grid = (P.ntiles + WPB - 1) / WPB;
-    warp_spmv<VT, MT, Epi, IPT, WPB><<<grid, WPB * 32, smem, s>>>(
+    warp_spmv<VT, MT, Epi, IPT, WPB, GNA><<<grid, WPB * 32, smem, s>>>(
         v, (const VT*)B.z[buf], e, P.coords.get(), P.ntiles, (VT*)B.carry, (VT*)B.head,
         B.part1, B.st);
   }
@@ -417,18 +424,25 @@ static SweepFn pick_pv(bool pv, bool ju) {
   return launch_sweep<VT, MT, true, false, EXACT, VAR, IPT>;
 }
 
+template <class VT, class MT, bool EXACT, int VAR>
+static SweepFn pick_warp_ipt(int ipt, bool pv, bool ju) {
+  switch (ipt) {
+    case 4: return pick_pv<VT, MT, EXACT, VAR, 4>(pv, ju);
+    case 16: return pick_pv<VT, MT, EXACT, VAR, 16>(pv, ju);
+    default: return pick_pv<VT, MT, EXACT, VAR, 8>(pv, ju);
+  }
+}
+
 template <class VT, class MT, bool EXACT>
 static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
-  if (var == VAR_CTA) {
-    switch (ipt) {
-      case 4: return pick_pv<VT, MT, EXACT, VAR_CTA, 4>(pv, ju);
-      default: return pick_pv<VT, MT, EXACT, VAR_CTA, 8>(pv, ju);
-    }
-  }
-  switch (ipt) {
-    case 4: return pick_pv<VT, MT, EXACT, VAR_WARP, 4>(pv, ju);
-    case 16: return pick_pv<VT, MT, EXACT, VAR_WARP, 16>(pv, ju);
-    default: return pick_pv<VT, MT, EXACT, VAR_WARP, 8>(pv, ju);
+  switch (var) {
+    case VAR_CTA:
+      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_CTA, 4>(pv, ju)
+                      : pick_pv<VT, MT, EXACT, VAR_CTA, 8>(pv, ju);
+    case VAR_WARP4: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP4>(ipt, pv, ju);
+    case VAR_WARP16: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP16>(ipt, pv, ju);
+    case VAR_WARPNA: return pick_warp_ipt<VT, MT, EXACT, VAR_WARPNA>(ipt, pv, ju);
+    default: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP>(ipt, pv, ju);
   }
 }
 
@@ -544,12 +558,25 @@ void pagerank(GraphHandleImpl& g, const PagerankParams& prm_in, double* out, boo
   // rows of a directed graph count a loop once unless ignored.
   double lfac = prm.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (prm.loops == 0 ? 2.0 : 1.0));
   Operator& op = g.op(which, prm.weighted, lfac, s);
-  const int var = prm.variant ? prm.variant : VAR_WARP;
-  const int ipt = prm.ipt ? prm.ipt : default_ipt(op, var);
+  // Kernel choice per phase (measured on R-MAT scale 24: one tile per warp,
+  // four warps per CTA; 8 items per lane for FP32 sweeps, 4 for FP64 sweeps).
+  const int var32 = prm.variant ? prm.variant : VAR_WARP4;
+  const int var64 = prm.variant ? prm.variant : VAR_WARP4;
+  const int ipt32 = prm.ipt ? prm.ipt : 8;
+  const int ipt64 = prm.ipt ? prm.ipt : 4;
   const bool rl = prm.relabel;
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
-  const uint32_t tile = tile_items(var, ipt);
-  const Partition& P = rl ? op.relabeled_partition(tile, s) : op.partition(tile, s);
+  const bool mixed_pre = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
+  const Partition* P32 = nullptr;
+  const Partition* P64 = nullptr;
+  if (mixed_pre) {
+    const uint32_t tile = tile_items(var32, ipt32);
+    P32 = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
+  }
+  if (prm.precision != PREC_FP32) {
+    const uint32_t tile = tile_items(var64, ipt64);
+    P64 = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
+  }
   const OpView<double> v64 = rl ? op.rview64() : op.view64();
   const OpView<float> v32 = rl ? op.rview32() : op.view32();
   const double* inv64 = rl ? R->inv_out64.get() : op.inv_out64.get();
@@ -559,8 +586,8 @@ void pagerank(GraphHandleImpl& g, const PagerankParams& prm_in, double* out, boo
 
   const bool pv = prm.personalization != nullptr;
   const bool ju = !pv || prm.dangling == 1;
-  const bool mixed = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
-  const uint32_t nt = P.ntiles;
+  const bool mixed = mixed_pre;
+  const uint32_t nt = std::max(P32 ? P32->ntiles : 0u, P64 ? P64->ntiles : 0u);
   const unsigned gv = grid_for(n, VT_THREADS, 1184);
 
   PrWorkspace* wsp = nullptr;
@@ -611,8 +638,8 @@ void pagerank(GraphHandleImpl& g, const PagerankParams& prm_in, double* out, boo
     SweepBuffers B{v64, v32, {ws.y32[0].get(), ws.y32[1].get()},
                    {ws.z32[0].get(), ws.z32[1].get()}, inv32, pdev, ws.carry32.get(),
                    ws.head32.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st};
-    SweepFn fn = pick_kernel<float, float, false>(var, ipt, pv, ju);
-    r32 = run_phase(fn, op, P, B, prm.damping, false, s, ws, hstate, &tms32, &tn32);
+    SweepFn fn = pick_kernel<float, float, false>(var32, ipt32, pv, ju);
+    r32 = run_phase(fn, op, *P32, B, prm.damping, false, s, ws, hstate, &tms32, &tn32);
     launches += r32.launches;
     if (r32.stopped && !r32.converged)
       throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +
@@ -639,9 +666,9 @@ void pagerank(GraphHandleImpl& g, const PagerankParams& prm_in, double* out, boo
                    {ws.z64[0].get(), ws.z64[1].get()}, inv64, pdev, ws.carry64.get(),
                    ws.head64.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1};
     bool use32 = op.has_vals && op.vals32_exact && !prm.fp64_values;
-    SweepFn fn = use32 ? pick_kernel<double, float, true>(var, ipt, pv, ju)
-                       : pick_kernel<double, double, true>(var, ipt, pv, ju);
-    r64 = run_phase(fn, op, P, B, prm.damping, true, s, ws, hstate, &tms64, &tn64);
+    SweepFn fn = use32 ? pick_kernel<double, float, true>(var64, ipt64, pv, ju)
+                       : pick_kernel<double, double, true>(var64, ipt64, pv, ju);
+    r64 = run_phase(fn, op, *P64, B, prm.damping, true, s, ws, hstate, &tms64, &tn64);
     launches += r64.launches;
     if (!r64.converged)
       throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +

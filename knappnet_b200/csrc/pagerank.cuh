@@ -44,7 +44,8 @@ struct PagerankInfo {
 struct Tuning {
   int ipt = 0;            // merge-path items per thread: 4, 8 or 16
   int relabel = 1;        // 1: sweep on the operator renumbered by column count
-  int variant = 0;        // sweep kernel: 1 CTA tiles, 2 warp tiles
+  int variant = 0;        // sweep kernel: 1 CTA tiles, 2-5 warp tiles (see pagerank.cu)
+  int carveout = -1;      // preferred shared-memory carveout percent (-1: driver default)
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

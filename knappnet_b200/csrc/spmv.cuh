@@ -234,7 +234,7 @@ struct WarpSmem {
   uint32_t rend[32 * IPT + 1];
 };
 
-template <class VT, class MT, class Epi, int IPT, int WPB>
+template <class VT, class MT, class Epi, int IPT, int WPB, int GNA = 0>
 __global__ void __launch_bounds__(WPB * 32)
 warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
           const TileCoord* __restrict__ coords, uint32_t ntiles, VT* __restrict__ carry,
@@ -270,7 +270,8 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
 #pragma unroll
     for (int q = 0; q < IPT; ++q) {
       const uint32_t k = lane + q * 32;
-      xv[q] = k < n_arcs ? ld_keep(xg + c[q], pol_keep) : VT(0);
+      xv[q] = k < n_arcs ? (GNA ? ld_keep_na(xg + c[q], pol_keep) : ld_keep(xg + c[q], pol_keep))
+                         : VT(0);
     }
 #pragma unroll
     for (int q = 0; q < IPT; ++q) {
@@ -294,18 +295,21 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
   const uint32_t stop = min(diag + (uint32_t)IPT, total);
   VT acc = VT(0);
   VT fval[IPT];
-  uint32_t fmask = 0;  // bit it: item it ended row (first finished row + popc below)
+  uint32_t fmask = 0;  // bit it: item it ended a row
   uint32_t first_row = 0xFFFFFFFFu;
+  // end of the current row (kept in a register; 2^32-1 past the last row)
+  uint32_t cur_end = ri < n_rows ? sm.rend[ri] : 0xFFFFFFFFu;
 #pragma unroll
   for (int it = 0; it < IPT; ++it) {
     fval[it] = VT(0);
     if (ri + aj < stop) {
-      if (ri < n_rows && aj >= sm.rend[ri]) {
+      if (aj >= cur_end) {
         fval[it] = acc;
         fmask |= 1u << it;
         if (first_row == 0xFFFFFFFFu) first_row = ri;
         acc = VT(0);
         ++ri;
+        cur_end = ri < n_rows ? sm.rend[ri] : 0xFFFFFFFFu;
       } else {
         acc += sm.prod[aj];
         ++aj;

@@ -388,3 +388,47 @@ def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel):
         K.set_tuning(K.TUNE_VARIANT, 0)
         K.set_tuning(K.TUNE_IPT, 0)
         K.set_tuning(K.TUNE_RELABEL, 1)
+
+
+# ------------------------------------------------------------------ batched personalised
+def seed_vectors(n, B, seed):
+    """B teleport vectors, each uniform over 1..64 seed nodes."""
+    rng = np.random.default_rng(seed)
+    P = np.zeros((B, n))
+    for b in range(B):
+        k = int(rng.integers(1, 65))
+        P[b, rng.choice(n, size=min(k, n), replace=False)] = 1.0
+    return P
+
+
+@pytest.mark.parametrize("precision,B", [(0, 40), (1, 40), (0, 300)])
+def test_pagerank_batch_matches_per_vector_oracle(precision, B):
+    kg, og = rmat_pair(11 if B > 100 else 12, True, seed=31)
+    P = seed_vectors(kg.n, B, 7)
+    out, info = kg.pagerank_batch(P, weighted=True, precision=precision, tol=1e-10)
+    assert out.shape == P.shape
+    worst = 0.0
+    for b in range(B):
+        ref = og.pagerank(weighted=True, personalization=P[b], tol=1e-10)
+        err = np.abs(out[b] - ref).sum()
+        worst = max(worst, err)
+        assert err <= (1e-12 if precision == 0 else 1e-9), (b, err)
+    assert info.max_column_iterations >= 1
+
+
+def test_pagerank_batch_options_and_errors():
+    kg, og = rmat_pair(10, True, seed=5)
+    P = seed_vectors(kg.n, 5, 3)
+    for opts in (dict(dangling=1), dict(directed=False), dict(loops=1, damping=0.7)):
+        out, _ = kg.pagerank_batch(P, weighted=True, **opts)
+        for b in range(5):
+            ref = og.pagerank(weighted=True, personalization=P[b], **opts)
+            assert np.abs(out[b] - ref).sum() <= 1e-12, opts
+    bad = P.copy()
+    bad[2, 0] = -1.0
+    with pytest.raises(K.EngineError, match="nonnegative"):
+        kg.pagerank_batch(bad)
+    zero = P.copy()
+    zero[1] = 0.0
+    with pytest.raises(K.EngineError, match="positive sum"):
+        kg.pagerank_batch(zero)
