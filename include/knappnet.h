@@ -153,6 +153,22 @@ NET_API int32_t net_pagerank_batch_device(const GraphHandle *h, double damping,
                                   double *d_out, NetBatchInfo *info, char *err,
                                   size_t err_len);
 
+/* PageRank on every graph of a packed batch: the handle holds `count`
+ * graphs side by side (graph k on nodes node_offsets[k] ..
+ * node_offsets[k + 1] - 1, no edge between graphs, e.g. ego networks built
+ * into one handle), and out receives, for every graph, what net_pagerank on
+ * that graph alone returns. One persistent CUDA launch solves all graphs.
+ * personalization is NULL (uniform per graph) or n values (rescaled per
+ * graph); iterations (NULL or count values) receives each graph's
+ * iteration count. */
+NET_API int32_t net_pagerank_graphs(const GraphHandle *h, int64_t count,
+                            const int64_t *node_offsets, double damping,
+                            int32_t directed, int32_t weighted,
+                            const double *personalization, int32_t dangling,
+                            int32_t loops, double tol, int64_t max_iter,
+                            double *out, int64_t *iterations,
+                            NetSolveInfo *info, char *err, size_t err_len);
+
 /* Builds a graph from device arrays: 32-bit endpoints and FP32 (d_w32) or
  * FP64 (d_w64) weights, either may be NULL. */
 NET_API int32_t net_graph_new_device(int64_t n, const uint32_t *d_src,
@@ -189,6 +205,21 @@ NET_API int32_t net_generate_rmat(int32_t scale, int64_t edge_factor, double a,
                           GraphHandle **out, int64_t *m_out, char *err,
                           size_t err_len);
 
+/* `count` G(n, m) graphs (the reference's generator, crates/engine/src/
+ * generate.rs:255-290): graph k has n[k] nodes and m[k] distinct edges drawn
+ * by Floyd's sampling from Philox stream (seed, k), sorted; its nodes are
+ * numbered after those of graphs 0..k-1, so the edges of all graphs form
+ * one packed batch for net_pagerank_graphs. src and tgt hold sum(m) values. */
+NET_API int32_t net_generate_gnm(int64_t count, const int64_t *n, const int64_t *m,
+                         int32_t directed, int32_t loops, uint64_t seed,
+                         int64_t *src, int64_t *tgt, char *err, size_t err_len);
+
+/* count sizes from the power law p(x) ~ x^-alpha on [lo, hi] (inverse
+ * transform of the continuous law, floored), size k from stream (seed, k). */
+NET_API int32_t net_power_law_sizes(int64_t count, double alpha, double lo,
+                            double hi, uint64_t seed, int64_t *out, char *err,
+                            size_t err_len);
+
 /* Timing of the merge-path sweep kernel in the last PageRank solve of the
  * calling thread, when enabled with net_set_sweep_timing(1), for the FP32
  * (phase 0) or FP64 (phase 1) sweeps: launches, their total device
@@ -203,7 +234,10 @@ NET_API void net_set_sweep_timing(int32_t on);
  * (1, default) or not (0); 2 = mixed precision: leave FP32 once the change is
  * below tol times this factor (default 8192); 3 = ... or below this floor
  * (default 2e-6); 4 = sweep kernel (0 automatic, 1 one merge-path tile per
- * CTA, 2 one tile per warp). Returns 1 for an unknown key or value. */
+ * CTA, 2 one tile per warp); 5 = preferred shared-memory carveout of the
+ * sweep (-1 driver default, 0..100 percent); 6 = threads per CTA of the
+ * packed-graph PageRank (0 tuned on first use, 128, 256, 512, 1024).
+ * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 
 /* Waits for the device; reports an asynchronous CUDA error if one occurred. */

@@ -96,6 +96,13 @@ def lib() -> ctypes.CDLL:
     L.net_pagerank_batch_device.argtypes = [h, f64, i32, i32, vp, i64, i32, i32, f64, i64, i32,
                                             vp, binfo_p, cp, sz]
     L.net_pagerank_batch_device.restype = i32
+    L.net_pagerank_graphs.argtypes = [h, i64, vp, f64, i32, i32, vp, i32, i32, f64, i64, vp, vp,
+                                      info_p, cp, sz]
+    L.net_pagerank_graphs.restype = i32
+    L.net_generate_gnm.argtypes = [i64, vp, vp, i32, i32, u64, vp, vp, cp, sz]
+    L.net_generate_gnm.restype = i32
+    L.net_power_law_sizes.argtypes = [i64, f64, f64, f64, u64, vp, cp, sz]
+    L.net_power_law_sizes.restype = i32
     L.net_graph_new_device.argtypes = [i64, vp, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
     L.net_graph_new_device.restype = i32
     L.net_graph_arc_count.argtypes = [h, i32]
@@ -251,6 +258,25 @@ class Graph:
                                         _ptr(out), ctypes.byref(info), err, ERR_LEN), err)
         return out, info
 
+    def pagerank_graphs(self, node_offsets, damping=0.85, directed=True, weighted=False,
+                        personalization=None, dangling=0, loops=0, tol=0.0, max_iter=0):
+        """PageRank of every graph packed in this handle (graph k on nodes
+        node_offsets[k]..node_offsets[k+1]-1): scores, per-graph iteration
+        counts, NetSolveInfo."""
+        off = np.ascontiguousarray(node_offsets, dtype=np.int64)
+        count = len(off) - 1
+        p = None if personalization is None else np.ascontiguousarray(personalization,
+                                                                       dtype=np.float64)
+        out = np.zeros(max(self.n, 1))
+        its = np.zeros(max(count, 1), dtype=np.int64)
+        info = NetSolveInfo()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_pagerank_graphs(self.h, count, _ptr(off), damping, int(directed),
+                                         int(weighted), _ptr(p), dangling, loops, tol, max_iter,
+                                         _ptr(out), _ptr(its), ctypes.byref(info), err, ERR_LEN),
+               err)
+        return out[: self.n], its[:count], info
+
     def pagerank_reference_call(self, damping=0.85, directed=True, weighted=False,
                                 personalization=None, dangling=0, loops=0, tol=0.0, max_iter=0,
                                 threads=0):
@@ -297,6 +323,27 @@ def generate_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, clean=T
     return Graph(1 << scale, directed=not symmetrize, _handle=h, _m=m.value, _weighted=lognormal)
 
 
+def generate_gnm(n, m, directed=False, loops=False, seed=1):
+    """G(n[k], m[k]) graphs packed one after another (net_generate_gnm):
+    returns (src, tgt) with global node numbers."""
+    n = np.ascontiguousarray(np.atleast_1d(n), dtype=np.int64)
+    m = np.ascontiguousarray(np.atleast_1d(m), dtype=np.int64)
+    tot = int(m.sum())
+    src = np.zeros(max(tot, 1), dtype=np.int64)
+    tgt = np.zeros(max(tot, 1), dtype=np.int64)
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_generate_gnm(len(n), _ptr(n), _ptr(m), int(directed), int(loops), seed,
+                                  _ptr(src), _ptr(tgt), err, ERR_LEN), err)
+    return src[:tot], tgt[:tot]
+
+
+def power_law_sizes(count, alpha=2.1, lo=50, hi=50_000, seed=1):
+    out = np.zeros(max(count, 1), dtype=np.int64)
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_power_law_sizes(count, alpha, lo, hi, seed, _ptr(out), err, ERR_LEN), err)
+    return out[:count]
+
+
 def sweep_timing(phase: int = 1):
     """(launches, total ms, algorithmic bytes per launch) of the merge-path
     sweep kernel in the last PageRank solve of this thread: FP32 sweeps
@@ -312,8 +359,8 @@ def set_sweep_timing(on: bool) -> None:
     lib().net_set_sweep_timing(int(on))
 
 
-TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT = \
-    0, 1, 2, 3, 4, 5
+TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT, \
+    TUNE_EGO_THREADS = 0, 1, 2, 3, 4, 5, 6
 
 
 def set_tuning(key: int, value: float) -> None:

@@ -13,6 +13,7 @@
 
 #include "../../include/knappnet.h"
 #include "batch.cuh"
+#include "ego.cuh"
 #include "eigen.cuh"
 #include "generate.cuh"
 #include "graph.cuh"
@@ -489,6 +490,69 @@ int32_t net_pagerank_batch_device(const GraphHandle* h, double damping, int32_t 
                     max_iter, precision, 1, d_out, info, err, err_len);
 }
 
+int32_t net_pagerank_graphs(const GraphHandle* h, int64_t count, const int64_t* node_offsets,
+                            double damping, int32_t directed, int32_t weighted,
+                            const double* personalization, int32_t dangling, int32_t loops,
+                            double tol, int64_t max_iter, double* out, int64_t* iterations,
+                            NetSolveInfo* info, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (dangling != 0 && dangling != 1)
+      throw Error("unknown dangling-node code " + std::to_string(dangling));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (count < 1 || count > 0xFFFFFFFll) throw Error("graph count out of range");
+    if (!node_offsets) throw Error("graph offsets are null");
+    knb::EgoInput in;
+    in.count = (uint32_t)count;
+    in.node_offsets = node_offsets;
+    in.damping = damping;
+    in.directed = directed != 0;
+    in.weighted = weighted != 0;
+    in.dangling = dangling;
+    in.loops = loops;
+    in.tol = tol > 0 ? tol : 1e-12;
+    in.max_iter = max_iter > 0 ? max_iter : 10000;
+    in.personalization = personalization;
+    in.iterations_out = iterations;
+    if (std::isnan(in.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    if (!(damping >= 0.0 && damping <= 1.0))
+      throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
+    if (g.n == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    if (in.weighted) check_nonnegative(g, "PageRank", s);
+    knb::EgoResult r;
+    knb::pagerank_graphs(g, in, out, &r, s);
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->iterations = r.total_iterations;
+      info->seconds = r.seconds;
+      info->converged = 1;
+      info->kernel_launches = 1;
+      info->reserved = r.threads;
+    }
+  });
+}
+
+int32_t net_generate_gnm(int64_t count, const int64_t* n, const int64_t* m, int32_t directed,
+                         int32_t loops, uint64_t seed, int64_t* src, int64_t* tgt, char* err,
+                         size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (count < 0) throw Error("negative graph count");
+    for (int64_t k = 0; k < count; ++k)
+      if (n[k] < 0 || m[k] < 0) throw Error("negative node or edge count");
+    knb::gnm_batch((uint64_t)count, n, m, directed != 0, loops != 0, seed, src, tgt, 0);
+  });
+}
+
+int32_t net_power_law_sizes(int64_t count, double alpha, double lo, double hi, uint64_t seed,
+                            int64_t* out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (count < 0 || !(alpha > 1.0) || !(lo >= 1.0) || !(hi >= lo))
+      throw Error("power law needs alpha > 1 and 1 <= lo <= hi");
+    knb::power_law_sizes((uint64_t)count, alpha, lo, hi, seed, out);
+  });
+}
+
 int64_t net_graph_arc_count(const GraphHandle* h, int32_t which) {
   if (!h) return -1;
   const knb::GraphHandleImpl& g = h->g;
@@ -620,6 +684,10 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 5:
       if (!(value >= -1 && value <= 100)) return 1;
       t.carveout = (int)value;
+      return 0;
+    case 6:
+      if (value != 0 && value != 128 && value != 256 && value != 512 && value != 1024) return 1;
+      knb::set_ego_threads((int)value);
       return 0;
     default:
       return 1;

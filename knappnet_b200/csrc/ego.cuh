@@ -1,0 +1,34 @@
+// PageRank on every graph of a packed batch (block-diagonal handle).
+#pragma once
+
+#include "graph.cuh"
+
+namespace knb {
+
+struct EgoInput {
+  uint32_t count = 0;
+  const int64_t* node_offsets = nullptr;  // count + 1, host
+  double damping = 0.85;
+  bool directed = true;
+  bool weighted = false;
+  int dangling = 0;
+  int loops = 0;
+  double tol = 1e-12;
+  int64_t max_iter = 10000;
+  const double* personalization = nullptr;  // host, n values or null
+  bool out_on_device = false;
+  int64_t* iterations_out = nullptr;        // host, count values or null
+};
+
+struct EgoResult {
+  double seconds = 0;
+  int threads = 0;
+  int64_t total_iterations = 0;
+  int64_t max_iterations = 0;
+};
+
+void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoResult* res,
+                     cudaStream_t s);
+void set_ego_threads(int threads);
+
+}  // namespace knb

@@ -180,3 +180,177 @@ RmatEdges generate_rmat(int scale, uint64_t edge_factor, double a, double b, dou
 }
 
 }  // namespace knb
+
+// ======================================================================= G(n, m)
+// Host generator of G(n, m) graphs with the reference's algorithm
+// (crates/engine/src/generate.rs:255-290): Floyd's sampling of m distinct
+// candidate pairs from stream (seed, rep), decoded and sorted.
+#include <algorithm>
+#include <cmath>
+#include <thread>
+#include <unordered_set>
+
+namespace knb {
+namespace {
+
+struct HostStream {
+  uint32_t k0, k1;
+  uint64_t stream, block = 0;
+  uint32_t buf[4];
+  int used = 4;
+  HostStream(uint64_t seed, uint64_t index)
+      : k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), stream(index) {}
+  uint32_t next_u32() {
+    if (used == 4) {
+      uint32_t c0 = (uint32_t)block, c1 = (uint32_t)(block >> 32), c2 = (uint32_t)stream,
+               c3 = (uint32_t)(stream >> 32), a = k0, b = k1;
+      for (int r = 0; r < 10; ++r) {
+        if (r) {
+          a += 0x9E3779B9u;
+          b += 0xBB67AE85u;
+        }
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ a, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ b;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+      }
+      buf[0] = c0;
+      buf[1] = c1;
+      buf[2] = c2;
+      buf[3] = c3;
+      ++block;
+      used = 0;
+    }
+    return buf[used++];
+  }
+  uint64_t next_u64() {
+    uint64_t hi = next_u32();
+    return hi << 32 | next_u32();
+  }
+  uint64_t below(uint64_t n) {
+    const uint64_t mx = ~0ull;
+    const uint64_t zone = mx - (mx % n + 1) % n;
+    for (;;) {
+      uint64_t x = next_u64();
+      if (x <= zone) return x % n;
+    }
+  }
+  double uniform() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+uint64_t pair_count(uint64_t n, bool directed, bool loops) {
+  if (directed) return loops ? n * n : n * (n ? n - 1 : 0);
+  return loops ? n * (n + 1) / 2 : n * (n ? n - 1 : 0) / 2;
+}
+
+uint64_t isqrt(uint64_t x) {
+  uint64_t r = (uint64_t)std::sqrt((double)x);
+  while (r > 0 && r * r > x) --r;
+  while ((r + 1) * (r + 1) <= x) ++r;
+  return r;
+}
+
+void decode(uint64_t k, uint64_t n, bool directed, bool loops, uint64_t* a, uint64_t* b) {
+  if (directed && loops) {
+    *a = k / n;
+    *b = k % n;
+  } else if (directed) {
+    uint64_t row = k / (n - 1), col = k % (n - 1);
+    *a = row;
+    *b = col >= row ? col + 1 : col;
+  } else if (!loops) {
+    uint64_t c = (1 + isqrt(1 + 8 * k)) / 2;
+    while (c * (c - 1) / 2 > k) --c;
+    while ((c + 1) * c / 2 <= k) ++c;
+    *a = k - c * (c - 1) / 2;
+    *b = c;
+  } else {
+    uint64_t c = (isqrt(1 + 8 * k) - 1) / 2;
+    while (c * (c + 1) / 2 > k) --c;
+    while ((c + 1) * (c + 2) / 2 <= k) ++c;
+    *a = k - c * (c + 1) / 2;
+    *b = c;
+  }
+}
+
+}  // namespace
+
+void gnm_edges(uint64_t n, uint64_t m, bool directed, bool loops, uint64_t seed, uint64_t rep,
+               int64_t offset, int64_t* src, int64_t* tgt) {
+  HostStream rng(seed, rep);
+  const uint64_t total = pair_count(n, directed, loops);
+  if (m > total) throw Error("a graph on " + std::to_string(n) + " nodes cannot hold " +
+                             std::to_string(m) + " edges");
+  std::vector<uint64_t> chosen;
+  chosen.reserve(m);
+  if (m * 2 <= total) {
+    std::unordered_set<uint64_t> set;
+    set.reserve(m * 2);
+    for (uint64_t j = total - m; j < total; ++j) {
+      uint64_t t = rng.below(j + 1);
+      if (!set.insert(t).second) set.insert(j);
+    }
+    chosen.assign(set.begin(), set.end());
+  } else {
+    std::unordered_set<uint64_t> skip;
+    for (uint64_t j = m; j < total; ++j) {
+      uint64_t t = rng.below(j + 1);
+      if (!skip.insert(t).second) skip.insert(j);
+    }
+    for (uint64_t k = 0; k < total; ++k)
+      if (!skip.count(k)) chosen.push_back(k);
+  }
+  std::vector<std::pair<uint64_t, uint64_t>> pairs(chosen.size());
+  for (size_t i = 0; i < chosen.size(); ++i) decode(chosen[i], n, directed, loops, &pairs[i].first, &pairs[i].second);
+  std::sort(pairs.begin(), pairs.end());
+  for (size_t i = 0; i < pairs.size(); ++i) {
+    src[i] = (int64_t)pairs[i].first + offset;
+    tgt[i] = (int64_t)pairs[i].second + offset;
+  }
+}
+
+// Graph k of a batch uses stream (seed, k) and node offset sum(n[0..k)).
+void gnm_batch(uint64_t count, const int64_t* n, const int64_t* m, bool directed, bool loops,
+               uint64_t seed, int64_t* src, int64_t* tgt, int threads) {
+  std::vector<int64_t> noff(count + 1, 0), eoff(count + 1, 0);
+  for (uint64_t k = 0; k < count; ++k) {
+    noff[k + 1] = noff[k] + n[k];
+    eoff[k + 1] = eoff[k] + m[k];
+  }
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  std::vector<std::thread> pool;
+  std::vector<std::string> errors(threads);
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([&, t] {
+      try {
+        for (uint64_t k = t; k < count; k += threads)
+          gnm_edges((uint64_t)n[k], (uint64_t)m[k], directed, loops, seed, k, noff[k],
+                    src + eoff[k], tgt + eoff[k]);
+      } catch (const std::exception& e) {
+        errors[t] = e.what();
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+  for (auto& e : errors)
+    if (!e.empty()) throw Error(e);
+}
+
+// Sizes from a power law p(x) ~ x^-alpha on [lo, hi] by inverse transform of
+// the continuous law, floored; size k from stream (seed, k).
+void power_law_sizes(uint64_t count, double alpha, double lo, double hi, uint64_t seed,
+                     int64_t* out) {
+  const double e = 1.0 - alpha;
+  const double a = std::pow(lo, e), b = std::pow(hi, e);
+  for (uint64_t k = 0; k < count; ++k) {
+    HostStream rng(seed, k);
+    const double u = rng.uniform();
+    double x = std::pow(a + u * (b - a), 1.0 / e);
+    int64_t v = (int64_t)std::floor(x);
+    out[k] = std::min<int64_t>(std::max<int64_t>(v, (int64_t)lo), (int64_t)hi);
+  }
+}
+
+}  // namespace knb

@@ -63,3 +63,31 @@ def test_reference_signatures_match_header():
     assert ("net_eigenvector(const GraphHandle *h, int32_t mode, int32_t weighted, int32_t "
             "scale, int32_t loops, double tol, int64_t max_iter, int32_t threads, double *out, "
             "double *eigenvalue, int32_t *connected, char *err, size_t err_len)" in text)
+
+
+def test_host_gnm_generator_matches_oracle(so):
+    # The library's G(n, m) restates crates/engine/src/generate.rs:255-290;
+    # both must give the same edges for the same stream.
+    import numpy as np
+    import knappnet_b200 as K
+    from oracle import oracle as O
+    for n, m, d, loops, seed in [(100, 300, False, False, 3), (50, 400, True, False, 4),
+                                 (30, 200, False, True, 5), (20, 300, True, True, 6),
+                                 (12, 60, False, False, 8)]:
+        s, t = K.generate_gnm([n], [m], d, loops, seed)
+        f, g = O.gnm(n, m, d, loops, seed, 0)
+        assert np.array_equal(s, f) and np.array_equal(t, g)
+    # a packed batch: graph k uses stream (seed, k) and global node numbers
+    s, t = K.generate_gnm([10, 20], [15, 30], False, False, 9)
+    f, g = O.gnm(20, 30, False, False, 9, 1)
+    assert np.array_equal(s[15:], f + 10) and np.array_equal(t[15:], g + 10)
+
+
+def test_power_law_sizes(so):
+    import numpy as np
+    import knappnet_b200 as K
+    x = K.power_law_sizes(20000, 2.1, 50, 50000, 3)
+    assert x.min() >= 50 and x.max() <= 50000
+    # mean of the truncated continuous law, floored: about 275 - 0.5
+    assert 240 < x.mean() < 310
+    assert np.array_equal(x, K.power_law_sizes(20000, 2.1, 50, 50000, 3))

@@ -432,3 +432,46 @@ def test_pagerank_batch_options_and_errors():
     zero[1] = 0.0
     with pytest.raises(K.EngineError, match="positive sum"):
         kg.pagerank_batch(zero)
+
+
+# ------------------------------------------------------------------ packed graphs
+@pytest.mark.parametrize("directed,weighted", [(False, False), (True, True)])
+def test_pagerank_graphs_matches_each_graph(directed, weighted):
+    sizes = K.power_law_sizes(60, 2.1, 5, 400, seed=4)
+    m = np.minimum(6 * sizes, sizes * (sizes - 1) // (1 if directed else 2))
+    src, tgt = K.generate_gnm(sizes, m, directed, False, seed=12)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    rng = np.random.default_rng(1)
+    w = rng.lognormal(size=len(src)) if weighted else None
+    g = K.Graph(int(off[-1]), src, tgt, w, directed)
+    out, its, info = g.pagerank_graphs(off, weighted=weighted, tol=1e-11)
+    for k in range(len(sizes)):
+        lo, hi = off[k], off[k + 1]
+        sel = (src >= lo) & (src < hi)
+        og = O.Graph(hi - lo, src[sel] - lo, tgt[sel] - lo, None if w is None else w[sel],
+                     directed)
+        ref = og.pagerank(weighted=weighted, tol=1e-11)
+        assert np.abs(out[lo:hi] - ref).sum() <= 1e-12, k
+        assert its[k] == og.last_iters, k
+    assert info.kernel_launches == 1
+
+
+def test_pagerank_graphs_options_and_errors():
+    sizes = np.array([7, 1, 30, 12])
+    src, tgt = K.generate_gnm(sizes, np.minimum(2 * sizes, sizes * (sizes - 1) // 2), False,
+                              False, seed=2)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    g = K.Graph(int(off[-1]), src, tgt, None, False)
+    p = np.arange(off[-1], dtype=float) % 3 + 1
+    out, _, _ = g.pagerank_graphs(off, personalization=p, dangling=1, loops=1, damping=0.7)
+    for k in range(len(sizes)):
+        lo, hi = off[k], off[k + 1]
+        sel = (src >= lo) & (src < hi)
+        og = O.Graph(hi - lo, src[sel] - lo, tgt[sel] - lo, None, False)
+        ref = og.pagerank(personalization=p[lo:hi], dangling=1, loops=1, damping=0.7)
+        assert np.abs(out[lo:hi] - ref).sum() <= 1e-12
+    bad = K.Graph(10, [0, 3], [4, 9], None, False)
+    with pytest.raises(K.EngineError, match="joins two different graphs"):
+        bad.pagerank_graphs([0, 5, 10])
+    with pytest.raises(K.EngineError, match="end at the node count"):
+        g.pagerank_graphs([0, 5])
