@@ -169,6 +169,36 @@ NET_API int32_t net_pagerank_graphs(const GraphHandle *h, int64_t count,
                             double *out, int64_t *iterations,
                             NetSolveInfo *info, char *err, size_t err_len);
 
+/* PageRank of the graph's structure with the edge weights d_weights (device,
+ * m values in input edge order, nonnegative) instead of its own; device
+ * pointers throughout. Weights are used as strengths (weighted PageRank). */
+NET_API int32_t net_pagerank_weights_device(const GraphHandle *h,
+                                    const double *d_weights, double damping,
+                                    int32_t directed,
+                                    const double *d_personalization,
+                                    int32_t dangling, int32_t loops, double tol,
+                                    int64_t max_iter, int32_t precision,
+                                    double *d_out, NetSolveInfo *info,
+                                    char *err, size_t err_len);
+
+/* Gradient of a loss with respect to the edge weights of weighted PageRank:
+ * given the scores d_scores (from net_pagerank_weights_device with the same
+ * arguments) and dL/dscores in d_grad_scores, writes dL/dweights (m values,
+ * input edge order) to d_grad_weights, by the adjoint solve
+ * (I - d M - d jump 1_D^T)^T lambda = dL/dscores and
+ * dL/dw_e = d f_e (x_j / s_j) (lambda_i - (M^T lambda)_j) for e = (j -> i).
+ * d_lambda (NULL or n values) receives the adjoint vector. tol bounds the
+ * L1 change of lambda relative to max(1, ||dL/dscores||_1). */
+NET_API int32_t net_pagerank_grad_device(const GraphHandle *h,
+                                 const double *d_weights, const double *d_scores,
+                                 const double *d_grad_scores, double damping,
+                                 int32_t directed,
+                                 const double *d_personalization,
+                                 int32_t dangling, int32_t loops, double tol,
+                                 int64_t max_iter, double *d_grad_weights,
+                                 double *d_lambda, NetSolveInfo *info,
+                                 char *err, size_t err_len);
+
 /* Builds a graph from device arrays: 32-bit endpoints and FP32 (d_w32) or
  * FP64 (d_w64) weights, either may be NULL. */
 NET_API int32_t net_graph_new_device(int64_t n, const uint32_t *d_src,

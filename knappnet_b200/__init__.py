@@ -103,6 +103,12 @@ def lib() -> ctypes.CDLL:
     L.net_generate_gnm.restype = i32
     L.net_power_law_sizes.argtypes = [i64, f64, f64, f64, u64, vp, cp, sz]
     L.net_power_law_sizes.restype = i32
+    L.net_pagerank_weights_device.argtypes = [h, vp, f64, i32, vp, i32, i32, f64, i64, i32, vp,
+                                              info_p, cp, sz]
+    L.net_pagerank_weights_device.restype = i32
+    L.net_pagerank_grad_device.argtypes = [h, vp, vp, vp, f64, i32, vp, i32, i32, f64, i64, vp,
+                                           vp, info_p, cp, sz]
+    L.net_pagerank_grad_device.restype = i32
     L.net_graph_new_device.argtypes = [i64, vp, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
     L.net_graph_new_device.restype = i32
     L.net_graph_arc_count.argtypes = [h, i32]

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/knappnet.h"
+#include "adjoint.cuh"
 #include "batch.cuh"
 #include "ego.cuh"
 #include "eigen.cuh"
@@ -550,6 +551,106 @@ int32_t net_power_law_sizes(int64_t count, double alpha, double lo, double hi, u
     if (count < 0 || !(alpha > 1.0) || !(lo >= 1.0) || !(hi >= lo))
       throw Error("power law needs alpha > 1 and 1 <= lo <= hi");
     knb::power_law_sizes((uint64_t)count, alpha, lo, hi, seed, out);
+  });
+}
+
+__global__ void first_bad_weight_dev(const double* __restrict__ w, uint64_t m,
+                                     unsigned long long* __restrict__ bad) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    if (!isfinite(w[e]) || w[e] < 0.0) atomicMin(bad, (unsigned long long)e);
+}
+
+static void check_device_weights(const knb::GraphHandleImpl& g, const double* d_w, cudaStream_t s) {
+  if (!d_w) throw Error("the weight vector is null");
+  if (!g.m) return;
+  knb::DevBuf<unsigned long long> bad(1);
+  KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+  first_bad_weight_dev<<<knb::grid_for(g.m, 256), 256, 0, s>>>(d_w, g.m, bad.get());
+  KNB_LAUNCH("first_bad_weight_dev");
+  uint64_t e = read_u64(bad.get(), s);
+  if (e != NONE)
+    throw Error("edge " + std::to_string(e) +
+                " has a negative or non-finite weight; PageRank requires non-negative weights");
+}
+
+int32_t net_pagerank_weights_device(const GraphHandle* h, const double* d_weights, double damping,
+                                    int32_t directed, const double* d_personalization,
+                                    int32_t dangling, int32_t loops, double tol, int64_t max_iter,
+                                    int32_t precision, double* d_out, NetSolveInfo* info,
+                                    char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (dangling != 0 && dangling != 1)
+      throw Error("unknown dangling-node code " + std::to_string(dangling));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (precision < 0 || precision > 2)
+      throw Error("unknown precision code " + std::to_string(precision));
+    if (!(damping >= 0.0 && damping <= 1.0))
+      throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
+    if (g.n == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    check_device_weights(g, d_weights, s);
+    knb::PagerankParams p;
+    p.damping = damping;
+    p.directed = directed != 0;
+    p.weighted = true;
+    p.personalization = d_personalization;
+    p.pers_on_device = true;
+    p.dangling = dangling;
+    p.loops = loops;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    p.precision = precision;
+    knb::PagerankInfo pi;
+    knb::pagerank_weights(g, d_weights, p, d_out, &pi, s);
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->iterations = pi.iterations;
+      info->iterations_fp32 = pi.iterations_fp32;
+      info->change = pi.change;
+      info->seconds = pi.seconds;
+      info->converged = pi.converged;
+      info->kernel_launches = pi.kernel_launches;
+    }
+  });
+}
+
+int32_t net_pagerank_grad_device(const GraphHandle* h, const double* d_weights,
+                                 const double* d_scores, const double* d_grad_scores,
+                                 double damping, int32_t directed,
+                                 const double* d_personalization, int32_t dangling, int32_t loops,
+                                 double tol, int64_t max_iter, double* d_grad_weights,
+                                 double* d_lambda, NetSolveInfo* info, char* err,
+                                 size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (dangling != 0 && dangling != 1)
+      throw Error("unknown dangling-node code " + std::to_string(dangling));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (!(damping >= 0.0 && damping < 1.0))
+      throw Error("damping is " + fmt_g(damping) + "; the adjoint needs 0 <= damping < 1");
+    if (!d_scores || !d_grad_scores || !d_grad_weights) throw Error("a device vector is null");
+    cudaStream_t s = knb::thread_stream();
+    check_device_weights(g, d_weights, s);
+    knb::AdjointParams p;
+    p.damping = damping;
+    p.directed = directed != 0;
+    p.dangling = dangling;
+    p.loops = loops;
+    p.personalization = d_personalization;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    knb::AdjointInfo ai;
+    knb::pagerank_grad(g, d_weights, d_scores, d_grad_scores, p, d_grad_weights, d_lambda, &ai, s);
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->iterations = ai.iterations;
+      info->change = ai.change;
+      info->seconds = ai.seconds;
+      info->converged = 1;
+      info->kernel_launches = ai.kernel_launches;
+    }
   });
 }
 

@@ -109,6 +109,10 @@ struct GraphHandleImpl {
   const DevCsr& in_rows() const { return directed ? inc : out; }
   const DevCsr& undirected_rows(cudaStream_t s);
   Operator& op(int which, bool weighted, double loop_factor, cudaStream_t s);
+  // An uncached operator whose arc values come from per-edge weights d_w
+  // (device, input edge order) instead of the graph's own.
+  std::unique_ptr<Operator> weighted_op(int which, const double* d_w, double loop_factor,
+                                        cudaStream_t s);
 };
 
 // Merge-path tile coordinates and split rows of a row-compressed matrix.

@@ -613,6 +613,82 @@ const Partition& Operator::relabeled_partition(uint32_t tile_items, cudaStream_t
   return ref;
 }
 
+// Arc values from per-edge weights given by the caller (input edge order),
+// through each arc's edge index.
+__global__ void op_values_from_edges(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                                     const uint32_t* __restrict__ edge, const double* __restrict__ w,
+                                     uint32_t n, double lf, double* __restrict__ v64,
+                                     float* __restrict__ v32, unsigned int* __restrict__ inexact) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    bool bad = false;
+    for (uint32_t k = off[r]; k < off[r + 1]; ++k) {
+      double x = w[edge[k]];
+      if (tgt[k] == r) x *= lf;
+      v64[k] = x;
+      float f = (float)x;
+      v32[k] = f;
+      if ((double)f != x) bad = true;
+    }
+    if (bad) atomicOr(inexact, 1u);
+  }
+}
+
+__global__ void row_sums_from_edges(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                                    const uint32_t* __restrict__ edge, const double* __restrict__ w,
+                                    uint32_t n, double lf, double* __restrict__ sum,
+                                    double* __restrict__ inv64, float* __restrict__ inv32,
+                                    unsigned int* __restrict__ dangling) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (uint32_t k = off[r]; k < off[r + 1]; ++k) {
+      double x = w[edge[k]];
+      if (tgt[k] == r) x *= lf;
+      s += x;
+    }
+    sum[r] = s;
+    double inv = s > 0.0 ? 1.0 / s : 0.0;
+    inv64[r] = inv;
+    inv32[r] = (float)inv;
+    if (!(s > 0.0)) atomicAdd(dangling, 1u);
+  }
+}
+
+std::unique_ptr<Operator> GraphHandleImpl::weighted_op(int which, const double* d_w, double lf,
+                                                       cudaStream_t s) {
+  auto o = std::make_unique<Operator>();
+  const DevCsr* rows = which == 0 ? &out : which == 1 ? &in_rows() : &undirected_rows(s);
+  const DevCsr* trans = which == 0 ? &in_rows() : which == 1 ? &out : rows;
+  o->rows = rows;
+  o->trans = trans;
+  o->n = n;
+  o->nnz = rows->arcs;
+  o->has_vals = true;
+  o->vals64.alloc(std::max<uint64_t>(o->nnz, 1));
+  o->vals32.alloc(std::max<uint64_t>(o->nnz, 1));
+  o->colsum.alloc(std::max<uint32_t>(n, 1));
+  o->inv_out64.alloc(std::max<uint32_t>(n, 1));
+  o->inv_out32.alloc(std::max<uint32_t>(n, 1));
+  DevBuf<unsigned int> flags(2);
+  KNB_CUDA(cudaMemsetAsync(flags.get(), 0, 8, s));
+  if (n) {
+    op_values_from_edges<<<grid_for(n, 256), 256, 0, s>>>(rows->off.get(), rows->tgt.get(),
+                                                          rows->edge.get(), d_w, n, lf,
+                                                          o->vals64.get(), o->vals32.get(),
+                                                          flags.get());
+    row_sums_from_edges<<<grid_for(n, 128), 128, 0, s>>>(trans->off.get(), trans->tgt.get(),
+                                                         trans->edge.get(), d_w, n, lf,
+                                                         o->colsum.get(), o->inv_out64.get(),
+                                                         o->inv_out32.get(), flags.get() + 1);
+    KNB_LAUNCH("weighted_op");
+  }
+  unsigned int hf[2] = {0, 0};
+  KNB_CUDA(cudaMemcpyAsync(hf, flags.get(), 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  o->vals32_exact = hf[0] == 0;
+  o->n_dangling = hf[1];
+  return o;
+}
+
 Operator& GraphHandleImpl::op(int which, bool wtd, double lf, cudaStream_t s) {
   std::lock_guard<std::mutex> lock(mu);
   auto key = std::make_tuple(which, wtd ? 1 : 0, (int)(lf * 2));

@@ -542,22 +542,35 @@ Tuning& tuning() {
   return t;
 }
 
-void pagerank(GraphHandleImpl& g, const PagerankParams& prm_in, double* out, bool out_on_device,
+int pagerank_rows(const GraphHandleImpl& g, bool directed) {
+  return (g.directed && directed) ? 1 : (g.directed ? 2 : 0);
+}
+
+double pagerank_loop_factor(int which, int loops) {
+  // Loop factor follows the orientation of the rows (eigenvector.rs:163-169):
+  // rows of a directed graph count a loop once unless ignored.
+  return loops == 2 ? 0.0 : (which == 1 ? 1.0 : (loops == 0 ? 2.0 : 1.0));
+}
+
+void pagerank(GraphHandleImpl& g, const PagerankParams& prm, double* out, bool out_on_device,
               PagerankInfo* info, cudaStream_t s) {
+  if (g.n == 0) return;
+  const int which = pagerank_rows(g, prm.directed);
+  Operator& op = g.op(which, prm.weighted, pagerank_loop_factor(which, prm.loops), s);
+  pagerank_op(op, prm, out, out_on_device, info, s);
+}
+
+void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool out_on_device,
+                 PagerankInfo* info, cudaStream_t s) {
   PagerankParams prm = prm_in;
   const Tuning& tu = tuning();
   if (tu.ipt) prm.ipt = tu.ipt;
   if (tu.variant) prm.variant = tu.variant;
-  prm.relabel = tu.relabel != 0;
+  prm.relabel = prm.relabel && tu.relabel != 0;
   prm.switch_factor = tu.switch_factor;
   prm.switch_floor = tu.switch_floor;
-  const uint32_t n = g.n;
+  const uint32_t n = op.n;
   if (n == 0) return;
-  int which = (g.directed && prm.directed) ? 1 : (g.directed ? 2 : 0);
-  // Loop factor follows the orientation of the rows (eigenvector.rs:163-169):
-  // rows of a directed graph count a loop once unless ignored.
-  double lfac = prm.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (prm.loops == 0 ? 2.0 : 1.0));
-  Operator& op = g.op(which, prm.weighted, lfac, s);
   // Kernel choice per phase (measured on R-MAT scale 24: one tile per warp,
   // four warps per CTA; 8 items per lane for FP32 sweeps, 4 for FP64 sweeps).
   const int var32 = prm.variant ? prm.variant : VAR_WARP4;

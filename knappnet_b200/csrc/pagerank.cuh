@@ -55,6 +55,13 @@ Tuning& tuning();
 // unless out_on_device). Throws knb::Error on failure (non-convergence too).
 void pagerank(GraphHandleImpl& g, const PagerankParams& prm, double* out, bool out_on_device,
               PagerankInfo* info, cudaStream_t s);
+// The same on a given pull operator (rows = arcs into a node).
+void pagerank_op(Operator& op, const PagerankParams& prm, double* out, bool out_on_device,
+                 PagerankInfo* info, cudaStream_t s);
+// Which rows PageRank pulls along (1 in-CSR, 2 directions ignored, 0 the
+// undirected CSR) and the diagonal factor of a self-loop in them.
+int pagerank_rows(const GraphHandleImpl& g, bool directed);
+double pagerank_loop_factor(int which, int loops);
 
 // Device time of the dominant kernel (the merge-path sweep) of the last solve
 // on this thread: launches and total milliseconds, measured with events.
