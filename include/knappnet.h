@@ -270,6 +270,26 @@ NET_API void net_set_sweep_timing(int32_t on);
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 
+/* PageRank (uniform teleport, weights as strengths when d_weights is not
+ * NULL) of one graph given as device arrays of its in-arcs: d_offsets (n + 1)
+ * and d_sources, d_weights (one per arc, or NULL), scores to d_out (n
+ * doubles); on `stream` (NULL: the default stream). It allocates no device
+ * memory, for callers that cannot call cudaMalloc (a host framework that has
+ * reserved the device memory for its own allocator, or a path that must not
+ * stall the device, which cudaMalloc and cudaFree may do): its scratch is a
+ * static device array of the library holding graphs of up to 262,144 (2^18)
+ * nodes (8 MiB, held on every device that loads the library); larger graphs
+ * are rejected with an error. The first call on a device looks up that
+ * array's address, so it should come before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialized by the caller. No counterpart in the reference. */
+NET_API int32_t net_pagerank_csr_static(int64_t n, const uint32_t *d_offsets,
+                                const uint32_t *d_sources,
+                                const double *d_weights, double damping,
+                                double tol, int64_t max_iter, double *d_out,
+                                int64_t *iterations, void *stream, char *err,
+                                size_t err_len);
+
 /* Waits for the device; reports an asynchronous CUDA error if one occurred. */
 NET_API int32_t net_device_sync(char *err, size_t err_len);
 
