@@ -284,12 +284,14 @@ def run_ours(args):
     r64m = roof(sw64m_ms, sw64m_n, bytes64)
     r64 = roof(sw64[1], sw64[0], sw64[2])
     # dominant kernel of the measured path: the sweep kind with most time
-    dom, dom_name = (r32, "tile_spmv<fp32>") if sw32_ms >= sw64m_ms else (r64m, "tile_spmv<fp64>")
+    dom, dom_name = ((r32, "warp_spmv<fp32> (merge-path warp tiles, 8 items per lane)")
+                     if sw32_ms >= sw64m_ms else
+                     (r64m, "warp_spmv<fp64> (merge-path warp tiles, 4 items per lane)"))
     traffic = None
     tfile = ROOT / "profiles" / "sweep_traffic.json"
     if tfile.exists():
         tdoc = json.loads(tfile.read_text())
-        key = "fp32" if dom_name.endswith("fp32>") else "fp64"
+        key = "fp32" if "<fp32>" in dom_name else "fp64"
         if key in tdoc:
             traffic = tdoc[key].get("bytes_per_launch_full_scale")
 

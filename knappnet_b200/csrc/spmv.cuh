@@ -228,10 +228,18 @@ tile_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
 // the partial sums of rows that continue past a lane are joined by one warp
 // segmented scan, whose value at lane l-1 is the carry into lane l's first
 // finished row.
+//
+// Products are stored with one pad element after every 128 bytes. Lane l's
+// merge-path items start near item l * IPT, so without padding the lanes of
+// one read step fall on 32 / IPT banks only; with it, consecutive lanes move
+// by IPT + IPT / (128 / sizeof(VT)) elements and spread over all banks, while
+// the coalesced writes (item lane + 32 q) stay conflict-free.
 template <class VT, int IPT>
 struct WarpSmem {
-  VT prod[32 * IPT];
+  static constexpr int PAD_SHIFT = sizeof(VT) == 8 ? 4 : 5;
+  VT prod[32 * IPT + ((32 * IPT) >> PAD_SHIFT)];
   uint32_t rend[32 * IPT + 1];
+  static __device__ __forceinline__ uint32_t slot(uint32_t k) { return k + (k >> PAD_SHIFT); }
 };
 
 template <class VT, class MT, class Epi, int IPT, int WPB, int GNA = 0>
@@ -276,7 +284,7 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
 #pragma unroll
     for (int q = 0; q < IPT; ++q) {
       const uint32_t k = lane + q * 32;
-      if (k < n_arcs) sm.prod[k] = op.vals ? wv[q] * xv[q] : xv[q];
+      if (k < n_arcs) sm.prod[WarpSmem<VT, IPT>::slot(k)] = op.vals ? wv[q] * xv[q] : xv[q];
     }
   }
   for (uint32_t r = lane; r < n_rows; r += 32) sm.rend[r] = op.off[i0 + r + 1] - j0;
@@ -311,7 +319,7 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
         ++ri;
         cur_end = ri < n_rows ? sm.rend[ri] : 0xFFFFFFFFu;
       } else {
-        acc += sm.prod[aj];
+        acc += sm.prod[WarpSmem<VT, IPT>::slot(aj)];
         ++aj;
       }
     }
