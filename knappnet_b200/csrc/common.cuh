@@ -6,6 +6,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 namespace knb {
 
@@ -91,6 +92,42 @@ __device__ __forceinline__ T warp_sum(T v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Sums of K <= 4 per-lane values over a warp by a reduce-scatter butterfly:
+// the first two exchanges also halve the number of values a lane carries,
+// so the K sums cost 2 + 1 + 3 shuffles instead of 5 K. Returns, in every
+// lane, the warp sum of value lane / 8 (lanes 8 K and up return a sum of
+// zeros). The association is fixed, so results are identical run to run.
+template <int K>
+__device__ __forceinline__ double warp_sum_scatter(const double* v, int lane) {
+  static_assert(K >= 1 && K <= 4, "at most 4 values");
+  constexpr unsigned F = 0xffffffffu;
+  const double v0 = v[0], v1 = K > 1 ? v[1] : 0.0, v2 = K > 2 ? v[2] : 0.0,
+               v3 = K > 3 ? v[3] : 0.0;
+  const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0;
+  // lanes 0-15 keep values 0 and 1, lanes 16-31 values 2 and 3
+  const double a0 = __shfl_xor_sync(F, h16 ? v0 : v2, 16);
+  const double a1 = __shfl_xor_sync(F, h16 ? v1 : v3, 16);
+  const double k0 = (h16 ? v2 : v0) + a0;
+  const double k1 = (h16 ? v3 : v1) + a1;
+  // then lanes with bit 3 clear keep the even value of the pair, set the odd
+  const double b = __shfl_xor_sync(F, h8 ? k0 : k1, 8);
+  double m = (h8 ? k1 : k0) + b;
+  m += __shfl_xor_sync(F, m, 4);
+  m += __shfl_xor_sync(F, m, 2);
+  m += __shfl_xor_sync(F, m, 1);
+  return m;
+}
+
+// Epilogues whose per-tile scalars are all plain sums declare SUMS = true.
+template <class E, class = void>
+struct EpiSums {
+  static constexpr bool value = false;
+};
+template <class E>
+struct EpiSums<E, std::void_t<decltype(E::SUMS)>> {
+  static constexpr bool value = E::SUMS;
+};
+
 template <class T>
 __device__ __forceinline__ T warp_max(T v) {
 #pragma unroll

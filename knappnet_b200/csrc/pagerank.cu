@@ -41,6 +41,7 @@ namespace knb {
 template <class VT, bool PV, bool JU, bool EXACT>
 struct PagerankEpi {
   static constexpr int NACC = 3;
+  static constexpr bool SUMS = true;  // total, dangling mass, change
   const VT* y_old;
   VT* y_new;
   VT* z_new;

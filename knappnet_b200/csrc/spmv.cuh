@@ -324,35 +324,66 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
       }
     }
   }
-  // 3. carries: inclusive segmented scan of (row at lane end, partial)
-  uint32_t key = ri;
+  // 3. carries: inclusive segmented scan of (row at lane end, partial). Row
+  //    keys never decrease along the lanes, so a lane's segment is the run of
+  //    lanes back to the last key change, found once from a ballot; the scan
+  //    then only shuffles values.
+  const uint32_t key = ri;
+  const uint32_t pkey = __shfl_up_sync(0xffffffffu, key, 1);
+  const uint32_t starts = __ballot_sync(0xffffffffu, lane == 0 || pkey != key);
+  const int seg0 = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
   VT v = acc;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t kk = __shfl_up_sync(0xffffffffu, key, o);
     VT vv = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o && kk == key) v += vv;
+    if (lane - o >= seg0) v += vv;
   }
-  const uint32_t pkey = __shfl_up_sync(0xffffffffu, key, 1);
   const VT pval = __shfl_up_sync(0xffffffffu, v, 1);
   const VT cin = (lane > 0 && pkey == first_row) ? pval : VT(0);
   if (lane == 31) carry[t] = v;  // the row open at the tile end (0 if none)
 
-  // 4. epilogue of the rows this lane finished
+  // 4. epilogue. With IPT >= 8 the finished row sums go to the product
+  //    buffer (free after the walk; a tile holds at most 32 * IPT rows), then
+  //    lane l takes rows l, l + 32, ...: the epilogue runs once per 32 rows,
+  //    with coalesced accesses to the per-node vectors, instead of once per
+  //    item slot. With fewer slots each lane runs its own rows directly.
   double a[NA > 0 ? NA : 1];
   Epi::init(a);
-  uint32_t r = first_row;
+  if constexpr (IPT >= 8) {
+    __syncwarp();
+    uint32_t r = first_row;
 #pragma unroll
-  for (int it = 0; it < IPT; ++it) {
-    if (fmask & (1u << it)) {
-      VT sum = fval[it];
-      if (r == first_row) sum += cin;
-      if (r == 0 && first_open) head[t] = sum;
-      else epi.row(i0 + r, sum, a);
-      ++r;
+    for (int it = 0; it < IPT; ++it) {
+      if (fmask & (1u << it)) {
+        VT sum = fval[it];
+        if (r == first_row) sum += cin;
+        sm.prod[r] = sum;
+        ++r;
+      }
+    }
+    __syncwarp();
+    for (uint32_t q = lane; q < n_rows; q += 32) {
+      const VT sum = sm.prod[q];
+      if (q == 0 && first_open) head[t] = sum;
+      else epi.row(i0 + q, sum, a);
+    }
+  } else {
+    uint32_t r = first_row;
+#pragma unroll
+    for (int it = 0; it < IPT; ++it) {
+      if (fmask & (1u << it)) {
+        VT sum = fval[it];
+        if (r == first_row) sum += cin;
+        if (r == 0 && first_open) head[t] = sum;
+        else epi.row(i0 + r, sum, a);
+        ++r;
+      }
     }
   }
-  if constexpr (NA > 0) {
+  if constexpr (NA > 0 && NA <= 4 && EpiSums<Epi>::value) {
+    const double w = warp_sum_scatter<NA>(a, lane);
+    if ((lane & 7) == 0 && (lane >> 3) < NA) part[(size_t)t * NA + (lane >> 3)] = w;
+  } else if constexpr (NA > 0) {
 #pragma unroll
     for (int s2 = 0; s2 < NA; ++s2) {
       double w = Epi::warp_combine(s2, a[s2]);
