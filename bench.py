@@ -158,9 +158,9 @@ def sum_over_ranks(dist, x: float) -> float:
     return float(t.item())
 
 
-def make_graph():
+def make_graph(scale: int = SCALE):
     import knappnet_b200 as K
-    g = K.generate_rmat(SCALE, EDGE_FACTOR, A, B, C, seed=SEED, clean=True, symmetrize=False,
+    g = K.generate_rmat(scale, EDGE_FACTOR, A, B, C, seed=SEED, clean=True, symmetrize=False,
                         lognormal=True, wseed=WSEED)
     K.device_sync()
     return g
@@ -192,7 +192,7 @@ def run_ours(args):
     import knappnet_b200 as K
     rank, world, local, dist = dist_setup(args.gpus)
     hbm, peak_kind = peaks()
-    g = make_graph()
+    g = make_graph(args.scale)
     n, m = g.n, g.m
 
     import torch
@@ -302,7 +302,7 @@ def run_ours(args):
         "ms_per_step": round(dev_s / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
         "data": "synthetic (R-MAT generated on the device from seeded Philox streams)",
-        "config": {"workload": "R-MAT scale 24, edge factor 16, a/b/c/d=.57/.19/.19/.05, "
+        "config": {"workload": f"R-MAT scale {args.scale}, edge factor 16, a/b/c/d=.57/.19/.19/.05, "
                                "directed, loops and duplicates removed, lognormal(0,1) FP32 "
                                "strengths; PageRank d=0.85, uniform teleport, tol 1e-9 (L1)",
                    "nodes": n, "arcs": m, "precision": "mixed (FP32 sweeps, FP64 sweeps)",
@@ -349,7 +349,7 @@ def run_reference(args):
         return
     from oracle import oracle as O
     import knappnet_b200 as K
-    g = make_graph()
+    g = make_graph(args.scale)
     n, m = g.n, g.m
     s, t, w = g.edges()
     K.lib()
@@ -379,7 +379,7 @@ def run_reference(args):
             "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (same R-MAT graph)",
-            "config": {"workload": "R-MAT scale 24, edge factor 16, directed, lognormal FP32 "
+            "config": {"workload": f"R-MAT scale {args.scale}, edge factor 16, directed, lognormal FP32 "
                                    "strengths; PageRank d=0.85, tol 1e-9", "nodes": n,
                        "arcs": m, "parallelism": f"{cores} CPU threads"},
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores,
@@ -400,6 +400,9 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=8.0,
                     help="seconds per reference-arm step")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scale", type=int, default=SCALE,
+                    help="R-MAT scale (the benchmark workload is 24; smaller scales "
+                         "serve profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -779,7 +779,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (!(value >= 0 && value <= 5) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 7) || value != (int)value) return 1;
       t.variant = (int)value;
       return 0;
     case 5:
@@ -789,6 +789,14 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 6:
       if (value != 0 && value != 128 && value != 256 && value != 512 && value != 1024) return 1;
       knb::set_ego_threads((int)value);
+      return 0;
+    case 7:
+      if (!(value >= -1 && value <= 4294967295.0) || value != (double)(int64_t)value) return 1;
+      t.hot_nodes = (int64_t)value;
+      return 0;
+    case 8:
+      if (value != 0 && value != 1) return 1;
+      t.persistent = (int)value;
       return 0;
     default:
       return 1;

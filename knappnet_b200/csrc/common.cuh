@@ -73,6 +73,23 @@ __device__ __forceinline__ double ld_keep(const double* p, uint64_t pol) {
   return v;
 }
 
+// 16-byte streamed loads (four u32 / f32, or two f64); the address must be
+// 16-byte aligned.
+__device__ __forceinline__ void ld_stream4(const uint32_t* p, uint64_t pol, uint32_t (&o)[4]) {
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=r"(o[0]), "=r"(o[1]), "=r"(o[2]), "=r"(o[3]) : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream4(const float* p, uint64_t pol, float (&o)[4]) {
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]) : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream4(const double* p, uint64_t pol, double (&o)[4]) {
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+      : "=d"(o[0]), "=d"(o[1]) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+      : "=d"(o[2]), "=d"(o[3]) : "l"(p + 2), "l"(pol));
+}
+
 // Gathers that skip L1 allocation (the L2 policy still applies).
 __device__ __forceinline__ float ld_keep_na(const float* p, uint64_t pol) {
   float v;

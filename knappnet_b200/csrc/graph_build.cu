@@ -567,12 +567,15 @@ const Relabeled& Operator::relabeled(cudaStream_t s) {
   r->perm.alloc(nn);
   r->iperm.alloc(nn);
   r->off.alloc((size_t)n + 1);
-  r->cols.alloc(std::max<uint64_t>(nnz, 1));
+  // arc arrays padded to the next multiple of 4 arcs, plus 4: the hot-node
+  // sweep reads them with 16-byte loads from 16-byte boundaries
+  const uint64_t arcs_padded = (nnz | 3) + 5;
+  r->cols.alloc(arcs_padded);
   r->inv_out64.alloc(nn);
   r->inv_out32.alloc(nn);
   if (has_vals) {
-    r->vals64.alloc(std::max<uint64_t>(nnz, 1));
-    r->vals32.alloc(std::max<uint64_t>(nnz, 1));
+    r->vals64.alloc(arcs_padded);
+    r->vals32.alloc(arcs_padded);
   }
   {
     DevBuf<uint64_t> keys(nn);

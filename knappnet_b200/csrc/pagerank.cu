@@ -26,7 +26,9 @@
 // max(tol * switch_factor, switch_floor): the FP32 perturbation of the
 // trajectory (about 1e-7 in L1) then decays over the remaining FP64 sweeps by
 // the same factor as the change, to well below the tolerance.
+#include <algorithm>
 #include <cfloat>
+#include <map>
 #include <mutex>
 #include <chrono>
 #include <cstring>
@@ -354,7 +356,44 @@ struct SweepBuffers {
   IterState* st;
 };
 
-enum SweepVariant : int { VAR_CTA = 1, VAR_WARP = 2, VAR_WARP4 = 3, VAR_WARP16 = 4, VAR_WARPNA = 5 };
+enum SweepVariant : int {
+  VAR_CTA = 1, VAR_WARP = 2, VAR_WARP4 = 3, VAR_WARP16 = 4, VAR_WARPNA = 5,
+  VAR_HOT = 6,    // hot-node cache, one CTA of 32 warps per SM
+  VAR_HOT16 = 7,  // hot-node cache, one CTA of 16 warps per SM
+};
+
+// SM count and the largest dynamic shared memory a CTA may opt into, per
+// device (queried once).
+struct DeviceLimits {
+  int sms = 0;
+  int smem_optin = 0;
+};
+static DeviceLimits device_limits() {
+  static std::mutex mu;
+  static std::map<int, DeviceLimits> cache;
+  int dev = 0;
+  KNB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  DeviceLimits d;
+  KNB_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+  KNB_CUDA(cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cache[dev] = d;
+  return d;
+}
+
+// Nodes the hot-node sweep keeps in shared memory: as many as fit beside
+// the warp buffers, at most n (and at most the tuning cap), in whole
+// 16-byte vectors.
+template <class VT>
+static uint32_t hot_nodes(uint32_t n, size_t warp_bytes, int smem_optin) {
+  const size_t room = (size_t)smem_optin > warp_bytes ? (size_t)smem_optin - warp_bytes : 0;
+  uint64_t hn = std::min<uint64_t>(room / sizeof(VT), n);
+  if (tuning().hot_nodes >= 0) hn = std::min<uint64_t>(hn, (uint64_t)tuning().hot_nodes);
+  hn -= hn % (16 / sizeof(VT));
+  return (uint32_t)hn;
+}
 
 template <class VT, class MT, bool PV, bool JU, bool EXACT, int VAR, int IPT>
 static void launch_sweep(const Operator& op, const Partition& P, const SweepBuffers& B, int buf,
@@ -371,7 +410,30 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
   OpView<MT> v;
   if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
   if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
-  if constexpr (VAR == VAR_CTA) {
+  if constexpr (VAR == VAR_HOT || VAR == VAR_HOT16) {
+    constexpr int WPB = VAR == VAR_HOT ? 32 : 16;
+    constexpr size_t wbytes = hot_warp_smem_bytes<VT, IPT, WPB>();
+    const DeviceLimits lim = device_limits();
+    const uint32_t hn = hot_nodes<VT>(op.n, wbytes, lim.smem_optin);
+    const size_t smem = wbytes + (size_t)hn * sizeof(VT);
+    auto fnp = hot_spmv<VT, MT, Epi, IPT, WPB>;
+    static std::mutex attr_mu;
+    static std::map<int, size_t> attr_set;  // per device: the largest size allowed so far
+    {
+      int dev = 0;
+      KNB_CUDA(cudaGetDevice(&dev));
+      std::lock_guard<std::mutex> lock(attr_mu);
+      size_t& allowed = attr_set[dev];
+      if (smem > allowed) {
+        KNB_CUDA(cudaFuncSetAttribute(fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        allowed = smem;
+      }
+    }
+    const unsigned grid = (unsigned)std::max(1, std::min<int>(lim.sms, (P.ntiles + WPB - 1) / WPB));
+    hot_spmv<VT, MT, Epi, IPT, WPB><<<grid, WPB * 32, smem, s>>>(
+        v, (const VT*)B.z[buf], hn, e, P.coords.get(), P.ntiles, (VT*)B.carry, (VT*)B.head,
+        B.part1, B.st);
+  } else if constexpr (VAR == VAR_CTA) {
     constexpr size_t smem = tile_smem_bytes<VT, IPT>();
     static bool attr_set = false;
     if (!attr_set) {
@@ -397,7 +459,28 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
       KNB_CUDA(cudaFuncSetAttribute(fnp, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     carve >= 0 ? carve : -1));
     }
-    const unsigned grid = (P.ntiles + WPB - 1) / WPB;
+    unsigned grid = (P.ntiles + WPB - 1) / WPB;
+    if (tuning().persistent) {
+      // the CTAs that fit on the GPU at once, each warp looping over tiles
+      static std::mutex occ_mu;
+      static std::map<std::pair<int, int>, int> occ;  // (device, carveout) -> CTAs per SM
+      int dev = 0;
+      KNB_CUDA(cudaGetDevice(&dev));
+      int per_sm = 0;
+      {
+        std::lock_guard<std::mutex> lock(occ_mu);
+        auto key = std::make_pair(dev, carve);
+        auto it = occ.find(key);
+        if (it == occ.end()) {
+          KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fnp, WPB * 32, smem));
+          occ[key] = per_sm;
+        } else {
+          per_sm = it->second;
+        }
+      }
+      const unsigned cap = (unsigned)std::max(1, per_sm) * (unsigned)device_limits().sms;
+      grid = std::min(grid, cap);
+    }
     warp_spmv<VT, MT, Epi, IPT, WPB, GNA><<<grid, WPB * 32, smem, s>>>(
         v, (const VT*)B.z[buf], e, P.coords.get(), P.ntiles, (VT*)B.carry, (VT*)B.head,
         B.part1, B.st);
@@ -443,6 +526,8 @@ static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
     case VAR_WARP4: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP4>(ipt, pv, ju);
     case VAR_WARP16: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP16>(ipt, pv, ju);
     case VAR_WARPNA: return pick_warp_ipt<VT, MT, EXACT, VAR_WARPNA>(ipt, pv, ju);
+    case VAR_HOT: return pick_warp_ipt<VT, MT, EXACT, VAR_HOT>(ipt, pv, ju);
+    case VAR_HOT16: return pick_warp_ipt<VT, MT, EXACT, VAR_HOT16>(ipt, pv, ju);
     default: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP>(ipt, pv, ju);
   }
 }
@@ -574,11 +659,15 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   if (n == 0) return;
   // Kernel choice per phase (measured on R-MAT scale 24: one tile per warp,
   // four warps per CTA; 8 items per lane for FP32 sweeps, 4 for FP64 sweeps).
-  const int var32 = prm.variant ? prm.variant : VAR_WARP4;
-  const int var64 = prm.variant ? prm.variant : VAR_WARP4;
+  const bool rl = prm.relabel;
+  int var32 = prm.variant ? prm.variant : VAR_WARP4;
+  int var64 = prm.variant ? prm.variant : VAR_WARP4;
+  // The hot-node sweep needs the renumbered operator: its most gathered
+  // nodes come first, and its arc arrays are padded for 16-byte loads.
+  if (!rl && (var32 == VAR_HOT || var32 == VAR_HOT16)) var32 = VAR_WARP4;
+  if (!rl && (var64 == VAR_HOT || var64 == VAR_HOT16)) var64 = VAR_WARP4;
   const int ipt32 = prm.ipt ? prm.ipt : 8;
   const int ipt64 = prm.ipt ? prm.ipt : 4;
-  const bool rl = prm.relabel;
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
   const bool mixed_pre = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
   const Partition* P32 = nullptr;

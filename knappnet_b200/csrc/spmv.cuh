@@ -242,62 +242,25 @@ struct WarpSmem {
   static __device__ __forceinline__ uint32_t slot(uint32_t k) { return k + (k >> PAD_SHIFT); }
 };
 
-template <class VT, class MT, class Epi, int IPT, int WPB, int GNA = 0>
-__global__ void __launch_bounds__(WPB * 32)
-warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
-          const TileCoord* __restrict__ coords, uint32_t ntiles, VT* __restrict__ carry,
-          VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st) {
-  constexpr int TILE = 32 * IPT;
+// Steps 2-4 of a warp tile once its products are staged in shared memory:
+// `prod(a)` is the product of the tile's arc a (0-based), `rend[r]` the
+// tile-relative end of row r, `rowbuf` a buffer of at least 32 * IPT values
+// that is free once the walk is over (it may alias the products).
+template <class VT, class Epi, int IPT, class Prod>
+__device__ __forceinline__ void warp_tile_finish(const Prod& prod, VT* rowbuf,
+                                                 const uint32_t* rend, uint32_t t, uint32_t i0,
+                                                 uint32_t n_rows, uint32_t n_arcs, bool first_open,
+                                                 const Epi& epi, VT* __restrict__ carry,
+                                                 VT* __restrict__ head, double* __restrict__ part,
+                                                 int lane) {
   constexpr int NA = Epi::NACC;
-  if (st && iteration_done(st)) return;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t t = blockIdx.x * WPB + wib;
-  if (t >= ntiles) return;
-  Epi epi = epi_in;
-  epi.prepare(st);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSmem<VT, IPT>& sm = reinterpret_cast<WarpSmem<VT, IPT>*>(smem_raw)[wib];
-
-  const uint32_t i0 = coords[t].row, j0 = coords[t].arc;
-  const uint32_t i1 = coords[t + 1].row, j1 = coords[t + 1].arc;
-  const uint32_t n_rows = i1 - i0, n_arcs = j1 - j0;
-  const uint64_t pol_stream = policy_evict_first();
-  const uint64_t pol_keep = policy_evict_last();
-
-  // 1. products (all index/value loads, then all gathers), row ends
-  {
-    uint32_t c[IPT];
-    VT wv[IPT];
-#pragma unroll
-    for (int q = 0; q < IPT; ++q) {
-      const uint32_t k = lane + q * 32;
-      c[q] = k < n_arcs ? ld_stream(op.cols + j0 + k, pol_stream) : 0u;
-      wv[q] = (op.vals && k < n_arcs) ? (VT)ld_stream(op.vals + j0 + k, pol_stream) : VT(1);
-    }
-    VT xv[IPT];
-#pragma unroll
-    for (int q = 0; q < IPT; ++q) {
-      const uint32_t k = lane + q * 32;
-      xv[q] = k < n_arcs ? (GNA ? ld_keep_na(xg + c[q], pol_keep) : ld_keep(xg + c[q], pol_keep))
-                         : VT(0);
-    }
-#pragma unroll
-    for (int q = 0; q < IPT; ++q) {
-      const uint32_t k = lane + q * 32;
-      if (k < n_arcs) sm.prod[WarpSmem<VT, IPT>::slot(k)] = op.vals ? wv[q] * xv[q] : xv[q];
-    }
-  }
-  for (uint32_t r = lane; r < n_rows; r += 32) sm.rend[r] = op.off[i0 + r + 1] - j0;
-  const bool first_open = i0 < op.n && j0 > op.off[i0];
-  __syncwarp();
-
   // 2. this lane's IPT items of the merge path
   const uint32_t total = n_rows + n_arcs;
   const uint32_t diag = min((uint32_t)(lane * IPT), total);
   uint32_t lo = diag > n_arcs ? diag - n_arcs : 0, hi = min(diag, n_rows);
   while (lo < hi) {
     uint32_t mid = (lo + hi) >> 1;
-    if (sm.rend[mid] <= diag - mid - 1) lo = mid + 1; else hi = mid;
+    if (rend[mid] <= diag - mid - 1) lo = mid + 1; else hi = mid;
   }
   uint32_t ri = lo, aj = diag - lo;
   const uint32_t stop = min(diag + (uint32_t)IPT, total);
@@ -306,7 +269,7 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
   uint32_t fmask = 0;  // bit it: item it ended a row
   uint32_t first_row = 0xFFFFFFFFu;
   // end of the current row (kept in a register; 2^32-1 past the last row)
-  uint32_t cur_end = ri < n_rows ? sm.rend[ri] : 0xFFFFFFFFu;
+  uint32_t cur_end = ri < n_rows ? rend[ri] : 0xFFFFFFFFu;
 #pragma unroll
   for (int it = 0; it < IPT; ++it) {
     fval[it] = VT(0);
@@ -317,9 +280,9 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
         if (first_row == 0xFFFFFFFFu) first_row = ri;
         acc = VT(0);
         ++ri;
-        cur_end = ri < n_rows ? sm.rend[ri] : 0xFFFFFFFFu;
+        cur_end = ri < n_rows ? rend[ri] : 0xFFFFFFFFu;
       } else {
-        acc += sm.prod[WarpSmem<VT, IPT>::slot(aj)];
+        acc += prod(aj);
         ++aj;
       }
     }
@@ -342,11 +305,11 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
   const VT cin = (lane > 0 && pkey == first_row) ? pval : VT(0);
   if (lane == 31) carry[t] = v;  // the row open at the tile end (0 if none)
 
-  // 4. epilogue. With IPT >= 8 the finished row sums go to the product
-  //    buffer (free after the walk; a tile holds at most 32 * IPT rows), then
-  //    lane l takes rows l, l + 32, ...: the epilogue runs once per 32 rows,
-  //    with coalesced accesses to the per-node vectors, instead of once per
-  //    item slot. With fewer slots each lane runs its own rows directly.
+  // 4. epilogue. With IPT >= 8 the finished row sums go to `rowbuf` (a tile
+  //    holds at most 32 * IPT rows), then lane l takes rows l, l + 32, ...:
+  //    the epilogue runs once per 32 rows, with coalesced accesses to the
+  //    per-node vectors, instead of once per item slot. With fewer slots each
+  //    lane runs its own rows directly.
   double a[NA > 0 ? NA : 1];
   Epi::init(a);
   if constexpr (IPT >= 8) {
@@ -357,13 +320,13 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
       if (fmask & (1u << it)) {
         VT sum = fval[it];
         if (r == first_row) sum += cin;
-        sm.prod[r] = sum;
+        rowbuf[r] = sum;
         ++r;
       }
     }
     __syncwarp();
     for (uint32_t q = lane; q < n_rows; q += 32) {
-      const VT sum = sm.prod[q];
+      const VT sum = rowbuf[q];
       if (q == 0 && first_open) head[t] = sum;
       else epi.row(i0 + q, sum, a);
     }
@@ -390,6 +353,186 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
       if (lane == 0) part[(size_t)t * NA + s2] = w;
     }
   }
+}
+
+// A warp takes tiles t = global warp, + all warps of the grid: launched with
+// one warp per tile it does one tile; launched with the CTAs that fit on the
+// GPU at once (a persistent grid) it loops, and a launch after convergence
+// retires a few thousand CTAs instead of one per tile.
+template <class VT, class MT, class Epi, int IPT, int WPB, int GNA = 0>
+__global__ void __launch_bounds__(WPB * 32)
+warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
+          const TileCoord* __restrict__ coords, uint32_t ntiles, VT* __restrict__ carry,
+          VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st) {
+  using S = WarpSmem<VT, IPT>;
+  if (st && iteration_done(st)) return;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint32_t t = blockIdx.x * WPB + wib;
+  if (t >= ntiles) return;
+  Epi epi = epi_in;
+  epi.prepare(st);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& sm = reinterpret_cast<S*>(smem_raw)[wib];
+  const uint64_t pol_stream = policy_evict_first();
+  const uint64_t pol_keep = policy_evict_last();
+  const uint32_t stride = gridDim.x * WPB;
+
+  for (; t < ntiles; t += stride) {
+    const uint32_t i0 = coords[t].row, j0 = coords[t].arc;
+    const uint32_t i1 = coords[t + 1].row, j1 = coords[t + 1].arc;
+    const uint32_t n_rows = i1 - i0, n_arcs = j1 - j0;
+
+    // 1. products (all index/value loads, then all gathers), row ends
+    {
+      uint32_t c[IPT];
+      VT wv[IPT];
+#pragma unroll
+      for (int q = 0; q < IPT; ++q) {
+        const uint32_t k = lane + q * 32;
+        c[q] = k < n_arcs ? ld_stream(op.cols + j0 + k, pol_stream) : 0u;
+        wv[q] = (op.vals && k < n_arcs) ? (VT)ld_stream(op.vals + j0 + k, pol_stream) : VT(1);
+      }
+      VT xv[IPT];
+#pragma unroll
+      for (int q = 0; q < IPT; ++q) {
+        const uint32_t k = lane + q * 32;
+        xv[q] = k < n_arcs ? (GNA ? ld_keep_na(xg + c[q], pol_keep) : ld_keep(xg + c[q], pol_keep))
+                           : VT(0);
+      }
+#pragma unroll
+      for (int q = 0; q < IPT; ++q) {
+        const uint32_t k = lane + q * 32;
+        if (k < n_arcs) sm.prod[S::slot(k)] = op.vals ? wv[q] * xv[q] : xv[q];
+      }
+    }
+    for (uint32_t r = lane; r < n_rows; r += 32) sm.rend[r] = op.off[i0 + r + 1] - j0;
+    const bool first_open = i0 < op.n && j0 > op.off[i0];
+    __syncwarp();
+    warp_tile_finish<VT, Epi, IPT>([&](uint32_t a) { return sm.prod[S::slot(a)]; }, sm.prod,
+                                   sm.rend, t, i0, n_rows, n_arcs, first_open, epi, carry, head,
+                                   part, lane);
+    __syncwarp();  // the next tile reuses this warp's buffers
+  }
+}
+
+// -------------------------------------------------------------------- kernel 1 (hot-node cache)
+// Persistent warp tiles with the most gathered part of the iterate in shared
+// memory. Nodes are numbered by decreasing column count (the relabelled
+// operator), so x[0, hot_n) holds the values a sweep gathers most: on R-MAT
+// scale 24 the first 40,960 nodes take 40% of all gathers. Each CTA (one per
+// SM) copies them into shared memory once per launch, and a gather of a
+// column below hot_n reads shared memory instead of sending a sector request
+// to L2 (the L1-to-L2 request path is what bounds the plain warp kernel).
+// Warps then loop over tiles t = global warp, + all warps.
+//
+// Column indices and values are read with 16-byte loads from the 16-byte
+// boundary at or below the tile's first arc, so each 128-byte line a tile
+// spans is requested once; the products are staged from that boundary with
+// 16-byte shared stores, and 16 bytes of padding after every 128 bytes keep
+// both the stores and the merge-path reads free of bank conflicts. The arc
+// arrays must be readable up to the next multiple of 4 arcs past the end
+// (the relabelled operator's arrays carry that padding).
+template <class VT, int IPT>
+struct alignas(16) HotWarpSmem {
+  static constexpr int GROUP = 16 / (int)sizeof(VT);   // elements per 16 bytes
+  static constexpr int ROW = 128 / (int)sizeof(VT);    // elements per 128 bytes
+  static constexpr int SPAN = 32 * IPT + 4;            // staged products, lead included
+  VT prod[SPAN + (SPAN / ROW + 1) * GROUP];
+  uint32_t rend[32 * IPT + 1];
+  static __device__ __forceinline__ uint32_t slot(uint32_t k) { return k + (k / ROW) * GROUP; }
+};
+
+template <class VT, class MT, class Epi, int IPT, int WPB>
+__global__ void __launch_bounds__(WPB * 32, 1)
+hot_spmv(OpView<MT> op, const VT* __restrict__ xg, uint32_t hot_n, Epi epi_in,
+         const TileCoord* __restrict__ coords, uint32_t ntiles, VT* __restrict__ carry,
+         VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st) {
+  using S = HotWarpSmem<VT, IPT>;
+  constexpr int NV = (8 * IPT + 1 + 31) / 32;  // 16-byte loads per lane per array
+  if (st && iteration_done(st)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  S& sm = reinterpret_cast<S*>(smem_raw)[wib];
+  VT* hot = reinterpret_cast<VT*>(smem_raw + sizeof(S) * WPB);
+  {
+    // hot_n is a multiple of 16 / sizeof(VT): whole 16-byte vectors
+    const uint4* src = reinterpret_cast<const uint4*>(xg);
+    uint4* dst = reinterpret_cast<uint4*>(hot);
+    const uint32_t nvec = hot_n / S::GROUP;
+    for (uint32_t i = threadIdx.x; i < nvec; i += WPB * 32) dst[i] = __ldg(src + i);
+  }
+  __syncthreads();
+  Epi epi = epi_in;
+  epi.prepare(st);
+  const uint64_t pol_stream = policy_evict_first();
+  const uint64_t pol_keep = policy_evict_last();
+
+  for (uint32_t t = blockIdx.x * WPB + wib; t < ntiles; t += gridDim.x * WPB) {
+    const uint32_t i0 = coords[t].row, j0 = coords[t].arc;
+    const uint32_t i1 = coords[t + 1].row, j1 = coords[t + 1].arc;
+    const uint32_t n_rows = i1 - i0, n_arcs = j1 - j0;
+    const uint32_t a0 = j0 & ~3u, lead = j0 - a0;
+    // 1. products: every index and value load, then every gather
+    {
+      uint32_t c[NV][4];
+      MT w[NV][4];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const uint32_t k0 = a0 + 4u * (lane + 32u * q);
+        if (k0 < j1) {
+          ld_stream4(op.cols + k0, pol_stream, c[q]);
+          if (op.vals) ld_stream4(op.vals + k0, pol_stream, w[q]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) c[q][e] = 0u;
+        }
+      }
+      VT x[NV][4];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const uint32_t k0 = a0 + 4u * (lane + 32u * q);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const uint32_t k = k0 + e;
+          const uint32_t col = c[q][e];
+          VT v = VT(0);
+          if (k >= j0 && k < j1) {
+            if (col < hot_n) v = hot[col];
+            else v = ld_keep(xg + col, pol_keep);
+          }
+          x[q][e] = v;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const uint32_t p = 4u * (lane + 32u * q);
+        if (a0 + p < j1) {
+          VT pr[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) pr[e] = op.vals ? (VT)w[q][e] * x[q][e] : x[q][e];
+          VT* dst = sm.prod + S::slot(p);
+          if constexpr (sizeof(VT) == 4) {
+            *reinterpret_cast<float4*>(dst) = make_float4(pr[0], pr[1], pr[2], pr[3]);
+          } else {
+            reinterpret_cast<double2*>(dst)[0] = make_double2(pr[0], pr[1]);
+            reinterpret_cast<double2*>(dst)[1] = make_double2(pr[2], pr[3]);
+          }
+        }
+      }
+    }
+    for (uint32_t r = lane; r < n_rows; r += 32) sm.rend[r] = op.off[i0 + r + 1] - j0;
+    const bool first_open = i0 < op.n && j0 > op.off[i0];
+    __syncwarp();
+    warp_tile_finish<VT, Epi, IPT>([&](uint32_t a) { return sm.prod[S::slot(a + lead)]; },
+                                   sm.prod, sm.rend, t, i0, n_rows, n_arcs, first_open, epi,
+                                   carry, head, part, lane);
+    __syncwarp();  // the next tile reuses this warp's buffers
+  }
+}
+
+template <class VT, int IPT, int WPB>
+constexpr size_t hot_warp_smem_bytes() {
+  return sizeof(HotWarpSmem<VT, IPT>) * WPB;
 }
 
 template <class VT, int IPT, int WPB>
