@@ -284,9 +284,11 @@ def run_ours(args):
     r64m = roof(sw64m_ms, sw64m_n, bytes64)
     r64 = roof(sw64[1], sw64[0], sw64[2])
     # dominant kernel of the measured path: the sweep kind with most time
-    dom, dom_name = ((r32, "warp_spmv<fp32> (merge-path warp tiles, 8 items per lane)")
+    dom, dom_name = ((r32, "warp_spmv<float> (persistent merge-path warp tiles, 16 warps per "
+                           "CTA, 8 items per lane)")
                      if sw32_ms >= sw64m_ms else
-                     (r64m, "warp_spmv<fp64> (merge-path warp tiles, 4 items per lane)"))
+                     (r64m, "warp_spmv<double> (persistent merge-path warp tiles, 16 warps per "
+                            "CTA, 4 items per lane)"))
     traffic = None
     tfile = ROOT / "profiles" / "sweep_traffic.json"
     if tfile.exists():

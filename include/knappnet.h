@@ -271,7 +271,7 @@ NET_API void net_set_sweep_timing(int32_t on);
  * 128, 256, 512, 1024); 7 = the most nodes kernels 6 and 7 keep in shared
  * memory (-1 as many as fit, 0 none); 8 = warp-tile sweeps launch one warp
  * per tile (0) or only the CTAs that fit on the GPU at once, each warp
- * looping over tiles (1).
+ * looping over tiles (1, default).
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 

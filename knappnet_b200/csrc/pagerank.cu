@@ -395,20 +395,14 @@ static uint32_t hot_nodes(uint32_t n, size_t warp_bytes, int smem_optin) {
   return (uint32_t)hn;
 }
 
-template <class VT, class MT, bool PV, bool JU, bool EXACT, int VAR, int IPT>
-static void launch_sweep(const Operator& op, const Partition& P, const SweepBuffers& B, int buf,
-                         double d, cudaStream_t s, unsigned g2, cudaEvent_t ev0, cudaEvent_t ev1) {
-  using Epi = PagerankEpi<VT, PV, JU, EXACT>;
-  Epi e;
-  e.y_old = (const VT*)B.y[buf];
-  e.y_new = (VT*)B.y[1 - buf];
-  e.z_new = (VT*)B.z[1 - buf];
-  e.inv_out = (const VT*)B.inv_out;
-  e.p = B.p;
-  e.d = d;
-  e.pu = 1.0 / (double)op.n;
-  OpView<MT> v;
-  if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
+// One merge-path sweep with epilogue `e`: the sweep kernel of variant VAR
+// gathering x, then the split-row kernel, whose CTAs also reduce the
+// epilogue's per-tile scalars and whose last CTA decides convergence.
+template <class VT, class MT, class Epi, int VAR, int IPT>
+static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>& v,
+                        const VT* x, const Epi& e, VT* carry, VT* head, double* part1,
+                        double* part2, IterState* st, cudaStream_t s, unsigned g2,
+                        cudaEvent_t ev0, cudaEvent_t ev1) {
   if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
   if constexpr (VAR == VAR_HOT || VAR == VAR_HOT16) {
     constexpr int WPB = VAR == VAR_HOT ? 32 : 16;
@@ -431,8 +425,8 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
     }
     const unsigned grid = (unsigned)std::max(1, std::min<int>(lim.sms, (P.ntiles + WPB - 1) / WPB));
     hot_spmv<VT, MT, Epi, IPT, WPB><<<grid, WPB * 32, smem, s>>>(
-        v, (const VT*)B.z[buf], hn, e, P.coords.get(), P.ntiles, (VT*)B.carry, (VT*)B.head,
-        B.part1, B.st);
+        v, x, hn, e, P.coords.get(), P.ntiles, carry, head,
+        part1, st);
   } else if constexpr (VAR == VAR_CTA) {
     constexpr size_t smem = tile_smem_bytes<VT, IPT>();
     static bool attr_set = false;
@@ -442,7 +436,7 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
       attr_set = true;
     }
     tile_spmv<VT, MT, Epi, IPT><<<P.ntiles, SPMV_THREADS, smem, s>>>(
-        v, (const VT*)B.z[buf], e, P.coords.get(), (VT*)B.carry, (VT*)B.head, B.part1, B.st);
+        v, x, e, P.coords.get(), carry, head, part1, st);
   } else {
     constexpr int WPB = VAR == VAR_WARP4 ? 4 : VAR == VAR_WARP16 ? 16 : 8;
     constexpr int GNA = VAR == VAR_WARPNA ? 1 : 0;
@@ -482,15 +476,33 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
       grid = std::min(grid, cap);
     }
     warp_spmv<VT, MT, Epi, IPT, WPB, GNA><<<grid, WPB * 32, smem, s>>>(
-        v, (const VT*)B.z[buf], e, P.coords.get(), P.ntiles, (VT*)B.carry, (VT*)B.head,
-        B.part1, B.st);
+        v, x, e, P.coords.get(), P.ntiles, carry, head,
+        part1, st);
   }
   KNB_LAUNCH("sweep");
   if (ev1) KNB_CUDA(cudaEventRecord(ev1, s));
   split_rows<VT, Epi><<<g2, SPMV_THREADS, 0, s>>>(P.split.get(), P.nsplit, P.nshort,
-                                                   (const VT*)B.carry, (const VT*)B.head, e,
-                                                   B.part1, P.ntiles, B.part2, B.st);
+                                                   carry, head, e,
+                                                   part1, P.ntiles, part2, st);
   KNB_LAUNCH("split_rows");
+}
+
+template <class VT, class MT, bool PV, bool JU, bool EXACT, int VAR, int IPT>
+static void launch_sweep(const Operator& op, const Partition& P, const SweepBuffers& B, int buf,
+                         double d, cudaStream_t s, unsigned g2, cudaEvent_t ev0, cudaEvent_t ev1) {
+  using Epi = PagerankEpi<VT, PV, JU, EXACT>;
+  Epi e;
+  e.y_old = (const VT*)B.y[buf];
+  e.y_new = (VT*)B.y[1 - buf];
+  e.z_new = (VT*)B.z[1 - buf];
+  e.inv_out = (const VT*)B.inv_out;
+  e.p = B.p;
+  e.d = d;
+  e.pu = 1.0 / (double)op.n;
+  OpView<MT> v;
+  if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
+  launch_spmv<VT, MT, Epi, VAR, IPT>(op, P, v, (const VT*)B.z[buf], e, (VT*)B.carry,
+                                     (VT*)B.head, B.part1, B.part2, B.st, s, g2, ev0, ev1);
   if (EXACT) {
     pr_exact_change<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
         (const double*)B.y[buf], (const double*)B.y[1 - buf], op.n, B.part3, B.st);
@@ -657,11 +669,12 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   prm.switch_floor = tu.switch_floor;
   const uint32_t n = op.n;
   if (n == 0) return;
-  // Kernel choice per phase (measured on R-MAT scale 24: one tile per warp,
-  // four warps per CTA; 8 items per lane for FP32 sweeps, 4 for FP64 sweeps).
+  // Kernel choice per phase (measured on R-MAT scale 24: warp tiles, sixteen
+  // warps per CTA, a persistent grid; 8 items per lane for FP32 sweeps, 4 for
+  // FP64 sweeps).
   const bool rl = prm.relabel;
-  int var32 = prm.variant ? prm.variant : VAR_WARP4;
-  int var64 = prm.variant ? prm.variant : VAR_WARP4;
+  int var32 = prm.variant ? prm.variant : VAR_WARP16;
+  int var64 = prm.variant ? prm.variant : VAR_WARP16;
   // The hot-node sweep needs the renumbered operator: its most gathered
   // nodes come first, and its arc arrays are padded for 16-byte loads.
   if (!rl && (var32 == VAR_HOT || var32 == VAR_HOT16)) var32 = VAR_WARP4;

@@ -47,7 +47,7 @@ struct Tuning {
   int variant = 0;        // sweep kernel: 1 CTA tiles, 2-5 warp tiles (see pagerank.cu)
   int carveout = -1;      // preferred shared-memory carveout percent (-1: driver default)
   int64_t hot_nodes = -1; // hot-node sweeps: cap on the nodes kept in shared memory (-1: none)
-  int persistent = 0;     // warp-tile sweeps: 1 launches only the CTAs that fit at once
+  int persistent = 1;     // warp-tile sweeps: 1 launches only the CTAs that fit at once
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

@@ -367,12 +367,15 @@ def test_lognormal_weights_match_box_muller():
 # Variants 6 and 7 keep the most gathered nodes in shared memory: a cap of
 # 1000 nodes splits the scale-12 graph's gathers between shared memory and
 # global memory, 0 sends all of them to global memory, -1 (no cap) holds the
-# whole iterate; relabel 0 falls back to the plain warp kernel.
-@pytest.mark.parametrize("variant,ipt,relabel,hot", [
-    (1, 4, 0, -1), (1, 8, 1, -1), (2, 4, 1, -1), (2, 8, 0, -1), (2, 8, 1, -1), (2, 16, 1, -1),
-    (6, 8, 1, -1), (6, 8, 1, 1000), (6, 8, 1, 0), (6, 4, 1, 1000), (6, 16, 1, 1000),
-    (7, 8, 1, 1000), (7, 4, 1, 1000), (6, 8, 0, -1)])
-def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot):
+# whole iterate; relabel 0 falls back to the plain warp kernel. Warp-tile
+# variants (2-4) run on a persistent grid (persist 1, the default) or with
+# one warp per tile (persist 0).
+@pytest.mark.parametrize("variant,ipt,relabel,hot,persist", [
+    (1, 4, 0, -1, 1), (1, 8, 1, -1, 1), (2, 4, 1, -1, 1), (2, 8, 0, -1, 1), (2, 8, 1, -1, 1),
+    (2, 16, 1, -1, 1), (3, 8, 1, -1, 0), (4, 8, 1, -1, 0), (4, 4, 1, -1, 1), (4, 8, 0, -1, 1),
+    (6, 8, 1, -1, 1), (6, 8, 1, 1000, 1), (6, 8, 1, 0, 1), (6, 4, 1, 1000, 1),
+    (6, 16, 1, 1000, 1), (7, 8, 1, 1000, 1), (7, 4, 1, 1000, 1), (6, 8, 0, -1, 1)])
+def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot, persist):
     kg, og = rmat_pair(12, True, seed=21)
     n = kg.n
     p = np.zeros(n)
@@ -382,6 +385,7 @@ def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot):
         K.set_tuning(K.TUNE_IPT, ipt)
         K.set_tuning(K.TUNE_RELABEL, relabel)
         K.set_tuning(K.TUNE_HOT_NODES, hot)
+        K.set_tuning(K.TUNE_PERSISTENT, persist)
         for opts in (dict(), dict(personalization=p), dict(directed=False)):
             b = og.pagerank(weighted=True, **opts)
             a = kg.pagerank(weighted=True, **opts)
@@ -396,6 +400,7 @@ def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot):
         K.set_tuning(K.TUNE_IPT, 0)
         K.set_tuning(K.TUNE_RELABEL, 1)
         K.set_tuning(K.TUNE_HOT_NODES, -1)
+        K.set_tuning(K.TUNE_PERSISTENT, 1)
 
 
 @pytest.mark.parametrize("variant", [6, 7])
