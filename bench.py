@@ -224,7 +224,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         wall0 = time.perf_counter()
         dev_s, sweeps, launches = 0.0, 0, 0
-        sw32_ms = sw32_n = sw64m_ms = sw64m_n = 0.0
+        sw32_ms = sw32_n = sw64m_ms = sw64m_n = swr_ms = swr_n = 0.0
         for _ in range(args.steps):
             infom = solve(K.PREC_MIXED)
             dev_s += infom.seconds
@@ -232,11 +232,14 @@ def run_ours(args):
             launches += infom.kernel_launches
             a = K.sweep_timing(0)
             b = K.sweep_timing(1)
+            c = K.sweep_timing(2)
             sw32_n += a[0]
             sw32_ms += a[1]
             sw64m_n += b[0]
             sw64m_ms += b[1]
-            bytes32, bytes64 = a[2], b[2]
+            swr_n += c[0]
+            swr_ms += c[1]
+            bytes32, bytes64, bytesr = a[2], b[2], c[2]
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
         barrier(dist)
@@ -282,20 +285,24 @@ def run_ours(args):
 
     r32 = roof(sw32_ms, sw32_n, bytes32)
     r64m = roof(sw64m_ms, sw64m_n, bytes64)
+    rr = roof(swr_ms, swr_n, bytesr)
     r64 = roof(sw64[1], sw64[0], sw64[2])
     # dominant kernel of the measured path: the sweep kind with most time
-    dom, dom_name = ((r32, "warp_spmv<float> (persistent merge-path warp tiles, 16 warps per "
-                           "CTA, 8 items per lane)")
-                     if sw32_ms >= sw64m_ms else
-                     (r64m, "warp_spmv<double> (persistent merge-path warp tiles, 16 warps per "
-                            "CTA, 4 items per lane)"))
+    kinds = [(sw32_ms, r32, "fp32", "warp_spmv<float> FP32 sweep (persistent merge-path warp "
+                                    "tiles, 16 warps per CTA, 8 items per lane)"),
+             (swr_ms, rr, "fp32", "warp_spmv<float> refinement sweep (FP32 gathers of the "
+                                  "correction, FP64 update; 16 warps per CTA, 8 items per lane)"),
+             (sw64m_ms, r64m, "fp64", "warp_spmv<double> FP64 sweep (16 warps per CTA, "
+                                      "4 items per lane)")]
+    _, dom, dom_kind, dom_name = max(kinds, key=lambda k: k[0])
     traffic = None
     tfile = ROOT / "profiles" / "sweep_traffic.json"
     if tfile.exists():
         tdoc = json.loads(tfile.read_text())
-        key = "fp32" if "<fp32>" in dom_name else "fp64"
-        if key in tdoc:
-            traffic = tdoc[key].get("bytes_per_launch_full_scale")
+        if dom_kind in tdoc and dom is r32:
+            traffic = tdoc[dom_kind].get("bytes_per_launch_full_scale")
+        elif dom is r64m and "fp64" in tdoc:
+            traffic = tdoc["fp64"].get("bytes_per_launch_full_scale")
 
     clock = clocks.summary()
     line = {
@@ -307,7 +314,9 @@ def run_ours(args):
         "config": {"workload": f"R-MAT scale {args.scale}, edge factor 16, a/b/c/d=.57/.19/.19/.05, "
                                "directed, loops and duplicates removed, lognormal(0,1) FP32 "
                                "strengths; PageRank d=0.85, uniform teleport, tol 1e-9 (L1)",
-                   "nodes": n, "arcs": m, "precision": "mixed (FP32 sweeps, FP64 sweeps)",
+                   "nodes": n, "arcs": m,
+                   "precision": "mixed (FP32 sweeps; one FP64 anchor sweep; refinement sweeps "
+                                "gathering the FP32 correction, FP64 update)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (arc arrays 2.1 GB per sweep)"},
         "gpu_launches": launches,
@@ -318,7 +327,8 @@ def run_ours(args):
                      "achieved": dom["achieved"] if dom else None, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": dom["frac"] if dom else None, "traffic": traffic,
-                     "fp32_sweep": r32, "fp64_sweep_in_mixed": r64m, "fp64_path_sweep": r64},
+                     "fp32_sweep": r32, "fp64_sweep_in_mixed": r64m, "refine_sweep": rr,
+                     "fp64_path_sweep": r64},
         "clocks": clock,
         "fp64_path": {"value": round(float(m) * info64.iterations / fp64_time / 1e9, 3),
                       "time_to_solution_ms": round(fp64_time * 1e3, 3),

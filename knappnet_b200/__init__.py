@@ -366,7 +366,7 @@ def set_sweep_timing(on: bool) -> None:
 
 
 TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT, \
-    TUNE_EGO_THREADS, TUNE_HOT_NODES, TUNE_PERSISTENT = 0, 1, 2, 3, 4, 5, 6, 7, 8
+    TUNE_EGO_THREADS, TUNE_HOT_NODES, TUNE_PERSISTENT, TUNE_REFINE = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9
 
 
 def set_tuning(key: int, value: float) -> None:

@@ -798,6 +798,10 @@ int32_t net_set_tuning(int32_t key, double value) {
       if (value != 0 && value != 1) return 1;
       t.persistent = (int)value;
       return 0;
+    case 9:
+      if (value != 0 && value != 1) return 1;
+      t.refine = (int)value;
+      return 0;
     default:
       return 1;
   }

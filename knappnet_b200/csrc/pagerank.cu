@@ -96,6 +96,69 @@ struct PagerankEpi {
   }
 };
 
+// Refinement sweeps of the mixed path. After the FP32 phase one FP64
+// "anchor" sweep fixes y_ref (its input iterate) and keeps the row sums
+// s_ref = A (y_ref / out); every later iterate is held as y = y_ref + e with
+// e in FP32, and a refinement sweep gathers z_e = e / out in FP32 (FP32
+// arc values, FP32 accumulation) and forms s = s_ref + A z_e in FP64. The
+// update, the sums and the stopping rule are those of the FP64 sweep
+// (PagerankEpi<double>), on the same trajectory: the FP32 rounding now
+// applies to e, which is about 1e-5 of y once the FP32 phase has ended, so
+// each sweep perturbs the iterate by about 1e-12 instead of 1e-7.
+// ANCHOR: the FP64 sweep that computes s_ref (row sums of the FP64 z).
+template <class VT, bool ANCHOR, bool PV, bool JU, bool EXACT>
+struct RefineEpi {
+  static constexpr int NACC = 3;
+  static constexpr bool SUMS = true;
+  const double* y_ref;
+  double* s_ref;        // written by the anchor sweep, read by refinement sweeps
+  const float* e_old;   // refinement sweeps: e of the input iterate
+  float* e_new;
+  float* z_new;         // e_new / out in FP32 (0 for dangling nodes)
+  const float* inv_out;
+  const double* p;
+  double d;
+  double pu;
+  double c_it = 0, c_dt = 0;
+
+  __device__ __forceinline__ void prepare(const IterState* st) {
+    c_it = st->inv_total;
+    c_dt = st->dterm;
+  }
+  static __device__ __forceinline__ void init(double* a) { a[0] = a[1] = a[2] = 0.0; }
+  static __device__ __forceinline__ double identity(int) { return 0.0; }
+  static __device__ __forceinline__ double combine(int, double a, double b) { return a + b; }
+  static __device__ __forceinline__ double warp_combine(int, double v) { return warp_sum(v); }
+
+  __device__ __forceinline__ void row(uint32_t g, VT s_in, double* a) const {
+    double s;
+    if constexpr (ANCHOR) {
+      s = (double)s_in;
+      s_ref[g] = s;
+    } else {
+      s = s_ref[g] + (double)s_in;
+    }
+    const double pg = PV ? p[g] : pu;
+    const double jg = JU ? pu : pg;
+    const double u = d * (s * c_it + c_dt * jg) + (1.0 - d) * pg;
+    const double yr = y_ref[g];
+    const double yo = ANCHOR ? yr : yr + (double)e_old[g];
+    const float en = (float)(u - yr);
+    const double us = yr + (double)en;  // the iterate as stored
+    const float io = inv_out[g];
+    e_new[g] = en;
+    z_new[g] = en * io;
+    a[0] += us;
+    if (io == 0.0f) a[1] += us;
+    a[2] += fabs(us - yo * c_it);
+  }
+
+  __device__ void finish(IterState* st, const double* tot) const {
+    PagerankEpi<double, PV, JU, EXACT> base;
+    base.finish(st, tot);
+  }
+};
+
 // ======================================================================= vertex kernels
 constexpr int VT_THREADS = 256;
 
@@ -175,6 +238,46 @@ __global__ void pr_exact_change(const double* __restrict__ y_old, const double* 
     if (r[0] <= st->tol) st->converged = 1;
     else if (st->iter >= st->max_iter) st->stopped = 1;
     st->ticket2 = 0;
+  }
+}
+
+// The exact change for refinement sweeps, whose iterates are y_ref + e
+// (e_old null: the anchor sweep, whose input iterate is y_ref itself).
+__global__ void pr_exact_change_ref(const double* __restrict__ y_ref,
+                                    const float* __restrict__ e_old,
+                                    const float* __restrict__ e_new, uint32_t n,
+                                    double* __restrict__ part, IterState* st) {
+  if (!st->ambiguous || st->converged || st->stopped) return;
+  __shared__ double sh[VT_THREADS / 32];
+  const double T = st->total, ip = st->prev_inv_total;
+  double a = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double yr = y_ref[i];
+    const double yo = e_old ? yr + (double)e_old[i] : yr;
+    a += fabs((yr + (double)e_new[i]) / T - yo * ip);
+  }
+  a = block_sum(a, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = a;
+  if (!last_block(&st->ticket2)) return;
+  double r[1];
+  reduce_parts<1>(part, gridDim.x, r, sh);
+  if (threadIdx.x == 0) {
+    st->change = r[0];
+    st->ambiguous = 0;
+    if (r[0] <= st->tol) st->converged = 1;
+    else if (st->iter >= st->max_iter) st->stopped = 1;
+    st->ticket2 = 0;
+  }
+}
+
+// out = (y_ref + e) / T in the caller's node order.
+__global__ void pr_output_ref(const double* __restrict__ y_ref, const float* __restrict__ e,
+                              const IterState* __restrict__ st, uint32_t n,
+                              const uint32_t* __restrict__ iperm, double* __restrict__ out) {
+  const double T = st->total;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t k = iperm ? iperm[i] : i;
+    out[i] = (y_ref[k] + (double)e[k]) / T;
   }
 }
 
@@ -288,11 +391,12 @@ struct PrWorkspace : Workspace {
   DevBuf<IterState> st;        // 0: FP32 phase, 1: FP64 phase, 2: personalization
   IterState* hstate = nullptr;  // pinned, 3 slots
   cudaEvent_t t0 = nullptr, t1 = nullptr, done[2] = {nullptr, nullptr};
+  cudaEvent_t a0 = nullptr, a1 = nullptr;  // anchor-sweep timing
   std::vector<cudaEvent_t> pool;  // sweep-timing events
 
   ~PrWorkspace() override {
     if (hstate) cudaFreeHost(hstate);
-    for (cudaEvent_t e : {t0, t1, done[0], done[1]})
+    for (cudaEvent_t e : {t0, t1, done[0], done[1], a0, a1})
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : pool) cudaEventDestroy(e);
   }
@@ -301,6 +405,8 @@ struct PrWorkspace : Workspace {
       KNB_CUDA(cudaMallocHost(&hstate, 3 * sizeof(IterState)));
       KNB_CUDA(cudaEventCreate(&t0));
       KNB_CUDA(cudaEventCreate(&t1));
+      KNB_CUDA(cudaEventCreate(&a0));
+      KNB_CUDA(cudaEventCreate(&a1));
       KNB_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
       KNB_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
       st.alloc(3);
@@ -354,6 +460,8 @@ struct SweepBuffers {
   double* part2;
   double* part3;
   IterState* st;
+  const double* y_ref = nullptr;  // refinement sweeps: the anchor iterate (FP64)
+  double* s_ref = nullptr;        //   and its row sums
 };
 
 enum SweepVariant : int {
@@ -544,14 +652,114 @@ static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
   }
 }
 
+// ----------------------------------------------------------------------- refinement
+// A refinement sweep (RefineEpi): e = B.y[buf] and z_e = B.z[buf] (FP32) in,
+// B.y[1 - buf] and B.z[1 - buf] out; FP32 arc values.
+template <bool PV, bool JU, int VAR, int IPT>
+static void launch_refine(const Operator& op, const Partition& P, const SweepBuffers& B, int buf,
+                          double d, cudaStream_t s, unsigned g2, cudaEvent_t ev0,
+                          cudaEvent_t ev1) {
+  using Epi = RefineEpi<float, false, PV, JU, true>;
+  Epi e;
+  e.y_ref = B.y_ref;
+  e.s_ref = B.s_ref;
+  e.e_old = (const float*)B.y[buf];
+  e.e_new = (float*)B.y[1 - buf];
+  e.z_new = (float*)B.z[1 - buf];
+  e.inv_out = (const float*)B.inv_out;
+  e.p = B.p;
+  e.d = d;
+  e.pu = 1.0 / (double)op.n;
+  launch_spmv<float, float, Epi, VAR, IPT>(op, P, B.v32, (const float*)B.z[buf], e,
+                                           (float*)B.carry, (float*)B.head, B.part1, B.part2,
+                                           B.st, s, g2, ev0, ev1);
+  pr_exact_change_ref<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
+      B.y_ref, (const float*)B.y[buf], (const float*)B.y[1 - buf], op.n, B.part3, B.st);
+  KNB_LAUNCH("pr_exact_change_ref");
+}
+
+// The anchor sweep: an FP64 sweep gathering z_ref = y_ref / out that keeps
+// its row sums in B.s_ref and writes e and z_e of its result to B.y[0] and
+// B.z[0]. MT: the arc value type (FP32 when every value is exact in FP32).
+template <class MT, bool PV, bool JU, int VAR, int IPT>
+static void launch_anchor(const Operator& op, const Partition& P, const SweepBuffers& B,
+                          const double* z_ref, double* carry64, double* head64, double d,
+                          cudaStream_t s, unsigned g2, cudaEvent_t ev0, cudaEvent_t ev1) {
+  using Epi = RefineEpi<double, true, PV, JU, true>;
+  Epi e;
+  e.y_ref = B.y_ref;
+  e.s_ref = B.s_ref;
+  e.e_old = nullptr;
+  e.e_new = (float*)B.y[0];
+  e.z_new = (float*)B.z[0];
+  e.inv_out = (const float*)B.inv_out;
+  e.p = B.p;
+  e.d = d;
+  e.pu = 1.0 / (double)op.n;
+  OpView<MT> v;
+  if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
+  launch_spmv<double, MT, Epi, VAR, IPT>(op, P, v, z_ref, e, carry64, head64, B.part1, B.part2,
+                                         B.st, s, g2, ev0, ev1);
+  pr_exact_change_ref<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
+      B.y_ref, nullptr, (const float*)B.y[0], op.n, B.part3, B.st);
+  KNB_LAUNCH("pr_exact_change_ref");
+}
+
+using AnchorFn = void (*)(const Operator&, const Partition&, const SweepBuffers&, const double*,
+                          double*, double*, double, cudaStream_t, unsigned, cudaEvent_t,
+                          cudaEvent_t);
+
+// Refinement and anchor sweeps come in the warp-tile variants (4, 8 or 16
+// warps per CTA) with 4 or 8 items per lane; other settings use 16 warps.
+template <int VAR, int IPT>
+static SweepFn pick_refine_pv(bool pv, bool ju) {
+  if (!pv) return launch_refine<false, true, VAR, IPT>;
+  if (ju) return launch_refine<true, true, VAR, IPT>;
+  return launch_refine<true, false, VAR, IPT>;
+}
+template <int VAR>
+static SweepFn pick_refine_ipt(int ipt, bool pv, bool ju) {
+  return ipt == 4 ? pick_refine_pv<VAR, 4>(pv, ju) : pick_refine_pv<VAR, 8>(pv, ju);
+}
+static SweepFn pick_refine(int var, int ipt, bool pv, bool ju) {
+  switch (var) {
+    case VAR_WARP: return pick_refine_ipt<VAR_WARP>(ipt, pv, ju);
+    case VAR_WARP4: return pick_refine_ipt<VAR_WARP4>(ipt, pv, ju);
+    default: return pick_refine_ipt<VAR_WARP16>(ipt, pv, ju);
+  }
+}
+template <class MT, int VAR, int IPT>
+static AnchorFn pick_anchor_pv(bool pv, bool ju) {
+  if (!pv) return launch_anchor<MT, false, true, VAR, IPT>;
+  if (ju) return launch_anchor<MT, true, true, VAR, IPT>;
+  return launch_anchor<MT, true, false, VAR, IPT>;
+}
+template <class MT, int VAR>
+static AnchorFn pick_anchor_ipt(int ipt, bool pv, bool ju) {
+  return ipt == 8 ? pick_anchor_pv<MT, VAR, 8>(pv, ju) : pick_anchor_pv<MT, VAR, 4>(pv, ju);
+}
+template <class MT>
+static AnchorFn pick_anchor(int var, int ipt, bool pv, bool ju) {
+  switch (var) {
+    case VAR_WARP: return pick_anchor_ipt<MT, VAR_WARP>(ipt, pv, ju);
+    case VAR_WARP4: return pick_anchor_ipt<MT, VAR_WARP4>(ipt, pv, ju);
+    default: return pick_anchor_ipt<MT, VAR_WARP16>(ipt, pv, ju);
+  }
+}
+static bool refine_variant(int var) {
+  return var == VAR_WARP || var == VAR_WARP4 || var == VAR_WARP16;
+}
+
 static uint32_t tile_items(int var, int ipt) {
   return (uint32_t)((var == VAR_CTA ? SPMV_THREADS : 32) * ipt);
 }
 
 // ======================================================================= timing
-static thread_local SweepTiming g_timing[2];
+static thread_local SweepTiming g_timing[3];
 static thread_local bool g_timing_on = false;
-SweepTiming last_sweep_timing(int phase) { return g_timing[phase & 1]; }
+SweepTiming last_sweep_timing(int phase) {
+  return (phase >= 0 && phase < 3) ? g_timing[phase] : SweepTiming{};
+}
 void set_sweep_timing(bool on) { g_timing_on = on; }
 
 // Algorithmic bytes of one sweep (counted once each): row offsets 4(n+1),
@@ -563,6 +771,22 @@ static double sweep_bytes(const Operator& op, size_t vt, size_t mt, bool pv) {
   double b = 4.0 * (n + 1) + 4.0 * nnz + (op.has_vals ? mt * nnz : 0.0) + 5.0 * vt * n;
   if (pv) b += 8.0 * n;
   return b;
+}
+
+// Refinement sweep: offsets, indices and FP32 values of the arcs, z_e
+// gathered once (4n), y_ref and s_ref read (16n), e and inv_out read (8n),
+// e and z_e written (8n), plus p when personalised. The anchor sweep reads
+// MT values and the FP64 z once (8n), y_ref (8n) and inv_out (4n), and
+// writes s_ref (8n), e and z_e (8n).
+static double refine_bytes(const Operator& op, bool pv) {
+  double n = op.n, nnz = (double)op.nnz;
+  return 4.0 * (n + 1) + 4.0 * nnz + (op.has_vals ? 4.0 * nnz : 0.0) + 36.0 * n +
+         (pv ? 8.0 * n : 0.0);
+}
+static double anchor_bytes(const Operator& op, size_t mt, bool pv) {
+  double n = op.n, nnz = (double)op.nnz;
+  return 4.0 * (n + 1) + 4.0 * nnz + (op.has_vals ? mt * nnz : 0.0) + 36.0 * n +
+         (pv ? 8.0 * n : 0.0);
 }
 
 // ======================================================================= phases
@@ -580,7 +804,7 @@ struct PhaseResult {
 static PhaseResult run_phase(SweepFn fn, const Operator& op, const Partition& P,
                              const SweepBuffers& B, double d, bool exact, cudaStream_t s,
                              PrWorkspace& ws, IterState* h_state /* pinned, 2 slots */,
-                             double* timing_ms, int64_t* timing_n) {
+                             double* timing_ms, int64_t* timing_n, int32_t iter0 = 0) {
   const int U = 8;
   const unsigned g2 = SPLIT_CTAS;
   PhaseResult r;
@@ -618,7 +842,7 @@ static PhaseResult run_phase(SweepFn fn, const Operator& op, const Partition& P,
   // Only sweeps that did work count for the timing (later ones exit at once).
   if (g_timing_on) {
     for (size_t k = 0; k + 1 < nev; k += 2) {
-      if ((int64_t)(k / 2) < fin.iter) {
+      if ((int64_t)(k / 2) < fin.iter - iter0) {
         float ms = 0;
         KNB_CUDA(cudaEventElapsedTime(&ms, ws.pool[k], ws.pool[k + 1]));
         *timing_ms += ms;
@@ -679,8 +903,17 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   // nodes come first, and its arc arrays are padded for 16-byte loads.
   if (!rl && (var32 == VAR_HOT || var32 == VAR_HOT16)) var32 = VAR_WARP4;
   if (!rl && (var64 == VAR_HOT || var64 == VAR_HOT16)) var64 = VAR_WARP4;
-  const int ipt32 = prm.ipt ? prm.ipt : 8;
-  const int ipt64 = prm.ipt ? prm.ipt : 4;
+  int ipt32 = prm.ipt ? prm.ipt : 8;
+  int ipt64 = prm.ipt ? prm.ipt : 4;
+  // Mixed precision with refinement: one FP64 anchor sweep, then refinement
+  // sweeps with FP32 gathers (RefineEpi); both run on warp tiles.
+  const bool refine = prm.precision == PREC_MIXED && tu.refine != 0;
+  const int var_r = refine_variant(var32) ? var32 : VAR_WARP16;  // refinement sweeps
+  const int ipt_r = ipt32 == 4 ? 4 : 8;
+  if (refine) {  // the anchor sweep takes the FP64 settings
+    if (!refine_variant(var64)) var64 = VAR_WARP16;
+    ipt64 = ipt64 == 8 ? 8 : 4;
+  }
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
   const bool mixed_pre = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
   const Partition* P32 = nullptr;
@@ -693,6 +926,11 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
     const uint32_t tile = tile_items(var64, ipt64);
     P64 = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
   }
+  const Partition* PR = nullptr;
+  if (refine) {
+    const uint32_t tile = tile_items(var_r, ipt_r);
+    PR = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
+  }
   const OpView<double> v64 = rl ? op.rview64() : op.view64();
   const OpView<float> v32 = rl ? op.rview32() : op.view32();
   const double* inv64 = rl ? R->inv_out64.get() : op.inv_out64.get();
@@ -703,7 +941,8 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   const bool pv = prm.personalization != nullptr;
   const bool ju = !pv || prm.dangling == 1;
   const bool mixed = mixed_pre;
-  const uint32_t nt = std::max(P32 ? P32->ntiles : 0u, P64 ? P64->ntiles : 0u);
+  const uint32_t nt = std::max({P32 ? P32->ntiles : 0u, P64 ? P64->ntiles : 0u,
+                                PR ? PR->ntiles : 0u});
   const unsigned gv = grid_for(n, VT_THREADS, 1184);
 
   PrWorkspace* wsp = nullptr;
@@ -736,8 +975,8 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
 
   IterState init{};
   int launches = pv ? 3 : 0;
-  double tms32 = 0, tms64 = 0;
-  int64_t tn32 = 0, tn64 = 0;
+  double tms32 = 0, tms64 = 0, tmsr = 0;
+  int64_t tn32 = 0, tn64 = 0, tnr = 0;
   PhaseResult r32, r64;
   const int64_t cap = prm.max_iter;
   double tol32 = std::max(prm.tol * prm.switch_factor, prm.switch_floor);
@@ -778,13 +1017,35 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
       KNB_LAUNCH("pr_init");
     }
     ++launches;
-    SweepBuffers B{v64, v32, {ws.y64[0].get(), ws.y64[1].get()},
-                   {ws.z64[0].get(), ws.z64[1].get()}, inv64, pdev, ws.carry64.get(),
-                   ws.head64.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1};
     bool use32 = op.has_vals && op.vals32_exact && !prm.fp64_values;
-    SweepFn fn = use32 ? pick_kernel<double, float, true>(var64, ipt64, pv, ju)
-                       : pick_kernel<double, double, true>(var64, ipt64, pv, ju);
-    r64 = run_phase(fn, op, *P64, B, prm.damping, true, s, ws, hstate, &tms64, &tn64);
+    if (refine) {
+      // y_ref = y64[0] (from pr_switch), s_ref in z64[1]; e and z_e reuse
+      // the FP32 iterate buffers, free once pr_switch has read them.
+      SweepBuffers R{v64, v32, {ws.y32[0].get(), ws.y32[1].get()},
+                     {ws.z32[0].get(), ws.z32[1].get()}, inv32, pdev, ws.carry32.get(),
+                     ws.head32.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1,
+                     ws.y64[0].get(), ws.z64[1].get()};
+      AnchorFn af = use32 ? pick_anchor<float>(var64, ipt64, pv, ju)
+                          : pick_anchor<double>(var64, ipt64, pv, ju);
+      af(op, *P64, R, ws.z64[0].get(), ws.carry64.get(), ws.head64.get(), prm.damping, s,
+         SPLIT_CTAS, g_timing_on ? ws.a0 : nullptr, g_timing_on ? ws.a1 : nullptr);
+      launches += 3;
+      SweepFn fr = pick_refine(var_r, ipt_r, pv, ju);
+      r64 = run_phase(fr, op, *PR, R, prm.damping, true, s, ws, hstate, &tmsr, &tnr, 1);
+      if (g_timing_on) {
+        float ms = 0;
+        KNB_CUDA(cudaEventElapsedTime(&ms, ws.a0, ws.a1));
+        tms64 += ms;
+        tn64 += 1;
+      }
+    } else {
+      SweepBuffers B{v64, v32, {ws.y64[0].get(), ws.y64[1].get()},
+                     {ws.z64[0].get(), ws.z64[1].get()}, inv64, pdev, ws.carry64.get(),
+                     ws.head64.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1};
+      SweepFn fn = use32 ? pick_kernel<double, float, true>(var64, ipt64, pv, ju)
+                         : pick_kernel<double, double, true>(var64, ipt64, pv, ju);
+      r64 = run_phase(fn, op, *P64, B, prm.damping, true, s, ws, hstate, &tms64, &tn64);
+    }
     launches += r64.launches;
     if (!r64.converged)
       throw Error("PageRank did not converge to tolerance " + std::to_string(prm.tol) +
@@ -798,6 +1059,9 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   }
   if (prm.precision == PREC_FP32) {
     pr_output<float><<<gv, VT_THREADS, 0, s>>>(y32_last, st, n, iperm, outp);
+  } else if (refine) {
+    pr_output_ref<<<gv, VT_THREADS, 0, s>>>(ws.y64[0].get(), ws.y32[(r64.iter - 1) & 1].get(),
+                                            st + 1, n, iperm, outp);
   } else {
     pr_output<double><<<gv, VT_THREADS, 0, s>>>(ws.y64[r64.iter & 1].get(), st + 1, n, iperm,
                                                  outp);
@@ -820,7 +1084,10 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   }
   const bool use32v = op.has_vals && op.vals32_exact && !prm.fp64_values;
   g_timing[0] = {tn32, tms32, sweep_bytes(op, 4, 4, pv)};
-  g_timing[1] = {tn64, tms64, sweep_bytes(op, 8, use32v ? 4 : 8, pv)};
+  g_timing[1] = {tn64, tms64,
+                 refine ? anchor_bytes(op, use32v ? 4 : 8, pv)
+                        : sweep_bytes(op, 8, use32v ? 4 : 8, pv)};
+  g_timing[2] = {tnr, tmsr, refine_bytes(op, pv)};
 }
 
 }  // namespace knb

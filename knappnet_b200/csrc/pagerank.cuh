@@ -7,7 +7,7 @@ namespace knb {
 
 enum Precision : int32_t {
   PREC_FP64 = 0,   // every sweep in FP64 (arc values FP64 unless exact in FP32)
-  PREC_MIXED = 1,  // FP32 sweeps, then FP64 sweeps on the same trajectory
+  PREC_MIXED = 1,  // FP32 sweeps, then FP64-accurate sweeps on the same trajectory
   PREC_FP32 = 2,   // FP32 sweeps only (no FP64 refinement; diagnostics)
 };
 
@@ -48,6 +48,7 @@ struct Tuning {
   int carveout = -1;      // preferred shared-memory carveout percent (-1: driver default)
   int64_t hot_nodes = -1; // hot-node sweeps: cap on the nodes kept in shared memory (-1: none)
   int persistent = 1;     // warp-tile sweeps: 1 launches only the CTAs that fit at once
+  int refine = 1;         // mixed: 1 anchor + refinement sweeps, 0 plain FP64 sweeps
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };
@@ -72,7 +73,8 @@ struct SweepTiming {
   double ms = 0;
   double bytes_per_launch = 0;  // algorithmic bytes of one sweep
 };
-// phase 0: FP32 sweeps, phase 1: FP64 sweeps
+// phase 0: FP32 sweeps, 1: FP64 sweeps (the anchor sweep in mixed solves
+// with refinement), 2: refinement sweeps
 SweepTiming last_sweep_timing(int phase);
 void set_sweep_timing(bool on);
 

@@ -175,18 +175,28 @@ def rmat_pair(scale, weighted, symmetrize=False, seed=3):
     return kg, og
 
 
-@pytest.mark.parametrize("weighted", [False, True])
-def test_pagerank_rmat_fp64_and_mixed(weighted):
+# refine 1 (default): after the FP32 sweeps, one FP64 anchor sweep and
+# refinement sweeps gathering the FP32 correction; refine 0: FP64 sweeps.
+@pytest.mark.parametrize("weighted,refine", [(False, 1), (True, 1), (True, 0)])
+def test_pagerank_rmat_fp64_and_mixed(weighted, refine):
     kg, og = rmat_pair(14, weighted)
     ref = og.pagerank(weighted=weighted, tol=1e-9)
     x64, i64 = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_FP64)
     assert np.abs(x64 - ref).sum() <= 1e-12
     assert i64.iterations == og.last_iters
-    xm, im = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_MIXED)
+    try:
+        K.set_tuning(K.TUNE_REFINE, refine)
+        xm, im = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_MIXED)
+    finally:
+        K.set_tuning(K.TUNE_REFINE, 1)
     assert np.abs(xm - ref).sum() <= 1e-9, np.abs(xm - ref).sum()
     assert im.iterations_fp32 > 0
     top = np.argsort(-ref, kind="stable")[:100]
     assert np.array_equal(np.argsort(-xm, kind="stable")[:100], top)
+    # the mixed path follows the FP64 trajectory: same stopping sweep, and
+    # far inside the 1e-9 bar
+    assert im.iterations == i64.iterations
+    assert np.abs(xm - x64).sum() <= 1e-10, np.abs(xm - x64).sum()
 
 
 def test_pagerank_personalized_and_undirected_rmat():
