@@ -289,7 +289,8 @@ def run_ours(args):
     r64 = roof(sw64[1], sw64[0], sw64[2])
     # dominant kernel of the measured path: the sweep kind with most time
     kinds = [(sw32_ms, r32, "fp32", "warp_spmv<float> FP32 sweep (persistent merge-path warp "
-                                    "tiles, 16 warps per CTA, 8 items per lane)"),
+                                    "tiles, 16 warps per CTA, 8 items per lane, L1 allocation "
+                                    "only for the 24,576 most gathered columns)"),
              (swr_ms, rr, "fp32", "warp_spmv<float> refinement sweep (FP32 gathers of the "
                                   "correction, FP64 update; 16 warps per CTA, 8 items per lane)"),
              (sw64m_ms, r64m, "fp64", "warp_spmv<double> FP64 sweep (16 warps per CTA, "

@@ -265,13 +265,17 @@ NET_API void net_set_sweep_timing(int32_t on);
  * below tol times this factor (default 8192); 3 = ... or below this floor
  * (default 2e-6); 4 = sweep kernel (0 automatic, 1 one merge-path tile per
  * CTA, 2-5 one tile per warp, 6 and 7 persistent warp tiles with the most
- * gathered nodes in shared memory, 32 or 16 warps per SM); 5 = preferred
+ * gathered nodes in shared memory, 32 or 16 warps per SM, 8 warp tiles whose
+ * gathers allocate in L1 only for the most gathered columns); 5 = preferred
  * shared-memory carveout of the sweep (-1 driver default, 0..100 percent);
  * 6 = threads per CTA of the packed-graph PageRank (0 tuned on first use,
  * 128, 256, 512, 1024); 7 = the most nodes kernels 6 and 7 keep in shared
- * memory (-1 as many as fit, 0 none); 8 = warp-tile sweeps launch one warp
+ * memory (-1 as many as fit, 0 none), or the columns below which kernel 8
+ * gathers allocate in L1 (-1: 24,576); 8 = warp-tile sweeps launch one warp
  * per tile (0) or only the CTAs that fit on the GPU at once, each warp
- * looping over tiles (1, default).
+ * looping over tiles (1, default); 9 = mixed precision ends with one FP64
+ * anchor sweep and refinement sweeps that gather the FP32 correction (1,
+ * default) or with FP64 sweeps (0).
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 

@@ -199,7 +199,7 @@ void pagerank_grad(GraphHandleImpl& g, const double* d_w, const double* d_x, con
       e.pu = 1.0 / n;
       warp_spmv<double, double, AdjointEpi, IPT, WPB><<<grid, WPB * 32, smem, s>>>(
           v, lam[k & 1].get(), e, P.coords.get(), P.ntiles, carry.get(), head.get(), part1.get(),
-          st.get());
+          st.get(), 0xFFFFFFFFu);
       split_rows<double, AdjointEpi><<<SPLIT_CTAS, SPMV_THREADS, 0, s>>>(
           P.split.get(), P.nsplit, P.nshort, carry.get(), head.get(), e, part1.get(), P.ntiles,
           part2.get(), st.get());
@@ -218,7 +218,8 @@ void pagerank_grad(GraphHandleImpl& g, const double* d_w, const double* d_x, con
   {
     RowSumEpi e{r.get()};
     warp_spmv<double, double, RowSumEpi, IPT, WPB><<<grid, WPB * 32, smem, s>>>(
-        v, lam_final, e, P.coords.get(), P.ntiles, carry.get(), head.get(), part1.get(), nullptr);
+        v, lam_final, e, P.coords.get(), P.ntiles, carry.get(), head.get(), part1.get(), nullptr,
+        0xFFFFFFFFu);
     split_rows<double, RowSumEpi><<<SPLIT_CTAS, SPMV_THREADS, 0, s>>>(
         P.split.get(), P.nsplit, P.nshort, carry.get(), head.get(), e, part1.get(), P.ntiles,
         part2.get(), nullptr);

@@ -779,7 +779,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (!(value >= 0 && value <= 7) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 8) || value != (int)value) return 1;
       t.variant = (int)value;
       return 0;
     case 5:

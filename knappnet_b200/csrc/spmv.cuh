@@ -245,15 +245,15 @@ struct WarpSmem {
 // Steps 2-4 of a warp tile once its products are staged in shared memory:
 // `prod(a)` is the product of the tile's arc a (0-based), `rend[r]` the
 // tile-relative end of row r, `rowbuf` a buffer of at least 32 * IPT values
-// that is free once the walk is over (it may alias the products).
+// that is free once the walk is over (it may alias the products). The
+// epilogue's scalars accumulate into this lane's `a` (see
+// warp_store_partials).
 template <class VT, class Epi, int IPT, class Prod>
 __device__ __forceinline__ void warp_tile_finish(const Prod& prod, VT* rowbuf,
                                                  const uint32_t* rend, uint32_t t, uint32_t i0,
                                                  uint32_t n_rows, uint32_t n_arcs, bool first_open,
                                                  const Epi& epi, VT* __restrict__ carry,
-                                                 VT* __restrict__ head, double* __restrict__ part,
-                                                 int lane) {
-  constexpr int NA = Epi::NACC;
+                                                 VT* __restrict__ head, double* a, int lane) {
   // 2. this lane's IPT items of the merge path
   const uint32_t total = n_rows + n_arcs;
   const uint32_t diag = min((uint32_t)(lane * IPT), total);
@@ -310,8 +310,6 @@ __device__ __forceinline__ void warp_tile_finish(const Prod& prod, VT* rowbuf,
   //    the epilogue runs once per 32 rows, with coalesced accesses to the
   //    per-node vectors, instead of once per item slot. With fewer slots each
   //    lane runs its own rows directly.
-  double a[NA > 0 ? NA : 1];
-  Epi::init(a);
   if constexpr (IPT >= 8) {
     __syncwarp();
     uint32_t r = first_row;
@@ -343,34 +341,60 @@ __device__ __forceinline__ void warp_tile_finish(const Prod& prod, VT* rowbuf,
       }
     }
   }
+}
+
+// One partial per warp: the warp's epilogue scalars (accumulated over all
+// its tiles, in tile order per lane) joined over the lanes in a fixed order
+// and stored at part[idx * NACC + s].
+template <class Epi>
+__device__ __forceinline__ void warp_store_partials(const double* a, double* __restrict__ part,
+                                                    uint32_t idx, int lane) {
+  constexpr int NA = Epi::NACC;
   if constexpr (NA > 0 && NA <= 4 && EpiSums<Epi>::value) {
     const double w = warp_sum_scatter<NA>(a, lane);
-    if ((lane & 7) == 0 && (lane >> 3) < NA) part[(size_t)t * NA + (lane >> 3)] = w;
+    if ((lane & 7) == 0 && (lane >> 3) < NA) part[(size_t)idx * NA + (lane >> 3)] = w;
   } else if constexpr (NA > 0) {
 #pragma unroll
     for (int s2 = 0; s2 < NA; ++s2) {
       double w = Epi::warp_combine(s2, a[s2]);
-      if (lane == 0) part[(size_t)t * NA + s2] = w;
+      if (lane == 0) part[(size_t)idx * NA + s2] = w;
     }
   }
+}
+
+// Up to 32 bytes of gathered values per lane (8 FP32 or 4 FP64 items) the
+// kernel is built for 48 resident warps per SM (at most 42 registers);
+// wider tiles keep the registers they need.
+template <class VT, int IPT, int WPB>
+constexpr int warp_min_blocks() {
+  return (IPT * (int)sizeof(VT) <= 32 && 48 / WPB > 0) ? 48 / WPB : 1;
 }
 
 // A warp takes tiles t = global warp, + all warps of the grid: launched with
 // one warp per tile it does one tile; launched with the CTAs that fit on the
 // GPU at once (a persistent grid) it loops, and a launch after convergence
-// retires a few thousand CTAs instead of one per tile.
+// retires a few thousand CTAs instead of one per tile. Each warp leaves one
+// partial of the epilogue's scalars, at part[global warp]: the partials
+// number min(warps launched, ntiles).
+// GNA: gathers allocate in L1 (0), never (1), or only for columns below
+// l1_hot (2), so that the most gathered values stay in L1 while one-off
+// gathers pass through.
 template <class VT, class MT, class Epi, int IPT, int WPB, int GNA = 0>
-__global__ void __launch_bounds__(WPB * 32)
+__global__ void __launch_bounds__(WPB * 32, (warp_min_blocks<VT, IPT, WPB>()))
 warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
           const TileCoord* __restrict__ coords, uint32_t ntiles, VT* __restrict__ carry,
-          VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st) {
+          VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st,
+          uint32_t l1_hot) {
   using S = WarpSmem<VT, IPT>;
   if (st && iteration_done(st)) return;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  uint32_t t = blockIdx.x * WPB + wib;
+  const uint32_t gw = blockIdx.x * WPB + wib;
+  uint32_t t = gw;
   if (t >= ntiles) return;
   Epi epi = epi_in;
   epi.prepare(st);
+  double acc[Epi::NACC > 0 ? Epi::NACC : 1];
+  Epi::init(acc);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S& sm = reinterpret_cast<S*>(smem_raw)[wib];
   const uint64_t pol_stream = policy_evict_first();
@@ -396,8 +420,14 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
 #pragma unroll
       for (int q = 0; q < IPT; ++q) {
         const uint32_t k = lane + q * 32;
-        xv[q] = k < n_arcs ? (GNA ? ld_keep_na(xg + c[q], pol_keep) : ld_keep(xg + c[q], pol_keep))
-                           : VT(0);
+        VT x = VT(0);
+        if (k < n_arcs) {
+          if constexpr (GNA == 1) x = ld_keep_na(xg + c[q], pol_keep);
+          else if constexpr (GNA == 2)
+            x = c[q] < l1_hot ? ld_keep(xg + c[q], pol_keep) : ld_keep_na(xg + c[q], pol_keep);
+          else x = ld_keep(xg + c[q], pol_keep);
+        }
+        xv[q] = x;
       }
 #pragma unroll
       for (int q = 0; q < IPT; ++q) {
@@ -410,9 +440,10 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
     __syncwarp();
     warp_tile_finish<VT, Epi, IPT>([&](uint32_t a) { return sm.prod[S::slot(a)]; }, sm.prod,
                                    sm.rend, t, i0, n_rows, n_arcs, first_open, epi, carry, head,
-                                   part, lane);
+                                   acc, lane);
     __syncwarp();  // the next tile reuses this warp's buffers
   }
+  warp_store_partials<Epi>(acc, part, gw, lane);
 }
 
 // -------------------------------------------------------------------- kernel 1 (hot-node cache)
@@ -466,8 +497,12 @@ hot_spmv(OpView<MT> op, const VT* __restrict__ xg, uint32_t hot_n, Epi epi_in,
   epi.prepare(st);
   const uint64_t pol_stream = policy_evict_first();
   const uint64_t pol_keep = policy_evict_last();
+  const uint32_t gw = blockIdx.x * WPB + wib;
+  if (gw >= ntiles) return;
+  double acc[Epi::NACC > 0 ? Epi::NACC : 1];
+  Epi::init(acc);
 
-  for (uint32_t t = blockIdx.x * WPB + wib; t < ntiles; t += gridDim.x * WPB) {
+  for (uint32_t t = gw; t < ntiles; t += gridDim.x * WPB) {
     const uint32_t i0 = coords[t].row, j0 = coords[t].arc;
     const uint32_t i1 = coords[t + 1].row, j1 = coords[t + 1].arc;
     const uint32_t n_rows = i1 - i0, n_arcs = j1 - j0;
@@ -525,9 +560,10 @@ hot_spmv(OpView<MT> op, const VT* __restrict__ xg, uint32_t hot_n, Epi epi_in,
     __syncwarp();
     warp_tile_finish<VT, Epi, IPT>([&](uint32_t a) { return sm.prod[S::slot(a + lead)]; },
                                    sm.prod, sm.rend, t, i0, n_rows, n_arcs, first_open, epi,
-                                   carry, head, part, lane);
+                                   carry, head, acc, lane);
     __syncwarp();  // the next tile reuses this warp's buffers
   }
+  warp_store_partials<Epi>(acc, part, gw, lane);
 }
 
 template <class VT, int IPT, int WPB>
@@ -551,8 +587,10 @@ constexpr size_t tile_smem_bytes() {
 // of tile `last`. Rows spanning few tiles take one thread (carries added in
 // tile order); long rows (hubs) take one warp: lane l adds tiles first+l,
 // first+l+32, ... in order, then a fixed butterfly joins the lanes. Each CTA
-// also reduces a fixed slice of the per-tile partials; the last CTA to finish
-// adds the per-CTA results in CTA order and hands them to Epi::finish. Every
+// also reduces a fixed slice of the sweep's `npart` partials (one per tile
+// from tile_spmv, one per warp from the warp-tile kernels); the last CTA to
+// finish adds the per-CTA results in CTA order and hands them to
+// Epi::finish. Every
 // sum has a fixed association, so results do not change from run to run.
 // Partials written by other CTAs are read with ld.global.cg (L2, not L1).
 constexpr int SPLIT_CTAS = 296;
@@ -562,7 +600,7 @@ __global__ void __launch_bounds__(SPMV_THREADS)
 split_rows(const SplitRow* __restrict__ sr, uint32_t nsr, uint32_t nshort,
            const VT* __restrict__ carry,
            const VT* __restrict__ head, Epi epi_in, const double* __restrict__ part1,
-           uint32_t ntiles, double* __restrict__ part2, IterState* st) {
+           uint32_t npart, double* __restrict__ part2, IterState* st) {
   constexpr int T = SPMV_THREADS;
   constexpr int NA = Epi::NACC;
   if (st && iteration_done(st)) return;
@@ -594,9 +632,9 @@ split_rows(const SplitRow* __restrict__ sr, uint32_t nsr, uint32_t nshort,
     }
   }
   if constexpr (NA > 0) {
-    // this CTA's slice of the per-tile partials, in tile order per thread
-    const uint32_t per = (ntiles + gridDim.x - 1) / gridDim.x;
-    const uint32_t q0 = blockIdx.x * per, q1 = min(ntiles, q0 + per);
+    // this CTA's slice of the sweep's partials, in order per thread
+    const uint32_t per = (npart + gridDim.x - 1) / gridDim.x;
+    const uint32_t q0 = blockIdx.x * per, q1 = min(npart, q0 + per);
     for (uint32_t q = q0 + tid; q < q1; q += T)
 #pragma unroll
       for (int s = 0; s < NA; ++s) a[s] = Epi::combine(s, a[s], __ldcg(part1 + (size_t)q * NA + s));

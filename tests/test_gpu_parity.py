@@ -378,13 +378,15 @@ def test_lognormal_weights_match_box_muller():
 # 1000 nodes splits the scale-12 graph's gathers between shared memory and
 # global memory, 0 sends all of them to global memory, -1 (no cap) holds the
 # whole iterate; relabel 0 falls back to the plain warp kernel. Warp-tile
-# variants (2-4) run on a persistent grid (persist 1, the default) or with
-# one warp per tile (persist 0).
+# variants (2-4, 8) run on a persistent grid (persist 1, the default) or with
+# one warp per tile (persist 0); variant 8 lets only gathers of columns below
+# the cap allocate in L1.
 @pytest.mark.parametrize("variant,ipt,relabel,hot,persist", [
     (1, 4, 0, -1, 1), (1, 8, 1, -1, 1), (2, 4, 1, -1, 1), (2, 8, 0, -1, 1), (2, 8, 1, -1, 1),
     (2, 16, 1, -1, 1), (3, 8, 1, -1, 0), (4, 8, 1, -1, 0), (4, 4, 1, -1, 1), (4, 8, 0, -1, 1),
     (6, 8, 1, -1, 1), (6, 8, 1, 1000, 1), (6, 8, 1, 0, 1), (6, 4, 1, 1000, 1),
-    (6, 16, 1, 1000, 1), (7, 8, 1, 1000, 1), (7, 4, 1, 1000, 1), (6, 8, 0, -1, 1)])
+    (6, 16, 1, 1000, 1), (7, 8, 1, 1000, 1), (7, 4, 1, 1000, 1), (6, 8, 0, -1, 1),
+    (8, 8, 1, 1000, 1), (8, 4, 1, 0, 1), (8, 8, 1, 0, 0)])
 def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot, persist):
     kg, og = rmat_pair(12, True, seed=21)
     n = kg.n
