@@ -291,7 +291,7 @@ def run_ours(args):
     kinds = [(sw32_ms, r32, "fp32", "warp_spmv<float> FP32 sweep (persistent merge-path warp "
                                     "tiles, 16 warps per CTA, 8 items per lane, L1 allocation "
                                     "only for the 24,576 most gathered columns)"),
-             (swr_ms, rr, "fp32", "warp_spmv<float> refinement sweep (FP32 gathers of the "
+             (swr_ms, rr, "refine", "warp_spmv<float> refinement sweep (FP32 gathers of the "
                                   "correction, FP64 update; 16 warps per CTA, 8 items per lane)"),
              (sw64m_ms, r64m, "fp64", "warp_spmv<double> FP64 sweep (16 warps per CTA, "
                                       "4 items per lane)")]
@@ -300,10 +300,8 @@ def run_ours(args):
     tfile = ROOT / "profiles" / "sweep_traffic.json"
     if tfile.exists():
         tdoc = json.loads(tfile.read_text())
-        if dom_kind in tdoc and dom is r32:
+        if dom_kind in tdoc:
             traffic = tdoc[dom_kind].get("bytes_per_launch_full_scale")
-        elif dom is r64m and "fp64" in tdoc:
-            traffic = tdoc["fp64"].get("bytes_per_launch_full_scale")
 
     clock = clocks.summary()
     line = {
