@@ -121,41 +121,25 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus: int):
+    from knappnet_b200 import ranks
     if n_gpus <= 1 and "WORLD_SIZE" not in os.environ:
         return 0, 1, 0, None
-    import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                            device_id=torch.device("cuda", local))
-    return rank, world, local, dist
+    return ranks.init("nccl", timeout_s=300.0)
 
 
 def barrier(dist):
-    if dist is not None:
-        dist.barrier()
+    from knappnet_b200 import ranks
+    ranks.barrier(dist)
 
 
 def max_over_ranks(dist, x: float) -> float:
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from knappnet_b200 import ranks
+    return ranks.max_over_ranks(dist, x)
 
 
 def sum_over_ranks(dist, x: float) -> float:
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from knappnet_b200 import ranks
+    return ranks.sum_over_ranks(dist, x)
 
 
 def make_graph(scale: int = SCALE):

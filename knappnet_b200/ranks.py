@@ -1,0 +1,94 @@
+"""One process per GPU: rank set-up, reductions over ranks, and the splits of
+the workloads that shard with no exchange.
+
+PageRank on one graph needs an exchange of the iterate every sweep to
+shard, so the benchmark runs independent replicas, one per GPU, and reports
+the arcs all ranks processed over the slowest rank's time. The batched and
+packed-graph workloads split with no exchange at all: teleport vectors by
+contiguous column ranges, packed graphs by contiguous graph ranges balanced
+by their nodes plus arcs. Reductions run on the process group's own device
+(CUDA tensors for NCCL, CPU tensors for gloo), so the same code serves the
+GPU runs and the CPU tests.
+"""
+from __future__ import annotations
+
+import os
+from datetime import timedelta
+
+import numpy as np
+
+
+def rank_env():
+    """(rank, world, local rank) from the torchrun environment (0, 1, 0
+    when launched as a single process)."""
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def init(backend: str = "nccl", timeout_s: float = 300.0):
+    """Joins the process group of a torchrun launch; returns (rank, world,
+    local, dist) with dist None for a single process."""
+    rank, world, local = rank_env()
+    if world <= 1 and "WORLD_SIZE" not in os.environ:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    kw = {}
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        kw["device_id"] = torch.device("cuda", local)
+    dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s), **kw)
+    return rank, world, local, dist
+
+
+def _reduce(dist, x: float, op) -> float:
+    if dist is None:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def max_over_ranks(dist, x: float) -> float:
+    """The largest x over all ranks (device time of the slowest rank)."""
+    return _reduce(dist, x, None if dist is None else dist.ReduceOp.MAX)
+
+
+def sum_over_ranks(dist, x: float) -> float:
+    """The sum of x over all ranks (units processed by the whole job)."""
+    return _reduce(dist, x, None if dist is None else dist.ReduceOp.SUM)
+
+
+def barrier(dist) -> None:
+    if dist is not None:
+        dist.barrier()
+
+
+def split_columns(batch: int, world: int, rank: int):
+    """The contiguous range [lo, hi) of teleport vectors this rank solves:
+    sizes differ by at most one and the ranges cover 0..batch exactly."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must lie in 0..world-1")
+    q, r = divmod(int(batch), world)
+    lo = rank * q + min(rank, r)
+    return lo, lo + q + (1 if rank < r else 0)
+
+
+def split_graphs(node_offsets, arc_counts, world: int, rank: int):
+    """The contiguous range [g0, g1) of packed graphs this rank solves, cut
+    where the running work (nodes plus arcs per graph) crosses rank/world of
+    the total, so ranks get nearly equal work; the ranges cover all graphs
+    exactly once, in order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must lie in 0..world-1")
+    off = np.asarray(node_offsets, dtype=np.int64)
+    work = np.diff(off) + np.asarray(arc_counts, dtype=np.int64)
+    cum = np.concatenate([[0], np.cumsum(work)])
+    total = cum[-1]
+    cuts = [int(np.searchsorted(cum, total * k / world, side="left")) for k in range(world + 1)]
+    cuts[0], cuts[-1] = 0, len(work)
+    for k in range(1, world + 1):
+        cuts[k] = max(cuts[k], cuts[k - 1])
+    return cuts[rank], cuts[rank + 1]
