@@ -71,6 +71,24 @@ NET_API int32_t net_pagerank(const GraphHandle *h, double damping, int32_t direc
                      int64_t max_iter, int32_t threads, double *out,
                      char *err, size_t err_len);
 
+/* Katz centrality x = alpha A' x + beta; beta holds 1 or n values; an alpha
+ * not below 1 / lambda_max is an error; normalized != 0 scales to unit
+ * Euclidean norm; mode 1 out, 2 in, 3 all. Replaces netcapi.h:472-476
+ * (crates/capi/src/spectral.rs:107-140). */
+NET_API int32_t net_katz(const GraphHandle *h, double alpha, const double *beta,
+                         int64_t beta_len, int32_t mode, int32_t weighted, int32_t loops,
+                         int32_t normalized, double tol, int64_t max_iter, int32_t threads,
+                         double *out, char *err, size_t err_len);
+
+/* Bonacich power centrality (I - exponent A)^-1 A 1, scaled so the squares
+ * sum to n, or (rescale != 0) so the scores sum to 1; when |exponent|
+ * lambda_max >= 1 a dense solve (at most 5,000 nodes); a singular system is
+ * an error. Replaces netcapi.h:481-486 (crates/capi/src/spectral.rs:149-179). */
+NET_API int32_t net_bonacich_power(const GraphHandle *h, double exponent, int32_t mode,
+                                   int32_t weighted, int32_t loops, int32_t rescale,
+                                   double tol, int64_t max_iter, int32_t threads,
+                                   double *out, char *err, size_t err_len);
+
 /* Eigenvector centrality; out holds n doubles; *eigenvalue receives the
  * principal eigenvalue and *connected 1 if the graph is (strongly)
  * connected. Replaces netcapi.h:455-459 (crates/capi/src/topography.rs:208-249). */

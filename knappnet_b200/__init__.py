@@ -80,6 +80,10 @@ def lib() -> ctypes.CDLL:
     L.net_eigenvector.argtypes = [h, i32, i32, i32, i32, f64, i64, i32, vp,
                                   ctypes.POINTER(f64), ctypes.POINTER(i32), cp, sz]
     L.net_eigenvector.restype = i32
+    L.net_katz.argtypes = [h, f64, vp, i64, i32, i32, i32, i32, f64, i64, i32, vp, cp, sz]
+    L.net_katz.restype = i32
+    L.net_bonacich_power.argtypes = [h, f64, i32, i32, i32, i32, f64, i64, i32, vp, cp, sz]
+    L.net_bonacich_power.restype = i32
     L.net_pagerank_ex.argtypes = [h, f64, i32, i32, vp, i32, i32, f64, i64, i32, vp, info_p,
                                   cp, sz]
     L.net_pagerank_ex.restype = i32
@@ -294,6 +298,27 @@ class Graph:
         _check(lib().net_pagerank(self.h, damping, int(directed), int(weighted), _ptr(p),
                                   dangling, loops, tol, max_iter, threads, _ptr(out), err,
                                   ERR_LEN), err)
+        return out[: self.n]
+
+    def katz(self, alpha=0.1, beta=1.0, mode=2, weighted=False, loops=1, normalized=True,
+             tol=0.0, max_iter=0, threads=0):
+        """net_katz: Katz centrality; beta is one value or n values."""
+        b = np.ascontiguousarray(np.atleast_1d(beta), dtype=np.float64)
+        out = np.zeros(max(self.n, 1))
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_katz(self.h, alpha, _ptr(b), len(b), mode, int(weighted), loops,
+                              int(normalized), tol, max_iter, threads, _ptr(out), err, ERR_LEN),
+               err)
+        return out[: self.n]
+
+    def bonacich(self, exponent=1.0, mode=1, weighted=False, loops=2, rescale=False, tol=0.0,
+                 max_iter=0, threads=0):
+        """net_bonacich_power: Bonacich power centrality."""
+        out = np.zeros(max(self.n, 1))
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_bonacich_power(self.h, exponent, mode, int(weighted), loops,
+                                        int(rescale), tol, max_iter, threads, _ptr(out), err,
+                                        ERR_LEN), err)
         return out[: self.n]
 
     def eigenvector(self, mode=2, weighted=False, scale=0, loops=0, tol=0.0, max_iter=0,

@@ -16,6 +16,7 @@
 #include "batch.cuh"
 #include "ego.cuh"
 #include "eigen.cuh"
+#include "katz.cuh"
 #include "generate.cuh"
 #include "graph.cuh"
 #include "pagerank.cuh"
@@ -374,6 +375,73 @@ static int32_t eigen_impl(const GraphHandle* h, int32_t mode, int32_t weighted, 
       info->eigenvalue = r.eigenvalue;
       info->connected = r.connected ? 1 : 0;
     }
+  });
+}
+
+// net_katz and net_bonacich_power: codes decoded and options checked in the
+// order of crates/capi/src/spectral.rs:107-179 and spectral.rs:365-385,
+// 596-611.
+static void series_codes(int32_t mode, int32_t loops) {
+  if (mode < 1 || mode > 3) throw Error("unknown degree mode code " + std::to_string(mode));
+  if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+}
+
+int32_t net_katz(const GraphHandle* h, double alpha, const double* beta, int64_t beta_len,
+                 int32_t mode, int32_t weighted, int32_t loops, int32_t normalized, double tol,
+                 int64_t max_iter, int32_t threads, double* out, char* err, size_t err_len) {
+  (void)threads;
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (beta_len < 0) throw Error("beta length must be non-negative");
+    if (beta_len > 0 && !beta) throw Error("beta is NULL");
+    series_codes(mode, loops);
+    knb::SeriesParams p;
+    p.mode = mode;
+    p.weighted = weighted != 0;
+    p.loops = loops;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    if (!std::isfinite(alpha) || alpha < 0.0)
+      throw Error("alpha is " + fmt_g(alpha) +
+                  "; it must be a nonnegative number below 1 / lambda_max");
+    const uint32_t n = g.n;
+    std::vector<double> b;
+    if (beta_len == 1) b.assign(n, beta[0]);
+    else if ((uint64_t)beta_len == n) b.assign(beta, beta + n);
+    else
+      throw Error("beta: expected length " + std::to_string(n) + ", found " +
+                  std::to_string(beta_len));
+    for (double v : b)
+      if (!std::isfinite(v)) throw Error("beta must be finite");
+    if (n == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    if (p.weighted) check_nonnegative(g, "Katz centrality", s);
+    knb::SeriesResult r;
+    knb::katz(g, alpha, b, normalized != 0, p, out, &r, s);
+  });
+}
+
+int32_t net_bonacich_power(const GraphHandle* h, double exponent, int32_t mode, int32_t weighted,
+                           int32_t loops, int32_t rescale, double tol, int64_t max_iter,
+                           int32_t threads, double* out, char* err, size_t err_len) {
+  (void)threads;
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    series_codes(mode, loops);
+    knb::SeriesParams p;
+    p.mode = mode;
+    p.weighted = weighted != 0;
+    p.loops = loops;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    if (!std::isfinite(exponent)) throw Error("the exponent must be finite");
+    if (g.n == 0) return;
+    cudaStream_t s = knb::thread_stream();
+    if (p.weighted) check_nonnegative(g, "power centrality", s);
+    knb::SeriesResult r;
+    knb::bonacich_power(g, exponent, rescale != 0, p, out, &r, s);
   });
 }
 

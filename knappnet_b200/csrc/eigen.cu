@@ -234,13 +234,7 @@ __global__ void uf_label(const uint32_t* __restrict__ root, const uint32_t* __re
   }
 }
 
-struct Comps {
-  std::vector<uint32_t> membership;
-  std::vector<uint32_t> sizes;
-  size_t count() const { return sizes.size(); }
-};
-
-static Comps weak_components(GraphHandleImpl& g, cudaStream_t s) {
+Comps weak_components(GraphHandleImpl& g, cudaStream_t s) {
   const uint32_t n = g.n;
   DevBuf<uint32_t> parent(n), root(n), flag(n + 1), label(n);
   uf_init<<<grid_for(n, ET), ET, 0, s>>>(parent.get(), n);
@@ -262,8 +256,8 @@ static Comps weak_components(GraphHandleImpl& g, cudaStream_t s) {
 }
 
 // Tarjan's algorithm with an explicit stack over the out-CSR (host).
-static Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint32_t>& tgt,
-                               uint32_t n) {
+Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint32_t>& tgt,
+                        uint32_t n) {
   const uint32_t UNSEEN = 0xFFFFFFFFu;
   std::vector<uint32_t> index(n, UNSEEN), low(n, 0), comp(n, UNSEEN), stack;
   std::vector<uint8_t> on(n, 0);

@@ -2,6 +2,8 @@
 // matrices and thick-restart Lanczos for symmetric ones.
 #pragma once
 
+#include <vector>
+
 #include "graph.cuh"
 
 namespace knb {
@@ -24,6 +26,20 @@ struct EigenResult {
   double seconds = 0;
   int kernel_launches = 0;
 };
+
+// Component labels (0..count-1) and sizes.
+struct Comps {
+  std::vector<uint32_t> membership;
+  std::vector<uint32_t> sizes;
+  size_t count() const { return sizes.size(); }
+};
+// Weak components of the handle's edges (device union-find; each
+// component's label follows its smallest node).
+Comps weak_components(GraphHandleImpl& g, cudaStream_t s);
+// Strong components of the directed graph in host CSR form (Tarjan's
+// algorithm with an explicit stack), labelled in order of smallest node.
+Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint32_t>& tgt,
+                        uint32_t n);
 
 // Writes n scores to `out` (host). Throws knb::Error on failure.
 void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenResult* r,

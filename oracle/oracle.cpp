@@ -1098,6 +1098,246 @@ Eigenvector eigenvector_centrality(const Graph& g, const EigenvectorOptions& o) 
   return r;
 }
 
+// ======================================================== Katz, Bonacich
+// spectral.rs:409-445: x = b + t A x by fixed-point iteration; stops when
+// the change times q / (1 - q) (at least 1) is at most tol times the
+// largest |x_i|, or when every score is 0.
+static std::vector<double> solve_series(const SparseOp& op, const std::vector<double>& b, double t,
+                                        double q, double tol, size_t max_iter, const char* what,
+                                        size_t* iters) {
+  const size_t n = b.size();
+  std::vector<double> x = b;
+  *iters = 0;
+  if (t == 0.0) return x;
+  const double factor = std::max(q / (1.0 - q), 1.0);
+  std::vector<double> y(n, 0.0);
+  for (size_t it = 0; it < max_iter; ++it) {
+    op.apply(x.data(), y.data());
+    double change = 0.0, top = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      y[i] = b[i] + t * y[i];
+      change = std::max(change, std::fabs(y[i] - x[i]));
+      top = std::max(top, std::fabs(y[i]));
+    }
+    std::swap(x, y);
+    *iters = it + 1;
+    if (change * factor <= tol * top || top == 0.0) return x;
+  }
+  throw Error{std::string(what) + " did not converge to tolerance " + fmt_g(tol) + " within " +
+              std::to_string(max_iter) + " iterations"};
+}
+
+// spectral.rs:529-537.
+static Error too_large(const char* name, double t, double lambda) {
+  return Error{std::string(name) + " = " + fmt_g(t) +
+               " is not below 1 / lambda_max: the largest eigenvalue of the adjacency matrix "
+               "is at least " + fmt_g(lambda) + ", so 1 / lambda_max is at most " +
+               fmt_g(1.0 / lambda)};
+}
+
+// spectral.rs:539-553: arcs i -> j for each positive entry (i, j).
+static Graph pattern_graph(const SparseOp& op) {
+  const size_t n = op.dim();
+  std::vector<int64_t> s, t;
+  for (size_t i = 0; i < n; ++i)
+    for (uint64_t k = op.off[i]; k < op.off[i + 1]; ++k)
+      if ((op.has_vals ? op.vals[k] : 1.0) > 0.0) {
+        s.push_back((int64_t)i);
+        t.push_back((int64_t)op.cols[k]);
+      }
+  return graph_from_edges(n, s.data(), t.data(), nullptr, s.size(), true);
+}
+
+// spectral.rs:447-527: checks that t times the spectral radius is below 1
+// and returns an upper bound on the radius (the largest over strong
+// components, each bounded by Collatz ratios of power iteration on A + I).
+static double check_attenuation(const Graph& g, const SparseOp& op, double t, const char* name,
+                                size_t max_iter) {
+  const size_t n = op.dim();
+  const double limit = 1.0 / t;
+  Components comp = g.directed ? components(pattern_graph(op), true) : components(g, false);
+  const size_t k = comp.count();
+  std::vector<size_t> start(k + 1, 0);
+  for (uint32_t c : comp.membership) start[c + 1] += 1;
+  for (size_t c = 0; c < k; ++c) start[c + 1] += start[c];
+  std::vector<uint32_t> members(n);
+  std::vector<size_t> cursor(start.begin(), start.end() - 1);
+  for (size_t v = 0; v < n; ++v) members[cursor[comp.membership[v]]++] = (uint32_t)v;
+  std::vector<uint32_t> index(n, 0xFFFFFFFFu);
+  double radius = 0.0;
+  for (size_t c = 0; c < k; ++c) {
+    std::vector<uint32_t> nodes(members.begin() + start[c], members.begin() + start[c + 1]);
+    if (nodes.size() == 1) {
+      const size_t v = nodes[0];
+      double diag = 0.0;
+      for (uint64_t q = op.off[v]; q < op.off[v + 1]; ++q)
+        if (op.cols[q] == v) diag += op.has_vals ? op.vals[q] : 1.0;
+      if (diag >= limit) throw too_large(name, t, diag);
+      radius = std::max(radius, diag);
+      continue;
+    }
+    for (size_t i = 0; i < nodes.size(); ++i) index[nodes[i]] = (uint32_t)i;
+    SparseOp sub = op.submatrix(nodes, index);
+    for (uint32_t v : nodes) index[v] = 0xFFFFFFFFu;
+    const size_t m = sub.dim();
+    std::vector<double> x(m, 1.0), y(m, 0.0);
+    bool decided = false;
+    for (size_t it = 0; it < max_iter; ++it) {
+      sub.apply(x.data(), y.data());
+      double lo = std::numeric_limits<double>::infinity(), hi = 0.0, top = 0.0;
+      for (size_t i = 0; i < m; ++i) {
+        const double r = y[i] / x[i];
+        lo = std::fmin(lo, r);
+        hi = std::fmax(hi, r);
+        y[i] += x[i];
+        top = std::fmax(top, y[i]);
+      }
+      if (lo >= limit) throw too_large(name, t, lo);
+      if (hi < limit) {
+        radius = std::max(radius, hi);
+        decided = true;
+        break;
+      }
+      for (size_t i = 0; i < m; ++i) x[i] = y[i] / top;
+    }
+    if (!decided)
+      throw Error{std::string(name) + " = " + fmt_g(t) +
+                  " is too close to 1 / lambda_max to decide whether the series converges; "
+                  "choose a smaller value"};
+  }
+  return radius;
+}
+
+// spectral.rs:346-363: a constant or per-node vector.
+static std::vector<double> per_node(const std::vector<double>& v, size_t n, const char* what) {
+  std::vector<double> out;
+  if (v.size() == 1) out.assign(n, v[0]);
+  else if (v.size() == n) out = v;
+  else
+    throw Error{std::string(what) + ": expected length " + std::to_string(n) + ", found " +
+                std::to_string(v.size())};
+  for (double x : out)
+    if (!std::isfinite(x)) throw Error{std::string(what) + " must be finite"};
+  return out;
+}
+
+// spectral.rs:365-407.
+std::vector<double> katz(const Graph& g, const KatzOptions& o, size_t* iters) {
+  check_iteration(o.tol, o.max_iter);
+  const size_t n = g.n;
+  *iters = 0;
+  if (!std::isfinite(o.alpha) || o.alpha < 0.0)
+    throw Error{"alpha is " + fmt_g(o.alpha) +
+                "; it must be a nonnegative number below 1 / lambda_max"};
+  std::vector<double> beta = per_node(o.beta, n, "beta");
+  if (n == 0) return {};
+  if (o.weighted) check_nonnegative(g, "Katz centrality");
+  Graph holder;
+  SparseOp op = matrix(g, o.mode, o.weighted, o.loops, o.threads, &holder);
+  const double q = o.alpha > 0.0 ? o.alpha * check_attenuation(g, op, o.alpha, "alpha", o.max_iter)
+                                 : 0.0;
+  std::vector<double> x = solve_series(op, beta, o.alpha, q, o.tol, o.max_iter,
+                                       "Katz centrality", iters);
+  if (o.normalized) {
+    double ss = 0.0;
+    for (double v : x) ss += v * v;
+    const double norm = std::sqrt(ss);
+    if (norm > 0.0)
+      for (double& v : x) v /= norm;
+  }
+  return x;
+}
+
+// linalg.rs:357-384 and 433-467.
+bool dense_solve_rowmajor(std::vector<double> a, size_t n, std::vector<double>* xio, double tol) {
+  std::vector<double>& x = *xio;
+  double mag = 0.0;
+  for (double v : a) mag = std::max(mag, std::fabs(v));
+  mag = std::max(mag, std::numeric_limits<double>::min());
+  const double threshold = tol * mag;
+  for (size_t k = 0; k < n; ++k) {
+    size_t p = k;
+    for (size_t r = k + 1; r < n; ++r)
+      if (std::fabs(a[r * n + k]) > std::fabs(a[p * n + k])) p = r;
+    if (std::fabs(a[p * n + k]) <= threshold) return false;
+    if (p != k) {
+      for (size_t c = 0; c < n; ++c) std::swap(a[k * n + c], a[p * n + c]);
+      std::swap(x[k], x[p]);
+    }
+    const double pivot = a[k * n + k];
+    for (size_t i = k + 1; i < n; ++i) {
+      const double f = a[i * n + k] / pivot;
+      if (f == 0.0) continue;
+      a[i * n + k] = 0.0;
+      for (size_t j = k + 1; j < n; ++j) a[i * n + j] = a[i * n + j] - f * a[k * n + j];
+      x[i] -= f * x[k];
+    }
+  }
+  for (size_t k = n; k-- > 0;) {
+    double s = x[k];
+    for (size_t j = k + 1; j < n; ++j) s -= a[k * n + j] * x[j];
+    x[k] = s / a[k * n + k];
+  }
+  return true;
+}
+
+// spectral.rs:590-655 (DENSE_MAX 5000) and 657-672.
+std::vector<double> bonacich_power(const Graph& g, const BonacichOptions& o, size_t* iters,
+                                   bool* dense) {
+  check_iteration(o.tol, o.max_iter);
+  *iters = 0;
+  *dense = false;
+  if (!std::isfinite(o.exponent)) throw Error{"the exponent must be finite"};
+  const size_t n = g.n;
+  if (n == 0) return {};
+  if (o.weighted) check_nonnegative(g, "power centrality");
+  Graph holder;
+  SparseOp op = matrix(g, o.mode, o.weighted, o.loops, o.threads, &holder);
+  std::vector<double> ones(n, 1.0), b(n, 0.0);
+  op.apply(ones.data(), b.data());
+  const double beta = o.exponent;
+  bool series = true;
+  double q = 0.0;
+  if (beta != 0.0) {
+    try {
+      q = check_attenuation(g, op, std::fabs(beta), "|exponent|", o.max_iter) * std::fabs(beta);
+    } catch (const Error&) {
+      series = false;
+    }
+  }
+  std::vector<double> y;
+  if (series) {
+    y = solve_series(op, b, beta, q, o.tol, o.max_iter, "power centrality", iters);
+  } else {
+    if (n > 5000)
+      throw Error{"|exponent| x lambda_max >= 1, so power centrality needs a dense linear "
+                  "solve, which is limited to 5000 nodes; use a smaller |exponent|"};
+    std::vector<double> a(n * n, 0.0);
+    for (size_t i = 0; i < n; ++i) a[i * n + i] = 1.0;
+    for (size_t i = 0; i < n; ++i)
+      for (uint64_t k = op.off[i]; k < op.off[i + 1]; ++k) {
+        const size_t j = op.cols[k];
+        a[i * n + j] = a[i * n + j] - beta * (op.has_vals ? op.vals[k] : 1.0);
+      }
+    y = b;
+    if (!dense_solve_rowmajor(a, n, &y, 1e-12))
+      throw Error{"I - exponent x A is singular (exponent is the reciprocal of an eigenvalue), "
+                  "so power centrality is undefined; choose another exponent"};
+    *dense = true;
+  }
+  double sq = 0.0;
+  for (double v : y) sq += v * v;
+  const double alpha = std::sqrt((double)n / sq);
+  if (o.rescale) {
+    double total = 0.0;
+    for (double v : y) total += v;
+    for (double& v : y) v /= total;
+  } else {
+    for (double& v : y) v *= alpha;
+  }
+  return y;
+}
+
 // ======================================================== G(n, m)
 // generate.rs:148-155.
 static uint64_t pair_count(uint64_t n, bool directed, bool loops) {

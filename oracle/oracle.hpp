@@ -147,6 +147,38 @@ struct Eigenvector {
 };
 Eigenvector eigenvector_centrality(const Graph& g, const EigenvectorOptions& o);
 
+// spectral.rs:308-344 (KatzOptions) and 555-594 (BonacichOptions).
+struct KatzOptions {
+  double alpha = 0.1;
+  std::vector<double> beta{1.0};  // one value, or one per node
+  Mode mode = Mode::In;
+  bool weighted = false;
+  Loops loops = Loops::Once;
+  bool normalized = true;
+  double tol = 1e-12;
+  size_t max_iter = 10000;
+  size_t threads = 0;
+};
+std::vector<double> katz(const Graph& g, const KatzOptions& o, size_t* iters);
+
+struct BonacichOptions {
+  double exponent = 1.0;
+  Mode mode = Mode::Out;
+  bool weighted = false;
+  Loops loops = Loops::Ignore;
+  bool rescale = false;
+  double tol = 1e-12;
+  size_t max_iter = 10000;
+  size_t threads = 0;
+};
+std::vector<double> bonacich_power(const Graph& g, const BonacichOptions& o, size_t* iters,
+                                   bool* dense);
+
+// linalg.rs:433-467: Gaussian elimination with partial pivoting on the
+// row-major n x n matrix `a`; false when a pivot is at most tol times the
+// largest magnitude of `a`.
+bool dense_solve_rowmajor(std::vector<double> a, size_t n, std::vector<double>* x, double tol);
+
 // linalg.rs:478-720: eigenvalues ascending, eigenvectors in columns of the
 // row-major n x n matrix `vecs` (vecs[i * n + j] = component i of vector j).
 bool symmetric_eigen(const std::vector<double>& a, size_t n, std::vector<double>* vals,

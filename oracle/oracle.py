@@ -73,6 +73,12 @@ def lib() -> ctypes.CDLL:
     L.orc_eigenvector_ex.restype = i32
     L.orc_symmetric_eigen.argtypes = [i64, vp, vp, vp]
     L.orc_symmetric_eigen.restype = i32
+    L.orc_katz.argtypes = [vp, f64, vp, i64, i32, i32, i32, i32, f64, i64, i32, vp,
+                           ctypes.POINTER(i64), cp, sz]
+    L.orc_katz.restype = i32
+    L.orc_bonacich_power.argtypes = [vp, f64, i32, i32, i32, i32, f64, i64, i32, vp,
+                                     ctypes.POINTER(i64), ctypes.POINTER(i32), cp, sz]
+    L.orc_bonacich_power.restype = i32
     _lib = L
     return L
 
@@ -189,6 +195,36 @@ class Graph:
             raise OracleError(err.value.decode())
         self.last_iters = it.value
         return out[: self.n], val.value, bool(conn.value)
+
+
+    def katz(self, alpha=0.1, beta=1.0, mode=2, weighted=False, loops=1, normalized=True,
+             tol=0.0, max_iter=0, threads=0):
+        """net_katz (spectral.rs:365-407); beta is one value or n values."""
+        b = np.ascontiguousarray(np.atleast_1d(beta), dtype=np.float64)
+        out = np.zeros(max(self.n, 1))
+        it = ctypes.c_int64()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_katz(self.h, alpha, _ptr(b), len(b), mode, int(weighted), loops,
+                          int(normalized), tol, max_iter, threads, _ptr(out), ctypes.byref(it),
+                          err, ERR_LEN):
+            raise OracleError(err.value.decode())
+        self.last_iters = it.value
+        return out[: self.n]
+
+    def bonacich(self, exponent=1.0, mode=1, weighted=False, loops=2, rescale=False, tol=0.0,
+                 max_iter=0, threads=0):
+        """net_bonacich_power (spectral.rs:596-655)."""
+        out = np.zeros(max(self.n, 1))
+        it = ctypes.c_int64()
+        dense = ctypes.c_int32()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_bonacich_power(self.h, exponent, mode, int(weighted), loops, int(rescale),
+                                    tol, max_iter, threads, _ptr(out), ctypes.byref(it),
+                                    ctypes.byref(dense), err, ERR_LEN):
+            raise OracleError(err.value.decode())
+        self.last_iters = it.value
+        self.last_dense = bool(dense.value)
+        return out[: self.n]
 
 
 def symmetric_eigen(a: np.ndarray):

@@ -235,6 +235,56 @@ int32_t orc_eigenvector(const OrcGraph* h, int32_t mode, int32_t weighted, int32
                             eigenvalue, connected, nullptr, err, err_len);
 }
 
+// net_katz / net_bonacich_power (crates/capi/src/spectral.rs:107-179), plus
+// the iteration count and (Bonacich) whether the dense solve was used.
+int32_t orc_katz(const OrcGraph* h, double alpha, const double* beta, int64_t beta_len,
+                 int32_t mode, int32_t weighted, int32_t loops, int32_t normalized, double tol,
+                 int64_t max_iter, int32_t threads, double* out, int64_t* iters, char* err,
+                 size_t err_len) {
+  return guard(err, err_len, [&] {
+    const Graph& g = handle(h);
+    if (beta_len < 0) throw Error{"beta length must be nonnegative"};
+    KatzOptions o;
+    o.alpha = alpha;
+    o.beta.assign(beta, beta + beta_len);
+    o.mode = mode_from_code(mode);
+    o.weighted = weighted != 0;
+    o.loops = loops_from_code(loops);
+    o.normalized = normalized != 0;
+    o.tol = tol > 0 ? tol : 1e-12;
+    o.max_iter = max_iter > 0 ? (size_t)max_iter : 10000;
+    o.threads = threads > 0 ? (size_t)threads : 0;
+    size_t it = 0;
+    std::vector<double> x = katz(g, o, &it);
+    if (!x.empty()) memcpy(out, x.data(), x.size() * 8);
+    if (iters) *iters = (int64_t)it;
+  });
+}
+
+int32_t orc_bonacich_power(const OrcGraph* h, double exponent, int32_t mode, int32_t weighted,
+                           int32_t loops, int32_t rescale, double tol, int64_t max_iter,
+                           int32_t threads, double* out, int64_t* iters, int32_t* dense,
+                           char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    const Graph& g = handle(h);
+    BonacichOptions o;
+    o.exponent = exponent;
+    o.mode = mode_from_code(mode);
+    o.weighted = weighted != 0;
+    o.loops = loops_from_code(loops);
+    o.rescale = rescale != 0;
+    o.tol = tol > 0 ? tol : 1e-12;
+    o.max_iter = max_iter > 0 ? (size_t)max_iter : 10000;
+    o.threads = threads > 0 ? (size_t)threads : 0;
+    size_t it = 0;
+    bool dn = false;
+    std::vector<double> x = bonacich_power(g, o, &it, &dn);
+    if (!x.empty()) memcpy(out, x.data(), x.size() * 8);
+    if (iters) *iters = (int64_t)it;
+    if (dense) *dense = dn ? 1 : 0;
+  });
+}
+
 // Eigenvalues ascending and eigenvectors (columns of the row-major n x n
 // `vecs`) of the symmetric matrix `a`; 1 if the QL iteration fails.
 int32_t orc_symmetric_eigen(int64_t n, const double* a, double* vals, double* vecs) {

@@ -26,13 +26,17 @@ import yaml
 
 HERE = Path(__file__).resolve().parent
 
-# Variants on the spectral-centrality path. Variants that first simplify or
-# symmetrize the network through net_graph_simplify (eigenvector_sna,
-# eigenvector_ucinet) are outside it.
+# Variants on the spectral-centrality path: PageRank, Katz and Bonacich power
+# centrality (spectral.yaml), eigenvector centrality (topography.yaml).
+# Variants that first simplify or symmetrize the network through
+# net_graph_simplify (eigenvector_sna, eigenvector_ucinet, bonacich_sna) are
+# outside it.
 VARIANTS = {
     "spectral.yaml": ["pagerank", "pagerank_networkx", "pagerank_weighted",
                       "pagerank_personalized", "pagerank_personalized_networkx",
-                      "pagerank_uniform_dangling", "pagerank_undirected"],
+                      "pagerank_uniform_dangling", "pagerank_undirected",
+                      "katz", "katz_weighted", "katz_igraph", "katz_exogenous",
+                      "bonacich", "bonacich_negative", "bonacich_unit", "bonacich_rescale"],
     "topography.yaml": ["eigenvector", "eigenvector_networkx", "eigenvector_weighted",
                         "eigenvector_weighted_networkx", "eigenvector_undirected"],
 }
@@ -106,7 +110,8 @@ def main():
     doc = {
         "about": "validation fixtures and golden values of the reference engine "
                  "(validation/fixtures, validation/golden/{definition,networkx}) for "
-                 "PageRank and eigenvector centrality; generated by make_golden.py",
+                 "PageRank, Katz, Bonacich power and eigenvector centrality; generated "
+                 "by make_golden.py",
         "oracle_versions": versions,
         "manifest": manifest,
         "fixtures": fixtures,

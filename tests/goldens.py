@@ -64,8 +64,35 @@ def make_graph(graph_cls, fx: dict):
                      np.asarray(fx["tgt"], dtype=np.int64), w, fx["directed"])
 
 
+def spectral_radius(g, mode: str, weighted: bool, loops: str) -> float:
+    """Largest eigenvalue of the matrix a measure uses, from the engine's own
+    eigenvector centrality (validation/bindings/spectral.py:140-151)."""
+    _, lam, _ = g.eigenvector(mode=MODES[mode], weighted=weighted, scale=0, loops=LOOPS[loops])
+    return lam
+
+
+def relative(e: dict, key: str, g, mode: str, weighted: bool, loops: str) -> float:
+    """`key` as given, or `key_fraction` / lambda_max
+    (validation/bindings/spectral.py:154-161)."""
+    if key in e:
+        return float(e[key])
+    lam = spectral_radius(g, mode, weighted, loops)
+    if lam <= 0.0:
+        return float(e[key + "_fraction"])
+    return float(e[key + "_fraction"]) / lam
+
+
 def run_variant(g, fx: dict, variant: str):
-    """Runs the manifest's engine options for `variant` on graph `g`."""
+    """Runs the manifest's engine options for `variant` on graph `g`; a
+    measure the engine rejects gives an empty vector, as in the reference's
+    harness (validation/bindings/spectral.py:163-169)."""
+    try:
+        return _run_variant(g, fx, variant)
+    except RuntimeError:  # the engines' error types derive from RuntimeError
+        return []
+
+
+def _run_variant(g, fx: dict, variant: str):
     e = load()["manifest"][variant]["engine"]
     n = fx["n"]
     if e["fn"] == "pagerank":
@@ -82,6 +109,20 @@ def run_variant(g, fx: dict, variant: str):
                                    scale=SCALES[e.get("scale", "max")],
                                    loops=LOOPS[e.get("loops", "twice")])
         return vals
+    if e["fn"] == "katz":
+        mode, weighted, loops = e.get("mode", "in"), bool(e.get("weighted", False)), \
+            e.get("loops", "once")
+        alpha = relative(e, "alpha", g, mode, weighted, loops)
+        b = e.get("beta", 1.0)
+        beta = np.asarray(node_rule(b, n) if isinstance(b, str) else [float(b)])
+        return g.katz(alpha=alpha, beta=beta, mode=MODES[mode], weighted=weighted,
+                      loops=LOOPS[loops], normalized=bool(e.get("normalized", True)))
+    if e["fn"] == "bonacich":
+        mode, weighted, loops = e.get("mode", "out"), bool(e.get("weighted", False)), \
+            e.get("loops", "ignore")
+        exponent = relative(e, "exponent", g, "in" if mode == "out" else mode, weighted, loops)
+        return g.bonacich(exponent=exponent, mode=MODES[mode], weighted=weighted,
+                          loops=LOOPS[loops], rescale=bool(e.get("rescale", False)))
     raise ValueError(e["fn"])
 
 

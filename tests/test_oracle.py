@@ -329,3 +329,53 @@ def test_rmat_quadrant_frequencies():
     q = s * 2 + t
     freq = np.bincount(q, minlength=4) / len(q)
     assert np.allclose(freq, [0.57, 0.19, 0.19, 0.05], atol=0.01)
+
+
+# ------------------------------------------------------------------ Katz, Bonacich
+def katz_bonacich_known_answers(G, err):
+    """The reference's hand values (crates/engine/src/metrics/spectral.rs:
+    992-1040), on an engine whose graphs are built by G(n, src, tgt, w,
+    directed) and whose failures raise `err`."""
+    # 0 -> 1 -> 2: x = 1 + alpha A^T x gives 1, 1 + a, 1 + a + a^2
+    dag = G(3, [0, 1], [1, 2], None, True)
+    assert np.array_equal(dag.katz(alpha=10.0, normalized=False), [1.0, 11.0, 111.0])
+    small = G(5, [0, 0, 1, 2, 3, 2], [1, 2, 2, 0, 2, 4], None, True)
+    want = [1.3445378151, 1.2689075630, 1.7226890756, 1.0, 1.3445378151]
+    assert np.allclose(small.katz(alpha=0.2, normalized=False, loops=2), want, atol=1e-9, rtol=0)
+    with pytest.raises(err, match="lambda_max"):
+        small.katz(alpha=0.76, normalized=False, loops=2)
+    # star around 0 with an extra edge 1 - 4
+    star = G(5, [0, 0, 0, 1], [1, 2, 3, 4], None, False)
+    assert np.allclose(star.bonacich(exponent=0.5),
+                       [1.4696735043, 1.1238679739, 0.7780624435, 0.7780624435, 0.6051596782],
+                       atol=1e-9, rtol=0)
+    assert np.allclose(star.bonacich(exponent=-0.5),
+                       [1.8605210188, -0.6201736729, -0.6201736729, -0.6201736729,
+                        0.6201736729], atol=1e-9, rtol=0)
+    assert abs(star.bonacich(exponent=0.5, rescale=True).sum() - 1.0) < 1e-12
+    # exponent 1 lies beyond 1 / lambda_max (about 1.9): the dense solve,
+    # (I - A) y proportional to A 1, squares summing to n
+    y = star.bonacich(exponent=1.0)
+    a = np.zeros((5, 5))
+    for s, t in ((0, 1), (0, 2), (0, 3), (1, 4)):
+        a[s, t] = a[t, s] = 1.0
+    lhs, rhs = (np.eye(5) - a) @ y, a @ np.ones(5)
+    k = lhs @ rhs / (rhs @ rhs)
+    assert np.allclose(lhs, k * rhs, atol=1e-9)
+    assert abs((y * y).sum() - 5.0) < 1e-9
+    # errors the reference raises
+    with pytest.raises(err, match="alpha"):
+        small.katz(alpha=-1.0)
+    with pytest.raises(err):
+        small.katz(alpha=0.1, beta=[1.0, 2.0])
+    with pytest.raises(err, match="finite"):
+        star.bonacich(exponent=float("inf"))
+
+
+def test_oracle_katz_bonacich_known_answers():
+    katz_bonacich_known_answers(O.Graph, O.OracleError)
+    g = O.Graph(5, [0, 0, 0, 1], [1, 2, 3, 4], None, False)
+    g.bonacich(exponent=1.0)
+    assert g.last_dense
+    g.bonacich(exponent=0.5)
+    assert not g.last_dense
