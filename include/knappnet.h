@@ -89,6 +89,15 @@ NET_API int32_t net_bonacich_power(const GraphHandle *h, double exponent, int32_
                                    double tol, int64_t max_iter, int32_t threads,
                                    double *out, char *err, size_t err_len);
 
+/* Hub and authority scores (n doubles each); *value receives the largest
+ * eigenvalue of A^T A, *unique 1 if the leading singular value is simple;
+ * scale 0 largest 1, 1 sum 1, 2 unit norm. Replaces netcapi.h:489-493
+ * (crates/capi/src/spectral.rs:189-230). */
+NET_API int32_t net_hits(const GraphHandle *h, int32_t weighted, int32_t loops, int32_t scale,
+                         double tol, int64_t max_iter, int32_t threads, double *hubs,
+                         double *authorities, double *value, int32_t *unique, char *err,
+                         size_t err_len);
+
 /* Eigenvector centrality; out holds n doubles; *eigenvalue receives the
  * principal eigenvalue and *connected 1 if the graph is (strongly)
  * connected. Replaces netcapi.h:455-459 (crates/capi/src/topography.rs:208-249). */

@@ -84,6 +84,9 @@ def lib() -> ctypes.CDLL:
     L.net_katz.restype = i32
     L.net_bonacich_power.argtypes = [h, f64, i32, i32, i32, i32, f64, i64, i32, vp, cp, sz]
     L.net_bonacich_power.restype = i32
+    L.net_hits.argtypes = [h, i32, i32, i32, f64, i64, i32, vp, vp, ctypes.POINTER(f64),
+                           ctypes.POINTER(i32), cp, sz]
+    L.net_hits.restype = i32
     L.net_pagerank_ex.argtypes = [h, f64, i32, i32, vp, i32, i32, f64, i64, i32, vp, info_p,
                                   cp, sz]
     L.net_pagerank_ex.restype = i32
@@ -320,6 +323,19 @@ class Graph:
                                         int(rescale), tol, max_iter, threads, _ptr(out), err,
                                         ERR_LEN), err)
         return out[: self.n]
+
+    def hits(self, weighted=False, loops=0, scale=0, tol=0.0, max_iter=0, threads=0):
+        """net_hits: hubs, authorities, the largest eigenvalue of A^T A and
+        whether the leading singular value is simple."""
+        hubs = np.zeros(max(self.n, 1))
+        auths = np.zeros(max(self.n, 1))
+        val = ctypes.c_double()
+        uniq = ctypes.c_int32()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_hits(self.h, int(weighted), loops, scale, tol, max_iter, threads,
+                              _ptr(hubs), _ptr(auths), ctypes.byref(val), ctypes.byref(uniq),
+                              err, ERR_LEN), err)
+        return hubs[: self.n], auths[: self.n], val.value, bool(uniq.value)
 
     def eigenvector(self, mode=2, weighted=False, scale=0, loops=0, tol=0.0, max_iter=0,
                     threads=0, precision=0):

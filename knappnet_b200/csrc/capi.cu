@@ -445,6 +445,38 @@ int32_t net_bonacich_power(const GraphHandle* h, double exponent, int32_t mode, 
   });
 }
 
+// net_hits: codes decoded as crates/capi/src/spectral.rs:189-230.
+int32_t net_hits(const GraphHandle* h, int32_t weighted, int32_t loops, int32_t scale, double tol,
+                 int64_t max_iter, int32_t threads, double* hubs, double* authorities,
+                 double* value, int32_t* unique, char* err, size_t err_len) {
+  (void)threads;
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (scale < 0 || scale > 2)
+      throw Error("unknown hub and authority scale code " + std::to_string(scale));
+    knb::HitsParams p;
+    p.weighted = weighted != 0;
+    p.loops = loops;
+    p.scale = scale;
+    p.tol = tol > 0 ? tol : 1e-12;
+    p.max_iter = max_iter > 0 ? max_iter : 10000;
+    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
+    cudaStream_t s = knb::thread_stream();
+    if (p.weighted) check_nonnegative(g, "hub and authority scores", s);
+    double v = 0.0;
+    int u = 0;
+    if (g.n == 0) {
+      v = 0.0;
+      u = 0;
+    } else {
+      knb::hits(g, p, hubs, authorities, &v, &u, s);
+    }
+    if (value) *value = v;
+    if (unique) *unique = u;
+  });
+}
+
 int32_t net_eigenvector(const GraphHandle* h, int32_t mode, int32_t weighted, int32_t scale,
                         int32_t loops, double tol, int64_t max_iter, int32_t threads, double* out,
                         double* eigenvalue, int32_t* connected, char* err, size_t err_len) {

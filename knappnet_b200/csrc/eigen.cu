@@ -397,6 +397,43 @@ __global__ void sub_copy(OpView<double> op, const uint32_t* __restrict__ nodes, 
   }
 }
 
+// Submatrices that keep only the entries whose column is mapped (local[c]
+// != 2^32 - 1), as SparseOp::submatrix (eigenvector.rs:589-624).
+__global__ void sub_lengths_mapped(OpView<double> op, const uint32_t* __restrict__ nodes,
+                                   uint32_t k, const uint32_t* __restrict__ local,
+                                   uint32_t* __restrict__ len) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    const uint32_t v = nodes[i];
+    uint32_t c = 0;
+    for (uint32_t q = op.off[v]; q < op.off[v + 1]; ++q) c += local[op.cols[q]] != 0xFFFFFFFFu;
+    len[i] = c;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) len[k] = 0;
+}
+
+__global__ void sub_copy_mapped(OpView<double> op, const uint32_t* __restrict__ nodes,
+                                uint32_t k, const uint32_t* __restrict__ local,
+                                const uint32_t* __restrict__ soff, uint32_t* __restrict__ scols,
+                                double* __restrict__ s64) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+    const uint32_t v = nodes[i];
+    uint32_t o = soff[i];
+    for (uint32_t q = op.off[v]; q < op.off[v + 1]; ++q) {
+      const uint32_t c = local[op.cols[q]];
+      if (c == 0xFFFFFFFFu) continue;
+      scols[o] = c;
+      if (s64) s64[o] = op.vals ? op.vals[q] : 1.0;
+      ++o;
+    }
+  }
+}
+
+__global__ void unscatter_local(const uint32_t* __restrict__ nodes, uint32_t k,
+                                uint32_t* __restrict__ local) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
+    local[nodes[i]] = 0xFFFFFFFFu;
+}
+
 __global__ void scatter_local(const uint32_t* __restrict__ nodes, uint32_t k,
                               uint32_t* __restrict__ local) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
@@ -856,10 +893,16 @@ struct Leading {
 
 // Thick-restart Lanczos (eigenvector.rs:746-878) on device operator A from
 // the all-ones vector; the unit eigenvector is left in `xout` (device).
+// With B given, the operator is B A (HITS: A_b^T A_b), applied as two
+// products in FP64; with `start` given (device, dim values), the process
+// starts from it instead of the all-ones vector.
 static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t max_matvecs,
                               bool mixed, double* xout, Leading* res, int* launches,
-                              cudaStream_t s) {
-  const size_t dim = A.n;
+                              cudaStream_t s, const DevOp* B = nullptr,
+                              const double* start = nullptr) {
+  const size_t dim = B ? B->n : A.n;
+  if (B) mixed = false;
+  DevBuf<double> tmp(B ? std::max<size_t>(A.n, 1) : 0);
   const int m = (int)std::max<size_t>(
       1, std::min<size_t>(std::min<size_t>(dim, MAXB), std::max<size_t>((1ull << 27) / dim, 8)));
   const int keep = std::max(1, std::min(8, m >= 2 ? m - 2 : 0));
@@ -872,6 +915,7 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
   DevBuf<LzState> st(1);
   DevBuf<IterState> ist(1);
   SpmvScratch sc;
+  if (B) sc.ensure(std::max(A.part->ntiles, B->part->ntiles));  // no growth between products
   LzState* hst = nullptr;
   KNB_CUDA(cudaMallocHost(&hst, sizeof(LzState)));
   struct F {
@@ -885,8 +929,16 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
   KNB_CUDA(cudaMemsetAsync(st.get(), 0, sizeof(LzState), s));
   KNB_CUDA(cudaMemsetAsync(ist.get(), 0, sizeof(IterState), s));
   KNB_CUDA(cudaMemsetAsync(hm_d.get(), 0, (size_t)m * m * 8, s));
-  // v0 = ones / ||ones|| (blocked norm as the reference's Blocks::dot)
-  fill_value<<<gv, 256, 0, s>>>(x.get(), (uint32_t)dim, 1.0);
+  auto apply = [&](const double* xin, const float* x32in, double* yout,
+                   const IterState* istp) -> int {
+    if (!B) return spmv(A, xin, x32in, yout, sc, istp, s);
+    const int l = spmv(A, xin, nullptr, tmp.get(), sc, istp, s);
+    return l + spmv(*B, tmp.get(), nullptr, yout, sc, istp, s);
+  };
+  // v0 = start / ||start|| (blocked norm as the reference's Blocks::dot),
+  // start = ones unless given
+  if (start) KNB_CUDA(cudaMemcpyAsync(x.get(), start, dim * 8, cudaMemcpyDeviceToDevice, s));
+  else fill_value<<<gv, 256, 0, s>>>(x.get(), (uint32_t)dim, 1.0);
   lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
   read_state();
   const double norm0 = std::sqrt(hst->xx);
@@ -917,7 +969,7 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
         }
         const double* vj = V.get() + (size_t)jj * dim;
         lz_begin<<<1, 32, 0, s>>>(st.get(), ist.get());
-        *launches += 1 + spmv(A, vj, use32 ? v32.get() : nullptr, w.get(), sc, ist.get(), s);
+        *launches += 1 + apply(vj, use32 ? v32.get() : nullptr, w.get(), ist.get());
         const int cols = jj + 1, lo = cols >= 2 ? cols - 2 : 0;
         lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
         lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
@@ -990,7 +1042,7 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
         KNB_CUDA(cudaMemcpyAsync(svec.get(), cf.data(), size * 8, cudaMemcpyHostToDevice, s));
         lz_combine<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), x.get());
         if (matvecs >= max_matvecs) return false;
-        *launches += 1 + spmv(A, x.get(), nullptr, y.get(), sc, nullptr, s);
+        *launches += 1 + apply(x.get(), nullptr, y.get(), nullptr);
         ++matvecs;
         lz_dots<<<nb, VB_T, 0, s>>>(x.get(), y.get(), dim, part.get(), st.get());
         lz_resid<<<gv, VB_T, 0, s>>>(x.get(), y.get(), dim, part.get(), st.get());
@@ -1069,6 +1121,258 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
       ++j;
     }
   }
+}
+
+// ======================================================================= HITS
+static std::string fmt_g(double v);
+
+namespace {
+
+// The rows `nodes` of `op` with columns renumbered by `local` (device, all
+// 2^32 - 1 outside the submatrix); FP64 values (1 when op has none).
+void mapped_submatrix(const OpView<double>& op, const std::vector<uint32_t>& nodes,
+                      const uint32_t* local, DevBuf<uint32_t>& nodes_d, DevOp& A,
+                      cudaStream_t s) {
+  const uint32_t kn = (uint32_t)nodes.size();
+  KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), nodes.data(), (size_t)kn * 4, cudaMemcpyHostToDevice,
+                           s));
+  A.own_off.alloc((size_t)kn + 1);
+  sub_lengths_mapped<<<grid_for(kn + 1, 256), 256, 0, s>>>(op, nodes_d.get(), kn, local,
+                                                           A.own_off.get());
+  const uint64_t nnz =
+      exclusive_scan<uint32_t>(A.own_off.get(), A.own_off.get(), (size_t)kn + 1, s);
+  A.n = kn;
+  A.nnz = nnz;
+  A.own_cols.alloc(std::max<uint64_t>(nnz, 1));
+  A.own_v64.alloc(std::max<uint64_t>(nnz, 1));
+  sub_copy_mapped<<<grid_for(kn, 128), 128, 0, s>>>(op, nodes_d.get(), kn, local,
+                                                    A.own_off.get(), A.own_cols.get(),
+                                                    A.own_v64.get());
+  KNB_LAUNCH("mapped submatrix");
+  A.off = A.own_off.get();
+  A.cols = A.own_cols.get();
+  A.v64 = A.own_v64.get();
+  A.v32 = nullptr;
+  A.own_part = build_partition(kn, nnz, A.off, SPMV_THREADS * EIG_IPT, s);
+  A.part = A.own_part.get();
+}
+
+void host_csr(const Operator& op, std::vector<uint32_t>* off, std::vector<uint32_t>* cols,
+              std::vector<double>* vals, cudaStream_t s) {
+  off->resize((size_t)op.n + 1);
+  cols->resize(op.nnz);
+  KNB_CUDA(cudaMemcpyAsync(off->data(), op.rows->off.get(), ((size_t)op.n + 1) * 4,
+                           cudaMemcpyDeviceToHost, s));
+  if (op.nnz)
+    KNB_CUDA(cudaMemcpyAsync(cols->data(), op.rows->tgt.get(), op.nnz * 4,
+                             cudaMemcpyDeviceToHost, s));
+  vals->clear();
+  if (op.has_vals) {
+    vals->resize(op.nnz);
+    if (op.nnz)
+      KNB_CUDA(cudaMemcpyAsync(vals->data(), op.vals64.get(), op.nnz * 8, cudaMemcpyDeviceToHost,
+                               s));
+  }
+  KNB_CUDA(cudaStreamSynchronize(s));
+}
+
+void hits_rescale(std::vector<double>& x, int how) {
+  for (double& v : x)
+    if (v < 0.0) v = 0.0;
+  double d = 0.0;
+  if (how == 0) {
+    for (double v : x) d = std::max(d, v);
+  } else if (how == 1) {
+    for (double v : x) d += v;
+  } else {
+    for (double v : x) d += v * v;
+    d = std::sqrt(d);
+  }
+  if (d > 0.0)
+    for (double& v : x) v /= d;
+}
+
+}  // namespace
+
+void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* auth_out,
+          double* value, int* unique, cudaStream_t s) {
+  const uint32_t n = g.n;
+  // A: rows are arcs out of each node (matrix(g, Out, ...)); A^T: the in-CSR
+  // of a directed graph (the reference's stable transpose has the same
+  // entry order), A itself for an undirected one.
+  const bool hdir = g.directed;
+  const double lf = p.loops == 2 ? 0.0 : (!hdir && p.loops == 0 ? 2.0 : 1.0);
+  Operator& A = g.op(0, p.weighted, lf, s);
+  Operator& At = hdir ? g.op(1, p.weighted, lf, s) : A;
+  std::vector<uint32_t> aoff, acols, toff, tcols;
+  std::vector<double> avals, tvals;
+  host_csr(A, &aoff, &acols, &avals, s);
+  if (hdir) host_csr(At, &toff, &tcols, &tvals, s);
+  const std::vector<uint32_t>& Toff = hdir ? toff : aoff;
+  const std::vector<uint32_t>& Tcols = hdir ? tcols : acols;
+  const std::vector<double>& Tvals = hdir ? tvals : avals;
+  auto av = [&](uint64_t k) { return avals.empty() ? 1.0 : avals[k]; };
+  auto tv = [&](uint64_t k) { return Tvals.empty() ? 1.0 : Tvals[k]; };
+  // blocks of the bipartite graph (hubs 0..n, authorities n..2n) joined by
+  // positive entries (spectral.rs:757-813)
+  std::vector<uint32_t> parent(2 * (size_t)n);
+  std::iota(parent.begin(), parent.end(), 0u);
+  auto find = [&](uint32_t v) {
+    while (parent[v] != v) {
+      parent[v] = parent[parent[v]];
+      v = parent[v];
+    }
+    return v;
+  };
+  bool any = false;
+  std::vector<char> has_in(n, 0), has_out(n, 0);
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint64_t k = aoff[i]; k < aoff[i + 1]; ++k)
+      if (av(k) > 0.0) {
+        any = true;
+        has_out[i] = 1;
+        has_in[acols[k]] = 1;
+        const uint32_t x = find(i), y = find(n + acols[k]);
+        if (x != y) parent[std::max(x, y)] = std::min(x, y);
+      }
+  if (!any) {
+    for (uint32_t i = 0; i < n; ++i) hubs_out[i] = auth_out[i] = std::nan("");
+    *value = 0.0;
+    *unique = 0;
+    return;
+  }
+  std::vector<uint32_t> block_of(2 * (size_t)n, 0xFFFFFFFFu);
+  std::vector<std::vector<uint32_t>> bh, ba;
+  for (uint32_t v = 0; v < 2 * n; ++v) {
+    const bool present = v < n ? has_out[v] : has_in[v - n];
+    if (!present) continue;
+    const uint32_t root = find(v);
+    if (block_of[root] == 0xFFFFFFFFu) {
+      block_of[root] = (uint32_t)bh.size();
+      bh.emplace_back();
+      ba.emplace_back();
+    }
+    (v < n ? bh : ba)[block_of[root]].push_back(v < n ? v : v - n);
+  }
+  // bounds on each block's sigma^2 (spectral.rs:814-836)
+  std::vector<double> row_sum(n, 0.0), col_sum(n, 0.0), col_sq(n, 0.0);
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint64_t k = aoff[i]; k < aoff[i + 1]; ++k) row_sum[i] += av(k);
+  for (uint32_t j = 0; j < n; ++j) {
+    double q = 0.0, acc = 0.0;
+    bool open = false;
+    uint32_t c = 0;
+    for (uint64_t k = Toff[j]; k < Toff[j + 1]; ++k) {
+      col_sum[j] += tv(k);
+      if (open && Tcols[k] == c) {
+        acc += tv(k);
+      } else {
+        if (open) q += acc * acc;
+        c = Tcols[k];
+        acc = tv(k);
+        open = true;
+      }
+    }
+    if (open) q += acc * acc;
+    col_sq[j] = q;
+  }
+  const size_t kb = bh.size();
+  std::vector<double> upper(kb, 0.0), lower(kb, 0.0);
+  for (size_t b = 0; b < kb; ++b) {
+    double rm = 0.0, cm = 0.0, lm = 0.0;
+    for (uint32_t i : bh[b]) rm = std::max(rm, row_sum[i]);
+    for (uint32_t j : ba[b]) {
+      cm = std::max(cm, col_sum[j]);
+      lm = std::max(lm, col_sq[j]);
+    }
+    upper[b] = rm * cm;
+    lower[b] = lm;
+  }
+  std::vector<size_t> order(kb);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return lower[x] > lower[y]; });
+  // leading eigenpair of each block that may hold the largest value
+  DevBuf<uint32_t> hub_index(n), auth_index(n), nodes_h(n), nodes_a(n);
+  KNB_CUDA(cudaMemsetAsync(hub_index.get(), 0xFF, (size_t)n * 4, s));
+  KNB_CUDA(cudaMemsetAsync(auth_index.get(), 0xFF, (size_t)n * 4, s));
+  const OpView<double> a64{A.n, A.nnz, A.rows->off.get(), A.rows->tgt.get(),
+                           A.has_vals ? A.vals64.get() : nullptr};
+  const OpView<double> t64{At.n, At.nnz, At.rows->off.get(), At.rows->tgt.get(),
+                           At.has_vals ? At.vals64.get() : nullptr};
+  const double TIE = 1e-9;
+  double best = 0.0;
+  struct Solved {
+    size_t b;
+    double value;
+    std::vector<double> v, sv;
+  };
+  std::vector<Solved> solved;
+  int launches = 0;
+  for (size_t b : order) {
+    if (upper[b] < best * (1.0 - TIE)) continue;
+    const uint32_t nh = (uint32_t)bh[b].size(), na = (uint32_t)ba[b].size();
+    KNB_CUDA(cudaMemcpyAsync(nodes_h.get(), bh[b].data(), (size_t)nh * 4, cudaMemcpyHostToDevice, s));
+    KNB_CUDA(cudaMemcpyAsync(nodes_a.get(), ba[b].data(), (size_t)na * 4, cudaMemcpyHostToDevice, s));
+    scatter_local<<<grid_for(nh, 256), 256, 0, s>>>(nodes_h.get(), nh, hub_index.get());
+    scatter_local<<<grid_for(na, 256), 256, 0, s>>>(nodes_a.get(), na, auth_index.get());
+    DevOp ab, abt;
+    DevBuf<uint32_t> tmp_nodes(std::max(nh, na));
+    mapped_submatrix(a64, bh[b], auth_index.get(), tmp_nodes, ab, s);
+    mapped_submatrix(t64, ba[b], hub_index.get(), tmp_nodes, abt, s);
+    unscatter_local<<<grid_for(nh, 256), 256, 0, s>>>(nodes_h.get(), nh, hub_index.get());
+    unscatter_local<<<grid_for(na, 256), 256, 0, s>>>(nodes_a.get(), na, auth_index.get());
+    // Kleinberg's first authority vector A_b^T 1
+    DevBuf<double> ones(std::max<uint32_t>(nh, 1)), sdev(std::max<uint32_t>(na, 1)), vdev(na);
+    fill_value<<<grid_for(nh, 256), 256, 0, s>>>(ones.get(), nh, 1.0);
+    SpmvScratch sc;
+    launches += 6 + spmv(abt, ones.get(), nullptr, sdev.get(), sc, nullptr, s);
+    Leading res;
+    if (!symmetric_leading(ab, p.tol, 0.0, p.max_iter, false, vdev.get(), &res, &launches, s,
+                           &abt, sdev.get()))
+      throw Error("hub and authority scores did not converge to tolerance " + fmt_g(p.tol) +
+                  " within " + std::to_string(p.max_iter) +
+                  " matrix-vector products; a larger iteration cap may help");
+    Solved sol;
+    sol.b = b;
+    sol.value = res.value;
+    sol.v.resize(na);
+    sol.sv.resize(na);
+    KNB_CUDA(cudaMemcpyAsync(sol.v.data(), vdev.get(), (size_t)na * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(sol.sv.data(), sdev.get(), (size_t)na * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    best = std::max(best, res.value);
+    solved.push_back(std::move(sol));
+  }
+  std::vector<double> auth(n, 0.0);
+  int tied = 0;
+  for (const Solved& sol : solved) {
+    if (sol.value < best * (1.0 - TIE)) continue;
+    ++tied;
+    double weight = 0.0;
+    for (size_t i = 0; i < sol.v.size(); ++i) weight += sol.v[i] * sol.sv[i];
+    for (size_t i = 0; i < ba[sol.b].size(); ++i) auth[ba[sol.b][i]] = sol.v[i] * weight;
+  }
+  // hubs = A auth (device product)
+  DevBuf<double> ad(n), hd(n);
+  KNB_CUDA(cudaMemcpyAsync(ad.get(), auth.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+  DevOp full;
+  full.n = A.n;
+  full.nnz = A.nnz;
+  full.off = A.rows->off.get();
+  full.cols = A.rows->tgt.get();
+  full.v64 = A.has_vals ? A.vals64.get() : nullptr;
+  full.part = &A.partition(SPMV_THREADS * EIG_IPT, s);
+  SpmvScratch sc;
+  spmv(full, ad.get(), nullptr, hd.get(), sc, nullptr, s);
+  std::vector<double> hubs(n);
+  KNB_CUDA(cudaMemcpyAsync(hubs.data(), hd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  hits_rescale(auth, p.scale);
+  hits_rescale(hubs, p.scale);
+  memcpy(hubs_out, hubs.data(), (size_t)n * 8);
+  memcpy(auth_out, auth.data(), (size_t)n * 8);
+  *value = best;
+  *unique = tied == 1 ? 1 : 0;
 }
 
 // ======================================================================= driver

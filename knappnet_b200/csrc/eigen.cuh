@@ -45,6 +45,22 @@ Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint
 void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenResult* r,
                  cudaStream_t s);
 
+// Hubs and authorities (reference: crates/engine/src/metrics/spectral.rs:
+// 676-903): blocks of the bipartite hub-authority graph, bounds on each
+// block's leading value, thick-restart Lanczos on A_b^T A_b from A_b^T 1
+// for the blocks that may hold the largest, ties combined. Writes n hub and
+// n authority scores (host), the largest eigenvalue of A^T A and whether
+// the leading singular value is simple.
+struct HitsParams {
+  bool weighted = false;
+  int loops = 0;   // 0 twice, 1 once, 2 ignore
+  int scale = 0;   // 0 largest 1, 1 sum 1, 2 unit norm
+  double tol = 1e-12;
+  int64_t max_iter = 10000;
+};
+void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs, double* auths, double* value,
+          int* unique, cudaStream_t s);
+
 // Dense symmetric eigensolver for the projected Lanczos problems: EISPACK
 // tred2 + tql2 order (reference: crates/engine/src/linalg.rs:478-720).
 // a is row-major n x n; eigenvalues ascending, eigenvectors in the columns of

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <numeric>
 #include <thread>
@@ -817,10 +818,11 @@ static Leading finish_vector(std::vector<double> x, double value, size_t matvecs
   return Leading{value, std::move(x), matvecs};
 }
 
-// eigenvector.rs:746-878.
-static bool symmetric_leading(const SparseOp& a, const std::vector<double>& start, double tol,
-                              double shift, size_t max_matvecs, Leading* res) {
-  size_t dim = a.dim();
+// eigenvector.rs:746-878: the operator is given as `apply` (y = M x) on
+// vectors of `dim` entries.
+using Apply = std::function<void(const double*, double*)>;
+static bool symmetric_leading(size_t dim, const Apply& apply, const std::vector<double>& start,
+                              double tol, double shift, size_t max_matvecs, Leading* res) {
   size_t m = std::max<size_t>(
       1, std::min(std::min(dim, MAX_BASIS), std::max<size_t>(MAX_BASIS_DOUBLES / dim, 8)));
   size_t keep = std::max<size_t>(1, std::min(KEEP, m >= 2 ? m - 2 : 0));
@@ -840,7 +842,7 @@ static bool symmetric_leading(const SparseOp& a, const std::vector<double>& star
     bool restart = false;
     while (!restart) {
       if (matvecs >= max_matvecs) return false;
-      a.apply(v.data(), w.data());
+      apply(v.data(), w.data());
       ++matvecs;
       double before, beta;
       basis.orthogonalize(j + 1, w.data(), blocks, &coef, &before, &beta);
@@ -863,7 +865,7 @@ static bool symmetric_leading(const SparseOp& a, const std::vector<double>& star
           for (size_t l = 0; l < size; ++l) cf[l] = s[l * size + top];
           std::vector<double> x = basis.combine(size, cf);
           if (matvecs >= max_matvecs) return false;
-          a.apply(x.data(), y.data());
+          apply(x.data(), y.data());
           ++matvecs;
           double xx = blocks.dot(x.data(), x.data());
           double value = blocks.dot(x.data(), y.data()) / xx;
@@ -1017,7 +1019,8 @@ static std::vector<double> symmetric_components(const Graph& h, const SparseOp& 
     }
     std::vector<double> ones(nodes.size(), 1.0);
     Leading res;
-    if (!symmetric_leading(*a, ones, o.tol, 1.0, o.max_iter, &res))
+    if (!symmetric_leading(a->dim(), [a](const double* x, double* y) { a->apply(x, y); }, ones,
+                           o.tol, 1.0, o.max_iter, &res))
       throw Error{"eigenvector centrality did not converge to tolerance " + fmt_g(o.tol) +
                   " within " + std::to_string(o.max_iter) +
                   " matrix-vector products; a larger iteration cap may help"};
@@ -1336,6 +1339,196 @@ std::vector<double> bonacich_power(const Graph& g, const BonacichOptions& o, siz
     for (double& v : y) v *= alpha;
   }
   return y;
+}
+
+// ======================================================== HITS
+// SparseOp::transpose (eigenvector.rs:627-656): a stable counting sort by
+// column, so row j lists the rows holding column j in increasing order.
+static SparseOp transpose_op(const SparseOp& a, size_t ncol) {
+  SparseOp t;
+  t.has_vals = a.has_vals;
+  t.threads = a.threads;
+  t.off.assign(ncol + 1, 0);
+  for (uint32_t j : a.cols) t.off[j + 1] += 1;
+  for (size_t c = 0; c < ncol; ++c) t.off[c + 1] += t.off[c];
+  std::vector<uint64_t> cur(t.off.begin(), t.off.end() - 1);
+  t.cols.assign(a.cols.size(), 0);
+  if (a.has_vals) t.vals.assign(a.cols.size(), 0.0);
+  for (size_t v = 0; v < a.dim(); ++v)
+    for (uint64_t k = a.off[v]; k < a.off[v + 1]; ++k) {
+      const uint64_t slot = cur[a.cols[k]]++;
+      t.cols[slot] = (uint32_t)v;
+      if (a.has_vals) t.vals[slot] = a.vals[k];
+    }
+  return t;
+}
+
+static double entry(const SparseOp& a, uint64_t k) { return a.has_vals ? a.vals[k] : 1.0; }
+
+// spectral.rs:905-922: sum of squares of row v, parallel entries merged.
+static double merged_squares(const SparseOp& a, size_t v) {
+  double q = 0.0, acc = 0.0;
+  bool open = false;
+  uint32_t c = 0;
+  for (uint64_t k = a.off[v]; k < a.off[v + 1]; ++k) {
+    if (open && a.cols[k] == c) {
+      acc += entry(a, k);
+    } else {
+      if (open) q += acc * acc;
+      c = a.cols[k];
+      acc = entry(a, k);
+      open = true;
+    }
+  }
+  if (open) q += acc * acc;
+  return q;
+}
+
+// spectral.rs:924-938.
+static void hits_rescale(std::vector<double>& x, int how) {
+  for (double& v : x)
+    if (v < 0.0) v = 0.0;
+  double d = 0.0;
+  if (how == 0) {
+    for (double v : x) d = std::max(d, v);
+  } else if (how == 1) {
+    for (double v : x) d += v;
+  } else {
+    for (double v : x) d += v * v;
+    d = std::sqrt(d);
+  }
+  if (d > 0.0)
+    for (double& v : x) v /= d;
+}
+
+// spectral.rs:748-903.
+Hits hits(const Graph& g, const HitsOptions& o) {
+  check_iteration(o.tol, o.max_iter);
+  const size_t n = g.n;
+  if (o.weighted) check_nonnegative(g, "hub and authority scores");
+  Graph holder;
+  SparseOp a = matrix(g, Mode::Out, o.weighted, o.loops, o.threads, &holder);
+  SparseOp at = transpose_op(a, n);
+  // blocks of the bipartite graph (hubs 0..n, authorities n..2n)
+  std::vector<size_t> parent(2 * n);
+  std::iota(parent.begin(), parent.end(), 0);
+  std::function<size_t(size_t)> find = [&](size_t v) {
+    while (parent[v] != v) {
+      parent[v] = parent[parent[v]];
+      v = parent[v];
+    }
+    return v;
+  };
+  bool any = false;
+  for (size_t i = 0; i < n; ++i)
+    for (uint64_t k = a.off[i]; k < a.off[i + 1]; ++k)
+      if (entry(a, k) > 0.0) {
+        any = true;
+        size_t x = find(i), y = find(n + a.cols[k]);
+        if (x != y) parent[std::max(x, y)] = std::min(x, y);
+      }
+  Hits r;
+  if (!any) {
+    r.hubs.assign(n, std::numeric_limits<double>::quiet_NaN());
+    r.authorities.assign(n, std::numeric_limits<double>::quiet_NaN());
+    r.value = 0.0;
+    r.unique = false;
+    return r;
+  }
+  std::vector<char> has_in(n, 0), has_out(n, 0);
+  for (size_t j = 0; j < n; ++j)
+    for (uint64_t k = at.off[j]; k < at.off[j + 1]; ++k)
+      if (entry(at, k) > 0.0) has_in[j] = 1;
+  for (size_t i = 0; i < n; ++i)
+    for (uint64_t k = a.off[i]; k < a.off[i + 1]; ++k)
+      if (entry(a, k) > 0.0) has_out[i] = 1;
+  std::vector<size_t> block_of(2 * n, SIZE_MAX);
+  std::vector<std::vector<uint32_t>> bh, ba;
+  for (size_t v = 0; v < 2 * n; ++v) {
+    const bool present = v < n ? has_out[v] : has_in[v - n];
+    if (!present) continue;
+    const size_t root = find(v);
+    if (block_of[root] == SIZE_MAX) {
+      block_of[root] = bh.size();
+      bh.emplace_back();
+      ba.emplace_back();
+    }
+    if (v < n) bh[block_of[root]].push_back((uint32_t)v);
+    else ba[block_of[root]].push_back((uint32_t)(v - n));
+  }
+  std::vector<double> row_sum(n, 0.0), col_sum(n, 0.0), col_sq(n, 0.0);
+  for (size_t i = 0; i < n; ++i)
+    for (uint64_t k = a.off[i]; k < a.off[i + 1]; ++k) row_sum[i] += entry(a, k);
+  for (size_t j = 0; j < n; ++j) {
+    for (uint64_t k = at.off[j]; k < at.off[j + 1]; ++k) col_sum[j] += entry(at, k);
+    col_sq[j] = merged_squares(at, j);
+  }
+  const size_t kb = bh.size();
+  std::vector<double> upper(kb, 0.0), lower(kb, 0.0);
+  for (size_t b = 0; b < kb; ++b) {
+    double rmax = 0.0, cmax = 0.0, lmax = 0.0;
+    for (uint32_t i : bh[b]) rmax = std::max(rmax, row_sum[i]);
+    for (uint32_t j : ba[b]) {
+      cmax = std::max(cmax, col_sum[j]);
+      lmax = std::max(lmax, col_sq[j]);
+    }
+    upper[b] = rmax * cmax;
+    lower[b] = lmax;
+  }
+  std::vector<size_t> order(kb);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t x, size_t y) { return lower[x] > lower[y]; });
+  std::vector<uint32_t> hub_index(n, 0xFFFFFFFFu), auth_index(n, 0xFFFFFFFFu);
+  double best = 0.0;
+  struct Solved {
+    size_t b;
+    double value;
+    std::vector<double> v, s;
+  };
+  std::vector<Solved> solved;
+  for (size_t b : order) {
+    if (upper[b] < best * (1.0 - TIE)) continue;
+    for (size_t i = 0; i < bh[b].size(); ++i) hub_index[bh[b][i]] = (uint32_t)i;
+    for (size_t i = 0; i < ba[b].size(); ++i) auth_index[ba[b][i]] = (uint32_t)i;
+    SparseOp ab = a.submatrix(bh[b], auth_index);
+    SparseOp abt = at.submatrix(ba[b], hub_index);
+    for (uint32_t v : bh[b]) hub_index[v] = 0xFFFFFFFFu;
+    for (uint32_t v : ba[b]) auth_index[v] = 0xFFFFFFFFu;
+    std::vector<double> ones(bh[b].size(), 1.0), sv(ba[b].size(), 0.0);
+    abt.apply(ones.data(), sv.data());
+    std::vector<double> tmp(ab.dim(), 0.0);
+    Leading res;
+    if (!symmetric_leading(ba[b].size(),
+                           [&](const double* x, double* y) {
+                             ab.apply(x, tmp.data());
+                             abt.apply(tmp.data(), y);
+                           },
+                           sv, o.tol, 0.0, o.max_iter, &res))
+      throw Error{"hub and authority scores did not converge to tolerance " + fmt_g(o.tol) +
+                  " within " + std::to_string(o.max_iter) +
+                  " matrix-vector products; a larger iteration cap may help"};
+    best = std::max(best, res.value);
+    solved.push_back({b, res.value, std::move(res.vector), std::move(sv)});
+  }
+  std::vector<double> auth(n, 0.0);
+  size_t tied = 0;
+  for (const Solved& sv : solved) {
+    if (sv.value < best * (1.0 - TIE)) continue;
+    ++tied;
+    double weight = 0.0;
+    for (size_t i = 0; i < sv.v.size(); ++i) weight += sv.v[i] * sv.s[i];
+    for (size_t i = 0; i < ba[sv.b].size(); ++i) auth[ba[sv.b][i]] = sv.v[i] * weight;
+  }
+  std::vector<double> hubs(n, 0.0);
+  a.apply(auth.data(), hubs.data());
+  hits_rescale(auth, o.scale);
+  hits_rescale(hubs, o.scale);
+  r.hubs = std::move(hubs);
+  r.authorities = std::move(auth);
+  r.value = best;
+  r.unique = tied == 1;
+  return r;
 }
 
 // ======================================================== G(n, m)

@@ -174,6 +174,22 @@ struct BonacichOptions {
 std::vector<double> bonacich_power(const Graph& g, const BonacichOptions& o, size_t* iters,
                                    bool* dense);
 
+// spectral.rs:676-746 (HitsScale, HitsOptions, Hits).
+struct HitsOptions {
+  bool weighted = false;
+  Loops loops = Loops::Twice;
+  int scale = 0;  // 0 largest 1, 1 sum 1, 2 unit norm
+  double tol = 1e-12;
+  size_t max_iter = 10000;
+  size_t threads = 0;
+};
+struct Hits {
+  std::vector<double> hubs, authorities;
+  double value = 0;
+  bool unique = false;
+};
+Hits hits(const Graph& g, const HitsOptions& o);
+
 // linalg.rs:433-467: Gaussian elimination with partial pivoting on the
 // row-major n x n matrix `a`; false when a pivot is at most tol times the
 // largest magnitude of `a`.

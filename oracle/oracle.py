@@ -79,6 +79,9 @@ def lib() -> ctypes.CDLL:
     L.orc_bonacich_power.argtypes = [vp, f64, i32, i32, i32, i32, f64, i64, i32, vp,
                                      ctypes.POINTER(i64), ctypes.POINTER(i32), cp, sz]
     L.orc_bonacich_power.restype = i32
+    L.orc_hits.argtypes = [vp, i32, i32, i32, f64, i64, i32, vp, vp, ctypes.POINTER(f64),
+                           ctypes.POINTER(i32), cp, sz]
+    L.orc_hits.restype = i32
     _lib = L
     return L
 
@@ -225,6 +228,21 @@ class Graph:
         self.last_iters = it.value
         self.last_dense = bool(dense.value)
         return out[: self.n]
+
+
+    def hits(self, weighted=False, loops=0, scale=0, tol=0.0, max_iter=0, threads=0):
+        """net_hits (spectral.rs:748-903): hubs, authorities, the largest
+        eigenvalue of A^T A and whether the leading singular value is simple."""
+        hubs = np.zeros(max(self.n, 1))
+        auths = np.zeros(max(self.n, 1))
+        val = ctypes.c_double()
+        uniq = ctypes.c_int32()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        if lib().orc_hits(self.h, int(weighted), loops, scale, tol, max_iter, threads,
+                          _ptr(hubs), _ptr(auths), ctypes.byref(val), ctypes.byref(uniq), err,
+                          ERR_LEN):
+            raise OracleError(err.value.decode())
+        return hubs[: self.n], auths[: self.n], val.value, bool(uniq.value)
 
 
 def symmetric_eigen(a: np.ndarray):

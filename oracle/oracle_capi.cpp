@@ -285,6 +285,29 @@ int32_t orc_bonacich_power(const OrcGraph* h, double exponent, int32_t mode, int
   });
 }
 
+// net_hits (crates/capi/src/spectral.rs:189-230).
+int32_t orc_hits(const OrcGraph* h, int32_t weighted, int32_t loops, int32_t scale, double tol,
+                 int64_t max_iter, int32_t threads, double* hubs, double* auths, double* value,
+                 int32_t* unique, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    const Graph& g = handle(h);
+    HitsOptions o;
+    o.weighted = weighted != 0;
+    o.loops = loops_from_code(loops);
+    if (scale < 0 || scale > 2)
+      throw Error{"unknown hub and authority scale code " + std::to_string(scale)};
+    o.scale = scale;
+    o.tol = tol > 0 ? tol : 1e-12;
+    o.max_iter = max_iter > 0 ? (size_t)max_iter : 10000;
+    o.threads = threads > 0 ? (size_t)threads : 0;
+    Hits r = hits(g, o);
+    if (!r.hubs.empty()) memcpy(hubs, r.hubs.data(), r.hubs.size() * 8);
+    if (!r.authorities.empty()) memcpy(auths, r.authorities.data(), r.authorities.size() * 8);
+    *value = r.value;
+    *unique = r.unique ? 1 : 0;
+  });
+}
+
 // Eigenvalues ascending and eigenvectors (columns of the row-major n x n
 // `vecs`) of the symmetric matrix `a`; 1 if the QL iteration fails.
 int32_t orc_symmetric_eigen(int64_t n, const double* a, double* vals, double* vecs) {

@@ -26,8 +26,8 @@ import yaml
 
 HERE = Path(__file__).resolve().parent
 
-# Variants on the spectral-centrality path: PageRank, Katz and Bonacich power
-# centrality (spectral.yaml), eigenvector centrality (topography.yaml).
+# Variants on the spectral-centrality path: PageRank, Katz, Bonacich power
+# centrality and hubs and authorities (spectral.yaml), eigenvector centrality (topography.yaml).
 # Variants that first simplify or symmetrize the network through
 # net_graph_simplify (eigenvector_sna, eigenvector_ucinet, bonacich_sna) are
 # outside it.
@@ -36,7 +36,9 @@ VARIANTS = {
                       "pagerank_personalized", "pagerank_personalized_networkx",
                       "pagerank_uniform_dangling", "pagerank_undirected",
                       "katz", "katz_weighted", "katz_igraph", "katz_exogenous",
-                      "bonacich", "bonacich_negative", "bonacich_unit", "bonacich_rescale"],
+                      "bonacich", "bonacich_negative", "bonacich_unit", "bonacich_rescale",
+                      "hits_authorities", "hits_hubs", "hits_authorities_networkx",
+                      "hits_hubs_networkx"],
     "topography.yaml": ["eigenvector", "eigenvector_networkx", "eigenvector_weighted",
                         "eigenvector_weighted_networkx", "eigenvector_undirected"],
 }
@@ -110,7 +112,7 @@ def main():
     doc = {
         "about": "validation fixtures and golden values of the reference engine "
                  "(validation/fixtures, validation/golden/{definition,networkx}) for "
-                 "PageRank, Katz, Bonacich power and eigenvector centrality; generated "
+                 "PageRank, Katz, Bonacich power, HITS and eigenvector centrality; generated "
                  "by make_golden.py",
         "oracle_versions": versions,
         "manifest": manifest,

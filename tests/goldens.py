@@ -19,6 +19,7 @@ MODES = {"out": 1, "in": 2, "all": 3}
 LOOPS = {"twice": 0, "once": 1, "ignore": 2}
 DANGLING = {"personalized": 0, "uniform": 1}
 SCALES = {"max": 0, "unit": 1}
+HITS_SCALES = {"max": 0, "sum": 1, "unit": 2}
 
 
 @lru_cache(maxsize=1)
@@ -123,6 +124,11 @@ def _run_variant(g, fx: dict, variant: str):
         exponent = relative(e, "exponent", g, "in" if mode == "out" else mode, weighted, loops)
         return g.bonacich(exponent=exponent, mode=MODES[mode], weighted=weighted,
                           loops=LOOPS[loops], rescale=bool(e.get("rescale", False)))
+    if e["fn"] == "hits":
+        hubs, auths, _, _ = g.hits(weighted=bool(e.get("weighted", False)),
+                                   loops=LOOPS[e.get("loops", "twice")],
+                                   scale=HITS_SCALES[e.get("scale", "max")])
+        return hubs if e["which"] == "hubs" else auths
     raise ValueError(e["fn"])
 
 

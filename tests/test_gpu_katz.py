@@ -107,3 +107,37 @@ def test_katz_rmat20_fixed_point():
     res = np.abs(x - (1.0 + alpha * (A @ x))).max()
     assert res <= 1e-10 * np.abs(x).max(), res
     kg.close()
+
+
+# ------------------------------------------------------------------ HITS
+def test_hits_known_answers():
+    from test_oracle import hits_known_answers
+    hits_known_answers(K.Graph)
+
+
+@pytest.mark.parametrize("weighted,symmetrize", [(False, False), (True, False), (True, True)])
+def test_hits_rmat_matches_oracle(weighted, symmetrize):
+    kg, og = pair(12, weighted, 51, symmetrize=symmetrize)
+    for loops in (0, 1, 2):
+        for scale in (0, 1, 2):
+            a = kg.hits(weighted=weighted, loops=loops, scale=scale)
+            b = og.hits(weighted=weighted, loops=loops, scale=scale)
+            assert abs(a[2] - b[2]) <= 1e-9 * b[2]
+            assert a[3] == b[3]
+            assert close(a[0], b[0], 1e-8) and close(a[1], b[1], 1e-8), (loops, scale)
+
+
+def test_hits_rmat20_singular_vector_equation():
+    """Scale 20, directed: A^T A a = value a, hubs proportional to A a."""
+    import scipy.sparse as sp
+    kg = K.generate_rmat(20, 16, seed=20240612, clean=True)
+    hubs, auths, value, unique = kg.hits(scale=2)
+    off, cols, _ = kg.csr(0)
+    A = sp.csr_matrix((np.ones(len(cols)), cols.astype(np.int32), off.astype(np.int64)),
+                      shape=(kg.n, kg.n))
+    ata = A.T @ (A @ auths)
+    assert unique
+    assert np.abs(ata - value * auths).max() <= 1e-8 * value * np.abs(auths).max()
+    h = A @ auths
+    assert np.abs(hubs - h / np.linalg.norm(h)).max() <= 1e-12
+    kg.close()

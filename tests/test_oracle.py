@@ -379,3 +379,26 @@ def test_oracle_katz_bonacich_known_answers():
     assert g.last_dense
     g.bonacich(exponent=0.5)
     assert not g.last_dense
+
+
+# ------------------------------------------------------------------ HITS
+def hits_known_answers(G):
+    """The reference's hand values (spectral.rs:1073-1092)."""
+    small = G(5, [0, 0, 1, 2, 3, 2], [1, 2, 2, 0, 2, 4], None, True)
+    hubs, auths, value, unique = small.hits()
+    h = 0.5 ** 0.5
+    assert np.allclose(hubs, [1.0, h, 0.0, h, 0.0], atol=1e-9, rtol=0)
+    assert np.allclose(auths, [0.0, 2 ** 0.5 - 1.0, 1.0, 0.0, 0.0], atol=1e-9, rtol=0)
+    assert unique
+    # a directed 4-cycle: A^T A = I, every block ties, equal scores stay put
+    cyc = G(4, [0, 1, 2, 3], [1, 2, 3, 0], None, True)
+    hubs, _, _, unique = cyc.hits()
+    assert not unique
+    assert np.array_equal(hubs, [1.0] * 4)
+    empty = G(3, [], [], None, True)
+    hubs, auths, value, _ = empty.hits()
+    assert np.isnan(hubs).all() and np.isnan(auths).all() and value == 0.0
+
+
+def test_oracle_hits_known_answers():
+    hits_known_answers(O.Graph)
