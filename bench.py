@@ -384,6 +384,211 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- other configurations
+# One JSON line per configuration, for the workloads the benchmark line does
+# not cover: device time (median of `--steps` runs after `--warmup`),
+# accuracy against the CPU restatement of the reference (oracle/), and the
+# restatement's time on this host where it finishes in a bounded sample.
+
+def _median_device(fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    return statistics.median(fn() for _ in range(max(steps, 1)))
+
+
+def run_c1(args):
+    """ER G(10,000, 50,000) undirected, FP64 PageRank at tol 1e-12."""
+    import knappnet_b200 as K
+    from oracle import oracle as O
+    s, t = K.generate_gnm(10_000, 50_000, False, False, seed=20240701)
+    g = K.Graph(10_000, s, t, None, False)
+    og = O.Graph(10_000, s, t, None, False)
+    last = {}
+
+    def gpu():
+        x, info = g.pagerank_ex(tol=1e-12, precision=K.PREC_FP64)
+        last["x"], last["it"] = x, info.iterations
+        return info.seconds
+    sec = _median_device(gpu, args.steps, args.warmup)
+    t0 = time.perf_counter()
+    ref = og.pagerank(tol=1e-12)
+    cpu = time.perf_counter() - t0
+    return {"workload": "c1: ER G(n=10000, m=50000) undirected, PageRank FP64, tol 1e-12",
+            "metric": "solve ms", "value": round(sec * 1e3, 4), "unit": "ms",
+            "higher_is_better": False, "iterations": last["it"],
+            "oracle_iterations": og.last_iters,
+            "l1_vs_oracle": float(np.abs(last["x"] - ref).sum()),
+            "cpu_restatement_ms": round(cpu * 1e3, 3),
+            "cores": O.threads_for(0, 10_000, 50_000)}
+
+
+def run_c2(args):
+    """Symmetrised R-MAT 20, eigenvector centrality by Lanczos, tol 1e-10:
+    FP64 products against FP32 products with FP64 reorthogonalisation."""
+    import knappnet_b200 as K
+    from oracle import oracle as O
+    g = K.generate_rmat(20, 16, seed=20240702, clean=True, symmetrize=True)
+    out = {"workload": "c2: R-MAT 20 symmetrised (a/b/c/d .57/.19/.19/.05, cleaned), "
+                       "eigenvector centrality mode all, Lanczos, tol 1e-10",
+           "nodes": g.n, "edges": g.m}
+    res = {}
+    for prec in (0, 1):
+        keep = {}
+
+        def gpu():
+            x, info = g.eigenvector_ex(mode=3, tol=1e-10, precision=prec)
+            keep["x"], keep["info"] = x, info
+            return info.seconds
+        sec = _median_device(gpu, args.steps, args.warmup)
+        res[prec] = (sec, keep["x"], keep["info"])
+    s, t, _ = g.edges()
+    og = O.Graph(g.n, s, t, None, False)
+    t0 = time.perf_counter()
+    ox, olam, _ = og.eigenvector(mode=3, tol=1e-10)
+    cpu = time.perf_counter() - t0
+    for prec, name in ((0, "fp64"), (1, "fp32_products")):
+        sec, x, info = res[prec]
+        out[name] = {"ms": round(sec * 1e3, 3), "matvecs": int(info.iterations),
+                     "matvecs_fp32": int(info.iterations_fp32),
+                     "eigenvalue": info.eigenvalue,
+                     "eigenvalue_rel_vs_oracle": abs(info.eigenvalue - olam) / olam,
+                     "linf_vs_oracle": float(np.abs(x - ox).max()),
+                     "l1_vs_oracle": float(np.abs(x - ox).sum())}
+    out.update({"metric": "Lanczos solve ms (FP32 products)", "value": out["fp32_products"]["ms"],
+                "unit": "ms", "higher_is_better": False,
+                "cpu_restatement_ms": round(cpu * 1e3, 1),
+                "cores": O.threads_for(0, g.n, g.m)})
+    return out
+
+
+def run_c4a(args):
+    """R-MAT 22 directed, 256 personalisation vectors (1-64 seeds each), one
+    batched solve, mixed precision."""
+    import knappnet_b200 as K
+    from oracle import oracle as O
+    g = K.generate_rmat(22, 16, seed=20240703, clean=True)
+    n, B = g.n, 256
+    rng = np.random.default_rng(20240704)
+    P = np.zeros((B, n))
+    for b in range(B):
+        k = int(rng.integers(1, 65))
+        P[b, rng.choice(n, size=k, replace=False)] = 1.0 / k
+    keep = {}
+
+    def gpu():
+        x, info = g.pagerank_batch(P, precision=K.PREC_MIXED, tol=1e-10)
+        keep["x"], keep["info"] = x, info
+        return info.seconds
+    sec = _median_device(gpu, args.steps, args.warmup)
+    info = keep["info"]
+    s, t, _ = g.edges()
+    og = O.Graph(n, s, t, None, True)
+    errs, cpu = [], 0.0
+    for b in (0, 1):
+        t0 = time.perf_counter()
+        ref = og.pagerank(personalization=P[b], tol=1e-10)
+        cpu += time.perf_counter() - t0
+        errs.append(float(np.abs(keep["x"][b] - ref).sum()))
+    arcs = int(g.csr(1)[0][-1])
+    return {"workload": "c4a: R-MAT 22 directed, 256 personalisation vectors (uniform over "
+                        "1-64 seed nodes), batched SpMM PageRank, mixed precision, tol 1e-10",
+            "metric": "GTEPS*B per sweep", "unit": "GTEPS*B/sweep", "higher_is_better": True,
+            "value": round(arcs * B * info.sweeps / sec / 1e9, 2),
+            "solve_ms": round(sec * 1e3, 2), "sweeps": int(info.sweeps),
+            "sweeps_fp32": int(info.sweeps_fp32), "arcs": arcs,
+            "l1_vs_oracle_sampled_columns": errs,
+            "cpu_restatement_ms_per_vector": round(cpu / 2 * 1e3, 1),
+            "cpu_restatement_ms_all_vectors_estimated": round(cpu / 2 * B * 1e3, 0),
+            "cores": O.threads_for(0, n, arcs // 2)}
+
+
+def run_c4b(args):
+    """10,000 ego graphs, power-law sizes 50-50,000, mean degree 12, one
+    persistent launch."""
+    import knappnet_b200 as K
+    from oracle import oracle as O
+    sizes = K.power_law_sizes(10_000, 2.1, 50, 50_000, seed=20240705)
+    m = np.minimum(6 * sizes, sizes * (sizes - 1) // 2)
+    src, tgt = K.generate_gnm(sizes, m, False, False, seed=20240706)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    g = K.Graph(int(off[-1]), src, tgt, None, False)
+    keep = {}
+
+    def gpu():
+        out, its, info = g.pagerank_graphs(off, tol=1e-12)
+        keep["x"], keep["its"], keep["info"] = out, its, info
+        return info.seconds
+    sec = _median_device(gpu, args.steps, args.warmup)
+    # the restatement, graph by graph, on a sample of 200 graphs, scaled by
+    # nodes plus arcs
+    rng = np.random.default_rng(9)
+    pick = rng.choice(len(sizes), 200, replace=False)
+    cpu, work, worst = 0.0, 0, 0.0
+    for k in pick:
+        lo, hi = off[k], off[k + 1]
+        sel = (src >= lo) & (src < hi)
+        og = O.Graph(hi - lo, src[sel] - lo, tgt[sel] - lo, None, False)
+        t0 = time.perf_counter()
+        ref = og.pagerank(tol=1e-12)
+        cpu += time.perf_counter() - t0
+        work += int(hi - lo) + 2 * int(sel.sum())
+        worst = max(worst, float(np.abs(keep["x"][lo:hi] - ref).sum()))
+    total_work = int(off[-1]) + 2 * int(m.sum())
+    return {"workload": "c4b: 10,000 undirected G(n, 6n) ego graphs, sizes power law "
+                        "(exponent 2.1) on [50, 50000], PageRank FP64 tol 1e-12, one launch",
+            "metric": "batch ms", "value": round(sec * 1e3, 3), "unit": "ms",
+            "higher_is_better": False, "nodes": int(off[-1]), "edges": int(m.sum()),
+            "kernel_launches": int(keep["info"].kernel_launches),
+            "max_iterations": int(keep["its"].max()),
+            "l1_vs_oracle_worst_of_200": worst,
+            "cpu_restatement_ms_estimated": round(cpu * total_work / work * 1e3, 1),
+            "cores": 1}
+
+
+def run_c5(args):
+    """Differentiable PageRank on directed R-MAT 20 with lognormal weights:
+    forward solve, adjoint solve and edge-gradient scatter through
+    torch.autograd.Function."""
+    import torch
+    import knappnet_b200 as K
+    from knappnet_b200 import autograd as AG
+    g = K.generate_rmat(20, 16, seed=20240707, clean=True, lognormal=True, wseed=20240708)
+    _, _, w = g.edges()
+    rng = np.random.default_rng(20240709)
+    wp = w * np.maximum(1 + 0.1 * rng.standard_normal(len(w)), 1e-3)
+    target = AG.pagerank(torch.tensor(wp, device="cuda"), g, tol=1e-12).detach()
+    wt = torch.tensor(w, dtype=torch.float64, device="cuda", requires_grad=True)
+
+    def step():
+        wt.grad = None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        loss = ((AG.pagerank(wt, g, tol=1e-12) - target) ** 2).sum()
+        loss.backward()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+    sec = _median_device(step, args.steps, args.warmup)
+    grad = wt.grad.detach().cpu().numpy()
+    v = rng.standard_normal(len(w)) * w
+    h = 1e-4
+
+    def loss_at(x):
+        y = AG.pagerank(torch.tensor(x, dtype=torch.float64, device="cuda"), g, tol=1e-13)
+        return ((y - target) ** 2).sum().item()
+    fd = (loss_at(w + h * v) - loss_at(w - h * v)) / (2 * h)
+    an = float(grad @ v)
+    return {"workload": "c5: R-MAT 20 directed, lognormal(0,1) FP32 weights, L = |x - x*|^2, "
+                        "x* from weights perturbed by 10%, forward + adjoint + edge gradients",
+            "metric": "forward+backward ms", "value": round(sec * 1e3, 3), "unit": "ms",
+            "higher_is_better": False, "edges": int(len(w)),
+            "directional_fd_rel_error": abs(fd - an) / abs(an)}
+
+
+WORKLOADS = {"c1": run_c1, "c2": run_c2, "c4a": run_c4a, "c4b": run_c4b, "c5": run_c5}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,13 +600,23 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=8.0,
                     help="seconds per reference-arm step")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["c3", "c1", "c2", "c4a", "c4b", "c5"], default="c3",
+                    help="c3 (default) is the benchmark line; the others print one JSON line "
+                         "each for the other configurations")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale (the benchmark workload is 24; smaller scales "
                          "serve profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload != "c3":
+        if args.impl == "reference" or int(os.environ.get("RANK", 0)) != 0:
+            return
+        line = WORKLOADS[args.workload](args)
+        line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                     "data": "synthetic (seeded Philox generators)"})
+        print(json.dumps(line), flush=True)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
