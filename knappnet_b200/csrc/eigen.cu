@@ -346,26 +346,54 @@ __global__ void fill_value(double* x, uint32_t n, double v) {
 
 // Row sum and the sum of squares with parallel entries merged
 // (eigenvector.rs:566-584).
+// Row sums and the sums of squares of rows with parallel entries merged
+// (rows are sorted by column, so parallel entries are adjacent), one warp
+// per row: lanes take 32 consecutive entries at a time; a ballot marks where
+// runs of equal columns start, a segmented scan gives each run's sum at its
+// last lane, and the run open at the chunk's end carries into the next.
 __global__ void op_row_sums(OpView<double> op, double* __restrict__ s_out,
                             double* __restrict__ q_out) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < op.n; v += gridDim.x * blockDim.x) {
-    double s = 0, q = 0, acc = 0;
-    uint32_t c = 0xFFFFFFFFu;
-    for (uint32_t k = op.off[v]; k < op.off[v + 1]; ++k) {
-      uint32_t j = op.cols[k];
-      double w = op.vals ? op.vals[k] : 1.0;
+  const unsigned F = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < op.n; v += nw) {
+    const uint32_t b = op.off[v], e = op.off[v + 1];
+    double s = 0.0, q = 0.0, cacc = 0.0;
+    uint32_t ccol = 0xFFFFFFFFu;  // column of the run open at the previous chunk's end
+    for (uint32_t base = b; base < e; base += 32) {
+      const uint32_t k = base + lane;
+      const bool valid = k < e;
+      const uint32_t j = valid ? op.cols[k] : 0xFFFFFFFEu;
+      const double w = valid ? (op.vals ? op.vals[k] : 1.0) : 0.0;
       s += w;
-      if (j == c) {
-        acc += w;
-      } else {
-        if (c != 0xFFFFFFFFu) q += acc * acc;
-        c = j;
-        acc = w;
+      uint32_t pj = __shfl_up_sync(F, j, 1);
+      if (lane == 0) pj = ccol;
+      const bool start = j != pj;
+      const uint32_t starts = __ballot_sync(F, start);
+      // the run carried from the previous chunk ends where this chunk starts anew
+      if (lane == 0 && (starts & 1u) && ccol != 0xFFFFFFFFu) q += cacc * cacc;
+      const uint32_t upto = starts & (0xffffffffu >> (31 - lane));
+      const int seg0 = upto ? 31 - __clz(upto) : -1;  // -1: the run continues from ccol
+      double r = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double rr = __shfl_up_sync(F, r, o);
+        if (lane - o >= (seg0 < 0 ? 0 : seg0)) r += rr;
       }
+      if (seg0 < 0) r += cacc;
+      const bool next_start = __shfl_down_sync(F, start, 1);
+      if (valid && lane < 31 && k + 1 < e && next_start) q += r * r;
+      const int last = (int)min(31u, e - 1 - base);
+      cacc = __shfl_sync(F, r, last);
+      ccol = __shfl_sync(F, j, last);
     }
-    if (c != 0xFFFFFFFFu) q += acc * acc;
-    s_out[v] = s;
-    q_out[v] = q;
+    q = warp_sum(q);
+    s = warp_sum(s);
+    if (lane == 0) {
+      if (e > b) q += cacc * cacc;
+      s_out[v] = s;
+      q_out[v] = q;
+    }
   }
 }
 
@@ -380,18 +408,21 @@ __global__ void sub_lengths(const uint32_t* __restrict__ off, const uint32_t* __
   if (blockIdx.x == 0 && threadIdx.x == 0) len[k] = 0;
 }
 
+// One warp per row (long rows copy at full width).
 __global__ void sub_copy(OpView<double> op, const uint32_t* __restrict__ nodes, uint32_t k,
                          const uint32_t* __restrict__ local, const uint32_t* __restrict__ soff,
                          uint32_t* __restrict__ scols, double* __restrict__ s64,
                          float* __restrict__ s32) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
-    uint32_t v = nodes[i];
-    uint32_t o = soff[i];
-    for (uint32_t q = op.off[v]; q < op.off[v + 1]; ++q, ++o) {
-      scols[o] = local[op.cols[q]];
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < k; i += nw) {
+    const uint32_t v = nodes[i];
+    const uint32_t b = op.off[v], e = op.off[v + 1], o = soff[i];
+    for (uint32_t q = b + lane; q < e; q += 32) {
+      scols[o + q - b] = local[op.cols[q]];
       if (op.vals) {
-        s64[o] = op.vals[q];
-        s32[o] = (float)op.vals[q];
+        s64[o + q - b] = op.vals[q];
+        s32[o + q - b] = (float)op.vals[q];
       }
     }
   }
@@ -399,14 +430,21 @@ __global__ void sub_copy(OpView<double> op, const uint32_t* __restrict__ nodes, 
 
 // Submatrices that keep only the entries whose column is mapped (local[c]
 // != 2^32 - 1), as SparseOp::submatrix (eigenvector.rs:589-624).
+// Submatrices that keep only the entries whose column is mapped (local[c]
+// != 2^32 - 1), in row order, as SparseOp::submatrix (eigenvector.rs:
+// 589-624); one warp per row, kept entries compacted by ballot.
 __global__ void sub_lengths_mapped(OpView<double> op, const uint32_t* __restrict__ nodes,
                                    uint32_t k, const uint32_t* __restrict__ local,
                                    uint32_t* __restrict__ len) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < k; i += nw) {
     const uint32_t v = nodes[i];
     uint32_t c = 0;
-    for (uint32_t q = op.off[v]; q < op.off[v + 1]; ++q) c += local[op.cols[q]] != 0xFFFFFFFFu;
-    len[i] = c;
+    for (uint32_t q = op.off[v] + lane; q < op.off[v + 1]; q += 32)
+      c += local[op.cols[q]] != 0xFFFFFFFFu;
+    c = warp_sum(c);
+    if (lane == 0) len[i] = c;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) len[k] = 0;
 }
@@ -415,15 +453,23 @@ __global__ void sub_copy_mapped(OpView<double> op, const uint32_t* __restrict__ 
                                 uint32_t k, const uint32_t* __restrict__ local,
                                 const uint32_t* __restrict__ soff, uint32_t* __restrict__ scols,
                                 double* __restrict__ s64) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < k; i += nw) {
     const uint32_t v = nodes[i];
+    const uint32_t b = op.off[v], e = op.off[v + 1];
     uint32_t o = soff[i];
-    for (uint32_t q = op.off[v]; q < op.off[v + 1]; ++q) {
-      const uint32_t c = local[op.cols[q]];
-      if (c == 0xFFFFFFFFu) continue;
-      scols[o] = c;
-      if (s64) s64[o] = op.vals ? op.vals[q] : 1.0;
-      ++o;
+    for (uint32_t base = b; base < e; base += 32) {
+      const uint32_t q = base + lane;
+      const uint32_t c = q < e ? local[op.cols[q]] : 0xFFFFFFFFu;
+      const bool keep = c != 0xFFFFFFFFu;
+      const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const uint32_t pos = o + __popc(mask & ((1u << lane) - 1u));
+        scols[pos] = c;
+        if (s64) s64[pos] = op.vals ? op.vals[q] : 1.0;
+      }
+      o += __popc(mask);
     }
   }
 }
@@ -1137,7 +1183,7 @@ void mapped_submatrix(const OpView<double>& op, const std::vector<uint32_t>& nod
   KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), nodes.data(), (size_t)kn * 4, cudaMemcpyHostToDevice,
                            s));
   A.own_off.alloc((size_t)kn + 1);
-  sub_lengths_mapped<<<grid_for(kn + 1, 256), 256, 0, s>>>(op, nodes_d.get(), kn, local,
+  sub_lengths_mapped<<<grid_for((uint64_t)kn * 32, 256), 256, 0, s>>>(op, nodes_d.get(), kn, local,
                                                            A.own_off.get());
   const uint64_t nnz =
       exclusive_scan<uint32_t>(A.own_off.get(), A.own_off.get(), (size_t)kn + 1, s);
@@ -1145,7 +1191,7 @@ void mapped_submatrix(const OpView<double>& op, const std::vector<uint32_t>& nod
   A.nnz = nnz;
   A.own_cols.alloc(std::max<uint64_t>(nnz, 1));
   A.own_v64.alloc(std::max<uint64_t>(nnz, 1));
-  sub_copy_mapped<<<grid_for(kn, 128), 128, 0, s>>>(op, nodes_d.get(), kn, local,
+  sub_copy_mapped<<<grid_for((uint64_t)kn * 32, 256), 256, 0, s>>>(op, nodes_d.get(), kn, local,
                                                     A.own_off.get(), A.own_cols.get(),
                                                     A.own_v64.get());
   KNB_LAUNCH("mapped submatrix");
@@ -1528,7 +1574,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
     const Comps& comps = strong;  // weak components of h
     const size_t k = comps.count();
     DevBuf<double> sdev(n), qdev(n);
-    op_row_sums<<<grid_for(n, 256), 256, 0, s>>>(v64, sdev.get(), qdev.get());
+    op_row_sums<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>(v64, sdev.get(), qdev.get());
     ++launches;
     std::vector<double> rs(n), rq(n);
     KNB_CUDA(cudaMemcpyAsync(rs.data(), sdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
@@ -1591,7 +1637,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
           A.own_v64.alloc(std::max<uint64_t>(nnz, 1));
           A.own_v32.alloc(std::max<uint64_t>(nnz, 1));
         }
-        sub_copy<<<grid_for(kn, 128), 128, 0, s>>>(v64, nodes_d.get(), kn, local.get(),
+        sub_copy<<<grid_for((uint64_t)kn * 32, 256), 256, 0, s>>>(v64, nodes_d.get(), kn, local.get(),
                                                    A.own_off.get(), A.own_cols.get(),
                                                    op.has_vals ? A.own_v64.get() : nullptr,
                                                    op.has_vals ? A.own_v32.get() : nullptr);

@@ -88,12 +88,14 @@ __global__ void fill_d(double* x, uint32_t n, double v) {
 
 // Entries inside a component of two or more nodes keep their value; the
 // rest become 0 (the product of a component's own submatrix).
+// One warp per row.
 __global__ void mask_values(OpView<double> op, const uint32_t* __restrict__ comp,
                             const uint8_t* __restrict__ big, double* __restrict__ mv) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < op.n; v += gridDim.x * blockDim.x) {
+  const uint32_t lane = threadIdx.x & 31, nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < op.n; v += nw) {
     const uint32_t c = comp[v];
     const bool keep = big[c] != 0;
-    for (uint32_t k = op.off[v]; k < op.off[v + 1]; ++k)
+    for (uint32_t k = op.off[v] + lane; k < op.off[v + 1]; k += 32)
       mv[k] = (keep && comp[op.cols[k]] == c) ? (op.vals ? op.vals[k] : 1.0) : 0.0;
   }
 }
@@ -505,7 +507,8 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
   DevBuf<double> mv(std::max<uint64_t>(op.nnz, 1)), x(n), ratio(n), ynext(n), cx((size_t)nch * 3),
       value_b(nbig), top(k);
   const OpView<double> v0 = op.view64();
-  mask_values<<<grid_for(n, KT), KT, 0, s>>>(v0, d_comp.get(), d_active.get(), mv.get());
+  mask_values<<<grid_for((uint64_t)n * 32, KT), KT, 0, s>>>(v0, d_comp.get(), d_active.get(),
+                                                          mv.get());
   fill_d<<<grid_for(n, KT), KT, 0, s>>>(x.get(), n, 1.0);
   KNB_LAUNCH("collatz set-up");
   const OpView<double> vm{v0.n, v0.nnz, v0.off, v0.cols, mv.get()};
