@@ -25,6 +25,9 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -939,35 +942,77 @@ struct Leading {
 
 // Thick-restart Lanczos (eigenvector.rs:746-878) on device operator A from
 // the all-ones vector; the unit eigenvector is left in `xout` (device).
+// Buffers of the Lanczos process, kept between calls by callers that solve
+// repeatedly (they only grow).
+struct LzBuffers {
+  DevBuf<double> tmp, V, w, y, x, rot, hm, svec, part;
+  DevBuf<float> v32;
+  DevBuf<LzState> st;
+  DevBuf<IterState> ist;
+  SpmvScratch sc;
+  LzState* hst = nullptr;
+  LzBuffers() = default;
+  LzBuffers(const LzBuffers&) = delete;
+  LzBuffers& operator=(const LzBuffers&) = delete;
+  ~LzBuffers() {
+    if (hst) cudaFreeHost(hst);
+  }
+  template <class T>
+  static void grow(DevBuf<T>& b, size_t count) {
+    if (b.n < count) b.alloc(count);
+  }
+  void ensure(size_t dim, size_t m, bool mixed, size_t tmp_n, size_t part_n) {
+    grow(tmp, tmp_n);
+    grow(V, m * dim);
+    grow(rot, m * dim);
+    grow(w, dim);
+    grow(y, dim);
+    grow(x, dim);
+    grow(hm, (size_t)MAXB * MAXB);
+    grow(svec, (size_t)MAXB * MAXB);
+    grow(part, part_n);
+    if (mixed) grow(v32, dim);
+    grow(st, 1);
+    grow(ist, 1);
+    if (!hst) KNB_CUDA(cudaMallocHost(&hst, sizeof(LzState)));
+  }
+};
+
 // With B given, the operator is B A (HITS: A_b^T A_b), applied as two
 // products in FP64; with `start` given (device, dim values), the process
-// starts from it instead of the all-ones vector.
+// starts from it instead of the all-ones vector. `buf`: buffers to reuse
+// (null: this call's own).
 static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t max_matvecs,
                               bool mixed, double* xout, Leading* res, int* launches,
                               cudaStream_t s, const DevOp* B = nullptr,
-                              const double* start = nullptr) {
+                              const double* start = nullptr, LzBuffers* buf = nullptr) {
   const size_t dim = B ? B->n : A.n;
   if (B) mixed = false;
-  DevBuf<double> tmp(B ? std::max<size_t>(A.n, 1) : 0);
   const int m = (int)std::max<size_t>(
       1, std::min<size_t>(std::min<size_t>(dim, MAXB), std::max<size_t>((1ull << 27) / dim, 8)));
   const int keep = std::max(1, std::min(8, m >= 2 ? m - 2 : 0));
   const unsigned nb = (unsigned)((dim + VB - 1) / VB);
   const unsigned gv = grid_for(dim, 256, 148 * 16);
-  DevBuf<double> V((size_t)m * dim), w(dim), y(dim), x(dim), rot((size_t)m * dim);
-  DevBuf<float> v32(mixed ? dim : 0);
-  DevBuf<double> hm_d((size_t)m * m), svec(MAXB * MAXB);
-  DevBuf<double> part(std::max<size_t>((size_t)nb * (MAXB + 1), (size_t)gv * 2) + 64);
-  DevBuf<LzState> st(1);
-  DevBuf<IterState> ist(1);
-  SpmvScratch sc;
+  LzBuffers own;
+  LzBuffers& L = buf ? *buf : own;
+  L.ensure(dim, (size_t)m, mixed, B ? std::max<size_t>(A.n, 1) : 0,
+           std::max<size_t>((size_t)nb * (MAXB + 1), (size_t)gv * 2) + 64);
+  DevBuf<double>& tmp = L.tmp;
+  DevBuf<double>& V = L.V;
+  DevBuf<double>& w = L.w;
+  DevBuf<double>& y = L.y;
+  DevBuf<double>& x = L.x;
+  DevBuf<double>& rot = L.rot;
+  DevBuf<float>& v32 = L.v32;
+  DevBuf<double>& hm_d = L.hm;
+  DevBuf<double>& svec = L.svec;
+  DevBuf<double>& part = L.part;
+  DevBuf<LzState>& st = L.st;
+  DevBuf<IterState>& ist = L.ist;
+  SpmvScratch& sc = L.sc;
   if (B) sc.ensure(std::max(A.part->ntiles, B->part->ntiles));  // no growth between products
-  LzState* hst = nullptr;
-  KNB_CUDA(cudaMallocHost(&hst, sizeof(LzState)));
-  struct F {
-    LzState* p;
-    ~F() { cudaFreeHost(p); }
-  } fh{hst};
+  else sc.ensure(A.part->ntiles);
+  LzState* hst = L.hst;
   auto read_state = [&] {
     KNB_CUDA(cudaMemcpyAsync(hst, st.get(), sizeof(LzState), cudaMemcpyDeviceToHost, s));
     KNB_CUDA(cudaStreamSynchronize(s));
@@ -1440,6 +1485,25 @@ static void scale_host(std::vector<double>& x, int how) {
     for (double& v : x) v /= d;
 }
 
+// What an eigenvector solve on one operator can reuse: its components and
+// whether any of them is cyclic; for symmetric operators the per-component
+// bounds and order, the submatrices of the components solved so far (with
+// their partitions), and the Lanczos buffers. Held for the length of a
+// solve, so concurrent solves on one operator take turns.
+struct EigPlan : Workspace {
+  std::mutex mu;
+  bool ready = false;
+  Comps comps;
+  unsigned int cyclic = 0;
+  bool sym_ready = false;
+  std::vector<double> upper, lower;
+  std::vector<size_t> order, start;
+  std::vector<uint32_t> members;
+  std::map<size_t, std::unique_ptr<DevOp>> subs;
+  DevBuf<uint32_t> local, nodes_d;
+  LzBuffers lz;
+};
+
 void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenResult* r,
                  cudaStream_t s) {
   const uint32_t n = g.n;
@@ -1459,33 +1523,45 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
   const double lf = p.loops == 2 ? 0.0 : (!hdir && p.loops == 0 ? 2.0 : 1.0);
   Operator& op = g.op(which, p.weighted, lf, s);
   const unsigned gv = grid_for(n, 256, 148 * 16);
-
-  // components: strong (directed h) or weak
-  Comps strong;
-  if (hdir) {
-    std::vector<uint32_t> off(n + 1), tgt(g.out.arcs);
-    KNB_CUDA(cudaMemcpyAsync(off.data(), g.out.off.get(), ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
-    if (g.out.arcs)
-      KNB_CUDA(cudaMemcpyAsync(tgt.data(), g.out.tgt.get(), g.out.arcs * 4, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaStreamSynchronize(s));
-    strong = strong_components(off, tgt, n);
-  } else {
-    strong = weak_components(g, s);
-    launches += 5;
+  EigPlan* planp = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(op.mu);
+    if (!op.eig_ws) op.eig_ws = std::make_unique<EigPlan>();
+    planp = static_cast<EigPlan*>(op.eig_ws.get());
   }
-  r->connected = strong.count() == 1;
-
-  // cyclic?
+  EigPlan& plan = *planp;
+  std::lock_guard<std::mutex> plan_lock(plan.mu);
   OpView<double> v64 = op.view64();
-  DevBuf<uint32_t> comp(n);
-  DevBuf<unsigned int> flag(1);
-  KNB_CUDA(cudaMemcpyAsync(comp.get(), strong.membership.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
-  KNB_CUDA(cudaMemsetAsync(flag.get(), 0, 4, s));
-  cyclic_arcs<<<grid_for(n, 256), 256, 0, s>>>(v64, comp.get(), flag.get());
-  ++launches;
-  unsigned int cyc = 0;
-  KNB_CUDA(cudaMemcpyAsync(&cyc, flag.get(), 4, cudaMemcpyDeviceToHost, s));
-  KNB_CUDA(cudaStreamSynchronize(s));
+
+  // components: strong (directed h) or weak; whether any is cyclic
+  if (!plan.ready) {
+    if (hdir) {
+      std::vector<uint32_t> off(n + 1), tgt(g.out.arcs);
+      KNB_CUDA(cudaMemcpyAsync(off.data(), g.out.off.get(), ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
+      if (g.out.arcs)
+        KNB_CUDA(cudaMemcpyAsync(tgt.data(), g.out.tgt.get(), g.out.arcs * 4, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      plan.comps = strong_components(off, tgt, n);
+    } else {
+      plan.comps = weak_components(g, s);
+      launches += 5;
+    }
+    DevBuf<uint32_t> comp(n);
+    DevBuf<unsigned int> flag(1);
+    KNB_CUDA(cudaMemcpyAsync(comp.get(), plan.comps.membership.data(), (size_t)n * 4,
+                             cudaMemcpyHostToDevice, s));
+    KNB_CUDA(cudaMemsetAsync(flag.get(), 0, 4, s));
+    cyclic_arcs<<<grid_for(n, 256), 256, 0, s>>>(v64, comp.get(), flag.get());
+    ++launches;
+    KNB_CUDA(cudaMemcpyAsync(&plan.cyclic, flag.get(), 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    plan.local.alloc(n);
+    plan.nodes_d.alloc(n);
+    plan.ready = true;
+  }
+  const Comps& strong = plan.comps;
+  r->connected = strong.count() == 1;
+  const unsigned int cyc = plan.cyclic;
   DevBuf<double> xd(n);
   std::vector<double> x(n);
   if (!cyc) {
@@ -1573,33 +1649,41 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
     // symmetric: Lanczos per weak component (eigenvector.rs:383-479)
     const Comps& comps = strong;  // weak components of h
     const size_t k = comps.count();
-    DevBuf<double> sdev(n), qdev(n);
-    op_row_sums<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>(v64, sdev.get(), qdev.get());
-    ++launches;
-    std::vector<double> rs(n), rq(n);
-    KNB_CUDA(cudaMemcpyAsync(rs.data(), sdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaMemcpyAsync(rq.data(), qdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaStreamSynchronize(s));
-    std::vector<double> upper(k, 0.0), sum(k, 0.0), square(k, 0.0), lower(k);
-    for (uint32_t v = 0; v < n; ++v) {
-      uint32_t c = comps.membership[v];
-      upper[c] = std::max(upper[c], rs[v]);
-      sum[c] += rs[v];
-      square[c] = std::max(square[c], rq[v]);
+    if (!plan.sym_ready) {
+      DevBuf<double> sdev(n), qdev(n);
+      op_row_sums<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>(v64, sdev.get(), qdev.get());
+      ++launches;
+      std::vector<double> rs(n), rq(n);
+      KNB_CUDA(cudaMemcpyAsync(rs.data(), sdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaMemcpyAsync(rq.data(), qdev.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      std::vector<double> sum(k, 0.0), square(k, 0.0);
+      plan.upper.assign(k, 0.0);
+      plan.lower.assign(k, 0.0);
+      for (uint32_t v = 0; v < n; ++v) {
+        uint32_t c = comps.membership[v];
+        plan.upper[c] = std::max(plan.upper[c], rs[v]);
+        sum[c] += rs[v];
+        square[c] = std::max(square[c], rq[v]);
+      }
+      for (size_t c = 0; c < k; ++c)
+        plan.lower[c] = std::max(sum[c] / (double)comps.sizes[c], std::sqrt(square[c]));
+      plan.order.resize(k);
+      std::iota(plan.order.begin(), plan.order.end(), 0);
+      std::stable_sort(plan.order.begin(), plan.order.end(),
+                       [&](size_t a, size_t b) { return plan.lower[b] < plan.lower[a]; });
+      plan.start.assign(k + 1, 0);
+      for (uint32_t c : comps.membership) plan.start[c + 1]++;
+      for (size_t c = 0; c < k; ++c) plan.start[c + 1] += plan.start[c];
+      plan.members.resize(n);
+      std::vector<size_t> cur(plan.start.begin(), plan.start.end() - 1);
+      for (uint32_t v = 0; v < n; ++v) plan.members[cur[comps.membership[v]]++] = v;
+      plan.sym_ready = true;
     }
-    for (size_t c = 0; c < k; ++c)
-      lower[c] = std::max(sum[c] / (double)comps.sizes[c], std::sqrt(square[c]));
-    std::vector<size_t> order(k);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return lower[b] < lower[a]; });
-    std::vector<size_t> start(k + 1, 0);
-    for (uint32_t c : comps.membership) start[c + 1]++;
-    for (size_t c = 0; c < k; ++c) start[c + 1] += start[c];
-    std::vector<uint32_t> members(n);
-    {
-      std::vector<size_t> cur(start.begin(), start.end() - 1);
-      for (uint32_t v = 0; v < n; ++v) members[cur[comps.membership[v]]++] = v;
-    }
+    const std::vector<double>& upper = plan.upper;
+    const std::vector<size_t>& order = plan.order;
+    const std::vector<size_t>& start = plan.start;
+    const std::vector<uint32_t>& members = plan.members;
     double best = 0.0;
     int64_t matvecs = 0, matvecs32 = 0;
     struct Solved {
@@ -1608,12 +1692,17 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
       DevBuf<double> u;
     };
     std::vector<Solved> solved;
-    DevBuf<uint32_t> local(n), nodes_d(n);
+    DevBuf<uint32_t>& local = plan.local;
+    DevBuf<uint32_t>& nodes_d = plan.nodes_d;
     const double TIE = 1e-9;
     for (size_t c : order) {
       if (upper[c] <= 0.0 || upper[c] < best * (1.0 - TIE)) continue;
       const uint32_t kn = (uint32_t)(start[c + 1] - start[c]);
-      DevOp A;
+      DevOp whole;
+      std::unique_ptr<DevOp>& cached = plan.subs[c];
+      const bool build_sub = k != 1 && !cached;
+      if (build_sub) cached = std::make_unique<DevOp>();
+      DevOp& A = k == 1 ? whole : *cached;
       if (k == 1) {
         A.n = n;
         A.nnz = op.nnz;
@@ -1622,7 +1711,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
         A.v64 = op.has_vals ? op.vals64.get() : nullptr;
         A.v32 = op.has_vals ? op.vals32.get() : nullptr;
         A.part = &op.partition(SPMV_THREADS * EIG_IPT, s);
-      } else {
+      } else if (build_sub) {
         KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), members.data() + start[c], (size_t)kn * 4,
                                  cudaMemcpyHostToDevice, s));
         scatter_local<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d.get(), kn, local.get());
@@ -1655,7 +1744,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
       sv.u.alloc(kn);
       Leading res;
       if (!symmetric_leading(A, p.tol, 1.0, p.max_iter, p.precision == 1, sv.u.get(), &res,
-                             &launches, s))
+                             &launches, s, nullptr, nullptr, &plan.lz))
         throw Error("eigenvector centrality did not converge to tolerance " + fmt_g(p.tol) +
                     " within " + std::to_string(p.max_iter) +
                     " matrix-vector products; a larger iteration cap may help");

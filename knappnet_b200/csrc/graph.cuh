@@ -79,6 +79,7 @@ struct Operator {
   const DevCsr* trans = nullptr;  // adjacency whose row lengths are this operator's column counts
   std::unique_ptr<Relabeled> relabel;
   std::unique_ptr<Workspace> pr_ws;  // PageRank's (pagerank.cu), created on first use
+  std::unique_ptr<Workspace> eig_ws;  // eigenvector centrality's (eigen.cu), created on first use
 
   const Relabeled& relabeled(cudaStream_t s);
   const Partition& relabeled_partition(uint32_t tile_items, cudaStream_t s);
