@@ -791,6 +791,54 @@ __global__ void lz_sign_clamp(double* x, size_t dim, const LzState* st) {
   }
 }
 
+// xinf = max |x| (one pass; the last CTA combines the CTA maxima).
+__global__ void __launch_bounds__(VB_T)
+lz_absmax(const double* __restrict__ x, size_t dim, double* __restrict__ part, LzState* st) {
+  double m = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(x[i]));
+  __shared__ double sh[VB_T / 32];
+  m = warp_max(m);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = m;
+  __syncthreads();
+  if (w == 0) {
+    m = warp_max(lane < VB_T / 32 ? sh[lane] : 0.0);
+    if (lane == 0) part[blockIdx.x] = m;
+  }
+  if (!lz_last(&st->ticket)) return;
+  if (threadIdx.x < 32) {
+    const volatile double* p = part;
+    double a = 0.0;
+    for (uint32_t q = threadIdx.x; q < gridDim.x; q += 32) a = fmax(a, p[q]);
+    a = warp_max(a);
+    if (threadIdx.x == 0) {
+      st->xinf = a;
+      st->ticket = 0;
+    }
+  }
+}
+
+// x /= max |x| (how 0) or ||x|| (how 1), unless that is 0 (the scale
+// option of eigenvector.rs:440-452 on non-negative scores).
+__global__ void scale_by_state(double* x, size_t dim, const LzState* st, int how) {
+  const double d = how == 0 ? st->xinf : sqrt(st->xx);
+  if (!(d > 0.0)) return;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = x[i] / d;
+}
+
+// x[nodes[i]] = u[i] sum(u): a component's unit vector weighted by its sum.
+__global__ void scatter_by_sum(const uint32_t* __restrict__ nodes, uint32_t k,
+                               const double* __restrict__ u, const LzState* st,
+                               double* __restrict__ x) {
+  const double f = st->sum;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x)
+    x[nodes[i]] = u[i] * f;
+}
+
 __global__ void scale_by(double* x, size_t dim, double f, int divide) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dim;
        i += (size_t)gridDim.x * blockDim.x)
@@ -1500,7 +1548,9 @@ struct EigPlan : Workspace {
   std::vector<size_t> order, start;
   std::vector<uint32_t> members;
   std::map<size_t, std::unique_ptr<DevOp>> subs;
-  DevBuf<uint32_t> local, nodes_d;
+  std::map<size_t, DevBuf<double>> vecs;  // each solved component's unit vector
+  DevBuf<uint32_t> local, members_d;
+  DevBuf<double> xd;
   LzBuffers lz;
 };
 
@@ -1555,16 +1605,15 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
     ++launches;
     KNB_CUDA(cudaMemcpyAsync(&plan.cyclic, flag.get(), 4, cudaMemcpyDeviceToHost, s));
     KNB_CUDA(cudaStreamSynchronize(s));
-    plan.local.alloc(n);
-    plan.nodes_d.alloc(n);
     plan.ready = true;
   }
   const Comps& strong = plan.comps;
   r->connected = strong.count() == 1;
   const unsigned int cyc = plan.cyclic;
-  DevBuf<double> xd(n);
-  std::vector<double> x(n);
+  if (plan.xd.n < n) plan.xd.alloc(n);
+  DevBuf<double>& xd = plan.xd;
   if (!cyc) {
+    std::vector<double> x(n);
     fill_value<<<gv, 256, 0, s>>>(xd.get(), n, 1.0);
     sink_scores<<<grid_for(n, 256), 256, 0, s>>>(v64, xd.get());
     launches += 2;
@@ -1678,22 +1727,24 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
       plan.members.resize(n);
       std::vector<size_t> cur(plan.start.begin(), plan.start.end() - 1);
       for (uint32_t v = 0; v < n; ++v) plan.members[cur[comps.membership[v]]++] = v;
+      plan.members_d.alloc(n);
+      KNB_CUDA(cudaMemcpyAsync(plan.members_d.get(), plan.members.data(), (size_t)n * 4,
+                               cudaMemcpyHostToDevice, s));
+      if (k > 1) plan.local.alloc(n);
       plan.sym_ready = true;
     }
     const std::vector<double>& upper = plan.upper;
     const std::vector<size_t>& order = plan.order;
     const std::vector<size_t>& start = plan.start;
-    const std::vector<uint32_t>& members = plan.members;
     double best = 0.0;
     int64_t matvecs = 0, matvecs32 = 0;
     struct Solved {
       size_t c;
       double value;
-      DevBuf<double> u;
+      double* u;
     };
     std::vector<Solved> solved;
     DevBuf<uint32_t>& local = plan.local;
-    DevBuf<uint32_t>& nodes_d = plan.nodes_d;
     const double TIE = 1e-9;
     for (size_t c : order) {
       if (upper[c] <= 0.0 || upper[c] < best * (1.0 - TIE)) continue;
@@ -1712,11 +1763,10 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
         A.v32 = op.has_vals ? op.vals32.get() : nullptr;
         A.part = &op.partition(SPMV_THREADS * EIG_IPT, s);
       } else if (build_sub) {
-        KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), members.data() + start[c], (size_t)kn * 4,
-                                 cudaMemcpyHostToDevice, s));
-        scatter_local<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d.get(), kn, local.get());
+        const uint32_t* nodes_d = plan.members_d.get() + start[c];
+        scatter_local<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d, kn, local.get());
         A.own_off.alloc((size_t)kn + 1);
-        sub_lengths<<<grid_for(kn + 1, 256), 256, 0, s>>>(op.rows->off.get(), nodes_d.get(), kn,
+        sub_lengths<<<grid_for(kn + 1, 256), 256, 0, s>>>(op.rows->off.get(), nodes_d, kn,
                                                           A.own_off.get());
         uint64_t nnz = exclusive_scan<uint32_t>(A.own_off.get(), A.own_off.get(), (size_t)kn + 1, s);
         A.n = kn;
@@ -1726,7 +1776,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
           A.own_v64.alloc(std::max<uint64_t>(nnz, 1));
           A.own_v32.alloc(std::max<uint64_t>(nnz, 1));
         }
-        sub_copy<<<grid_for((uint64_t)kn * 32, 256), 256, 0, s>>>(v64, nodes_d.get(), kn, local.get(),
+        sub_copy<<<grid_for((uint64_t)kn * 32, 256), 256, 0, s>>>(v64, nodes_d, kn, local.get(),
                                                    A.own_off.get(), A.own_cols.get(),
                                                    op.has_vals ? A.own_v64.get() : nullptr,
                                                    op.has_vals ? A.own_v32.get() : nullptr);
@@ -1741,9 +1791,11 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
       }
       Solved sv;
       sv.c = c;
-      sv.u.alloc(kn);
+      DevBuf<double>& u = plan.vecs[c];
+      if (u.n < kn) u.alloc(kn);
+      sv.u = u.get();
       Leading res;
-      if (!symmetric_leading(A, p.tol, 1.0, p.max_iter, p.precision == 1, sv.u.get(), &res,
+      if (!symmetric_leading(A, p.tol, 1.0, p.max_iter, p.precision == 1, sv.u, &res,
                              &launches, s, nullptr, nullptr, &plan.lz))
         throw Error("eigenvector centrality did not converge to tolerance " + fmt_g(p.tol) +
                     " within " + std::to_string(p.max_iter) +
@@ -1754,25 +1806,32 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
       sv.value = res.value;
       solved.push_back(std::move(sv));
     }
+    // tied components' vectors, each weighted by its sum, then the scale
+    // option; all on the device, one copy of the scores to the host
     fill_value<<<gv, 256, 0, s>>>(xd.get(), n, 0.0);
     ++launches;
+    LzBuffers::grow(plan.lz.st, 1);
+    LzBuffers::grow(plan.lz.part, std::max<size_t>(gv, 3 * ((size_t)n + VB - 1) / VB) + 64);
+    LzState* st = plan.lz.st.get();
+    double* part = plan.lz.part.get();
+    KNB_CUDA(cudaMemsetAsync(st, 0, sizeof(LzState), s));
     for (auto& sv : solved) {
       if (sv.value < best * (1.0 - TIE)) continue;
       const uint32_t kn = (uint32_t)(start[sv.c + 1] - start[sv.c]);
-      std::vector<double> u(kn);
-      KNB_CUDA(cudaMemcpyAsync(u.data(), sv.u.get(), (size_t)kn * 8, cudaMemcpyDeviceToHost, s));
-      KNB_CUDA(cudaStreamSynchronize(s));
-      double total = 0.0;
-      for (double v : u) total += v;
-      KNB_CUDA(cudaMemcpyAsync(nodes_d.get(), members.data() + start[sv.c], (size_t)kn * 4,
-                               cudaMemcpyHostToDevice, s));
-      scatter_scaled<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d.get(), kn, sv.u.get(), total, xd.get());
-      ++launches;
+      lz_dots<<<(unsigned)((kn + VB - 1) / VB), VB_T, 0, s>>>(sv.u, nullptr, kn, part, st);
+      scatter_by_sum<<<grid_for(kn, 256), 256, 0, s>>>(plan.members_d.get() + start[sv.c], kn,
+                                                       sv.u, st, xd.get());
+      launches += 2;
     }
-    KNB_CUDA(cudaMemcpyAsync(x.data(), xd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    if (p.scale == 0)
+      lz_absmax<<<gv, VB_T, 0, s>>>(xd.get(), n, part, st);
+    else
+      lz_dots<<<(unsigned)((n + VB - 1) / VB), VB_T, 0, s>>>(xd.get(), nullptr, n, part, st);
+    scale_by_state<<<gv, 256, 0, s>>>(xd.get(), n, st, p.scale == 0 ? 0 : 1);
+    launches += 2;
+    KNB_LAUNCH("eigenvector scores");
+    KNB_CUDA(cudaMemcpyAsync(out, xd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
     KNB_CUDA(cudaStreamSynchronize(s));
-    scale_host(x, p.scale);
-    memcpy(out, x.data(), (size_t)n * 8);
     r->eigenvalue = best;
     r->matvecs = matvecs;
     r->matvecs_fp32 = matvecs32;
