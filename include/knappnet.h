@@ -107,6 +107,23 @@ NET_API int32_t net_eigenvector(const GraphHandle *h, int32_t mode, int32_t weig
                         double *eigenvalue, int32_t *connected, char *err,
                         size_t err_len);
 
+/* Weak (kind 0) or strong (kind 1) components: membership receives n
+ * labels, numbered from 0 in order of each component's lowest-numbered
+ * node, count one value; strong components of an undirected graph are its
+ * weak ones. Replaces netcapi.h:517-520 (crates/capi/src/topography.rs:85-106). */
+NET_API int32_t net_components(const GraphHandle *h, int32_t kind, int32_t *membership,
+                               int64_t *count, char *err, size_t err_len);
+
+/* Freeman centralization, one double to out. This library provides the
+ * eigenvector measure (measure 3; igraph convention 0, direction ignored):
+ * n max(c) - sum(c) over the unweighted eigenvector centrality c scaled
+ * to max 1, divided by n - 2 when normalized (NaN below 3 nodes). The
+ * other measures (0 degree, 1 betweenness, 2 closeness) fail with a
+ * message. Replaces netcapi.h:534-539 (crates/capi/src/topography.rs:134-159). */
+NET_API int32_t net_centralization(const GraphHandle *h, int32_t measure, int32_t mode,
+                                   int32_t loops, int32_t normalized, int32_t convention,
+                                   int32_t threads, double *out, char *err, size_t err_len);
+
 /* ---- Extensions (no counterpart in the reference) ---------------------- */
 
 /* What a solve did. */

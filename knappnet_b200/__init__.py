@@ -80,6 +80,10 @@ def lib() -> ctypes.CDLL:
     L.net_eigenvector.argtypes = [h, i32, i32, i32, i32, f64, i64, i32, vp,
                                   ctypes.POINTER(f64), ctypes.POINTER(i32), cp, sz]
     L.net_eigenvector.restype = i32
+    L.net_components.argtypes = [h, i32, vp, ctypes.POINTER(i64), cp, sz]
+    L.net_components.restype = i32
+    L.net_centralization.argtypes = [h, i32, i32, i32, i32, i32, i32, ctypes.POINTER(f64), cp, sz]
+    L.net_centralization.restype = i32
     L.net_katz.argtypes = [h, f64, vp, i64, i32, i32, i32, i32, f64, i64, i32, vp, cp, sz]
     L.net_katz.restype = i32
     L.net_bonacich_power.argtypes = [h, f64, i32, i32, i32, i32, f64, i64, i32, vp, cp, sz]
@@ -336,6 +340,28 @@ class Graph:
                               _ptr(hubs), _ptr(auths), ctypes.byref(val), ctypes.byref(uniq),
                               err, ERR_LEN), err)
         return hubs[: self.n], auths[: self.n], val.value, bool(uniq.value)
+
+    def components(self, strong=False):
+        """Weak or strong components (net_components): labels numbered in
+        order of each component's lowest node, and their count."""
+        memb = np.zeros(max(self.n, 1), dtype=np.int32)
+        cnt = ctypes.c_int64()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_components(self.h, int(bool(strong)), _ptr(memb), ctypes.byref(cnt),
+                                    err, ERR_LEN), err)
+        return memb[: self.n], cnt.value
+
+    def centralization(self, measure=3, mode=3, loops=True, normalized=True, convention=0):
+        """Freeman centralization (net_centralization); this library
+        provides the eigenvector measure (3) under the igraph convention."""
+        out = ctypes.c_double()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_centralization(self.h, measure, mode, int(loops), int(normalized),
+                                        convention, 0, ctypes.byref(out), err, ERR_LEN), err)
+        return out.value
+
+    def centralization_eigenvector(self, normalized=True):
+        return self.centralization(3, 3, True, normalized, 0)
 
     def eigenvector(self, mode=2, weighted=False, scale=0, loops=0, tol=0.0, max_iter=0,
                     threads=0, precision=0):

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <limits>
 #include <new>
 #include <string>
 #include <vector>
@@ -491,6 +492,85 @@ int32_t net_eigenvector_ex(const GraphHandle* h, int32_t mode, int32_t weighted,
                            NetSolveInfo* info, char* err, size_t err_len) {
   return eigen_impl(h, mode, weighted, scale, loops, tol, max_iter, precision, out, eigenvalue,
                     connected, info, err, err_len);
+}
+
+int32_t net_components(const GraphHandle* h, int32_t kind, int32_t* membership, int64_t* count,
+                       char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    // ComponentKind::from_code (crates/engine/src/metrics/topography.rs:152-163)
+    if (kind != 0 && kind != 1) throw Error("unknown component kind code " + std::to_string(kind));
+    cudaStream_t s = knb::thread_stream();
+    knb::Comps c = kind == 1 && g.directed ? knb::strong_components(g, nullptr, false, nullptr, s)
+                                           : knb::weak_components(g, s);
+    for (uint32_t v = 0; v < g.n; ++v) {
+      if (c.membership[v] > (uint32_t)INT32_MAX)
+        throw Error("component count " + std::to_string(c.membership[v]) + " is too large");
+      membership[v] = (int32_t)c.membership[v];
+    }
+    *count = (int64_t)c.count();
+  });
+}
+
+int32_t net_centralization(const GraphHandle* h, int32_t measure, int32_t mode, int32_t loops,
+                           int32_t normalized, int32_t convention, int32_t threads, double* out,
+                           char* err, size_t err_len) {
+  (void)threads;
+  (void)loops;  // degree centralization only
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    // codes, then the convention and measure rules
+    // (crates/engine/src/metrics/topography.rs:320-334,376-387,475-498)
+    if (measure < 0 || measure > 3)
+      throw Error("unknown centralization measure code " + std::to_string(measure));
+    if (mode < 1 || mode > 3) throw Error("unknown degree mode code " + std::to_string(mode));
+    if (convention < 0 || convention > 3)
+      throw Error("unknown convention code " + std::to_string(convention));
+    static const char* names[] = {"igraph", "NetworkX", "sna", "UCINET"};
+    if (convention == 1)
+      throw Error("NetworkX has no centralization index; use the igraph, sna, or UCINET convention");
+    if (measure != 3)
+      throw Error("degree, betweenness and closeness centralization are outside this library, "
+                  "which provides the spectral measures only (measure 3, eigenvector)");
+    if (convention != 0)
+      throw Error(std::string("eigenvector centralization is provided for the igraph convention "
+                              "only, not ") + names[convention]);
+    if (g.directed && mode != 3)
+      throw Error("eigenvector centralization is provided with direction ignored (mode \"all\") only");
+    const uint32_t n = g.n;
+    if (n == 0) {
+      *out = std::numeric_limits<double>::quiet_NaN();
+      return;
+    }
+    // eigenvector centrality, direction ignored, unweighted, scaled to max
+    // 1, loops twice, default tolerance and cap; then Freeman's index
+    // n max - sum, over n - 2 when normalized (topography.rs:446-472,512-560)
+    knb::EigenParams p;
+    p.mode = 3;
+    p.weighted = false;
+    p.scale = 0;
+    p.loops = 0;
+    p.tol = 1e-12;
+    p.max_iter = 10000;
+    std::vector<double> x(n);
+    knb::EigenResult r;
+    knb::eigenvector(g, p, x.data(), &r, knb::thread_stream());
+    double mx = -std::numeric_limits<double>::infinity(), total = 0.0;
+    bool nan = false;
+    for (double v : x) {
+      mx = std::fmax(mx, v);
+      total += v;
+      nan = nan || std::isnan(v);
+    }
+    if (nan) mx = std::numeric_limits<double>::quiet_NaN();
+    const double raw = (double)n * mx - total;
+    if (!normalized) {
+      *out = raw;
+      return;
+    }
+    const double tmax = n < 3 ? std::numeric_limits<double>::quiet_NaN() : (double)n - 2.0;
+    *out = raw / tmax;
+  });
 }
 
 int32_t net_generate_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,

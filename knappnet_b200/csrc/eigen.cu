@@ -258,63 +258,234 @@ Comps weak_components(GraphHandleImpl& g, cudaStream_t s) {
   return c;
 }
 
-// Tarjan's algorithm with an explicit stack over the out-CSR (host).
-Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint32_t>& tgt,
-                        uint32_t n) {
-  const uint32_t UNSEEN = 0xFFFFFFFFu;
-  std::vector<uint32_t> index(n, UNSEEN), low(n, 0), comp(n, UNSEEN), stack;
-  std::vector<uint8_t> on(n, 0);
-  std::vector<std::pair<uint32_t, uint32_t>> frames;
-  uint32_t counter = 0, ncomp = 0;
-  for (uint32_t root = 0; root < n; ++root) {
-    if (index[root] != UNSEEN) continue;
-    frames.push_back({root, 0});
-    index[root] = low[root] = counter++;
-    stack.push_back(root);
-    on[root] = 1;
-    while (!frames.empty()) {
-      uint32_t v = frames.back().first;
-      uint32_t& pos = frames.back().second;
-      if (pos < off[v + 1] - off[v]) {
-        uint32_t w = tgt[off[v] + pos];
-        ++pos;
-        if (index[w] == UNSEEN) {
-          index[w] = low[w] = counter++;
-          stack.push_back(w);
-          on[w] = 1;
-          frames.push_back({w, 0});
-        } else if (on[w]) {
-          low[v] = std::min(low[v], index[w]);
-        }
-        continue;
-      }
-      frames.pop_back();
-      if (!frames.empty()) low[frames.back().first] = std::min(low[frames.back().first], low[v]);
-      if (low[v] == index[v]) {
-        for (;;) {
-          uint32_t w = stack.back();
-          stack.pop_back();
-          on[w] = 0;
-          comp[w] = ncomp;
-          if (w == v) break;
-        }
-        ++ncomp;
-      }
+// ======================================================================= strong components (device)
+// Strong components of the arcs (src[e], tgt[e]) on the device, as rounds
+// over the nodes not yet assigned to a component:
+//  1. trim: a node with no unassigned in-neighbour, or none out, other than
+//     itself, is a component of its own (repeated to a fixed point);
+//  2. colour: each node takes the largest id that reaches it through
+//     unassigned nodes (max propagation along the arcs to a fixed point);
+//  3. a node whose colour is its own id is the largest node of its
+//     component, which is the set of nodes of that colour that reach it: a
+//     path from such a node to the root never leaves the colour, so
+//     propagation backwards along the arcs inside the colour finds it.
+// Each round assigns at least the component of the largest unassigned id.
+// Every pass is one thread per arc (the arc list is balanced whatever the
+// degrees), and a pass that changes nothing ends its fixed point; passes
+// are enqueued four at a time between reads of their change flags.
+// Components are labelled in order of their smallest node, as Tarjan's
+// labels (crates/engine/src/metrics/topography.rs:183-221).
+constexpr uint32_t SCC_NONE = 0xFFFFFFFFu;
+
+// Arcs (src[e], tgt[e]) for e < m; with w given only arcs with w[e] > 0
+// take part; with `both` each arc also counts reversed. Loops never matter.
+struct SccArcs {
+  const uint32_t* src;
+  const uint32_t* tgt;
+  const double* w;
+  uint64_t m;
+  int both;
+};
+
+__device__ __forceinline__ bool scc_arc(const SccArcs& a, uint64_t e, const uint32_t* rep,
+                                        uint32_t* u, uint32_t* v) {
+  *u = a.src[e];
+  *v = a.tgt[e];
+  if (*u == *v) return false;
+  if (a.w && !(a.w[e] > 0.0)) return false;
+  return rep[*u] == SCC_NONE && rep[*v] == SCC_NONE;
+}
+
+__device__ __forceinline__ void scc_flag(bool c, unsigned int* flag) {
+  if (__syncthreads_or(c) && threadIdx.x == 0) *flag = 1u;
+}
+
+__global__ void scc_trim_mark(SccArcs a, const uint32_t* __restrict__ rep, uint8_t* hasin,
+                              uint8_t* hasout) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < a.m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t u, v;
+    if (!scc_arc(a, e, rep, &u, &v)) continue;
+    if (!hasout[u]) hasout[u] = 1;
+    if (!hasin[v]) hasin[v] = 1;
+    if (a.both) {
+      if (!hasout[v]) hasout[v] = 1;
+      if (!hasin[u]) hasin[u] = 1;
     }
   }
+}
+
+// changed: some node was assigned; left: some node is still unassigned.
+__global__ void scc_trim_assign(uint32_t n, uint32_t* rep, uint8_t* hasin, uint8_t* hasout,
+                                unsigned int* changed, unsigned int* left) {
+  bool c = false, l = false;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    if (rep[v] != SCC_NONE) continue;
+    if (!hasin[v] || !hasout[v]) {
+      rep[v] = v;
+      c = true;
+    } else {
+      l = true;
+    }
+    hasin[v] = 0;
+    hasout[v] = 0;
+  }
+  scc_flag(c, changed);
+  scc_flag(l, left);
+}
+
+__global__ void scc_color_init(uint32_t n, const uint32_t* __restrict__ rep, uint32_t* color) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (rep[v] == SCC_NONE) color[v] = v;
+}
+
+// Colours only grow, so a pass in which no thread raised one read settled
+// values throughout: that pass ends the fixed point.
+__global__ void scc_color_push(SccArcs a, const uint32_t* __restrict__ rep, uint32_t* color,
+                               unsigned int* changed) {
+  bool c = false;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < a.m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t u, v;
+    if (!scc_arc(a, e, rep, &u, &v)) continue;
+    const uint32_t cu = color[u], cv = color[v];
+    if (cv < cu) {
+      atomicMax(&color[v], cu);
+      c = true;
+    }
+    if (a.both && cu < cv) {
+      atomicMax(&color[u], cv);
+      c = true;
+    }
+  }
+  scc_flag(c, changed);
+}
+
+__global__ void scc_roots(uint32_t n, const uint32_t* __restrict__ rep,
+                          const uint32_t* __restrict__ color, uint8_t* mark) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (rep[v] == SCC_NONE) mark[v] = color[v] == v ? 1 : 0;
+}
+
+__global__ void scc_back(SccArcs a, const uint32_t* __restrict__ rep,
+                         const uint32_t* __restrict__ color, uint8_t* mark, unsigned int* changed) {
+  bool c = false;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < a.m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t u, v;
+    if (!scc_arc(a, e, rep, &u, &v)) continue;
+    if (color[u] != color[v]) continue;
+    const uint8_t mu = mark[u], mv = mark[v];
+    if (!mu && mv) {
+      mark[u] = 1;
+      c = true;
+    }
+    if (a.both && mu && !mv) {
+      mark[v] = 1;
+      c = true;
+    }
+  }
+  scc_flag(c, changed);
+}
+
+__global__ void scc_assign(uint32_t n, uint32_t* rep, const uint32_t* __restrict__ color,
+                           const uint8_t* __restrict__ mark) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (rep[v] == SCC_NONE && mark[v]) rep[v] = color[v];
+}
+
+__global__ void scc_smallest(uint32_t n, const uint32_t* __restrict__ rep, uint32_t* smallest) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    atomicMin(&smallest[rep[v]], v);
+}
+
+__global__ void scc_root_of(uint32_t n, const uint32_t* __restrict__ rep,
+                            const uint32_t* __restrict__ smallest, uint32_t* root,
+                            uint32_t* is_root) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t r = smallest[rep[v]];
+    root[v] = r;
+    is_root[v] = r == v;
+  }
+}
+
+static Comps strong_components_device(const SccArcs& a, uint32_t n, int* launches,
+                                      cudaStream_t s) {
   Comps c;
-  std::vector<uint32_t> relabel(n, UNSEEN);
-  c.membership.resize(n);
-  for (uint32_t v = 0; v < n; ++v) {
-    uint32_t r = comp[v];
-    if (relabel[r] == UNSEEN) {
-      relabel[r] = (uint32_t)c.sizes.size();
-      c.sizes.push_back(0);
+  if (n == 0) return c;
+  constexpr int BATCH = 4;
+  DevBuf<uint32_t> rep(n), color(n), smallest(n), root(n), flag((size_t)n + 1), label(n);
+  DevBuf<uint8_t> hasin(n), hasout(n), mark(n);
+  DevBuf<unsigned int> flags(2 * BATCH);
+  unsigned int hf[2 * BATCH];
+  KNB_CUDA(cudaMemsetAsync(rep.get(), 0xFF, (size_t)n * 4, s));
+  KNB_CUDA(cudaMemsetAsync(hasin.get(), 0, n, s));
+  KNB_CUDA(cudaMemsetAsync(hasout.get(), 0, n, s));
+  const unsigned gn = grid_for(n, ET, 148 * 16);
+  const unsigned ga = a.m ? grid_for(a.m, ET, 148 * 16) : 1;
+  int nl = 0;
+  // Runs `pass` (one pass, writing its change flag to flags[b]) to a fixed
+  // point; returns the batch slot of the pass that changed nothing.
+  auto settle = [&](auto pass) -> int {
+    for (uint64_t done = 0;; done += BATCH) {
+      if (done > (uint64_t)n + 2 * BATCH)
+        throw Error("strong components did not settle (internal error)");
+      KNB_CUDA(cudaMemsetAsync(flags.get(), 0, 2 * BATCH * 4, s));
+      for (int b = 0; b < BATCH; ++b) pass(b);
+      KNB_LAUNCH("strong components");
+      KNB_CUDA(cudaMemcpyAsync(hf, flags.get(), 2 * BATCH * 4, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      for (int b = 0; b < BATCH; ++b)
+        if (!hf[b]) return b;
     }
-    c.membership[v] = relabel[r];
-    c.sizes[relabel[r]]++;
+  };
+  for (;;) {
+    const int b = settle([&](int slot) {
+      if (a.m) scc_trim_mark<<<ga, ET, 0, s>>>(a, rep.get(), hasin.get(), hasout.get());
+      scc_trim_assign<<<gn, ET, 0, s>>>(n, rep.get(), hasin.get(), hasout.get(),
+                                        flags.get() + slot, flags.get() + BATCH + slot);
+      nl += 2;
+    });
+    if (!hf[BATCH + b]) break;
+    scc_color_init<<<gn, ET, 0, s>>>(n, rep.get(), color.get());
+    ++nl;
+    settle([&](int slot) {
+      scc_color_push<<<ga, ET, 0, s>>>(a, rep.get(), color.get(), flags.get() + slot);
+      ++nl;
+    });
+    scc_roots<<<gn, ET, 0, s>>>(n, rep.get(), color.get(), mark.get());
+    ++nl;
+    settle([&](int slot) {
+      scc_back<<<ga, ET, 0, s>>>(a, rep.get(), color.get(), mark.get(), flags.get() + slot);
+      ++nl;
+    });
+    scc_assign<<<gn, ET, 0, s>>>(n, rep.get(), color.get(), mark.get());
+    ++nl;
   }
+  // label in order of each component's smallest node
+  KNB_CUDA(cudaMemsetAsync(smallest.get(), 0xFF, (size_t)n * 4, s));
+  scc_smallest<<<gn, ET, 0, s>>>(n, rep.get(), smallest.get());
+  scc_root_of<<<gn, ET, 0, s>>>(n, rep.get(), smallest.get(), root.get(), flag.get());
+  KNB_LAUNCH("strong component labels");
+  const uint32_t k = exclusive_scan<uint32_t>(flag.get(), flag.get(), n, s);
+  DevBuf<uint32_t> sizes(std::max<uint32_t>(k, 1));
+  KNB_CUDA(cudaMemsetAsync(sizes.get(), 0, (size_t)std::max<uint32_t>(k, 1) * 4, s));
+  uf_label<<<gn, ET, 0, s>>>(root.get(), flag.get(), n, label.get(), sizes.get());
+  KNB_LAUNCH("uf_label");
+  nl += 3;
+  c.membership.resize(n);
+  c.sizes.resize(k);
+  KNB_CUDA(cudaMemcpyAsync(c.membership.data(), label.get(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  if (k) KNB_CUDA(cudaMemcpyAsync(c.sizes.data(), sizes.get(), (size_t)k * 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  if (launches) *launches += nl;
   return c;
+}
+
+Comps strong_components(GraphHandleImpl& g, const double* w, bool both, int* launches,
+                        cudaStream_t s) {
+  SccArcs a{g.src.get(), g.tgt.get(), w, g.m, both ? 1 : 0};
+  return strong_components_device(a, g.n, launches, s);
 }
 
 // ======================================================================= small kernels
@@ -1586,12 +1757,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
   // components: strong (directed h) or weak; whether any is cyclic
   if (!plan.ready) {
     if (hdir) {
-      std::vector<uint32_t> off(n + 1), tgt(g.out.arcs);
-      KNB_CUDA(cudaMemcpyAsync(off.data(), g.out.off.get(), ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
-      if (g.out.arcs)
-        KNB_CUDA(cudaMemcpyAsync(tgt.data(), g.out.tgt.get(), g.out.arcs * 4, cudaMemcpyDeviceToHost, s));
-      KNB_CUDA(cudaStreamSynchronize(s));
-      plan.comps = strong_components(off, tgt, n);
+      plan.comps = strong_components(g, nullptr, false, &launches, s);
     } else {
       plan.comps = weak_components(g, s);
       launches += 5;

@@ -36,10 +36,11 @@ struct Comps {
 // Weak components of the handle's edges (device union-find; each
 // component's label follows its smallest node).
 Comps weak_components(GraphHandleImpl& g, cudaStream_t s);
-// Strong components of the directed graph in host CSR form (Tarjan's
-// algorithm with an explicit stack), labelled in order of smallest node.
-Comps strong_components(const std::vector<uint32_t>& off, const std::vector<uint32_t>& tgt,
-                        uint32_t n);
+// Strong components of the handle's edges on the device, labelled in order
+// of smallest node. With w (device, one value per edge) only edges with
+// w > 0 take part; with `both` every edge also counts reversed.
+Comps strong_components(GraphHandleImpl& g, const double* w, bool both, int* launches,
+                        cudaStream_t s);
 
 // Writes n scores to `out` (host). Throws knb::Error on failure.
 void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenResult* r,

@@ -432,21 +432,9 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
   };
   Comps comp;
   if (g.directed) {
-    // strong components of the positive entries (spectral.rs:539-553)
-    std::vector<uint32_t> off((size_t)n + 1, 0);
-    for (uint64_t e = 0; e < g.m; ++e)
-      if (value(e) > 0.0) {
-        off[src[e] + 1] += 1;
-        if (rw.all && src[e] != tgt[e]) off[tgt[e] + 1] += 1;
-      }
-    for (uint32_t v = 0; v < n; ++v) off[v + 1] += off[v];
-    std::vector<uint32_t> pos(off.begin(), off.end() - 1), arcs(off[n]);
-    for (uint64_t e = 0; e < g.m; ++e)
-      if (value(e) > 0.0) {
-        arcs[pos[src[e]]++] = tgt[e];
-        if (rw.all && src[e] != tgt[e]) arcs[pos[tgt[e]]++] = src[e];
-      }
-    comp = strong_components(off, arcs, n);
+    // strong components of the positive entries (spectral.rs:539-553); a
+    // loop's factor leaves the pattern of the other entries as it is
+    comp = strong_components(g, weighted ? g.w.get() : nullptr, rw.all, nullptr, s);
   } else {
     comp = weak_components(g, s);
   }

@@ -200,6 +200,28 @@ class Graph:
         return out[: self.n], val.value, bool(conn.value)
 
 
+    def centralization_eigenvector(self, normalized=True):
+        """igraph's eigenvector centralization
+        (crates/engine/src/metrics/topography.rs:446-498,536-548): eigenvector
+        centrality with direction ignored, unweighted, loops twice, scaled
+        to max 1; then n max - sum (NaN if a score is NaN), over n - 2 when
+        normalized (NaN below 3 nodes); NaN for no nodes."""
+        n = self.n
+        if n == 0:
+            return float("nan")
+        x, _, _ = self.eigenvector(mode=3, weighted=False, scale=0, loops=0)
+        mx = float("-inf")
+        total = 0.0
+        for v in x.tolist():
+            mx = max(mx, v) if v == v else mx
+            total += v
+        if any(v != v for v in x.tolist()):
+            mx = float("nan")
+        raw = n * mx - total
+        if not normalized:
+            return raw
+        return raw / (n - 2.0) if n >= 3 else float("nan")
+
     def katz(self, alpha=0.1, beta=1.0, mode=2, weighted=False, loops=1, normalized=True,
              tol=0.0, max_iter=0, threads=0):
         """net_katz (spectral.rs:365-407); beta is one value or n values."""

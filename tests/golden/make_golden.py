@@ -27,7 +27,9 @@ import yaml
 HERE = Path(__file__).resolve().parent
 
 # Variants on the spectral-centrality path: PageRank, Katz, Bonacich power
-# centrality and hubs and authorities (spectral.yaml), eigenvector centrality (topography.yaml).
+# centrality and hubs and authorities (spectral.yaml), eigenvector centrality
+# and the components it is computed on (topography.yaml), eigenvector
+# centralization (roles.yaml).
 # Variants that first simplify or symmetrize the network through
 # net_graph_simplify (eigenvector_sna, eigenvector_ucinet, bonacich_sna) are
 # outside it.
@@ -40,7 +42,9 @@ VARIANTS = {
                       "hits_authorities", "hits_hubs", "hits_authorities_networkx",
                       "hits_hubs_networkx"],
     "topography.yaml": ["eigenvector", "eigenvector_networkx", "eigenvector_weighted",
-                        "eigenvector_weighted_networkx", "eigenvector_undirected"],
+                        "eigenvector_weighted_networkx", "eigenvector_undirected",
+                        "components_weak", "components_strong"],
+    "roles.yaml": ["centralization_eigenvector"],
 }
 ORACLES = ["definition", "networkx"]
 
@@ -78,6 +82,7 @@ def main():
                 "applies_to": e.get("applies_to", "any"),
                 "requires_weights": bool(e.get("requires_weights", False)),
                 "tolerance": e["tolerance"],
+                "compare": e.get("compare", "values"),
                 "source": f"validation/manifest.d/{fname}",
             }
 
@@ -112,7 +117,8 @@ def main():
     doc = {
         "about": "validation fixtures and golden values of the reference engine "
                  "(validation/fixtures, validation/golden/{definition,networkx}) for "
-                 "PageRank, Katz, Bonacich power, HITS and eigenvector centrality; generated "
+                 "PageRank, Katz, Bonacich power, HITS, eigenvector centrality, components "
+                 "and eigenvector centralization; generated "
                  "by make_golden.py",
         "oracle_versions": versions,
         "manifest": manifest,

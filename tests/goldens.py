@@ -124,12 +124,34 @@ def _run_variant(g, fx: dict, variant: str):
         exponent = relative(e, "exponent", g, "in" if mode == "out" else mode, weighted, loops)
         return g.bonacich(exponent=exponent, mode=MODES[mode], weighted=weighted,
                           loops=LOOPS[loops], rescale=bool(e.get("rescale", False)))
+    if e["fn"] == "components":
+        memb, _ = g.components(strong=e["kind"] == "strong")
+        return [float(v) for v in memb]
+    if e["fn"] == "centralization_eigenvector":
+        # validation/bindings/roles.py:207-212: one value, NaN when undefined
+        return [g.centralization_eigenvector(normalized=bool(e.get("normalized", True)))]
     if e["fn"] == "hits":
         hubs, auths, _, _ = g.hits(weighted=bool(e.get("weighted", False)),
                                    loops=LOOPS[e.get("loops", "twice")],
                                    scale=HITS_SCALES[e.get("scale", "max")])
         return hubs if e["which"] == "hubs" else auths
     raise ValueError(e["fn"])
+
+
+def canonical(values, mode: str):
+    """validation/compare.py:40-60 for the modes on this path: values as
+    given, or (partition) group labels renumbered by first appearance."""
+    if mode == "partition":
+        seen = {}
+        return [None if v is None else float(seen.setdefault(v, len(seen))) for v in values]
+    return list(values)
+
+
+def agree_variant(ours, theirs, variant: str):
+    """`agree` after putting both sides in the variant's comparison form."""
+    spec = load()["manifest"][variant]
+    mode = spec.get("compare", "values")
+    return agree(canonical(list(ours), mode), canonical(list(theirs), mode), spec["tolerance"])
 
 
 def agree(ours, theirs, tol: dict):

@@ -32,8 +32,7 @@ def test_golden(fx_name, variant, orc):
     fx = DOC["fixtures"][fx_name]
     g = goldens.make_graph(K.Graph, fx)
     got = goldens.run_variant(g, fx, variant)
-    ok, msg = goldens.agree(list(got), DOC["golden"][fx_name][variant][orc],
-                            DOC["manifest"][variant]["tolerance"])
+    ok, msg = goldens.agree_variant(got, DOC["golden"][fx_name][variant][orc], variant)
     assert ok, msg
 
 

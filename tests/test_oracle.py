@@ -28,8 +28,7 @@ def test_oracle_matches_golden(fx_name, variant, orc):
     fx = doc["fixtures"][fx_name]
     g = goldens.make_graph(O.Graph, fx)
     got = goldens.run_variant(g, fx, variant)
-    ok, msg = goldens.agree(list(got), doc["golden"][fx_name][variant][orc],
-                            doc["manifest"][variant]["tolerance"])
+    ok, msg = goldens.agree_variant(got, doc["golden"][fx_name][variant][orc], variant)
     assert ok, msg
 
 
