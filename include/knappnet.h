@@ -107,6 +107,26 @@ NET_API int32_t net_eigenvector(const GraphHandle *h, int32_t mode, int32_t weig
                         double *eigenvalue, int32_t *connected, char *err,
                         size_t err_len);
 
+/* The adjacency-matrix reading of a graph (sna, UCINET): parallel edges
+ * collapse, keeping the largest (keep 0) or smallest (keep 1) weight, and
+ * self-loops are dropped; undirected != 0 also symmetrizes a directed
+ * graph. Edges come out sorted by (from, to). Release *out with
+ * net_graph_free. Replaces netcapi.h:62-64 (crates/capi/src/topography.rs:42-56). */
+NET_API int32_t net_graph_simplify(const GraphHandle *h, int32_t undirected, int32_t keep,
+                                   GraphHandle **out, char *err, size_t err_len);
+
+/* Eigenvector centrality of a two-mode network: the leading singular
+ * vectors of the binary incidence matrix, each mode scaled to Euclidean
+ * length 1 (NaN for every node when there are no ties). types holds n codes
+ * (0 first mode, 1 second); tol <= 0 and max_iter <= 0 select 1e-12 and
+ * 10000. *eigenvalue receives the largest singular value, *connected 1 if
+ * the network is connected. Replaces netcapi.h:762-771
+ * (crates/capi/src/twomode.rs:293-320). */
+NET_API int32_t net_twomode_eigenvector(const GraphHandle *h, const int32_t *types, double tol,
+                                        int64_t max_iter, int32_t threads, double *out,
+                                        double *eigenvalue, int32_t *connected, char *err,
+                                        size_t err_len);
+
 /* Weak (kind 0) or strong (kind 1) components: membership receives n
  * labels, numbered from 0 in order of each component's lowest-numbered
  * node, count one value; strong components of an undirected graph are its

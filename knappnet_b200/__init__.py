@@ -80,6 +80,11 @@ def lib() -> ctypes.CDLL:
     L.net_eigenvector.argtypes = [h, i32, i32, i32, i32, f64, i64, i32, vp,
                                   ctypes.POINTER(f64), ctypes.POINTER(i32), cp, sz]
     L.net_eigenvector.restype = i32
+    L.net_graph_simplify.argtypes = [h, i32, i32, ctypes.POINTER(h), cp, sz]
+    L.net_graph_simplify.restype = i32
+    L.net_twomode_eigenvector.argtypes = [h, vp, f64, i64, i32, vp, ctypes.POINTER(f64),
+                                          ctypes.POINTER(i32), cp, sz]
+    L.net_twomode_eigenvector.restype = i32
     L.net_components.argtypes = [h, i32, vp, ctypes.POINTER(i64), cp, sz]
     L.net_components.restype = i32
     L.net_centralization.argtypes = [h, i32, i32, i32, i32, i32, i32, ctypes.POINTER(f64), cp, sz]
@@ -340,6 +345,31 @@ class Graph:
                               _ptr(hubs), _ptr(auths), ctypes.byref(val), ctypes.byref(uniq),
                               err, ERR_LEN), err)
         return hubs[: self.n], auths[: self.n], val.value, bool(uniq.value)
+
+    def simplify(self, undirected=False, keep=0):
+        """The adjacency-matrix reading (net_graph_simplify): loops dropped,
+        parallel edges merged keeping the largest (keep 0) or smallest
+        (keep 1) weight; undirected symmetrizes a directed graph."""
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_graph_simplify(self.h, int(bool(undirected)), int(keep), ctypes.byref(h),
+                                        err, ERR_LEN), err)
+        m = int(lib().net_graph_edge_count(h))
+        return Graph(self.n, directed=self.directed and not undirected, _handle=h, _m=m,
+                     _weighted=self.weighted)
+
+    def twomode_eigenvector(self, types, tol=0.0, max_iter=0):
+        """Two-mode eigenvector centrality (net_twomode_eigenvector):
+        (scores, largest singular value, connected)."""
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        out = np.zeros(max(self.n, 1))
+        val = ctypes.c_double()
+        conn = ctypes.c_int32()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_twomode_eigenvector(self.h, _ptr(t), tol, max_iter, 0, _ptr(out),
+                                             ctypes.byref(val), ctypes.byref(conn), err,
+                                             ERR_LEN), err)
+        return out[: self.n], val.value, bool(conn.value)
 
     def components(self, strong=False):
         """Weak or strong components (net_components): labels numbered in

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <exception>
 #include <limits>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -135,6 +136,73 @@ __global__ void degree_rows(const uint32_t* __restrict__ off1, const uint32_t* _
     }
     out[v] = s;
   }
+}
+
+// ---- simplify (crates/engine/src/metrics/topography.rs:96-141): the
+// adjacency-matrix reading of a graph. Loops are dropped; every arc (for an
+// undirected result every unordered pair, as (smaller, larger)) is kept
+// once, sorted by (from, to), with the largest (keep 0) or smallest (keep 1)
+// weight of its parallel edges. Keys pack (from << tb) | to, with the
+// sentinel n << tb (after every real key) for a loop.
+__global__ void simplify_keys(const uint32_t* __restrict__ src, const uint32_t* __restrict__ tgt,
+                              uint64_t m, int directed, int tb, uint64_t sentinel,
+                              uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = src[e], b = tgt[e];
+    uint64_t k = sentinel;
+    if (a != b) {
+      const bool keep_order = directed || a < b;
+      k = ((uint64_t)(keep_order ? a : b) << tb) | (uint64_t)(keep_order ? b : a);
+    }
+    keys[e] = k;
+    idx[e] = (uint32_t)e;
+  }
+}
+
+__device__ __forceinline__ bool simplify_head(const uint64_t* keys, uint64_t i, uint64_t sentinel) {
+  return keys[i] != sentinel && (i == 0 || keys[i] != keys[i - 1]);
+}
+
+__global__ void simplify_heads(const uint64_t* __restrict__ keys, uint64_t m, uint64_t sentinel,
+                               uint32_t* __restrict__ head) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    head[i] = simplify_head(keys, i, sentinel) ? 1u : 0u;
+}
+
+// One thread per run of equal keys (at its head): the pair and the run's
+// largest or smallest weight.
+__global__ void simplify_emit(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ idx,
+                              const uint32_t* __restrict__ pos, uint64_t m, uint64_t sentinel,
+                              int tb, const double* __restrict__ w, int keep_min,
+                              uint32_t* __restrict__ out_src, uint32_t* __restrict__ out_tgt,
+                              double* __restrict__ out_w) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if (!simplify_head(keys, i, sentinel)) continue;
+    const uint64_t k = keys[i];
+    const uint32_t p = pos[i];
+    out_src[p] = (uint32_t)(k >> tb);
+    out_tgt[p] = (uint32_t)(k & ((1ull << tb) - 1));
+    if (w) {
+      double x = w[idx[i]];
+      for (uint64_t j = i + 1; j < m && keys[j] == k; ++j) {
+        const double y = w[idx[j]];
+        x = keep_min ? fmin(x, y) : fmax(x, y);
+      }
+      out_w[p] = x;
+    }
+  }
+}
+
+// First edge whose two ends have the same node type.
+__global__ void same_mode_edge(const uint32_t* __restrict__ src, const uint32_t* __restrict__ tgt,
+                               uint64_t m, const uint8_t* __restrict__ type,
+                               unsigned long long* __restrict__ bad) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    if (type[src[e]] == type[tgt[e]]) atomicMin(bad, (unsigned long long)e);
 }
 
 unsigned long long read_u64(const unsigned long long* d, cudaStream_t s) {
@@ -492,6 +560,130 @@ int32_t net_eigenvector_ex(const GraphHandle* h, int32_t mode, int32_t weighted,
                            NetSolveInfo* info, char* err, size_t err_len) {
   return eigen_impl(h, mode, weighted, scale, loops, tol, max_iter, precision, out, eigenvalue,
                     connected, info, err, err_len);
+}
+
+int32_t net_graph_simplify(const GraphHandle* h, int32_t undirected, int32_t keep,
+                           GraphHandle** out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    // ParallelWeight::from_code (crates/engine/src/metrics/topography.rs:86-96)
+    if (keep != 0 && keep != 1)
+      throw Error("unknown parallel-edge weight code " + std::to_string(keep));
+    if (!out) throw Error("output handle pointer is null");
+    cudaStream_t s = knb::thread_stream();
+    const bool directed = g.directed && !undirected;
+    const uint64_t m = g.m;
+    int tb = 0;
+    while (tb < 32 && (1ull << tb) < (uint64_t)g.n) ++tb;
+    int hb = 0;
+    while (hb < 33 && (1ull << hb) < (uint64_t)g.n + 1) ++hb;
+    const uint64_t sentinel = (uint64_t)g.n << tb;
+    knb::DevBuf<uint64_t> keys(std::max<uint64_t>(m, 1));
+    knb::DevBuf<uint32_t> idx(std::max<uint64_t>(m, 1)), pos(std::max<uint64_t>(m, 1));
+    uint64_t mo = 0;
+    if (m) {
+      const unsigned gm = knb::grid_for(m, 256);
+      simplify_keys<<<gm, 256, 0, s>>>(g.src.get(), g.tgt.get(), m, directed ? 1 : 0, tb, sentinel,
+                                       keys.get(), idx.get());
+      KNB_LAUNCH("simplify_keys");
+      knb::radix_sort(keys.get(), idx.get(), m, tb + hb, s);
+      simplify_heads<<<gm, 256, 0, s>>>(keys.get(), m, sentinel, pos.get());
+      KNB_LAUNCH("simplify_heads");
+      mo = knb::exclusive_scan<uint32_t>(pos.get(), pos.get(), m, s);
+    }
+    knb::DevBuf<uint32_t> os(std::max<uint64_t>(mo, 1)), ot(std::max<uint64_t>(mo, 1));
+    knb::DevBuf<double> ow(g.weighted ? std::max<uint64_t>(mo, 1) : 0);
+    if (mo) {
+      simplify_emit<<<knb::grid_for(m, 256), 256, 0, s>>>(
+          keys.get(), idx.get(), pos.get(), m, sentinel, tb, g.weighted ? g.w.get() : nullptr,
+          keep, os.get(), ot.get(), g.weighted ? ow.get() : nullptr);
+      KNB_LAUNCH("simplify_emit");
+    }
+    char e2[512] = {0};
+    if (net_graph_new_device((int64_t)g.n, os.get(), ot.get(), nullptr,
+                             g.weighted ? ow.get() : nullptr, (int64_t)mo, directed ? 1 : 0, out,
+                             e2, sizeof e2))
+      throw Error(e2);
+  });
+}
+
+int32_t net_twomode_eigenvector(const GraphHandle* h, const int32_t* types, double tol,
+                                int64_t max_iter, int32_t threads, double* out,
+                                double* eigenvalue, int32_t* connected, char* err,
+                                size_t err_len) {
+  (void)threads;
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    // types_from, check_types (crates/capi/src/twomode.rs:50-66,
+    // crates/engine/src/metrics/bipartite.rs:93-111)
+    if (!types) throw Error("node types are missing");
+    const uint32_t n = g.n;
+    std::vector<uint8_t> t(std::max<uint32_t>(n, 1), 0);
+    for (uint32_t v = 0; v < n; ++v) {
+      if (types[v] != 0 && types[v] != 1)
+        throw Error("node " + std::to_string(v) + " has type code " + std::to_string(types[v]) +
+                    "; use 0 for the first mode and 1 for the second");
+      t[v] = (uint8_t)types[v];
+    }
+    const double tl = tol > 0 ? tol : 1e-12;
+    const int64_t mi = max_iter > 0 ? max_iter : 10000;
+    cudaStream_t s = knb::thread_stream();
+    if (g.m) {
+      knb::DevBuf<uint8_t> td(std::max<uint32_t>(n, 1));
+      knb::DevBuf<unsigned long long> bad(1);
+      KNB_CUDA(cudaMemcpyAsync(td.get(), t.data(), n, cudaMemcpyHostToDevice, s));
+      KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+      same_mode_edge<<<knb::grid_for(g.m, 256), 256, 0, s>>>(g.src.get(), g.tgt.get(), g.m,
+                                                             td.get(), bad.get());
+      KNB_LAUNCH("same_mode_edge");
+      const uint64_t e = read_u64(bad.get(), s);
+      if (e != NONE) {
+        uint32_t a = 0, b = 0;
+        KNB_CUDA(cudaMemcpyAsync(&a, g.src.get() + e, 4, cudaMemcpyDeviceToHost, s));
+        KNB_CUDA(cudaMemcpyAsync(&b, g.tgt.get() + e, 4, cudaMemcpyDeviceToHost, s));
+        KNB_CUDA(cudaStreamSynchronize(s));
+        throw Error("edge " + std::to_string(e) + " joins nodes " + std::to_string(a) + " and " +
+                    std::to_string(b) +
+                    ", which are in the same mode; in a two-mode network every edge joins the "
+                    "two modes");
+      }
+    }
+    // the binary affiliation graph (bipartite.rs:113-116), then eigenvector
+    // centrality with direction ignored, unweighted, unit scale, loops
+    // ignored; each mode's half scaled to length 1 (bipartite.rs:288-336)
+    GraphHandle* a = nullptr;
+    char e2[512] = {0};
+    if (net_graph_simplify(h, 1, 0, &a, e2, sizeof e2)) throw Error(e2);
+    std::unique_ptr<GraphHandle> own(a);
+    knb::EigenParams p;
+    p.mode = 3;
+    p.weighted = false;
+    p.scale = 1;
+    p.loops = 2;
+    p.tol = tl;
+    p.max_iter = mi;
+    knb::EigenResult r;
+    std::vector<double> x(std::max<uint32_t>(n, 1));
+    knb::eigenvector(a->g, p, x.data(), &r, s);
+    if (a->g.m == 0) {
+      for (uint32_t v = 0; v < n; ++v) out[v] = std::numeric_limits<double>::quiet_NaN();
+      if (eigenvalue) *eigenvalue = 0.0;
+      if (connected) *connected = r.connected ? 1 : 0;
+      return;
+    }
+    for (uint8_t mode = 0; mode < 2; ++mode) {
+      double ss = 0.0;
+      for (uint32_t v = 0; v < n; ++v)
+        if (t[v] == mode) ss += x[v] * x[v];
+      const double norm = std::sqrt(ss);
+      if (norm > 0.0)
+        for (uint32_t v = 0; v < n; ++v)
+          if (t[v] == mode) x[v] /= norm;
+    }
+    memcpy(out, x.data(), (size_t)n * 8);
+    if (eigenvalue) *eigenvalue = r.eigenvalue;
+    if (connected) *connected = r.connected ? 1 : 0;
+  });
 }
 
 int32_t net_components(const GraphHandle* h, int32_t kind, int32_t* membership, int64_t* count,

@@ -7,6 +7,7 @@ use it as the checker; the product library never imports it.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -138,6 +139,7 @@ class Graph:
         self.m = len(s)
         self.directed = bool(directed)
         self.weighted = w is not None
+        self._src, self._tgt, self._w = s, t, w
         h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(ERR_LEN)
         if lib().orc_graph_new(self.n, _ptr(s), _ptr(t), _ptr(w), self.m, int(directed),
@@ -199,6 +201,71 @@ class Graph:
         self.last_iters = it.value
         return out[: self.n], val.value, bool(conn.value)
 
+
+    def edges(self):
+        return self._src.copy(), self._tgt.copy(), (None if self._w is None else self._w.copy())
+
+    def simplify(self, undirected=False, keep=0):
+        """simplify (crates/engine/src/metrics/topography.rs:96-141): loops
+        dropped; each arc, or for an undirected result each pair as
+        (smaller, larger), once in (from, to) order with the largest (keep 0)
+        or smallest (keep 1) weight of its parallel edges."""
+        if keep not in (0, 1):
+            raise OracleError(f"unknown parallel-edge weight code {keep}")
+        directed = self.directed and not undirected
+        s, t, w = self._src, self._tgt, self._w
+        keepm = s != t
+        s, t = s[keepm], t[keepm]
+        x = np.ones(len(s)) if w is None else w[keepm]
+        if not directed:
+            lo, hi = np.minimum(s, t), np.maximum(s, t)
+            s, t = lo, hi
+        merged = {}
+        for a, b, v in zip(s.tolist(), t.tolist(), x.tolist()):
+            k = (a, b)
+            if k in merged:
+                merged[k] = min(merged[k], v) if keep else max(merged[k], v)
+            else:
+                merged[k] = v
+        keys = sorted(merged)
+        ms = np.array([k[0] for k in keys], dtype=np.int64)
+        mt = np.array([k[1] for k in keys], dtype=np.int64)
+        mw = None if w is None else np.array([merged[k] for k in keys])
+        return Graph(self.n, ms, mt, mw, directed)
+
+    def twomode_eigenvector(self, types, tol=0.0, max_iter=0):
+        """twomode_eigenvector (crates/engine/src/metrics/bipartite.rs:93-111,
+        113-116, 288-336; type codes as crates/capi/src/twomode.rs:50-66):
+        eigenvector centrality of the binary affiliation graph (undirected,
+        parallel edges merged), direction ignored, unweighted, unit scale,
+        loops ignored; each mode's half divided by its own Euclidean norm
+        (a sequential sum in node order); NaN everywhere without ties."""
+        types = [int(v) for v in types]
+        for v, c in enumerate(types):
+            if c not in (0, 1):
+                raise OracleError(f"node {v} has type code {c}; use 0 for the first mode "
+                                  "and 1 for the second")
+        for e, (a, b) in enumerate(zip(self._src.tolist(), self._tgt.tolist())):
+            if types[a] == types[b]:
+                raise OracleError(f"edge {e} joins nodes {a} and {b}, which are in the same "
+                                  "mode; in a two-mode network every edge joins the two modes")
+        aff = self.simplify(undirected=True, keep=0)
+        x, lam, conn = aff.eigenvector(mode=3, weighted=False, scale=1, loops=2, tol=tol,
+                                       max_iter=max_iter)
+        if aff.m == 0:
+            return np.full(self.n, np.nan), 0.0, conn
+        x = x.copy()
+        for mode in (0, 1):
+            ss = 0.0
+            for v in range(self.n):
+                if types[v] == mode:
+                    ss += x[v] * x[v]
+            norm = math.sqrt(ss)
+            if norm > 0.0:
+                for v in range(self.n):
+                    if types[v] == mode:
+                        x[v] /= norm
+        return x, lam, conn
 
     def centralization_eigenvector(self, normalized=True):
         """igraph's eigenvector centralization

@@ -30,21 +30,24 @@ HERE = Path(__file__).resolve().parent
 # centrality and hubs and authorities (spectral.yaml), eigenvector centrality
 # and the components it is computed on (topography.yaml), eigenvector
 # centralization (roles.yaml).
-# Variants that first simplify or symmetrize the network through
-# net_graph_simplify (eigenvector_sna, eigenvector_ucinet, bonacich_sna) are
-# outside it.
+# The sna and UCINET variants read the network through net_graph_simplify
+# first; two-mode eigenvector centrality (twomode.yaml) needs the node types
+# the two-mode fixtures record.
 VARIANTS = {
     "spectral.yaml": ["pagerank", "pagerank_networkx", "pagerank_weighted",
                       "pagerank_personalized", "pagerank_personalized_networkx",
                       "pagerank_uniform_dangling", "pagerank_undirected",
                       "katz", "katz_weighted", "katz_igraph", "katz_exogenous",
                       "bonacich", "bonacich_negative", "bonacich_unit", "bonacich_rescale",
+                      "bonacich_sna",
                       "hits_authorities", "hits_hubs", "hits_authorities_networkx",
                       "hits_hubs_networkx"],
     "topography.yaml": ["eigenvector", "eigenvector_networkx", "eigenvector_weighted",
                         "eigenvector_weighted_networkx", "eigenvector_undirected",
+                        "eigenvector_sna", "eigenvector_ucinet",
                         "components_weak", "components_strong"],
     "roles.yaml": ["centralization_eigenvector"],
+    "twomode.yaml": ["twomode_eigenvector"],
 }
 ORACLES = ["definition", "networkx"]
 
@@ -99,7 +102,7 @@ def main():
                     w.append(float(row["weight"]))
         fixtures[d.name] = {
             "n": meta["n"], "directed": meta["directed"], "weighted": meta["weighted"],
-            "tags": meta.get("tags", []), "src": src, "tgt": tgt,
+            "tags": meta.get("tags", []), "type": meta.get("type"), "src": src, "tgt": tgt,
             "w": w if meta["weighted"] else None,
         }
         g = {}
@@ -117,8 +120,8 @@ def main():
     doc = {
         "about": "validation fixtures and golden values of the reference engine "
                  "(validation/fixtures, validation/golden/{definition,networkx}) for "
-                 "PageRank, Katz, Bonacich power, HITS, eigenvector centrality, components "
-                 "and eigenvector centralization; generated "
+                 "PageRank, Katz, Bonacich power, HITS, eigenvector centrality (one- and "
+                 "two-mode), components and eigenvector centralization; generated "
                  "by make_golden.py",
         "oracle_versions": versions,
         "manifest": manifest,

@@ -83,6 +83,23 @@ def relative(e: dict, key: str, g, mode: str, weighted: bool, loops: str) -> flo
     return float(e[key + "_fraction"]) / lam
 
 
+def target(g, e: dict):
+    """The graph, or its adjacency-matrix reading (net_graph_simplify) when
+    the variant says `simple` or `symmetrize`
+    (validation/bindings/topography.py:64-85,157; spectral.py:118-137)."""
+    if e.get("symmetrize"):
+        return g.simplify(undirected=True, keep=0)
+    if e.get("simple"):
+        return g.simplify(undirected=False, keep=0)
+    return g
+
+
+def defined(values):
+    """NaN written as -1, as the topography and two-mode runners do
+    (validation/bindings/topography.py:17,60-61)."""
+    return [-1.0 if math.isnan(v) else float(v) for v in values]
+
+
 def run_variant(g, fx: dict, variant: str):
     """Runs the manifest's engine options for `variant` on graph `g`; a
     measure the engine rejects gives an empty vector, as in the reference's
@@ -105,11 +122,17 @@ def _run_variant(g, fx: dict, variant: str):
                           dangling=DANGLING[e.get("dangling", "personalized")],
                           loops=LOOPS[e.get("loops", "twice")])
     if e["fn"] == "eigenvector":
-        vals, _, _ = g.eigenvector(mode=MODES[e.get("mode", "in")],
-                                   weighted=bool(e.get("weighted", False)),
-                                   scale=SCALES[e.get("scale", "max")],
-                                   loops=LOOPS[e.get("loops", "twice")])
-        return vals
+        vals, _, _ = target(g, e).eigenvector(mode=MODES[e.get("mode", "in")],
+                                              weighted=bool(e.get("weighted", False)),
+                                              scale=SCALES[e.get("scale", "max")],
+                                              loops=LOOPS[e.get("loops", "twice")])
+        return defined(vals)
+    if e["fn"] == "twomode":
+        # validation/bindings/twomode.py:130-159 (the eigenvector measure)
+        if fx.get("type") is None:
+            return []
+        vals, _, _ = g.twomode_eigenvector(fx["type"])
+        return defined(vals)
     if e["fn"] == "katz":
         mode, weighted, loops = e.get("mode", "in"), bool(e.get("weighted", False)), \
             e.get("loops", "once")
@@ -121,8 +144,9 @@ def _run_variant(g, fx: dict, variant: str):
     if e["fn"] == "bonacich":
         mode, weighted, loops = e.get("mode", "out"), bool(e.get("weighted", False)), \
             e.get("loops", "ignore")
-        exponent = relative(e, "exponent", g, "in" if mode == "out" else mode, weighted, loops)
-        return g.bonacich(exponent=exponent, mode=MODES[mode], weighted=weighted,
+        t = target(g, e)
+        exponent = relative(e, "exponent", t, "in" if mode == "out" else mode, weighted, loops)
+        return t.bonacich(exponent=exponent, mode=MODES[mode], weighted=weighted,
                           loops=LOOPS[loops], rescale=bool(e.get("rescale", False)))
     if e["fn"] == "components":
         memb, _ = g.components(strong=e["kind"] == "strong")

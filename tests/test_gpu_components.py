@@ -3,8 +3,12 @@ oracle's union-find and Tarjan's algorithm (crates/engine/src/metrics/
 topography.rs:183-286): labels and counts bit-exact, on random graphs, on
 shapes that stress the rounds of trimming and colouring (long paths either
 way, a long cycle, chains of cycles, a cycle reached only through a long
-tail), and on R-MAT graphs; and eigenvector centralization (net_centralization,
-topography.rs:475-498) against the oracle's restatement.
+tail), and on R-MAT graphs; eigenvector centralization (net_centralization,
+topography.rs:475-498), the adjacency-matrix reading (net_graph_simplify,
+topography.rs:96-141: edges, order and merged weights bit-exact) and
+two-mode eigenvector centrality (net_twomode_eigenvector,
+crates/engine/src/metrics/bipartite.rs:288-336) against the oracle's
+restatements.
 """
 from __future__ import annotations
 
@@ -130,4 +134,81 @@ def test_centralization_codes():
     err = ctypes.create_string_buffer(256)
     assert K.lib().net_components(g.h, 2, memb.ctypes.data, ctypes.byref(cnt), err, 256) == 1
     assert err.value.decode() == "unknown component kind code 2"
+    g.close()
+
+
+def test_simplify_matches_oracle():
+    """net_graph_simplify vs the oracle's restatement of simplify
+    (topography.rs:96-141): the same edges in the same order and the same
+    merged weights, bit-exact."""
+    rng = SplitMix64(20241207)
+    for case in range(40):
+        n, src, tgt, w, directed = random_case(rng, 30)
+        weights = np.asarray(w) if case % 2 else None
+        g = K.Graph(n, np.asarray(src), np.asarray(tgt), weights, directed)
+        og = O.Graph(n, np.asarray(src), np.asarray(tgt), weights, directed)
+        for undirected in (False, True):
+            for keep in (0, 1):
+                a = g.simplify(undirected=undirected, keep=keep)
+                b = og.simplify(undirected=undirected, keep=keep)
+                sa, ta, wa = a.edges()
+                sb, tb, wb = b.edges()
+                assert a.directed == b.directed
+                assert np.array_equal(sa, sb) and np.array_equal(ta, tb), (case, undirected, keep)
+                if weights is None:
+                    assert wa is None
+                else:
+                    assert np.array_equal(wa, wb), (case, undirected, keep)
+                a.close()
+        g.close()
+    # a heavy multigraph: 200,000 arcs over 300 nodes
+    r = np.random.default_rng(11)
+    s, t = r.integers(0, 300, 200_000), r.integers(0, 300, 200_000)
+    w = r.uniform(0.1, 5.0, 200_000)
+    g = K.Graph(300, s, t, w, True)
+    og = O.Graph(300, s, t, w, True)
+    for undirected, keep in ((False, 0), (True, 1)):
+        sa, ta, wa = g.simplify(undirected, keep).edges()
+        sb, tb, wb = og.simplify(undirected, keep).edges()
+        assert np.array_equal(sa, sb) and np.array_equal(ta, tb) and np.array_equal(wa, wb)
+    with pytest.raises(RuntimeError, match="unknown parallel-edge weight code 2"):
+        g.simplify(keep=2)
+    g.close()
+
+
+def bipartite_case(r, n1, n2, m):
+    s = r.integers(0, n1, m)
+    t = n1 + r.integers(0, n2, m)
+    flip = r.random(m) < 0.5
+    src, tgt = np.where(flip, t, s), np.where(flip, s, t)
+    return n1 + n2, src, tgt, [0] * n1 + [1] * n2
+
+
+def test_twomode_eigenvector_matches_oracle():
+    r = np.random.default_rng(12)
+    for n1, n2, m, directed in ((5, 7, 12, False), (20, 30, 90, True), (50, 8, 400, False),
+                                (300, 200, 3000, True), (40, 40, 0, False)):
+        n, src, tgt, types = bipartite_case(r, n1, n2, m)
+        g = K.Graph(n, src, tgt, None, directed)
+        og = O.Graph(n, src, tgt, None, directed)
+        x, lam, conn = g.twomode_eigenvector(types)
+        rx, rlam, rconn = og.twomode_eigenvector(types)
+        assert conn == rconn
+        if m == 0:
+            assert np.isnan(x).all() and lam == 0.0
+        else:
+            assert abs(lam - rlam) <= 1e-10 * rlam
+            assert np.nanmax(np.abs(x - rx)) <= 1e-9, (n1, n2, m)
+            for mode in (0, 1):
+                sel = np.asarray(types) == mode
+                assert abs(np.sum(x[sel] ** 2) - 1.0) <= 1e-12
+        g.close()
+
+
+def test_twomode_eigenvector_errors():
+    g = K.Graph(4, np.array([0, 1, 0]), np.array([2, 3, 1]), None, False)
+    with pytest.raises(RuntimeError, match="node 1 has type code 2; use 0 for the first mode"):
+        g.twomode_eigenvector([0, 2, 1, 1])
+    with pytest.raises(RuntimeError, match="edge 2 joins nodes 0 and 1, which are in the same mode"):
+        g.twomode_eigenvector([0, 0, 1, 1])
     g.close()
