@@ -127,6 +127,14 @@ NET_API int32_t net_twomode_eigenvector(const GraphHandle *h, const int32_t *typ
                                         double *eigenvalue, int32_t *connected, char *err,
                                         size_t err_len);
 
+/* Newman's leading eigenvector communities of an undirected network with
+ * at most 3000 nodes: 0-based labels (by first appearance) to
+ * membership[0..n), the modularity on the input network to *q (NaN without
+ * edges), the number of divisions to *splits. Weights (weighted != 0) must
+ * be non-negative. Replaces netcapi.h:978-984 (crates/capi/src/groups.rs:334-356). */
+NET_API int32_t net_leading_eigen(const GraphHandle *h, int32_t weighted, int64_t *membership,
+                                  double *q, int64_t *splits, char *err, size_t err_len);
+
 /* Weak (kind 0) or strong (kind 1) components: membership receives n
  * labels, numbered from 0 in order of each component's lowest-numbered
  * node, count one value; strong components of an undirected graph are its

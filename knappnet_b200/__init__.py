@@ -85,6 +85,8 @@ def lib() -> ctypes.CDLL:
     L.net_twomode_eigenvector.argtypes = [h, vp, f64, i64, i32, vp, ctypes.POINTER(f64),
                                           ctypes.POINTER(i32), cp, sz]
     L.net_twomode_eigenvector.restype = i32
+    L.net_leading_eigen.argtypes = [h, i32, vp, ctypes.POINTER(f64), ctypes.POINTER(i64), cp, sz]
+    L.net_leading_eigen.restype = i32
     L.net_components.argtypes = [h, i32, vp, ctypes.POINTER(i64), cp, sz]
     L.net_components.restype = i32
     L.net_centralization.argtypes = [h, i32, i32, i32, i32, i32, i32, ctypes.POINTER(f64), cp, sz]
@@ -370,6 +372,17 @@ class Graph:
                                              ctypes.byref(val), ctypes.byref(conn), err,
                                              ERR_LEN), err)
         return out[: self.n], val.value, bool(conn.value)
+
+    def leading_eigen(self, weighted=False):
+        """Newman's leading eigenvector communities (net_leading_eigen):
+        (labels, modularity, divisions)."""
+        memb = np.zeros(max(self.n, 1), dtype=np.int64)
+        q = ctypes.c_double()
+        splits = ctypes.c_int64()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_leading_eigen(self.h, int(bool(weighted)), _ptr(memb), ctypes.byref(q),
+                                       ctypes.byref(splits), err, ERR_LEN), err)
+        return memb[: self.n], q.value, splits.value
 
     def components(self, strong=False):
         """Weak or strong components (net_components): labels numbered in

@@ -686,6 +686,24 @@ int32_t net_twomode_eigenvector(const GraphHandle* h, const int32_t* types, doub
   });
 }
 
+int32_t net_leading_eigen(const GraphHandle* h, int32_t weighted, int64_t* membership, double* q,
+                          int64_t* splits, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    // require_undirected, MAX_NODES, additive_weights
+    // (crates/engine/src/metrics/partition.rs:52-70, partition/leading_eigen.rs:57-68)
+    if (g.directed)
+      throw Error("The leading eigenvector method is defined here for undirected networks only; "
+                  "build the network as undirected first");
+    if (g.n > 3000)
+      throw Error("the leading eigenvector method uses a dense eigendecomposition and is limited "
+                  "to 3000 nodes");
+    cudaStream_t s = knb::thread_stream();
+    if (weighted) check_nonnegative(g, "modularity", s);
+    knb::leading_eigen(g, weighted != 0, membership, q, splits, nullptr, s);
+  });
+}
+
 int32_t net_components(const GraphHandle* h, int32_t kind, int32_t* membership, int64_t* count,
                        char* err, size_t err_len) {
   return guard(err, err_len, [&] {

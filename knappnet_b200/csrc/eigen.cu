@@ -26,6 +26,8 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <unordered_map>
+#include <deque>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -1204,7 +1206,8 @@ struct LzBuffers {
 static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t max_matvecs,
                               bool mixed, double* xout, Leading* res, int* launches,
                               cudaStream_t s, const DevOp* B = nullptr,
-                              const double* start = nullptr, LzBuffers* buf = nullptr) {
+                              const double* start = nullptr, LzBuffers* buf = nullptr,
+                              bool perron = true) {
   const size_t dim = B ? B->n : A.n;
   if (B) mixed = false;
   const int m = (int)std::max<size_t>(
@@ -1361,9 +1364,12 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
         const double xx = hst->xx, value = hst->value, rinf = hst->rinf, xinf = hst->xinf;
         const double need = tol * (std::max(value, 0.0) + shift) * xinf;
         if (rinf <= need) {
-          // finish_vector: sign, clamp, unit norm
-          lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
-          lz_sign_clamp<<<gv, 256, 0, s>>>(x.get(), dim, st.get());
+          // finish_vector: sign, clamp, unit norm (a signed eigenvector,
+          // perron false: unit norm only)
+          if (perron) {
+            lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
+            lz_sign_clamp<<<gv, 256, 0, s>>>(x.get(), dim, st.get());
+          }
           lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
           read_state();
           const double nrm = std::sqrt(hst->xx);
@@ -2010,6 +2016,288 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
   cudaEventDestroy(t1);
   r->seconds = ms * 1e-3;
   r->kernel_launches = launches;
+}
+
+// ======================================================================= leading eigenvector communities
+// Newman's leading eigenvector method (crates/engine/src/metrics/partition/
+// leading_eigen.rs:57-160): groups are divided by the signs of the leading
+// eigenvector of their generalized modularity matrix B(g), breadth first,
+// until no division has a positive eigenvalue and a positive gain.
+// The dense adjacency, the degrees, B(g), its row sums and the gain are
+// computed on the device in the reference's summation order (one thread per
+// row, in column order); the leading eigenpair comes from the thick-restart
+// Lanczos process above in FP64 on B(g) as a dense operator, without the
+// Perron clamp, started from a fixed hashed vector (B(g) 1 = 0, so the
+// all-ones start of eigenvector centrality would break down at once). Rows
+// of B(g) that are entirely zero (nodes without ties) have eigenvector
+// component exactly 0 for any eigenvalue other than 0, so they stay out of
+// the eigenproblem and take component 0, as the reference's dense solver
+// gives them (to rounding). The reference's scale sum runs over the whole
+// matrix in one sequence; here it is the sum of the per-row sums.
+
+// a[u n + v]: arcs of row u in CSR order (input order per target), a loop
+// adding twice its weight (leading_eigen.rs:70-80).
+__global__ void le_dense(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                         const double* __restrict__ w, uint32_t n, double* __restrict__ a) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    double* row = a + (size_t)u * n;
+    for (uint32_t k = off[u]; k < off[u + 1]; ++k) {
+      const uint32_t v = tgt[k];
+      const double x = w ? w[k] : 1.0;
+      if (v == u) row[u] = __dadd_rn(row[u], __dmul_rn(2.0, x));
+      else row[v] = __dadd_rn(row[v], x);
+    }
+  }
+}
+
+__global__ void le_row_sums(const double* __restrict__ a, uint32_t n, double* __restrict__ k) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const double* row = a + (size_t)u * n;
+    double t = 0.0;
+    for (uint32_t j = 0; j < n; ++j) t = __dadd_rn(t, row[j]);
+    k[u] = t;
+  }
+}
+
+// b[r ng + c] = a[i n + j] - k_i k_j / 2m for group members i = g[r], j = g[c].
+__global__ void le_build(const double* __restrict__ a, uint32_t n, const double* __restrict__ k,
+                         double two_m, const uint32_t* __restrict__ grp, uint32_t ng,
+                         double* __restrict__ b) {
+  const uint64_t total = (uint64_t)ng * ng;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(q / ng), c = (uint32_t)(q % ng);
+    const uint32_t i = grp[r], j = grp[c];
+    b[q] = __dsub_rn(a[(size_t)i * n + j], __ddiv_rn(__dmul_rn(k[i], k[j]), two_m));
+  }
+}
+
+// Per row: the diagonal minus the row's sum, then the sum of |b| over the row.
+__global__ void le_diag(double* __restrict__ b, uint32_t ng, double* __restrict__ absrow) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < ng; r += gridDim.x * blockDim.x) {
+    double* row = b + (size_t)r * ng;
+    double t = 0.0;
+    for (uint32_t c = 0; c < ng; ++c) t = __dadd_rn(t, row[c]);
+    row[r] = __dsub_rn(row[r], t);
+    double z = 0.0;
+    for (uint32_t c = 0; c < ng; ++c) z = __dadd_rn(z, fabs(row[c]));
+    absrow[r] = z;
+  }
+}
+
+// The dense operator over the rows `nz` of B(g) as a CSR matrix.
+__global__ void le_sub(const double* __restrict__ b, uint32_t ng, const uint32_t* __restrict__ nz,
+                       uint32_t dim, uint32_t* __restrict__ off, uint32_t* __restrict__ cols,
+                       double* __restrict__ vals) {
+  const uint64_t total = (uint64_t)dim * dim;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(q / dim), c = (uint32_t)(q % dim);
+    cols[q] = c;
+    vals[q] = b[(size_t)nz[r] * ng + nz[c]];
+    if (c == 0) off[r] = (uint32_t)q;
+    if (q == 0) off[dim] = (uint32_t)total;
+  }
+}
+
+// A fixed start vector with values in [-1, 1) from a hash of the index.
+__global__ void le_start(double* __restrict__ x, uint32_t dim) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < dim; r += gridDim.x * blockDim.x) {
+    uint64_t z = (uint64_t)r * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    x[r] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  }
+}
+
+// s_r times the sum over c of b[r][c] s_c, in column order.
+__global__ void le_gain_rows(const double* __restrict__ b, uint32_t ng, const double* __restrict__ sv,
+                             double* __restrict__ out) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < ng; r += gridDim.x * blockDim.x) {
+    const double* row = b + (size_t)r * ng;
+    double t = 0.0;
+    for (uint32_t c = 0; c < ng; ++c) t = __dadd_rn(t, __dmul_rn(row[c], sv[c]));
+    out[r] = __dmul_rn(sv[r], t);
+  }
+}
+
+void leading_eigen(GraphHandleImpl& g, bool weighted, int64_t* membership, double* q,
+                   int64_t* splits_out, int* launches_out, cudaStream_t s) {
+  const uint32_t n = g.n;
+  int launches = 0;
+  std::vector<size_t> memb(n, 0);
+  size_t splits = 0;
+  double two_m = 0.0;
+  DevBuf<double> a, k;
+  if (n > 0) {
+    a.alloc((size_t)n * n);
+    k.alloc(n);
+    KNB_CUDA(cudaMemsetAsync(a.get(), 0, (size_t)n * n * 8, s));
+    le_dense<<<grid_for(n, 128), 128, 0, s>>>(g.out.off.get(), g.out.tgt.get(),
+                                                weighted ? g.out.w.get() : nullptr, n, a.get());
+    le_row_sums<<<grid_for(n, 128), 128, 0, s>>>(a.get(), n, k.get());
+    KNB_LAUNCH("leading eigenvector adjacency");
+    launches += 2;
+    std::vector<double> hk(n);
+    KNB_CUDA(cudaMemcpyAsync(hk.data(), k.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    for (double v : hk) two_m += v;
+  }
+  if (two_m > 0.0) {
+    size_t next_label = 1;
+    std::deque<std::vector<uint32_t>> queue;
+    {
+      std::vector<uint32_t> all(n);
+      std::iota(all.begin(), all.end(), 0u);
+      queue.push_back(std::move(all));
+    }
+    DevBuf<double> b, absrow, vals, x, start, sv, rowgain;
+    DevBuf<uint32_t> grp, nzd, off, cols;
+    LzBuffers lz;
+    while (!queue.empty()) {
+      std::vector<uint32_t> group = std::move(queue.front());
+      queue.pop_front();
+      const uint32_t ng = (uint32_t)group.size();
+      if (ng < 2) continue;
+      const size_t nn = (size_t)ng * ng;
+      if (b.n < nn) b.alloc(nn);
+      if (grp.n < ng) {
+        grp.alloc(ng);
+        absrow.alloc(ng);
+        sv.alloc(ng);
+        rowgain.alloc(ng);
+      }
+      KNB_CUDA(cudaMemcpyAsync(grp.get(), group.data(), (size_t)ng * 4, cudaMemcpyHostToDevice, s));
+      le_build<<<grid_for(nn, 256), 256, 0, s>>>(a.get(), n, k.get(), two_m, grp.get(), ng, b.get());
+      le_diag<<<grid_for(ng, 128), 128, 0, s>>>(b.get(), ng, absrow.get());
+      KNB_LAUNCH("generalized modularity matrix");
+      launches += 2;
+      std::vector<double> habs(ng);
+      KNB_CUDA(cudaMemcpyAsync(habs.data(), absrow.get(), (size_t)ng * 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      double total = 0.0, maxrow = 0.0;
+      std::vector<uint32_t> nz;
+      for (uint32_t r = 0; r < ng; ++r) {
+        total += habs[r];
+        maxrow = std::max(maxrow, habs[r]);
+        if (habs[r] > 0.0) nz.push_back(r);
+      }
+      const double scale = total / (double)ng;
+      // leading eigenpair of B(g) over its nonzero rows
+      double lambda = 0.0;
+      std::vector<double> u(ng, 0.0);
+      if (!nz.empty()) {
+        const uint32_t dim = (uint32_t)nz.size();
+        const size_t nnz = (size_t)dim * dim;
+        if (nnz > 0xFFFFFFFFull) throw Error("group too large for the leading eigenvector method");
+        if (vals.n < nnz) {
+          vals.alloc(nnz);
+          cols.alloc(nnz);
+        }
+        if (off.n < (size_t)dim + 1) {
+          off.alloc((size_t)dim + 1);
+          nzd.alloc(dim);
+          x.alloc(dim);
+          start.alloc(dim);
+        }
+        KNB_CUDA(cudaMemcpyAsync(nzd.get(), nz.data(), (size_t)dim * 4, cudaMemcpyHostToDevice, s));
+        le_sub<<<grid_for(nnz, 256), 256, 0, s>>>(b.get(), ng, nzd.get(), dim, off.get(), cols.get(),
+                                                  vals.get());
+        le_start<<<grid_for(dim, 256), 256, 0, s>>>(start.get(), dim);
+        KNB_LAUNCH("modularity operator");
+        launches += 2;
+        DevOp A;
+        A.n = dim;
+        A.nnz = nnz;
+        A.off = off.get();
+        A.cols = cols.get();
+        A.v64 = vals.get();
+        A.own_part = build_partition(dim, nnz, A.off, SPMV_THREADS * EIG_IPT, s);
+        A.part = A.own_part.get();
+        Leading res;
+        if (!symmetric_leading(A, 1e-12, maxrow, 200000, false, x.get(), &res, &launches, s,
+                               nullptr, start.get(), &lz, false))
+          throw Error("the leading eigenvector method: the eigenvector of a group of " +
+                      std::to_string(ng) + " nodes did not converge");
+        lambda = res.value;
+        std::vector<double> hx(dim);
+        KNB_CUDA(cudaMemcpyAsync(hx.data(), x.get(), (size_t)dim * 8, cudaMemcpyDeviceToHost, s));
+        KNB_CUDA(cudaStreamSynchronize(s));
+        for (uint32_t r = 0; r < dim; ++r) u[nz[r]] = hx[r];
+      }
+      if (std::isnan(lambda) || lambda <= 1e-10 * scale) continue;
+      // the first component of largest magnitude decides the sign
+      uint32_t big = 0;
+      for (uint32_t r = 1; r < ng; ++r)
+        if (std::fabs(u[r]) > std::fabs(u[big])) big = r;
+      const double sign = u[big] < 0.0 ? -1.0 : 1.0;
+      const double tiny = 1e-12 * std::fabs(u[big]);
+      std::vector<double> sg(ng);
+      for (uint32_t r = 0; r < ng; ++r) sg[r] = sign * u[r] > tiny ? 1.0 : -1.0;
+      KNB_CUDA(cudaMemcpyAsync(sv.get(), sg.data(), (size_t)ng * 8, cudaMemcpyHostToDevice, s));
+      le_gain_rows<<<grid_for(ng, 128), 128, 0, s>>>(b.get(), ng, sv.get(), rowgain.get());
+      KNB_LAUNCH("modularity gain");
+      ++launches;
+      std::vector<double> hg(ng);
+      KNB_CUDA(cudaMemcpyAsync(hg.data(), rowgain.get(), (size_t)ng * 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      double gain = 0.0;
+      for (double v : hg) gain += v;
+      if (std::isnan(gain) || gain <= 1e-10 * scale * (double)ng) continue;
+      std::vector<uint32_t> plus, minus;
+      for (uint32_t r = 0; r < ng; ++r) (sg[r] > 0.0 ? plus : minus).push_back(group[r]);
+      if (plus.empty() || minus.empty()) continue;
+      for (uint32_t v : minus) memb[v] = next_label;
+      ++next_label;
+      ++splits;
+      queue.push_back(std::move(plus));
+      queue.push_back(std::move(minus));
+    }
+  } else {
+    std::iota(memb.begin(), memb.end(), (size_t)0);
+  }
+  // labels by first appearance (partition.rs:62-65)
+  std::unordered_map<size_t, int64_t> seen;
+  std::vector<int64_t> label(n);
+  for (uint32_t v = 0; v < n; ++v) {
+    auto it = seen.find(memb[v]);
+    if (it == seen.end()) it = seen.emplace(memb[v], (int64_t)seen.size()).first;
+    label[v] = it->second;
+  }
+  // modularity of the partition on the input network
+  // (crates/engine/src/metrics/community.rs:97-146, undirected, resolution 1)
+  const size_t kc = seen.size();
+  std::vector<double> inside(kc, 0.0), kout(kc, 0.0), kin(kc, 0.0);
+  double m = 0.0;
+  if (g.m) {
+    std::vector<uint32_t> hs(g.m), ht(g.m);
+    std::vector<double> hw(weighted ? g.m : 0);
+    KNB_CUDA(cudaMemcpyAsync(hs.data(), g.src.get(), g.m * 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(ht.data(), g.tgt.get(), g.m * 4, cudaMemcpyDeviceToHost, s));
+    if (weighted) KNB_CUDA(cudaMemcpyAsync(hw.data(), g.w.get(), g.m * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    for (uint64_t e = 0; e < g.m; ++e) {
+      const double xv = weighted ? hw[e] : 1.0;
+      const int64_t cs = label[hs[e]], ct = label[ht[e]];
+      m += xv;
+      kout[cs] += xv;
+      kin[ct] += xv;
+      if (cs == ct) inside[cs] += xv;
+    }
+  }
+  double qv = std::numeric_limits<double>::quiet_NaN();
+  if (m > 0.0) {
+    qv = 0.0;
+    for (size_t c = 0; c < kc; ++c) {
+      const double kk = kout[c] + kin[c];
+      qv += inside[c] / m - (kk / (2.0 * m)) * (kk / (2.0 * m));
+    }
+  }
+  for (uint32_t v = 0; v < n; ++v) membership[v] = label[v];
+  *q = qv;
+  *splits_out = (int64_t)splits;
+  if (launches_out) *launches_out = launches;
 }
 
 }  // namespace knb

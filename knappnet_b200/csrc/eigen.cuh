@@ -68,4 +68,11 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs, double* auths, 
 // vecs. Returns false if the QL iteration does not converge.
 bool symmetric_eigen(const double* a, int n, double* vals, double* vecs);
 
+// Newman's leading eigenvector communities of an undirected graph with at
+// most 3000 nodes (crates/engine/src/metrics/partition/leading_eigen.rs):
+// n labels by first appearance, the modularity on the input network and the
+// number of divisions.
+void leading_eigen(GraphHandleImpl& g, bool weighted, int64_t* membership, double* q,
+                   int64_t* splits, int* launches, cudaStream_t s);
+
 }  // namespace knb

@@ -32,7 +32,8 @@ HERE = Path(__file__).resolve().parent
 # centralization (roles.yaml).
 # The sna and UCINET variants read the network through net_graph_simplify
 # first; two-mode eigenvector centrality (twomode.yaml) needs the node types
-# the two-mode fixtures record.
+# the two-mode fixtures record; Newman's leading eigenvector communities
+# (groups.yaml) divide by the signs of a leading eigenvector.
 VARIANTS = {
     "spectral.yaml": ["pagerank", "pagerank_networkx", "pagerank_weighted",
                       "pagerank_personalized", "pagerank_personalized_networkx",
@@ -48,6 +49,7 @@ VARIANTS = {
                         "components_weak", "components_strong"],
     "roles.yaml": ["centralization_eigenvector"],
     "twomode.yaml": ["twomode_eigenvector"],
+    "groups.yaml": ["leading_eigen", "leading_eigen_membership", "leading_eigen_weighted"],
 }
 ORACLES = ["definition", "networkx"]
 
@@ -121,7 +123,8 @@ def main():
         "about": "validation fixtures and golden values of the reference engine "
                  "(validation/fixtures, validation/golden/{definition,networkx}) for "
                  "PageRank, Katz, Bonacich power, HITS, eigenvector centrality (one- and "
-                 "two-mode), components and eigenvector centralization; generated "
+                 "two-mode), components, eigenvector centralization and leading eigenvector "
+                 "communities; generated "
                  "by make_golden.py",
         "oracle_versions": versions,
         "manifest": manifest,

@@ -154,6 +154,12 @@ def _run_variant(g, fx: dict, variant: str):
     if e["fn"] == "centralization_eigenvector":
         # validation/bindings/roles.py:207-212: one value, NaN when undefined
         return [g.centralization_eigenvector(normalized=bool(e.get("normalized", True)))]
+    if e["fn"] == "leading_eigen":
+        # validation/bindings/groups.py:160-167,292-294,368-371
+        memb, q, _ = g.leading_eigen(weighted=bool(e.get("weighted", False)))
+        if e.get("output") == "membership":
+            return [float(v) for v in memb]
+        return [-1.0 if q != q else q]
     if e["fn"] == "hits":
         hubs, auths, _, _ = g.hits(weighted=bool(e.get("weighted", False)),
                                    loops=LOOPS[e.get("loops", "twice")],

@@ -212,3 +212,72 @@ def test_twomode_eigenvector_errors():
     with pytest.raises(RuntimeError, match="edge 2 joins nodes 0 and 1, which are in the same mode"):
         g.twomode_eigenvector([0, 0, 1, 1])
     g.close()
+
+
+def planted(r, sizes, p_in, p_out, weighted=False, isolates=0):
+    """Undirected planted-partition multigraph: blocks of the given sizes,
+    then `isolates` nodes without ties."""
+    n = sum(sizes) + isolates
+    block = np.repeat(np.arange(len(sizes)), sizes)
+    s, t = [], []
+    nb = sum(sizes)
+    for u in range(nb):
+        for v in range(u + 1, nb):
+            if r.random() < (p_in if block[u] == block[v] else p_out):
+                s.append(u)
+                t.append(v)
+    w = r.uniform(0.5, 2.0, len(s)) if weighted else None
+    return n, np.asarray(s, dtype=np.int64), np.asarray(t, dtype=np.int64), w
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_leading_eigen_matches_oracle(case):
+    """net_leading_eigen vs the oracle (EISPACK eigenvectors, the reference's
+    summation order): the same labels, the same number of divisions, the
+    modularity within 1e-12 relative."""
+    r = np.random.default_rng(100 + case)
+    shapes = [([30, 30, 30], 0.3, 0.02, False, 0), ([50, 40, 30, 20], 0.25, 0.01, True, 5),
+              ([120], 0.05, 0.0, False, 0), ([60, 60], 0.2, 0.05, True, 3),
+              ([200, 150, 100, 50], 0.08, 0.004, False, 10), ([25] * 12, 0.5, 0.01, True, 0)]
+    sizes, p_in, p_out, weighted, iso = shapes[case]
+    n, s, t, w = planted(r, sizes, p_in, p_out, weighted, iso)
+    g = K.Graph(n, s, t, w, False)
+    og = O.Graph(n, s, t, w, False)
+    memb, q, splits = g.leading_eigen(weighted=weighted)
+    rm, rq, rsplits = og.leading_eigen(weighted=weighted)
+    assert splits == rsplits
+    assert np.array_equal(memb, rm)
+    assert abs(q - rq) <= 1e-12 * abs(rq) + 1e-14
+    g.close()
+
+
+def test_leading_eigen_reference_cases_and_errors():
+    """The reference's own cases (partition/leading_eigen.rs:163-206)."""
+    g = K.Graph(6, np.array([0, 0, 1, 3, 3, 4, 2]), np.array([1, 2, 2, 4, 5, 5, 3]), None, False)
+    memb, q, splits = g.leading_eigen()
+    assert memb.tolist() == [0, 0, 0, 1, 1, 1] and splits == 1
+    assert abs(q - 5.0 / 14.0) < 1e-14
+    s, t = [], []
+    for c in range(4):
+        for i in range(5):
+            for j in range(i + 1, 5):
+                s.append(5 * c + i)
+                t.append(5 * c + j)
+        s.append(5 * c)
+        t.append((5 * c + 5) % 20)
+    memb, _, splits = K.Graph(20, np.array(s), np.array(t), None, False).leading_eigen()
+    assert splits == 3
+    for c in range(4):
+        assert len(set(memb[5 * c: 5 * c + 5].tolist())) == 1
+    s, t = zip(*[(i, j) for i in range(5) for j in range(i + 1, 5)])
+    memb, _, splits = K.Graph(5, np.array(s), np.array(t), None, False).leading_eigen()
+    assert memb.tolist() == [0] * 5 and splits == 0
+    memb, q, _ = K.Graph(3, np.array([], dtype=np.int64), np.array([], dtype=np.int64), None,
+                         False).leading_eigen()
+    assert memb.tolist() == [0, 1, 2] and np.isnan(q)
+    with pytest.raises(RuntimeError, match="undirected networks only"):
+        K.Graph(2, np.array([0]), np.array([1]), None, True).leading_eigen()
+    with pytest.raises(RuntimeError, match="the graph has no edge weights"):
+        K.Graph(2, np.array([0]), np.array([1]), None, False).leading_eigen(weighted=True)
+    with pytest.raises(RuntimeError, match="limited to 3000 nodes"):
+        K.Graph(3001, np.array([0]), np.array([1]), None, False).leading_eigen()
