@@ -586,7 +586,126 @@ def run_c5(args):
             "directional_fd_rel_error": abs(fd - an) / abs(an)}
 
 
-WORKLOADS = {"c1": run_c1, "c2": run_c2, "c4a": run_c4a, "c4b": run_c4b, "c5": run_c5}
+def run_next(args):
+    """The measures built on the same kernels beyond PageRank and eigenvector
+    centrality, one JSON line each: wall time of the C ABI call (host
+    buffers, set-up included; the median of the timed calls) against the
+    oracle's time for the same call on this host, and the largest difference
+    from the oracle."""
+    import knappnet_b200 as K
+    from oracle import oracle as O
+
+    def timed(fn):
+        keep = {}
+
+        def once():
+            t0 = time.perf_counter()
+            keep["r"] = fn()
+            return time.perf_counter() - t0
+        sec = _median_device(once, args.steps, args.warmup)
+        return sec, keep["r"]
+
+    def cpu(fn):
+        t0 = time.perf_counter()
+        r = fn()
+        return time.perf_counter() - t0, r
+
+    lines = []
+
+    def line(name, what, sec, csec, extra):
+        d = {"workload": name, "description": what, "metric": "call ms", "value": round(sec * 1e3, 3),
+             "unit": "ms", "higher_is_better": False, "oracle_ms": round(csec * 1e3, 1)}
+        d.update(extra)
+        lines.append(d)
+
+    # Katz and Bonacich power centrality, directed weighted R-MAT
+    g = K.generate_rmat(20, 16, seed=20240711, clean=True, lognormal=True, wseed=20240712)
+    s, t, w = g.edges()
+    og = O.Graph(g.n, s, t, w, True)
+    _, lam, _ = g.eigenvector(mode=2, weighted=True)
+    alpha = 0.5 / lam
+    sec, x = timed(lambda: g.katz(alpha=alpha, beta=1.0, mode=2, weighted=True))
+    csec, ox = cpu(lambda: og.katz(alpha=alpha, beta=1.0, mode=2, weighted=True))
+    line("katz", "R-MAT 20 directed, lognormal weights, mode in, alpha = 0.5 / lambda_max",
+         sec, csec, {"nodes": g.n, "edges": g.m,
+                     "max_rel_vs_oracle": float(np.abs(x - ox).max() / np.abs(ox).max())})
+    sec, hv = timed(lambda: g.hits())
+    csec, ohv = cpu(lambda: og.hits())
+    line("hits", "R-MAT 20 directed, unweighted, scale max", sec, csec,
+         {"nodes": g.n, "edges": g.m, "value_rel_vs_oracle": abs(hv[2] - ohv[2]) / ohv[2],
+          "max_abs_vs_oracle": float(max(np.nanmax(np.abs(hv[0] - ohv[0])),
+                                         np.nanmax(np.abs(hv[1] - ohv[1]))))})
+    g.close()
+    del og
+
+    # strong and weak components
+    g = K.generate_rmat(22, 16, seed=20240713, clean=True)
+    s, t, _ = g.edges()
+    og = O.Graph(g.n, s, t, None, True)
+    for strong in (True, False):
+        sec, (m, c) = timed(lambda: g.components(strong=strong))
+        csec, (om, oc) = cpu(lambda: og.components(strong=strong))
+        line("components_strong" if strong else "components_weak",
+             "R-MAT 22 directed, cleaned", sec, csec,
+             {"nodes": g.n, "edges": g.m, "components": int(c),
+              "labels_identical": bool(c == oc and np.array_equal(m.astype(np.int64),
+                                                                  om.astype(np.int64)))})
+    g.close()
+    del og
+
+    # adjacency-matrix reading of a multigraph, then two-mode eigenvector
+    g = K.generate_rmat(18, 16, seed=20240714, clean=False, lognormal=True, wseed=20240715)
+    s, t, w = g.edges()
+    og = O.Graph(g.n, s, t, w, True)
+    sec, a = timed(lambda: g.simplify(undirected=True, keep=0))
+    csec, oa = cpu(lambda: og.simplify(undirected=True, keep=0))
+    sa, ta, wa = a.edges()
+    sb, tb, wb = oa.edges()
+    line("simplify", "R-MAT 18 with loops and parallel arcs, lognormal weights, symmetrized, "
+         "largest weight kept", sec, csec,
+         {"edges_in": g.m, "edges_out": int(len(sa)),
+          "identical": bool(np.array_equal(sa, sb) and np.array_equal(ta, tb)
+                            and np.array_equal(wa, wb))})
+    a.close()
+    g.close()
+    del og, oa
+    rng = np.random.default_rng(20240716)
+    n1, n2, mm = 200_000, 100_000, 2_000_000
+    bs = rng.integers(0, n1, mm)
+    bt = n1 + rng.integers(0, n2, mm)
+    types = [0] * n1 + [1] * n2
+    g = K.Graph(n1 + n2, bs, bt, None, False)
+    og = O.Graph(n1 + n2, bs, bt, None, False)
+    sec, (x, lam, _) = timed(lambda: g.twomode_eigenvector(types))
+    csec, (ox, olam, _) = cpu(lambda: og.twomode_eigenvector(types))
+    line("twomode_eigenvector", "random two-mode network, 200,000 + 100,000 nodes, 2,000,000 ties",
+         sec, csec, {"singular_value_rel_vs_oracle": abs(lam - olam) / olam,
+                     "max_abs_vs_oracle": float(np.nanmax(np.abs(x - ox)))})
+    g.close()
+    del og
+
+    # leading eigenvector communities at the size limit's scale
+    rng = np.random.default_rng(20240717)
+    sizes = [250] * 8
+    blk = np.repeat(np.arange(8), 250)
+    iu, ju = np.triu_indices(2000, 1)
+    p = np.where(blk[iu] == blk[ju], 0.05, 0.002)
+    keep = rng.random(len(iu)) < p
+    ls, lt = iu[keep].astype(np.int64), ju[keep].astype(np.int64)
+    g = K.Graph(2000, ls, lt, None, False)
+    og = O.Graph(2000, ls, lt, None, False)
+    sec, (m, q, sp) = timed(lambda: g.leading_eigen())
+    csec, (om, oq, osp) = cpu(lambda: og.leading_eigen())
+    line("leading_eigen", "planted partition, 8 blocks of 250 nodes, p_in 0.05, p_out 0.002",
+         sec, csec, {"edges": int(len(ls)), "splits": int(sp), "modularity": q,
+                     "labels_identical": bool(np.array_equal(m, om) and sp == osp),
+                     "modularity_rel_vs_oracle": abs(q - oq) / abs(oq)})
+    g.close()
+    return lines
+
+
+WORKLOADS = {"c1": run_c1, "c2": run_c2, "c4a": run_c4a, "c4b": run_c4b, "c5": run_c5,
+             "next": run_next}
 
 
 def main():
@@ -600,9 +719,11 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=8.0,
                     help="seconds per reference-arm step")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["c3", "c1", "c2", "c4a", "c4b", "c5"], default="c3",
+    ap.add_argument("--workload", choices=["c3", "c1", "c2", "c4a", "c4b", "c5", "next"],
+                    default="c3",
                     help="c3 (default) is the benchmark line; the others print one JSON line "
-                         "each for the other configurations")
+                         "each for the other configurations (next: one per measure beyond "
+                         "PageRank and eigenvector centrality)")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale (the benchmark workload is 24; smaller scales "
                          "serve profiling captures)")
@@ -612,10 +733,11 @@ def main():
     if args.workload != "c3":
         if args.impl == "reference" or int(os.environ.get("RANK", 0)) != 0:
             return
-        line = WORKLOADS[args.workload](args)
-        line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-                     "data": "synthetic (seeded Philox generators)"})
-        print(json.dumps(line), flush=True)
+        result = WORKLOADS[args.workload](args)
+        for line in (result if isinstance(result, list) else [result]):
+            line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                         "data": "synthetic (seeded Philox generators)"})
+            print(json.dumps(line), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:
