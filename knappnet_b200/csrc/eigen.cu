@@ -1473,24 +1473,91 @@ void mapped_submatrix(const OpView<double>& op, const std::vector<uint32_t>& nod
   A.part = A.own_part.get();
 }
 
-void host_csr(const Operator& op, std::vector<uint32_t>* off, std::vector<uint32_t>* cols,
-              std::vector<double>* vals, cudaStream_t s) {
-  off->resize((size_t)op.n + 1);
-  cols->resize(op.nnz);
-  KNB_CUDA(cudaMemcpyAsync(off->data(), op.rows->off.get(), ((size_t)op.n + 1) * 4,
-                           cudaMemcpyDeviceToHost, s));
-  if (op.nnz)
-    KNB_CUDA(cudaMemcpyAsync(cols->data(), op.rows->tgt.get(), op.nnz * 4,
-                             cudaMemcpyDeviceToHost, s));
-  vals->clear();
-  if (op.has_vals) {
-    vals->resize(op.nnz);
-    if (op.nnz)
-      KNB_CUDA(cudaMemcpyAsync(vals->data(), op.vals64.get(), op.nnz * 8, cudaMemcpyDeviceToHost,
-                               s));
+// HITS blocks (spectral.rs:757-813) on the device: every positive entry
+// (i, j) of A joins hub i and authority n + j (one warp per row, the CAS
+// union of the components above) and marks both as present.
+__global__ void hits_union(OpView<double> a, uint32_t* parent, uint8_t* has_out, uint8_t* has_in,
+                           unsigned int* any) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  bool found = false;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += warps) {
+    for (uint32_t k = a.off[i] + lane; k < a.off[i + 1]; k += 32) {
+      const double v = a.vals ? a.vals[k] : 1.0;
+      if (!(v > 0.0)) continue;
+      const uint32_t j = a.cols[k];
+      found = true;
+      if (!has_out[i]) has_out[i] = 1;
+      if (!has_in[j]) has_in[j] = 1;
+      uint32_t x = uf_find(parent, i), y = uf_find(parent, a.n + j);
+      while (x != y) {
+        const uint32_t lo = x < y ? x : y, hi = x < y ? y : x;
+        const uint32_t old = atomicCAS(&parent[hi], hi, lo);
+        if (old == hi) break;
+        x = uf_find(parent, old);
+        y = uf_find(parent, lo);
+      }
+    }
   }
-  KNB_CUDA(cudaStreamSynchronize(s));
+  if (__any_sync(0xffffffffu, found) && lane == 0) *any = 1u;
 }
+
+// root[v] of every present node (hubs v < n with a positive entry in their
+// row, authorities n + j with one in column j; the others NONE), and the
+// flags of the roots. A block's root is its smallest node, so numbering the
+// roots in order numbers the blocks by first appearance.
+__global__ void hits_roots(uint32_t* parent, uint32_t n, const uint8_t* __restrict__ has_out,
+                           const uint8_t* __restrict__ has_in, uint32_t* __restrict__ root,
+                           uint32_t* __restrict__ is_root) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < 2 * n; v += gridDim.x * blockDim.x) {
+    const bool present = v < n ? has_out[v] != 0 : has_in[v - n] != 0;
+    const uint32_t r = present ? uf_find(parent, v) : 0xFFFFFFFFu;
+    root[v] = r;
+    is_root[v] = present && r == v;
+  }
+}
+
+__global__ void hits_label(const uint32_t* __restrict__ root, const uint32_t* __restrict__ rank,
+                           uint32_t n2, uint32_t* __restrict__ label) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n2; v += gridDim.x * blockDim.x)
+    label[v] = root[v] == 0xFFFFFFFFu ? 0xFFFFFFFFu : rank[root[v]];
+}
+
+// The bounds' per-node sums (spectral.rs:814-836), one thread per row in
+// CSR order: row sums of A; column sums of A and the squares of its merged
+// column entries (runs of one row within a row of the transpose).
+__global__ void hits_row_sum(OpView<double> a, double* __restrict__ row_sum) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (uint32_t k = a.off[i]; k < a.off[i + 1]; ++k) t = __dadd_rn(t, a.vals ? a.vals[k] : 1.0);
+    row_sum[i] = t;
+  }
+}
+
+__global__ void hits_col_sums(OpView<double> at, double* __restrict__ col_sum,
+                              double* __restrict__ col_sq) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < at.n; j += gridDim.x * blockDim.x) {
+    double sum = 0.0, q = 0.0, acc = 0.0;
+    bool open = false;
+    uint32_t c = 0;
+    for (uint32_t k = at.off[j]; k < at.off[j + 1]; ++k) {
+      const double v = at.vals ? at.vals[k] : 1.0;
+      sum = __dadd_rn(sum, v);
+      if (open && at.cols[k] == c) {
+        acc = __dadd_rn(acc, v);
+      } else {
+        if (open) q = __dadd_rn(q, __dmul_rn(acc, acc));
+        c = at.cols[k];
+        acc = v;
+        open = true;
+      }
+    }
+    if (open) q = __dadd_rn(q, __dmul_rn(acc, acc));
+    col_sum[j] = sum;
+    col_sq[j] = q;
+  }
+}
+
 
 void hits_rescale(std::vector<double>& x, int how) {
   for (double& v : x)
@@ -1520,77 +1587,62 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
   const double lf = p.loops == 2 ? 0.0 : (!hdir && p.loops == 0 ? 2.0 : 1.0);
   Operator& A = g.op(0, p.weighted, lf, s);
   Operator& At = hdir ? g.op(1, p.weighted, lf, s) : A;
-  std::vector<uint32_t> aoff, acols, toff, tcols;
-  std::vector<double> avals, tvals;
-  host_csr(A, &aoff, &acols, &avals, s);
-  if (hdir) host_csr(At, &toff, &tcols, &tvals, s);
-  const std::vector<uint32_t>& Toff = hdir ? toff : aoff;
-  const std::vector<uint32_t>& Tcols = hdir ? tcols : acols;
-  const std::vector<double>& Tvals = hdir ? tvals : avals;
-  auto av = [&](uint64_t k) { return avals.empty() ? 1.0 : avals[k]; };
-  auto tv = [&](uint64_t k) { return Tvals.empty() ? 1.0 : Tvals[k]; };
+  const OpView<double> a64{A.n, A.nnz, A.rows->off.get(), A.rows->tgt.get(),
+                           A.has_vals ? A.vals64.get() : nullptr};
+  const OpView<double> t64{At.n, At.nnz, At.rows->off.get(), At.rows->tgt.get(),
+                           At.has_vals ? At.vals64.get() : nullptr};
   // blocks of the bipartite graph (hubs 0..n, authorities n..2n) joined by
-  // positive entries (spectral.rs:757-813)
-  std::vector<uint32_t> parent(2 * (size_t)n);
-  std::iota(parent.begin(), parent.end(), 0u);
-  auto find = [&](uint32_t v) {
-    while (parent[v] != v) {
-      parent[v] = parent[parent[v]];
-      v = parent[v];
-    }
-    return v;
-  };
-  bool any = false;
-  std::vector<char> has_in(n, 0), has_out(n, 0);
-  for (uint32_t i = 0; i < n; ++i)
-    for (uint64_t k = aoff[i]; k < aoff[i + 1]; ++k)
-      if (av(k) > 0.0) {
-        any = true;
-        has_out[i] = 1;
-        has_in[acols[k]] = 1;
-        const uint32_t x = find(i), y = find(n + acols[k]);
-        if (x != y) parent[std::max(x, y)] = std::min(x, y);
-      }
+  // positive entries (spectral.rs:757-813), found on the device
+  const uint32_t n2 = 2 * n;
+  std::vector<uint32_t> label(n2);
+  unsigned int any = 0;
+  {
+    DevBuf<uint32_t> parent(n2), root(n2), flag((size_t)n2 + 1), lab(n2);
+    DevBuf<uint8_t> has_out(n), has_in(n);
+    DevBuf<unsigned int> anyd(1);
+    uf_init<<<grid_for(n2, ET), ET, 0, s>>>(parent.get(), n2);
+    KNB_CUDA(cudaMemsetAsync(has_out.get(), 0, n, s));
+    KNB_CUDA(cudaMemsetAsync(has_in.get(), 0, n, s));
+    KNB_CUDA(cudaMemsetAsync(anyd.get(), 0, 4, s));
+    hits_union<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>(a64, parent.get(), has_out.get(),
+                                                               has_in.get(), anyd.get());
+    hits_roots<<<grid_for(n2, ET), ET, 0, s>>>(parent.get(), n, has_out.get(), has_in.get(),
+                                               root.get(), flag.get());
+    KNB_LAUNCH("hub and authority blocks");
+    exclusive_scan<uint32_t>(flag.get(), flag.get(), n2, s);
+    hits_label<<<grid_for(n2, ET), ET, 0, s>>>(root.get(), flag.get(), n2, lab.get());
+    KNB_LAUNCH("hits_label");
+    KNB_CUDA(cudaMemcpyAsync(label.data(), lab.get(), (size_t)n2 * 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(&any, anyd.get(), 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+  }
   if (!any) {
     for (uint32_t i = 0; i < n; ++i) hubs_out[i] = auth_out[i] = std::nan("");
     *value = 0.0;
     *unique = 0;
     return;
   }
-  std::vector<uint32_t> block_of(2 * (size_t)n, 0xFFFFFFFFu);
   std::vector<std::vector<uint32_t>> bh, ba;
-  for (uint32_t v = 0; v < 2 * n; ++v) {
-    const bool present = v < n ? has_out[v] : has_in[v - n];
-    if (!present) continue;
-    const uint32_t root = find(v);
-    if (block_of[root] == 0xFFFFFFFFu) {
-      block_of[root] = (uint32_t)bh.size();
-      bh.emplace_back();
-      ba.emplace_back();
+  for (uint32_t v = 0; v < n2; ++v) {
+    const uint32_t b = label[v];
+    if (b == 0xFFFFFFFFu) continue;
+    if (b >= bh.size()) {
+      bh.resize((size_t)b + 1);
+      ba.resize((size_t)b + 1);
     }
-    (v < n ? bh : ba)[block_of[root]].push_back(v < n ? v : v - n);
+    (v < n ? bh : ba)[b].push_back(v < n ? v : v - n);
   }
   // bounds on each block's sigma^2 (spectral.rs:814-836)
-  std::vector<double> row_sum(n, 0.0), col_sum(n, 0.0), col_sq(n, 0.0);
-  for (uint32_t i = 0; i < n; ++i)
-    for (uint64_t k = aoff[i]; k < aoff[i + 1]; ++k) row_sum[i] += av(k);
-  for (uint32_t j = 0; j < n; ++j) {
-    double q = 0.0, acc = 0.0;
-    bool open = false;
-    uint32_t c = 0;
-    for (uint64_t k = Toff[j]; k < Toff[j + 1]; ++k) {
-      col_sum[j] += tv(k);
-      if (open && Tcols[k] == c) {
-        acc += tv(k);
-      } else {
-        if (open) q += acc * acc;
-        c = Tcols[k];
-        acc = tv(k);
-        open = true;
-      }
-    }
-    if (open) q += acc * acc;
-    col_sq[j] = q;
+  std::vector<double> row_sum(n), col_sum(n), col_sq(n);
+  {
+    DevBuf<double> rs(n), cs(n), cq(n);
+    hits_row_sum<<<grid_for(n, 128), 128, 0, s>>>(a64, rs.get());
+    hits_col_sums<<<grid_for(n, 128), 128, 0, s>>>(t64, cs.get(), cq.get());
+    KNB_LAUNCH("hub and authority bounds");
+    KNB_CUDA(cudaMemcpyAsync(row_sum.data(), rs.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(col_sum.data(), cs.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(col_sq.data(), cq.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
   }
   const size_t kb = bh.size();
   std::vector<double> upper(kb, 0.0), lower(kb, 0.0);
@@ -1611,10 +1663,6 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
   DevBuf<uint32_t> hub_index(n), auth_index(n), nodes_h(n), nodes_a(n);
   KNB_CUDA(cudaMemsetAsync(hub_index.get(), 0xFF, (size_t)n * 4, s));
   KNB_CUDA(cudaMemsetAsync(auth_index.get(), 0xFF, (size_t)n * 4, s));
-  const OpView<double> a64{A.n, A.nnz, A.rows->off.get(), A.rows->tgt.get(),
-                           A.has_vals ? A.vals64.get() : nullptr};
-  const OpView<double> t64{At.n, At.nnz, At.rows->off.get(), At.rows->tgt.get(),
-                           At.has_vals ? At.vals64.get() : nullptr};
   const double TIE = 1e-9;
   double best = 0.0;
   struct Solved {
