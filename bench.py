@@ -595,15 +595,22 @@ def run_next(args):
     import knappnet_b200 as K
     from oracle import oracle as O
 
-    def timed(fn):
+    def timed(fn, release=None):
+        """Median and minimum wall time of fn(); the previous call's result
+        is released outside the timed region."""
         keep = {}
-
-        def once():
+        times = []
+        for i in range(args.warmup + max(args.steps, 1)):
+            if "r" in keep and release is not None:
+                release(keep["r"])
+            keep.pop("r", None)
             t0 = time.perf_counter()
             keep["r"] = fn()
-            return time.perf_counter() - t0
-        sec = _median_device(once, args.steps, args.warmup)
-        return sec, keep["r"]
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+        timed.last_min = min(times)
+        return statistics.median(times), keep["r"]
 
     def cpu(fn):
         t0 = time.perf_counter()
@@ -614,7 +621,8 @@ def run_next(args):
 
     def line(name, what, sec, csec, extra):
         d = {"workload": name, "description": what, "metric": "call ms", "value": round(sec * 1e3, 3),
-             "unit": "ms", "higher_is_better": False, "oracle_ms": round(csec * 1e3, 1)}
+             "unit": "ms", "higher_is_better": False, "min_ms": round(timed.last_min * 1e3, 3),
+             "oracle_ms": round(csec * 1e3, 1)}
         d.update(extra)
         lines.append(d)
 
@@ -657,7 +665,7 @@ def run_next(args):
     g = K.generate_rmat(18, 16, seed=20240714, clean=False, lognormal=True, wseed=20240715)
     s, t, w = g.edges()
     og = O.Graph(g.n, s, t, w, True)
-    sec, a = timed(lambda: g.simplify(undirected=True, keep=0))
+    sec, a = timed(lambda: g.simplify(undirected=True, keep=0), release=lambda h: h.close())
     csec, oa = cpu(lambda: og.simplify(undirected=True, keep=0))
     sa, ta, wa = a.edges()
     sb, tb, wb = oa.edges()

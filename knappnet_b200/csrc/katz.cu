@@ -398,20 +398,25 @@ struct Scratch {
         part2((size_t)SPLIT_CTAS * 2 + 2), st(1) {}
 };
 
-// Host copies of the edge arrays.
-void host_edges(GraphHandleImpl& g, std::vector<uint32_t>* src, std::vector<uint32_t>* tgt,
-                std::vector<double>* w, cudaStream_t s) {
-  src->resize(g.m);
-  tgt->resize(g.m);
-  if (g.m) {
-    KNB_CUDA(cudaMemcpyAsync(src->data(), g.src.get(), g.m * 4, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaMemcpyAsync(tgt->data(), g.tgt.get(), g.m * 4, cudaMemcpyDeviceToHost, s));
+// A node's diagonal entry: the sum of its self-loop values (weight, or 1,
+// times the loop factor) in input order. Rows of the out-CSR are sorted by
+// target with ties in input order, so a thread finds its loops by binary
+// search and adds them in that order.
+__global__ void loop_diag(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                          const double* __restrict__ w, uint32_t n, double lf,
+                          double* __restrict__ diag) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t lo = off[i], hi = off[i + 1];
+    const uint32_t end = hi;
+    while (lo < hi) {
+      const uint32_t mid = lo + ((hi - lo) >> 1);
+      if (tgt[mid] < i) lo = mid + 1; else hi = mid;
+    }
+    double d = 0.0;
+    for (uint32_t k = lo; k < end && tgt[k] == i; ++k)
+      d = __dadd_rn(d, __dmul_rn(w ? w[k] : 1.0, lf));
+    diag[i] = d;
   }
-  if (g.weighted) {
-    w->resize(g.m);
-    if (g.m) KNB_CUDA(cudaMemcpyAsync(w->data(), g.w.get(), g.m * 8, cudaMemcpyDeviceToHost, s));
-  }
-  KNB_CUDA(cudaStreamSynchronize(s));
 }
 
 // check_attenuation (spectral.rs:447-527): returns the radius bound or
@@ -422,14 +427,6 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
   const uint32_t n = g.n;
   const double limit = 1.0 / t;
   *collatz = 0;
-  std::vector<uint32_t> src, tgt;
-  std::vector<double> w;
-  host_edges(g, &src, &tgt, &w, s);
-  auto value = [&](uint64_t e) {
-    double v = weighted ? w[e] : 1.0;
-    if (src[e] == tgt[e]) v *= rw.lf;
-    return v;
-  };
   Comps comp;
   if (g.directed) {
     // strong components of the positive entries (spectral.rs:539-553); a
@@ -441,8 +438,15 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
   const size_t k = comp.count();
   // single nodes: the diagonal (the sum of a node's self-loop entries)
   std::vector<double> diag(n, 0.0);
-  for (uint64_t e = 0; e < g.m; ++e)
-    if (src[e] == tgt[e]) diag[src[e]] += value(e);
+  if (n) {
+    DevBuf<double> dd(n);
+    loop_diag<<<grid_for(n, KT), KT, 0, s>>>(g.out.off.get(), g.out.tgt.get(),
+                                              weighted ? g.out.w.get() : nullptr, n, rw.lf,
+                                              dd.get());
+    KNB_LAUNCH("loop_diag");
+    KNB_CUDA(cudaMemcpyAsync(diag.data(), dd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+  }
   std::vector<uint32_t> first(k, 0xFFFFFFFFu);
   for (uint32_t v = 0; v < n; ++v)
     if (first[comp.membership[v]] == 0xFFFFFFFFu) first[comp.membership[v]] = v;
