@@ -81,14 +81,15 @@ __device__ __forceinline__ void row_product(const OpView<MT>& op, const VT* __re
 }
 
 // The PageRank update of row i for this lane's columns, and its per-column
-// sums (mass, dangling mass, L1 change) into red.
+// sums (mass, dangling mass, L1 change) into the warp's slice red[3][B] of
+// shared memory (column c belongs to lane c mod 32, so every slot has one
+// writer and takes its rows in order).
 template <class VT, int VW>
 __device__ __forceinline__ void row_update(uint32_t i, const VT (&s)[VW], int lane,
                                            const BatchScalars& bs, const ColState* cs,
                                            const VT* __restrict__ Yold, VT* __restrict__ Ynew,
                                            VT* __restrict__ Znew, const VT* __restrict__ inv_out,
-                                           const double* __restrict__ P,
-                                           double (&red)[3][VW]) {
+                                           const double* __restrict__ P, double* red) {
   const VT io = inv_out[i];
 #pragma unroll
   for (int v = 0; v < VW; ++v) {
@@ -102,24 +103,25 @@ __device__ __forceinline__ void row_update(uint32_t i, const VT (&s)[VW], int la
     const VT xo = Yold[q] * it;
     Ynew[q] = u;
     Znew[q] = u * io;
-    red[0][v] += (double)u;
-    if (io == VT(0)) red[1][v] += (double)u;
-    red[2][v] += fabs((double)u - (double)xo);
+    red[c] += (double)u;
+    if (io == VT(0)) red[bs.B + c] += (double)u;
+    red[2 * bs.B + c] += fabs((double)u - (double)xo);
   }
 }
 
-// Joins the lanes' per-column sums of a CTA in warp order into part[cta][3][B].
-template <int VW>
-__device__ __forceinline__ void cta_column_sums(double (&red)[3][VW], uint32_t B,
-                                                double* __restrict__ part, double* smem) {
+// Zeroes this warp's slice [3][B] of the per-warp column sums in smem.
+__device__ __forceinline__ double* warp_sums(double* smem, uint32_t B) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  // smem: [BW][3][B]
-  for (int s = 0; s < 3; ++s)
-#pragma unroll
-    for (int v = 0; v < VW; ++v) {
-      const uint32_t c = lane + 32 * v;
-      if (c < B) smem[((size_t)w * 3 + s) * B + c] = red[s][v];
-    }
+  double* red = smem + (size_t)w * 3 * B;
+  for (uint32_t q = lane; q < 3 * B; q += 32) red[q] = 0.0;
+  __syncwarp();
+  return red;
+}
+
+// Joins the warps' per-column sums of a CTA (smem [BW][3][B]) in warp order
+// into part[cta][3][B].
+__device__ __forceinline__ void cta_column_sums(uint32_t B, double* __restrict__ part,
+                                                const double* smem) {
   __syncthreads();
   for (uint32_t q = threadIdx.x; q < 3 * B; q += BT) {
     double a = 0;
@@ -138,11 +140,7 @@ spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ 
   if (*all_frozen) return;
   extern __shared__ double smem_b[];
   const int lane = threadIdx.x & 31;
-  double red[3][VW];
-#pragma unroll
-  for (int s = 0; s < 3; ++s)
-#pragma unroll
-    for (int v = 0; v < VW; ++v) red[s][v] = 0.0;
+  double* red = warp_sums(smem_b, bs.B);
   const uint32_t gw = blockIdx.x * BW + (threadIdx.x >> 5), nw = gridDim.x * BW;
   for (uint32_t r = gw; r < nranges; r += nw) {
     const RowRange rr = ranges[r];
@@ -154,7 +152,7 @@ spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ 
       row_update<VT, VW>(i, acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
     }
   }
-  cta_column_sums<VW>(red, bs.B, part, smem_b);
+  cta_column_sums(bs.B, part, smem_b);
 }
 
 // Partial products of the chunks of long rows.
@@ -189,11 +187,7 @@ spmm_long(const uint32_t* __restrict__ lrow, const uint32_t* __restrict__ lfirst
   if (*all_frozen) return;
   extern __shared__ double smem_b[];
   const int lane = threadIdx.x & 31;
-  double red[3][VW];
-#pragma unroll
-  for (int s = 0; s < 3; ++s)
-#pragma unroll
-    for (int v = 0; v < VW; ++v) red[s][v] = 0.0;
+  double* red = warp_sums(smem_b, bs.B);
   const uint32_t gw = blockIdx.x * BW + (threadIdx.x >> 5), nw = gridDim.x * BW;
   for (uint32_t q = gw; q < nlong; q += nw) {
     VT acc[VW];
@@ -207,7 +201,7 @@ spmm_long(const uint32_t* __restrict__ lrow, const uint32_t* __restrict__ lfirst
       }
     row_update<VT, VW>(lrow[q], acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
   }
-  cta_column_sums<VW>(red, bs.B, part, smem_b);
+  cta_column_sums(bs.B, part, smem_b);
 }
 
 // Per column: sums over the CTAs in order, the stopping rule, the scalars of
