@@ -61,14 +61,50 @@ struct BatchScalars {
   int32_t exact;
 };
 
-// Row sum of one row of A times Z for this lane's columns.
+// Arcs whose gathers one warp keeps in flight together: about 32 registers
+// of gathered values per lane.
+template <class VT, int VW>
+constexpr int arcs_in_flight() {
+  constexpr int u = 32 / (VW * (int)(sizeof(VT) / 4));
+  return u < 1 ? 1 : (u > 8 ? 8 : u);
+}
+
+// Row sum of one row of A times Z for this lane's columns. U arcs at a
+// time: their indices, then all their gathers, then the products added in
+// arc order (so each column's sum keeps the order of a one-arc loop).
 template <class VT, class MT, int VW>
 __device__ __forceinline__ void row_product(const OpView<MT>& op, const VT* __restrict__ Z,
                                             uint32_t B, uint32_t a0, uint32_t a1, int lane,
                                             VT (&acc)[VW]) {
+  constexpr int U = arcs_in_flight<VT, VW>();
 #pragma unroll
   for (int v = 0; v < VW; ++v) acc[v] = VT(0);
-  for (uint32_t k = a0; k < a1; ++k) {
+  uint32_t k = a0;
+  for (; k + U <= a1; k += U) {
+    uint32_t j[U];
+    VT w[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      j[u] = __ldg(op.cols + k + u);
+      w[u] = op.vals ? (VT)__ldg(op.vals + k + u) : VT(1);
+    }
+    VT z[U][VW];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const VT* zr = Z + (size_t)j[u] * B;
+#pragma unroll
+      for (int v = 0; v < VW; ++v) {
+        const uint32_t c = lane + 32 * v;
+        z[u][v] = c < B ? __ldg(zr + c) : VT(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int v = 0; v < VW; ++v)
+        if (lane + 32 * v < B) acc[v] += w[u] * z[u][v];
+  }
+  for (; k < a1; ++k) {
     const uint32_t j = __ldg(op.cols + k);
     const VT w = op.vals ? (VT)__ldg(op.vals + k) : VT(1);
     const VT* zr = Z + (size_t)j * B;
