@@ -30,7 +30,7 @@ constexpr int BT = 256;          // threads per CTA
 constexpr int BW = BT / 32;      // warps per CTA
 constexpr int MAXVW = 8;         // columns per lane (B <= 256 per launch)
 constexpr uint32_t LONG_ROW = 512;
-constexpr uint32_t RANGE_ARCS = 1024;
+constexpr uint32_t RANGE_ARCS = 256;
 
 struct RowRange {
   uint32_t lo, hi;
