@@ -463,10 +463,12 @@ def run_c2(args):
 
 def run_c4a(args):
     """R-MAT 22 directed, 256 personalisation vectors (1-64 seeds each), one
-    batched solve, mixed precision."""
+    batched solve, mixed precision (another scale with --scale, for
+    profiling captures)."""
     import knappnet_b200 as K
     from oracle import oracle as O
-    g = K.generate_rmat(22, 16, seed=20240703, clean=True)
+    scale = args.scale if args.scale != SCALE else 22
+    g = K.generate_rmat(scale, 16, seed=20240703, clean=True)
     n, B = g.n, 256
     rng = np.random.default_rng(20240704)
     P = np.zeros((B, n))
@@ -490,7 +492,7 @@ def run_c4a(args):
         cpu += time.perf_counter() - t0
         errs.append(float(np.abs(keep["x"][b] - ref).sum()))
     arcs = int(g.csr(1)[0][-1])
-    return {"workload": "c4a: R-MAT 22 directed, 256 personalisation vectors (uniform over "
+    return {"workload": f"c4a: R-MAT {scale} directed, 256 personalisation vectors (uniform over "
                         "1-64 seed nodes), batched SpMM PageRank, mixed precision, tol 1e-10",
             "metric": "GTEPS*B per sweep", "unit": "GTEPS*B/sweep", "higher_is_better": True,
             "value": round(arcs * B * info.sweeps / sec / 1e9, 2),
