@@ -18,6 +18,7 @@
 // nodes stay dangling for positive weights, so D does not move.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "adjoint.cuh"
@@ -136,11 +137,14 @@ void pagerank_weights(GraphHandleImpl& g, const double* d_w, const PagerankParam
                       double* d_out, PagerankInfo* info, cudaStream_t s) {
   if (g.n == 0) return;
   const int which = pagerank_rows(g, prm.directed);
-  auto op = g.weighted_op(which, d_w, pagerank_loop_factor(which, prm.loops), s);
+  const double lf = pagerank_loop_factor(which, prm.loops);
+  GraphHandleImpl::WeightSlot& slot = g.weight_slot(which, lf, s);
+  std::lock_guard<std::mutex> lock(slot.mu);
+  g.fill_weights(*slot.op, d_w, lf, s);
   PagerankParams p = prm;
   p.weighted = true;
-  p.relabel = false;  // a one-off operator: renumbering would cost more than it saves
-  pagerank_op(*op, p, d_out, true, info, s);
+  p.relabel = false;  // values change every call: no renumbered copy
+  pagerank_op(*slot.op, p, d_out, true, info, s);
 }
 
 void pagerank_grad(GraphHandleImpl& g, const double* d_w, const double* d_x, const double* d_gx,
@@ -151,9 +155,17 @@ void pagerank_grad(GraphHandleImpl& g, const double* d_w, const double* d_x, con
   if (n == 0) return;
   const int which = pagerank_rows(g, prm.directed);
   const double lf = pagerank_loop_factor(which, prm.loops);
-  auto fwd = g.weighted_op(which, d_w, lf, s);  // its column sums are the out-strengths
-  const int twhich = which == 1 ? 0 : which;    // pull along out-arcs
-  auto tr = g.weighted_op(twhich, d_w, lf, s);
+  // fwd: its column sums are the out-strengths; tr: pull along out-arcs
+  const int twhich = which == 1 ? 0 : which;
+  GraphHandleImpl::WeightSlot& fslot = g.weight_slot(which, lf, s);
+  GraphHandleImpl::WeightSlot& tslot = g.weight_slot(twhich, lf, s);
+  std::unique_lock<std::mutex> flock(fslot.mu, std::defer_lock), tlock(tslot.mu, std::defer_lock);
+  if (&fslot == &tslot) flock.lock();
+  else std::lock(flock, tlock);
+  Operator* fwd = fslot.op.get();
+  Operator* tr = tslot.op.get();
+  g.fill_weights(*fwd, d_w, lf, s);
+  if (tr != fwd) g.fill_weights(*tr, d_w, lf, s);
   const Partition& P = tr->partition(128, s);
   DevBuf<double> jump;
   if (prm.personalization && prm.dangling == 0) normalized_jump(prm.personalization, n, jump, s);

@@ -110,10 +110,18 @@ struct GraphHandleImpl {
   const DevCsr& in_rows() const { return directed ? inc : out; }
   const DevCsr& undirected_rows(cudaStream_t s);
   Operator& op(int which, bool weighted, double loop_factor, cudaStream_t s);
-  // An uncached operator whose arc values come from per-edge weights d_w
-  // (device, input edge order) instead of the graph's own.
-  std::unique_ptr<Operator> weighted_op(int which, const double* d_w, double loop_factor,
-                                        cudaStream_t s);
+  // Operators whose arc values come from per-edge weights d_w (device,
+  // input edge order) given per call, one per (rows, loop factor): the
+  // structure, partitions and workspaces stay, and each call rewrites the
+  // values (fill_weights) while it holds the slot's mutex.
+  struct WeightSlot {
+    std::mutex mu;
+    std::unique_ptr<Operator> op;
+  };
+  std::map<std::pair<int, int>, std::unique_ptr<WeightSlot>> wslots;  // guarded by mu
+  WeightSlot& weight_slot(int which, double loop_factor, cudaStream_t s);
+  // Arc values, column sums and their inverses of o from d_w.
+  void fill_weights(Operator& o, const double* d_w, double loop_factor, cudaStream_t s);
 };
 
 // Merge-path tile coordinates and split rows of a row-compressed matrix.

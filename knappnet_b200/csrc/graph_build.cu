@@ -656,40 +656,56 @@ __global__ void row_sums_from_edges(const uint32_t* __restrict__ off, const uint
   }
 }
 
-std::unique_ptr<Operator> GraphHandleImpl::weighted_op(int which, const double* d_w, double lf,
-                                                       cudaStream_t s) {
+// An operator over the chosen rows with value buffers allocated (not filled).
+static std::unique_ptr<Operator> weights_skeleton(GraphHandleImpl& g, int which, cudaStream_t s) {
   auto o = std::make_unique<Operator>();
-  const DevCsr* rows = which == 0 ? &out : which == 1 ? &in_rows() : &undirected_rows(s);
-  const DevCsr* trans = which == 0 ? &in_rows() : which == 1 ? &out : rows;
+  const DevCsr* rows = which == 0 ? &g.out : which == 1 ? &g.in_rows() : &g.undirected_rows(s);
+  const DevCsr* trans = which == 0 ? &g.in_rows() : which == 1 ? &g.out : rows;
   o->rows = rows;
   o->trans = trans;
-  o->n = n;
+  o->n = g.n;
   o->nnz = rows->arcs;
   o->has_vals = true;
   o->vals64.alloc(std::max<uint64_t>(o->nnz, 1));
   o->vals32.alloc(std::max<uint64_t>(o->nnz, 1));
-  o->colsum.alloc(std::max<uint32_t>(n, 1));
-  o->inv_out64.alloc(std::max<uint32_t>(n, 1));
-  o->inv_out32.alloc(std::max<uint32_t>(n, 1));
+  o->colsum.alloc(std::max<uint32_t>(g.n, 1));
+  o->inv_out64.alloc(std::max<uint32_t>(g.n, 1));
+  o->inv_out32.alloc(std::max<uint32_t>(g.n, 1));
+  return o;
+}
+
+void GraphHandleImpl::fill_weights(Operator& o, const double* d_w, double lf, cudaStream_t s) {
+  const DevCsr* rows = o.rows;
+  const DevCsr* trans = o.trans;
   DevBuf<unsigned int> flags(2);
   KNB_CUDA(cudaMemsetAsync(flags.get(), 0, 8, s));
   if (n) {
     op_values_from_edges<<<grid_for(n, 256), 256, 0, s>>>(rows->off.get(), rows->tgt.get(),
                                                           rows->edge.get(), d_w, n, lf,
-                                                          o->vals64.get(), o->vals32.get(),
+                                                          o.vals64.get(), o.vals32.get(),
                                                           flags.get());
     row_sums_from_edges<<<grid_for(n, 128), 128, 0, s>>>(trans->off.get(), trans->tgt.get(),
                                                          trans->edge.get(), d_w, n, lf,
-                                                         o->colsum.get(), o->inv_out64.get(),
-                                                         o->inv_out32.get(), flags.get() + 1);
+                                                         o.colsum.get(), o.inv_out64.get(),
+                                                         o.inv_out32.get(), flags.get() + 1);
     KNB_LAUNCH("weighted_op");
   }
   unsigned int hf[2] = {0, 0};
   KNB_CUDA(cudaMemcpyAsync(hf, flags.get(), 8, cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
-  o->vals32_exact = hf[0] == 0;
-  o->n_dangling = hf[1];
-  return o;
+  o.vals32_exact = hf[0] == 0;
+  o.n_dangling = hf[1];
+}
+
+GraphHandleImpl::WeightSlot& GraphHandleImpl::weight_slot(int which, double lf, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair(which, (int)(lf * 2));
+  auto& slot = wslots[key];
+  if (!slot) {
+    slot = std::make_unique<WeightSlot>();
+    slot->op = weights_skeleton(*this, which, s);
+  }
+  return *slot;
 }
 
 Operator& GraphHandleImpl::op(int which, bool wtd, double lf, cudaStream_t s) {
