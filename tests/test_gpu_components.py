@@ -281,3 +281,38 @@ def test_leading_eigen_reference_cases_and_errors():
         K.Graph(2, np.array([0]), np.array([1]), None, False).leading_eigen(weighted=True)
     with pytest.raises(RuntimeError, match="limited to 3000 nodes"):
         K.Graph(3001, np.array([0]), np.array([1]), None, False).leading_eigen()
+
+
+def test_zero_node_graph_every_entry_point():
+    """A graph without nodes: every entry point gives what the oracle gives
+    (equal results, NaN where undefined), or both refuse."""
+    e = np.array([], dtype=np.int64)
+    for directed in (True, False):
+        g = K.Graph(0, e, e, None, directed)
+        og = O.Graph(0, e, e, None, directed)
+        calls = [
+            ("components", lambda x: x.components(strong=True)[1]),
+            ("weak", lambda x: x.components(strong=False)[1]),
+            ("pagerank", lambda x: x.pagerank()),
+            ("eigenvector", lambda x: x.eigenvector(mode=3)[0]),
+            ("katz", lambda x: x.katz(alpha=0.1)),
+            ("hits", lambda x: x.hits()[0]),
+            ("centralization", lambda x: x.centralization_eigenvector()),
+            ("twomode", lambda x: x.twomode_eigenvector([])[0]),
+        ]
+        if not directed:
+            calls.append(("leading_eigen", lambda x: x.leading_eigen()[0]))
+        for name, fn in calls:
+            try:
+                ref = fn(og)
+            except RuntimeError:
+                with pytest.raises(RuntimeError):
+                    fn(g)
+                continue
+            got = fn(g)
+            assert np.array_equal(np.asarray(got, dtype=np.float64),
+                                  np.asarray(ref, dtype=np.float64), equal_nan=True), name
+        sg = g.simplify(undirected=True)
+        assert sg.n == 0 and sg.m == 0
+        sg.close()
+        g.close()
