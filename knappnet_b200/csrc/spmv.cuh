@@ -238,7 +238,11 @@ template <class VT, int IPT>
 struct WarpSmem {
   static constexpr int PAD_SHIFT = sizeof(VT) == 8 ? 4 : 5;
   VT prod[32 * IPT + ((32 * IPT) >> PAD_SHIFT)];
-  uint32_t rend[32 * IPT + 1];
+  // tile-relative row ends, at most 32 * IPT: 16 bits keep three 16-warp
+  // CTAs of the FP32 sweep under the 100 KB shared-memory carveout, so L1
+  // keeps the rest of the SM's 256 KB
+  uint16_t rend[32 * IPT + 1];
+  static_assert(32 * IPT < 65536, "row ends must fit in 16 bits");
   static __device__ __forceinline__ uint32_t slot(uint32_t k) { return k + (k >> PAD_SHIFT); }
 };
 
@@ -248,9 +252,9 @@ struct WarpSmem {
 // that is free once the walk is over (it may alias the products). The
 // epilogue's scalars accumulate into this lane's `a` (see
 // warp_store_partials).
-template <class VT, class Epi, int IPT, class Prod>
+template <class VT, class Epi, int IPT, class Prod, class RE>
 __device__ __forceinline__ void warp_tile_finish(const Prod& prod, VT* rowbuf,
-                                                 const uint32_t* rend, uint32_t t, uint32_t i0,
+                                                 const RE* rend, uint32_t t, uint32_t i0,
                                                  uint32_t n_rows, uint32_t n_arcs, bool first_open,
                                                  const Epi& epi, VT* __restrict__ carry,
                                                  VT* __restrict__ head, double* a, int lane) {
@@ -435,7 +439,8 @@ warp_spmv(OpView<MT> op, const VT* __restrict__ xg, Epi epi_in,
         if (k < n_arcs) sm.prod[S::slot(k)] = op.vals ? wv[q] * xv[q] : xv[q];
       }
     }
-    for (uint32_t r = lane; r < n_rows; r += 32) sm.rend[r] = op.off[i0 + r + 1] - j0;
+    for (uint32_t r = lane; r < n_rows; r += 32)
+      sm.rend[r] = (uint16_t)(op.off[i0 + r + 1] - j0);
     const bool first_open = i0 < op.n && j0 > op.off[i0];
     __syncwarp();
     warp_tile_finish<VT, Epi, IPT>([&](uint32_t a) { return sm.prod[S::slot(a)]; }, sm.prod,
