@@ -111,7 +111,7 @@ NET_API int32_t net_eigenvector(const GraphHandle *h, int32_t mode, int32_t weig
  * collapse, keeping the largest (keep 0) or smallest (keep 1) weight, and
  * self-loops are dropped; undirected != 0 also symmetrizes a directed
  * graph. Edges come out sorted by (from, to). Release *out with
- * net_graph_free. Replaces netcapi.h:62-64 (crates/capi/src/topography.rs:42-56). */
+ * net_graph_free. Replaces netcapi.h:59-65 (crates/capi/src/topography.rs:42-56). */
 NET_API int32_t net_graph_simplify(const GraphHandle *h, int32_t undirected, int32_t keep,
                                    GraphHandle **out, char *err, size_t err_len);
 
