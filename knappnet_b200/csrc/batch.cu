@@ -69,6 +69,16 @@ constexpr int arcs_in_flight() {
   return u < 1 ? 1 : (u > 8 ? 8 : u);
 }
 
+// The normalised teleport columns: dense node-major P[i * B + c], or, when
+// few entries are nonzero, each row's nonzero (column, value) pairs in
+// column order (rowptr over n + 1 rows).
+struct PersView {
+  const double* dense;
+  const uint32_t* rowptr;
+  const uint32_t* cols;
+  const double* vals;
+};
+
 // Row sum of one row of A times Z for this lane's columns. U arcs at a
 // time: their indices, then all their gathers, then the products added in
 // arc order (so each column's sum keeps the order of a one-arc loop).
@@ -125,15 +135,28 @@ __device__ __forceinline__ void row_update(uint32_t i, const VT (&s)[VW], int la
                                            const BatchScalars& bs, const ColState* cs,
                                            const VT* __restrict__ Yold, VT* __restrict__ Ynew,
                                            VT* __restrict__ Znew, const VT* __restrict__ inv_out,
-                                           const double* __restrict__ P, double* red) {
+                                           const PersView& pv, double* red) {
   const VT io = inv_out[i];
+  VT psp[VW];  // this lane's teleport values of row i (sparse teleport)
+#pragma unroll
+  for (int v = 0; v < VW; ++v) psp[v] = VT(0);
+  if (!pv.dense) {
+    for (uint32_t e = pv.rowptr[i]; e < pv.rowptr[i + 1]; ++e) {
+      const uint32_t c = pv.cols[e];
+      if ((c & 31u) != (uint32_t)lane) continue;
+      const VT x = (VT)pv.vals[e];
+#pragma unroll
+      for (int v = 0; v < VW; ++v)
+        if ((c >> 5) == (uint32_t)v) psp[v] = x;
+    }
+  }
 #pragma unroll
   for (int v = 0; v < VW; ++v) {
     const uint32_t c = lane + 32 * v;
     if (c >= bs.B || cs[c].frozen) continue;
     const VT it = (VT)cs[c].inv_total, dt = (VT)cs[c].dterm;
     const size_t q = (size_t)i * bs.B + c;
-    const VT pg = (VT)P[q];
+    const VT pg = pv.dense ? (VT)pv.dense[q] : psp[v];
     const VT jg = bs.jump_uniform ? (VT)bs.pu : pg;
     const VT u = (VT)bs.d * (s[v] * it + dt * jg) + (VT)(1.0 - bs.d) * pg;
     const VT xo = Yold[q] * it;
@@ -171,7 +194,7 @@ __global__ void __launch_bounds__(BT)
 spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ ranges,
           uint32_t nranges, BatchScalars bs, const ColState* __restrict__ cs,
           const VT* __restrict__ Yold, VT* __restrict__ Ynew, VT* __restrict__ Znew,
-          const VT* __restrict__ inv_out, const double* __restrict__ P,
+          const VT* __restrict__ inv_out, PersView P,
           double* __restrict__ part, const int32_t* __restrict__ all_frozen) {
   if (*all_frozen) return;
   extern __shared__ double smem_b[];
@@ -218,7 +241,7 @@ __global__ void __launch_bounds__(BT)
 spmm_long(const uint32_t* __restrict__ lrow, const uint32_t* __restrict__ lfirst, uint32_t nlong,
           const VT* __restrict__ scratch, BatchScalars bs, const ColState* __restrict__ cs,
           const VT* __restrict__ Yold, VT* __restrict__ Ynew, VT* __restrict__ Znew,
-          const VT* __restrict__ inv_out, const double* __restrict__ P,
+          const VT* __restrict__ inv_out, PersView P,
           double* __restrict__ part, const int32_t* __restrict__ all_frozen) {
   if (*all_frozen) return;
   extern __shared__ double smem_b[];
@@ -394,6 +417,33 @@ __global__ void pers_scatter(const double* __restrict__ pin, const double* __res
   }
 }
 
+// Nonzero teleport entries per node of a column group (column-major input).
+__global__ void pers_row_counts(const double* __restrict__ pin, uint32_t n, uint32_t B,
+                                uint32_t* __restrict__ cnt) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t k = 0;
+    for (uint32_t c = 0; c < B; ++c) k += pin[(size_t)c * n + i] != 0.0 ? 1u : 0u;
+    cnt[i] = k;
+  }
+}
+
+// Each node's nonzero entries, normalised as pers_scatter does, in column order.
+__global__ void pers_row_fill(const double* __restrict__ pin, const double* __restrict__ sums,
+                              uint32_t n, uint32_t B, const uint32_t* __restrict__ rowptr,
+                              uint32_t* __restrict__ cols, double* __restrict__ vals) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t e = rowptr[i];
+    for (uint32_t c = 0; c < B; ++c) {
+      const double v = pin[(size_t)c * n + i];
+      if (v != 0.0) {
+        cols[e] = c;
+        vals[e] = v / sums[c];
+        ++e;
+      }
+    }
+  }
+}
+
 // Output: column-major out[c * n + i] = Y_c[i] / T_c from the buffer the
 // column stopped in.
 template <class VT>
@@ -453,7 +503,7 @@ static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uin
                        const DevBuf<Chunk>& chunks, uint32_t nchunks, const DevBuf<uint32_t>& lrow,
                        const DevBuf<uint32_t>& lfirst, uint32_t nlong, const BatchScalars& bs,
                        ColState* cs, const VT* Yold, VT* Ynew, const VT* Zold, VT* Znew,
-                       const VT* inv_out, const double* P, VT* scratch, double* part,
+                       const VT* inv_out, const PersView& P, VT* scratch, double* part,
                        int32_t* all_frozen, unsigned grid, cudaStream_t s) {
   const size_t smem = (size_t)BW * 3 * bs.B * sizeof(double);
   static bool attr = false;
@@ -485,7 +535,7 @@ static int batch_sweep_vw(int vw, const OpView<MT>& op, const DevBuf<RowRange>& 
                           uint32_t nranges, const DevBuf<Chunk>& chunks, uint32_t nchunks,
                           const DevBuf<uint32_t>& lrow, const DevBuf<uint32_t>& lfirst,
                           uint32_t nlong, const BatchScalars& bs, ColState* cs, const VT* Yold,
-                          VT* Ynew, const VT* Zold, VT* Znew, const VT* inv_out, const double* P,
+                          VT* Ynew, const VT* Zold, VT* Znew, const VT* inv_out, const PersView& P,
                           VT* scratch, double* part, int32_t* all_frozen, unsigned grid,
                           cudaStream_t s) {
 #define KNB_SW(V)                                                                                 \
@@ -554,19 +604,38 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
   for (uint32_t c0 = 0; c0 < Btot; c0 += 256) {
     const uint32_t B = std::min<uint32_t>(256, Btot - c0);
     const int vw = vw_for(B);
-    DevBuf<double> P((size_t)n * B), sums(B);
+    DevBuf<double> Pd, sums(B), pvals;
+    DevBuf<uint32_t> prow((size_t)n + 1), pcols;
     DevBuf<int32_t> flags(2);
     KNB_CUDA(cudaMemsetAsync(flags.get(), 0, 8, s));
-    pers_columns<<<grid_for(B, BW, 1184), BT, 0, s>>>(pin.get() + (size_t)c0 * n, n, B, P.get(),
+    pers_columns<<<grid_for(B, BW, 1184), BT, 0, s>>>(pin.get() + (size_t)c0 * n, n, B, nullptr,
                                                       flags.get(), sums.get());
     int32_t hf[2];
     KNB_CUDA(cudaMemcpyAsync(hf, flags.get(), 8, cudaMemcpyDeviceToHost, s));
     KNB_CUDA(cudaStreamSynchronize(s));
     if (hf[0] & 1) throw Error("the personalization vector must hold finite, nonnegative values");
     if (hf[0] & 2) throw Error("the personalization vector must have a positive sum");
-    pers_scatter<<<grid_for((uint64_t)n * B, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n,
-                                                                 sums.get(), n, B, P.get());
-    launches += 2;
+    // Teleport columns: the nonzero entries per node when at most 1/16 of
+    // them are nonzero (seed-set personalisation), else dense; a sweep then
+    // reads only the rows that hold seeds.
+    KNB_CUDA(cudaMemsetAsync(prow.get(), 0, ((size_t)n + 1) * 4, s));
+    pers_row_counts<<<grid_for(n, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n, n, B, prow.get());
+    const uint32_t pnnz = exclusive_scan<uint32_t>(prow.get(), prow.get(), (size_t)n + 1, s);
+    PersView P{nullptr, nullptr, nullptr, nullptr};
+    if ((uint64_t)pnnz * 16 <= (uint64_t)n * B) {
+      pcols.alloc(std::max<uint32_t>(pnnz, 1));
+      pvals.alloc(std::max<uint32_t>(pnnz, 1));
+      pers_row_fill<<<grid_for(n, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n, sums.get(), n, B,
+                                                     prow.get(), pcols.get(), pvals.get());
+      P = PersView{nullptr, prow.get(), pcols.get(), pvals.get()};
+    } else {
+      Pd.alloc((size_t)n * B);
+      pers_scatter<<<grid_for((uint64_t)n * B, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n,
+                                                                   sums.get(), n, B, Pd.get());
+      P = PersView{Pd.get(), nullptr, nullptr, nullptr};
+    }
+    KNB_LAUNCH("teleport columns");
+    launches += 4;
     BatchScalars bs{prm.damping, 1.0 / n, n, B, prm.dangling == 1 ? 1 : 0, 0.0, 0, 0};
     DevBuf<ColState> cs(B);
     DevBuf<int32_t> all_frozen(1);
@@ -595,7 +664,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
         launches += batch_sweep_vw<float, float>(
             vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
             cs.get(), Y32[b].get(), Y32[1 - b].get(), Z32[b].get(), Z32[1 - b].get(),
-            op.inv_out32.get(), P.get(), sc32.get(), part.get(), all_frozen.get(), grid, s);
+            op.inv_out32.get(), P, sc32.get(), part.get(), all_frozen.get(), grid, s);
         ++k;
         if (k % 4 == 0) {
           int32_t af = 0;
@@ -651,12 +720,12 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
         launches += batch_sweep_vw<double, float>(
             vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
             cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
-            op.inv_out64.get(), P.get(), sc64.get(), part.get(), all_frozen.get(), grid, s);
+            op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
       else
         launches += batch_sweep_vw<double, double>(
             vw, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
             cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
-            op.inv_out64.get(), P.get(), sc64.get(), part.get(), all_frozen.get(), grid, s);
+            op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
       ++k;
       if (k % 4 == 0) {
         int32_t af = 0;

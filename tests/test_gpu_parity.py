@@ -468,6 +468,21 @@ def test_pagerank_batch_matches_per_vector_oracle(precision, B):
     assert info.max_column_iterations >= 1
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pagerank_batch_dense_teleport(precision):
+    """Teleport columns with every entry positive (the dense layout; seed
+    sets take the sparse one): each column matches its own oracle solve."""
+    kg, og = rmat_pair(11, True, seed=33)
+    rng = np.random.default_rng(34)
+    P = rng.uniform(0.1, 2.0, (24, kg.n))
+    P[3, ::2] = 0.0  # one column half empty
+    out, _ = kg.pagerank_batch(P, weighted=True, precision=precision, tol=1e-10)
+    for b in range(P.shape[0]):
+        ref = og.pagerank(weighted=True, personalization=P[b], tol=1e-10)
+        err = np.abs(out[b] - ref).sum()
+        assert err <= (1e-12 if precision == 0 else 1e-9), (b, err)
+
+
 def test_pagerank_batch_options_and_errors():
     kg, og = rmat_pair(10, True, seed=5)
     P = seed_vectors(kg.n, 5, 3)
