@@ -1577,23 +1577,34 @@ void hits_rescale(std::vector<double>& x, int how) {
 
 }  // namespace
 
-void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* auth_out,
-          double* value, int* unique, cudaStream_t s) {
-  const uint32_t n = g.n;
-  // A: rows are arcs out of each node (matrix(g, Out, ...)); A^T: the in-CSR
-  // of a directed graph (the reference's stable transpose has the same
-  // entry order), A itself for an undirected one.
-  const bool hdir = g.directed;
-  const double lf = p.loops == 2 ? 0.0 : (!hdir && p.loops == 0 ? 2.0 : 1.0);
-  Operator& A = g.op(0, p.weighted, lf, s);
-  Operator& At = hdir ? g.op(1, p.weighted, lf, s) : A;
-  const OpView<double> a64{A.n, A.nnz, A.rows->off.get(), A.rows->tgt.get(),
-                           A.has_vals ? A.vals64.get() : nullptr};
-  const OpView<double> t64{At.n, At.nnz, At.rows->off.get(), At.rows->tgt.get(),
-                           At.has_vals ? At.vals64.get() : nullptr};
+// What hubs and authorities on one operator can reuse: the blocks, their
+// upper bounds and order, each solved block's submatrices A_b and A_b^T with
+// Kleinberg's start vector A_b^T 1, and the Lanczos buffers. Held for the
+// length of a call, so concurrent calls on one operator take turns.
+struct HitsPlan : Workspace {
+  std::mutex mu;
+  bool ready = false, any = false;
+  std::vector<std::vector<uint32_t>> bh, ba;
+  std::vector<double> upper;
+  std::vector<size_t> order;
+  struct Block {
+    DevOp ab, abt;
+    DevBuf<double> sdev;
+    std::vector<double> sv;
+  };
+  std::map<size_t, std::unique_ptr<Block>> blocks;
+  DevBuf<uint32_t> hub_index, auth_index, nodes_h, nodes_a;
+  DevBuf<double> vdev;
+  LzBuffers lz;
+};
+
+// The blocks, their bounds and their order (spectral.rs:757-836), computed
+// once per operator.
+static void hits_prepare(HitsPlan& plan, const OpView<double>& a64, const OpView<double>& t64,
+                         uint32_t n, cudaStream_t s) {
+  const uint32_t n2 = 2 * n;
   // blocks of the bipartite graph (hubs 0..n, authorities n..2n) joined by
   // positive entries (spectral.rs:757-813), found on the device
-  const uint32_t n2 = 2 * n;
   std::vector<uint32_t> label(n2);
   unsigned int any = 0;
   {
@@ -1616,13 +1627,13 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
     KNB_CUDA(cudaMemcpyAsync(&any, anyd.get(), 4, cudaMemcpyDeviceToHost, s));
     KNB_CUDA(cudaStreamSynchronize(s));
   }
-  if (!any) {
-    for (uint32_t i = 0; i < n; ++i) hubs_out[i] = auth_out[i] = std::nan("");
-    *value = 0.0;
-    *unique = 0;
+  plan.any = any != 0;
+  if (!plan.any) {
+    plan.ready = true;
     return;
   }
-  std::vector<std::vector<uint32_t>> bh, ba;
+  std::vector<std::vector<uint32_t>>& bh = plan.bh;
+  std::vector<std::vector<uint32_t>>& ba = plan.ba;
   for (uint32_t v = 0; v < n2; ++v) {
     const uint32_t b = label[v];
     if (b == 0xFFFFFFFFu) continue;
@@ -1645,7 +1656,9 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
     KNB_CUDA(cudaStreamSynchronize(s));
   }
   const size_t kb = bh.size();
-  std::vector<double> upper(kb, 0.0), lower(kb, 0.0);
+  std::vector<double>& upper = plan.upper;
+  upper.assign(kb, 0.0);
+  std::vector<double> lower(kb, 0.0);
   for (size_t b = 0; b < kb; ++b) {
     double rm = 0.0, cm = 0.0, lm = 0.0;
     for (uint32_t i : bh[b]) rm = std::max(rm, row_sum[i]);
@@ -1656,43 +1669,94 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
     upper[b] = rm * cm;
     lower[b] = lm;
   }
-  std::vector<size_t> order(kb);
+  std::vector<size_t>& order = plan.order;
+  order.resize(kb);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return lower[x] > lower[y]; });
+  plan.hub_index.alloc(n);
+  plan.auth_index.alloc(n);
+  plan.nodes_h.alloc(n);
+  plan.nodes_a.alloc(n);
+  KNB_CUDA(cudaMemsetAsync(plan.hub_index.get(), 0xFF, (size_t)n * 4, s));
+  KNB_CUDA(cudaMemsetAsync(plan.auth_index.get(), 0xFF, (size_t)n * 4, s));
+  plan.ready = true;
+}
+
+void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* auth_out,
+          double* value, int* unique, cudaStream_t s) {
+  const uint32_t n = g.n;
+  // A: rows are arcs out of each node (matrix(g, Out, ...)); A^T: the in-CSR
+  // of a directed graph (the reference's stable transpose has the same
+  // entry order), A itself for an undirected one.
+  const bool hdir = g.directed;
+  const double lf = p.loops == 2 ? 0.0 : (!hdir && p.loops == 0 ? 2.0 : 1.0);
+  Operator& A = g.op(0, p.weighted, lf, s);
+  Operator& At = hdir ? g.op(1, p.weighted, lf, s) : A;
+  const OpView<double> a64{A.n, A.nnz, A.rows->off.get(), A.rows->tgt.get(),
+                           A.has_vals ? A.vals64.get() : nullptr};
+  const OpView<double> t64{At.n, At.nnz, At.rows->off.get(), At.rows->tgt.get(),
+                           At.has_vals ? At.vals64.get() : nullptr};
+  HitsPlan* planp = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(A.mu);
+    if (!A.hits_ws) A.hits_ws = std::make_unique<HitsPlan>();
+    planp = static_cast<HitsPlan*>(A.hits_ws.get());
+  }
+  HitsPlan& plan = *planp;
+  std::lock_guard<std::mutex> plan_lock(plan.mu);
+  if (!plan.ready) hits_prepare(plan, a64, t64, n, s);
+  if (!plan.any) {
+    for (uint32_t i = 0; i < n; ++i) hubs_out[i] = auth_out[i] = std::nan("");
+    *value = 0.0;
+    *unique = 0;
+    return;
+  }
+  const std::vector<std::vector<uint32_t>>& bh = plan.bh;
+  const std::vector<std::vector<uint32_t>>& ba = plan.ba;
+  const std::vector<double>& upper = plan.upper;
   // leading eigenpair of each block that may hold the largest value
-  DevBuf<uint32_t> hub_index(n), auth_index(n), nodes_h(n), nodes_a(n);
-  KNB_CUDA(cudaMemsetAsync(hub_index.get(), 0xFF, (size_t)n * 4, s));
-  KNB_CUDA(cudaMemsetAsync(auth_index.get(), 0xFF, (size_t)n * 4, s));
   const double TIE = 1e-9;
   double best = 0.0;
   struct Solved {
     size_t b;
     double value;
-    std::vector<double> v, sv;
+    std::vector<double> v;
+    const std::vector<double>* sv;
   };
   std::vector<Solved> solved;
   int launches = 0;
-  for (size_t b : order) {
+  for (size_t b : plan.order) {
     if (upper[b] < best * (1.0 - TIE)) continue;
     const uint32_t nh = (uint32_t)bh[b].size(), na = (uint32_t)ba[b].size();
-    KNB_CUDA(cudaMemcpyAsync(nodes_h.get(), bh[b].data(), (size_t)nh * 4, cudaMemcpyHostToDevice, s));
-    KNB_CUDA(cudaMemcpyAsync(nodes_a.get(), ba[b].data(), (size_t)na * 4, cudaMemcpyHostToDevice, s));
-    scatter_local<<<grid_for(nh, 256), 256, 0, s>>>(nodes_h.get(), nh, hub_index.get());
-    scatter_local<<<grid_for(na, 256), 256, 0, s>>>(nodes_a.get(), na, auth_index.get());
-    DevOp ab, abt;
-    DevBuf<uint32_t> tmp_nodes(std::max(nh, na));
-    mapped_submatrix(a64, bh[b], auth_index.get(), tmp_nodes, ab, s);
-    mapped_submatrix(t64, ba[b], hub_index.get(), tmp_nodes, abt, s);
-    unscatter_local<<<grid_for(nh, 256), 256, 0, s>>>(nodes_h.get(), nh, hub_index.get());
-    unscatter_local<<<grid_for(na, 256), 256, 0, s>>>(nodes_a.get(), na, auth_index.get());
-    // Kleinberg's first authority vector A_b^T 1
-    DevBuf<double> ones(std::max<uint32_t>(nh, 1)), sdev(std::max<uint32_t>(na, 1)), vdev(na);
-    fill_value<<<grid_for(nh, 256), 256, 0, s>>>(ones.get(), nh, 1.0);
-    SpmvScratch sc;
-    launches += 6 + spmv(abt, ones.get(), nullptr, sdev.get(), sc, nullptr, s);
+    std::unique_ptr<HitsPlan::Block>& blk = plan.blocks[b];
+    if (!blk) {
+      blk = std::make_unique<HitsPlan::Block>();
+      DevBuf<uint32_t>& nodes_h = plan.nodes_h;
+      DevBuf<uint32_t>& nodes_a = plan.nodes_a;
+      KNB_CUDA(cudaMemcpyAsync(nodes_h.get(), bh[b].data(), (size_t)nh * 4, cudaMemcpyHostToDevice, s));
+      KNB_CUDA(cudaMemcpyAsync(nodes_a.get(), ba[b].data(), (size_t)na * 4, cudaMemcpyHostToDevice, s));
+      scatter_local<<<grid_for(nh, 256), 256, 0, s>>>(nodes_h.get(), nh, plan.hub_index.get());
+      scatter_local<<<grid_for(na, 256), 256, 0, s>>>(nodes_a.get(), na, plan.auth_index.get());
+      DevBuf<uint32_t> tmp_nodes(std::max(nh, na));
+      mapped_submatrix(a64, bh[b], plan.auth_index.get(), tmp_nodes, blk->ab, s);
+      mapped_submatrix(t64, ba[b], plan.hub_index.get(), tmp_nodes, blk->abt, s);
+      unscatter_local<<<grid_for(nh, 256), 256, 0, s>>>(nodes_h.get(), nh, plan.hub_index.get());
+      unscatter_local<<<grid_for(na, 256), 256, 0, s>>>(nodes_a.get(), na, plan.auth_index.get());
+      // Kleinberg's first authority vector A_b^T 1
+      DevBuf<double> ones(std::max<uint32_t>(nh, 1));
+      blk->sdev.alloc(std::max<uint32_t>(na, 1));
+      fill_value<<<grid_for(nh, 256), 256, 0, s>>>(ones.get(), nh, 1.0);
+      SpmvScratch sc;
+      launches += 6 + spmv(blk->abt, ones.get(), nullptr, blk->sdev.get(), sc, nullptr, s);
+      blk->sv.resize(na);
+      KNB_CUDA(cudaMemcpyAsync(blk->sv.data(), blk->sdev.get(), (size_t)na * 8,
+                               cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+    }
+    if (plan.vdev.n < na) plan.vdev.alloc(na);
     Leading res;
-    if (!symmetric_leading(ab, p.tol, 0.0, p.max_iter, false, vdev.get(), &res, &launches, s,
-                           &abt, sdev.get()))
+    if (!symmetric_leading(blk->ab, p.tol, 0.0, p.max_iter, false, plan.vdev.get(), &res,
+                           &launches, s, &blk->abt, blk->sdev.get(), &plan.lz))
       throw Error("hub and authority scores did not converge to tolerance " + fmt_g(p.tol) +
                   " within " + std::to_string(p.max_iter) +
                   " matrix-vector products; a larger iteration cap may help");
@@ -1700,9 +1764,9 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
     sol.b = b;
     sol.value = res.value;
     sol.v.resize(na);
-    sol.sv.resize(na);
-    KNB_CUDA(cudaMemcpyAsync(sol.v.data(), vdev.get(), (size_t)na * 8, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaMemcpyAsync(sol.sv.data(), sdev.get(), (size_t)na * 8, cudaMemcpyDeviceToHost, s));
+    sol.sv = &blk->sv;
+    KNB_CUDA(cudaMemcpyAsync(sol.v.data(), plan.vdev.get(), (size_t)na * 8, cudaMemcpyDeviceToHost,
+                             s));
     KNB_CUDA(cudaStreamSynchronize(s));
     best = std::max(best, res.value);
     solved.push_back(std::move(sol));
@@ -1713,7 +1777,7 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
     if (sol.value < best * (1.0 - TIE)) continue;
     ++tied;
     double weight = 0.0;
-    for (size_t i = 0; i < sol.v.size(); ++i) weight += sol.v[i] * sol.sv[i];
+    for (size_t i = 0; i < sol.v.size(); ++i) weight += sol.v[i] * (*sol.sv)[i];
     for (size_t i = 0; i < ba[sol.b].size(); ++i) auth[ba[sol.b][i]] = sol.v[i] * weight;
   }
   // hubs = A auth (device product)
