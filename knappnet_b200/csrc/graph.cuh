@@ -81,6 +81,7 @@ struct Operator {
   std::unique_ptr<Workspace> pr_ws;  // PageRank's (pagerank.cu), created on first use
   std::unique_ptr<Workspace> eig_ws;  // eigenvector centrality's (eigen.cu), created on first use
   std::unique_ptr<Workspace> hits_ws;  // hubs and authorities' (eigen.cu), created on first use
+  std::unique_ptr<Workspace> series_ws;  // the Katz / Bonacich attenuation check's (katz.cu)
 
   const Relabeled& relabeled(cudaStream_t s);
   const Partition& relabeled_partition(uint32_t tile_items, cudaStream_t s);

@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -419,14 +420,25 @@ __global__ void loop_diag(const uint32_t* __restrict__ off, const uint32_t* __re
   }
 }
 
-// check_attenuation (spectral.rs:447-527): returns the radius bound or
-// throws. `collatz` receives the number of power-iteration steps.
-double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw, bool weighted,
-                         double t, const char* name, int64_t max_iter, int64_t* collatz,
-                         cudaStream_t s) {
+// What the attenuation check on one operator can reuse whatever t is: the
+// components, the diagonal of every single-node component (in label order),
+// the larger components' member lists and chunks, and the operator with the
+// entries that leave their component masked to 0. Held for the length of a
+// check, so concurrent calls on one operator take turns.
+struct SeriesPlan : Workspace {
+  std::mutex mu;
+  bool ready = false;
+  size_t k = 0;
+  std::vector<double> single_diag;
+  uint32_t nbig = 0, nch = 0;
+  DevBuf<uint32_t> d_comp, d_members, d_big, d_cc0, d_chc, d_chl, d_chh;
+  DevBuf<uint8_t> d_big_flags;
+  DevBuf<double> mv;
+};
+
+static void series_prepare(SeriesPlan& plan, GraphHandleImpl& g, const Operator& op,
+                           const Rows& rw, bool weighted, cudaStream_t s) {
   const uint32_t n = g.n;
-  const double limit = 1.0 / t;
-  *collatz = 0;
   Comps comp;
   if (g.directed) {
     // strong components of the positive entries (spectral.rs:539-553); a
@@ -436,6 +448,7 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
     comp = weak_components(g, s);
   }
   const size_t k = comp.count();
+  plan.k = k;
   // single nodes: the diagonal (the sum of a node's self-loop entries)
   std::vector<double> diag(n, 0.0);
   if (n) {
@@ -450,13 +463,9 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
   std::vector<uint32_t> first(k, 0xFFFFFFFFu);
   for (uint32_t v = 0; v < n; ++v)
     if (first[comp.membership[v]] == 0xFFFFFFFFu) first[comp.membership[v]] = v;
-  double radius = 0.0;
+  plan.single_diag.clear();
   for (size_t c = 0; c < k; ++c)
-    if (comp.sizes[c] == 1) {
-      const double d = diag[first[c]];
-      if (d >= limit) throw too_large(name, t, d);
-      radius = std::max(radius, d);
-    }
+    if (comp.sizes[c] == 1) plan.single_diag.push_back(diag[first[c]]);
   // larger components: nodes grouped by component, chunks of CHUNK nodes
   std::vector<uint32_t> big_comps, comp_chunk0, members, chunk_comp, chunk_lo, chunk_hi;
   std::vector<uint32_t> start(k + 1, 0);
@@ -482,31 +491,70 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
       }
     }
   comp_chunk0.push_back((uint32_t)chunk_comp.size());
-  if (big_comps.empty()) return radius;
-  const uint32_t nbig = (uint32_t)big_comps.size(), nch = (uint32_t)chunk_comp.size();
-  auto up32 = [&](const std::vector<uint32_t>& h) {
-    DevBuf<uint32_t> d(std::max<size_t>(h.size(), 1));
-    if (!h.empty())
-      KNB_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * 4, cudaMemcpyHostToDevice, s));
-    return d;
-  };
-  DevBuf<uint32_t> d_comp = up32(comp.membership), d_members = up32(members),
-                   d_big = up32(big_comps), d_cc0 = up32(comp_chunk0), d_chc = up32(chunk_comp),
-                   d_chl = up32(chunk_lo), d_chh = up32(chunk_hi);
+  plan.nbig = (uint32_t)big_comps.size();
+  plan.nch = (uint32_t)chunk_comp.size();
+  if (plan.nbig) {
+    auto up32 = [&](DevBuf<uint32_t>& d, const std::vector<uint32_t>& h) {
+      d.alloc(std::max<size_t>(h.size(), 1));
+      if (!h.empty())
+        KNB_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * 4, cudaMemcpyHostToDevice, s));
+    };
+    up32(plan.d_comp, comp.membership);
+    up32(plan.d_members, members);
+    up32(plan.d_big, big_comps);
+    up32(plan.d_cc0, comp_chunk0);
+    up32(plan.d_chc, chunk_comp);
+    up32(plan.d_chl, chunk_lo);
+    up32(plan.d_chh, chunk_hi);
+    plan.d_big_flags.alloc(std::max<size_t>(k, 1));
+    KNB_CUDA(cudaMemcpyAsync(plan.d_big_flags.get(), big.data(), k, cudaMemcpyHostToDevice, s));
+    plan.mv.alloc(std::max<uint64_t>(op.nnz, 1));
+    const OpView<double> v0 = op.view64();
+    mask_values<<<grid_for((uint64_t)n * 32, KT), KT, 0, s>>>(v0, plan.d_comp.get(),
+                                                            plan.d_big_flags.get(), plan.mv.get());
+    KNB_LAUNCH("collatz set-up");
+    KNB_CUDA(cudaStreamSynchronize(s));
+  }
+  plan.ready = true;
+}
+
+// check_attenuation (spectral.rs:447-527): returns the radius bound or
+// throws. `collatz` receives the number of power-iteration steps.
+double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw, bool weighted,
+                         double t, const char* name, int64_t max_iter, int64_t* collatz,
+                         cudaStream_t s) {
+  const uint32_t n = g.n;
+  const double limit = 1.0 / t;
+  *collatz = 0;
+  Operator& mop = const_cast<Operator&>(op);
+  SeriesPlan* planp = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(mop.mu);
+    if (!mop.series_ws) mop.series_ws = std::make_unique<SeriesPlan>();
+    planp = static_cast<SeriesPlan*>(mop.series_ws.get());
+  }
+  SeriesPlan& plan = *planp;
+  std::lock_guard<std::mutex> plan_lock(plan.mu);
+  if (!plan.ready) series_prepare(plan, g, op, rw, weighted, s);
+  double radius = 0.0;
+  for (double d : plan.single_diag) {
+    if (d >= limit) throw too_large(name, t, d);
+    radius = std::max(radius, d);
+  }
+  if (plan.nbig == 0) return radius;
+  const size_t k = plan.k;
+  const uint32_t nbig = plan.nbig, nch = plan.nch;
   DevBuf<uint8_t> d_active(k), d_status(nbig);
-  KNB_CUDA(cudaMemcpyAsync(d_active.get(), big.data(), k, cudaMemcpyHostToDevice, s));
+  KNB_CUDA(cudaMemcpyAsync(d_active.get(), plan.d_big_flags.get(), k, cudaMemcpyDeviceToDevice, s));
   KNB_CUDA(cudaMemsetAsync(d_status.get(), 0, nbig, s));
-  DevBuf<double> mv(std::max<uint64_t>(op.nnz, 1)), x(n), ratio(n), ynext(n), cx((size_t)nch * 3),
-      value_b(nbig), top(k);
+  DevBuf<double> x(n), ratio(n), ynext(n), cx((size_t)nch * 3), value_b(nbig), top(k);
   const OpView<double> v0 = op.view64();
-  mask_values<<<grid_for((uint64_t)n * 32, KT), KT, 0, s>>>(v0, d_comp.get(), d_active.get(),
-                                                          mv.get());
   fill_d<<<grid_for(n, KT), KT, 0, s>>>(x.get(), n, 1.0);
-  KNB_LAUNCH("collatz set-up");
-  const OpView<double> vm{v0.n, v0.nnz, v0.off, v0.cols, mv.get()};
-  const Partition& P = const_cast<Operator&>(op).partition(32 * K_IPT, s);
+  KNB_LAUNCH("collatz start");
+  const OpView<double> vm{v0.n, v0.nnz, v0.off, v0.cols, plan.mv.get()};
+  const Partition& P = mop.partition(32 * K_IPT, s);
   Scratch sc(P);
-  CollatzEpi e{d_comp.get(), d_active.get(), x.get(), ratio.get(), ynext.get()};
+  CollatzEpi e{plan.d_comp.get(), d_active.get(), x.get(), ratio.get(), ynext.get()};
   std::vector<uint8_t> status(nbig, 0);
   std::vector<double> vals(nbig, 0.0);
   bool done = false;
@@ -514,12 +562,12 @@ double attenuation_bound(GraphHandleImpl& g, const Operator& op, const Rows& rw,
     sweep(vm, P, x.get(), e, sc.carry.get(), sc.head.get(), sc.part1.get(), sc.part2.get(),
           nullptr, s);
     chunk_extrema<<<std::min<uint32_t>(nch, 148 * 8), KT, 0, s>>>(
-        d_members.get(), d_chc.get(), d_chl.get(), d_chh.get(), d_active.get(), ratio.get(),
-        ynext.get(), nch, cx.get());
-    collatz_decide<<<grid_for(nbig, KT), KT, 0, s>>>(d_big.get(), nbig, d_cc0.get(), cx.get(),
-                                                     limit, d_active.get(), d_status.get(),
-                                                     value_b.get(), top.get());
-    collatz_next<<<grid_for(n, KT), KT, 0, s>>>(d_comp.get(), d_active.get(), ynext.get(),
+        plan.d_members.get(), plan.d_chc.get(), plan.d_chl.get(), plan.d_chh.get(),
+        d_active.get(), ratio.get(), ynext.get(), nch, cx.get());
+    collatz_decide<<<grid_for(nbig, KT), KT, 0, s>>>(plan.d_big.get(), nbig, plan.d_cc0.get(),
+                                                     cx.get(), limit, d_active.get(),
+                                                     d_status.get(), value_b.get(), top.get());
+    collatz_next<<<grid_for(n, KT), KT, 0, s>>>(plan.d_comp.get(), d_active.get(), ynext.get(),
                                                 top.get(), n, x.get());
     KNB_LAUNCH("collatz step");
     *collatz = it + 1;
