@@ -591,9 +591,10 @@ def run_c5(args):
 def run_next(args):
     """The measures built on the same kernels beyond PageRank and eigenvector
     centrality, one JSON line each: wall time of the C ABI call (host
-    buffers, set-up included; the median of the timed calls) against the
-    oracle's time for the same call on this host, and the largest difference
-    from the oracle."""
+    buffers; the median and minimum of the timed calls, which reuse the
+    set-up kept per operator, and the first call on the handle, which builds
+    it) against the oracle's time for the same call on this host, and the
+    largest difference from the oracle."""
     import knappnet_b200 as K
     from oracle import oracle as O
 
@@ -609,6 +610,8 @@ def run_next(args):
             t0 = time.perf_counter()
             keep["r"] = fn()
             dt = time.perf_counter() - t0
+            if i == 0:
+                timed.first = dt
             if i >= args.warmup:
                 times.append(dt)
         timed.last_min = min(times)
@@ -624,7 +627,7 @@ def run_next(args):
     def line(name, what, sec, csec, extra):
         d = {"workload": name, "description": what, "metric": "call ms", "value": round(sec * 1e3, 3),
              "unit": "ms", "higher_is_better": False, "min_ms": round(timed.last_min * 1e3, 3),
-             "oracle_ms": round(csec * 1e3, 1)}
+             "first_call_ms": round(timed.first * 1e3, 3), "oracle_ms": round(csec * 1e3, 1)}
         d.update(extra)
         lines.append(d)
 
