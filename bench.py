@@ -28,8 +28,8 @@ With --impl reference the reference arm runs instead: the CPU restatement
 net_pagerank call on the same graph, one bounded sample per step.
 
 Multi-GPU (torchrun, one process per GPU): independent replicas of the same
-solve (PageRank on one graph does not shard without an exchange per
-iteration); value is the arcs all ranks processed per
+solve (PageRank on one graph does not shard without an all-gather of the
+iterate every iteration); value is the arcs all ranks processed per
 iteration-second, timed as the maximum over ranks.
 """
 from __future__ import annotations
