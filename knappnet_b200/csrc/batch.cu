@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "batch.cuh"
@@ -61,13 +62,10 @@ struct BatchScalars {
   int32_t exact;
 };
 
-// Arcs whose gathers one warp keeps in flight together: about 32 registers
-// of gathered values per lane.
-template <class VT, int VW>
-constexpr int arcs_in_flight() {
-  constexpr int u = 32 / (VW * (int)(sizeof(VT) / 4));
-  return u < 1 ? 1 : (u > 8 ? 8 : u);
-}
+// Arcs whose gathers one warp keeps in flight together (U): 1, 2 or 4,
+// picked per operator by timing (tune_arcs_in_flight). The products are
+// added in arc order whatever U is, so the choice never changes a result.
+constexpr int U_CANDIDATES[] = {1, 2, 4};
 
 // The normalised teleport columns: dense node-major P[i * B + c], or, when
 // few entries are nonzero, each row's nonzero (column, value) pairs in
@@ -82,11 +80,10 @@ struct PersView {
 // Row sum of one row of A times Z for this lane's columns. U arcs at a
 // time: their indices, then all their gathers, then the products added in
 // arc order (so each column's sum keeps the order of a one-arc loop).
-template <class VT, class MT, int VW>
+template <class VT, class MT, int VW, int U>
 __device__ __forceinline__ void row_product(const OpView<MT>& op, const VT* __restrict__ Z,
                                             uint32_t B, uint32_t a0, uint32_t a1, int lane,
                                             VT (&acc)[VW]) {
-  constexpr int U = arcs_in_flight<VT, VW>();
 #pragma unroll
   for (int v = 0; v < VW; ++v) acc[v] = VT(0);
   uint32_t k = a0;
@@ -189,7 +186,7 @@ __device__ __forceinline__ void cta_column_sums(uint32_t B, double* __restrict__
   }
 }
 
-template <class VT, class MT, int VW>
+template <class VT, class MT, int VW, int U>
 __global__ void __launch_bounds__(BT)
 spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ ranges,
           uint32_t nranges, BatchScalars bs, const ColState* __restrict__ cs,
@@ -207,7 +204,7 @@ spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ 
       const uint32_t a0 = op.off[i], a1 = op.off[i + 1];
       if (a1 - a0 > LONG_ROW) continue;  // long rows: spmm_chunks / spmm_long
       VT acc[VW];
-      row_product<VT, MT, VW>(op, Z, bs.B, a0, a1, lane, acc);
+      row_product<VT, MT, VW, U>(op, Z, bs.B, a0, a1, lane, acc);
       row_update<VT, VW>(i, acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
     }
   }
@@ -215,7 +212,7 @@ spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ 
 }
 
 // Partial products of the chunks of long rows.
-template <class VT, class MT, int VW>
+template <class VT, class MT, int VW, int U>
 __global__ void __launch_bounds__(BT)
 spmm_chunks(OpView<MT> op, const VT* __restrict__ Z, const Chunk* __restrict__ chunks,
             uint32_t nchunks, uint32_t B, VT* __restrict__ scratch,
@@ -226,7 +223,7 @@ spmm_chunks(OpView<MT> op, const VT* __restrict__ Z, const Chunk* __restrict__ c
   for (uint32_t q = gw; q < nchunks; q += nw) {
     const Chunk ch = chunks[q];
     VT acc[VW];
-    row_product<VT, MT, VW>(op, Z, B, ch.a0, ch.a1, lane, acc);
+    row_product<VT, MT, VW, U>(op, Z, B, ch.a0, ch.a1, lane, acc);
 #pragma unroll
     for (int v = 0; v < VW; ++v) {
       const uint32_t c = lane + 32 * v;
@@ -498,17 +495,20 @@ static void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
   if (!h.empty()) KNB_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
-template <class VT, class MT, int VW>
+// One sweep: the row products and updates, then (finish) the per-column
+// sums, stopping rule and next sweep's scalars. Without finish the sweep
+// only rewrites Ynew, Znew, the chunk scratch and the partials.
+template <class VT, class MT, int VW, int U>
 static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uint32_t nranges,
                        const DevBuf<Chunk>& chunks, uint32_t nchunks, const DevBuf<uint32_t>& lrow,
                        const DevBuf<uint32_t>& lfirst, uint32_t nlong, const BatchScalars& bs,
                        ColState* cs, const VT* Yold, VT* Ynew, const VT* Zold, VT* Znew,
                        const VT* inv_out, const PersView& P, VT* scratch, double* part,
-                       int32_t* all_frozen, unsigned grid, cudaStream_t s) {
+                       int32_t* all_frozen, unsigned grid, bool finish, cudaStream_t s) {
   const size_t smem = (size_t)BW * 3 * bs.B * sizeof(double);
   static bool attr = false;
   if (!attr) {
-    KNB_CUDA(cudaFuncSetAttribute(spmm_rows<VT, MT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    KNB_CUDA(cudaFuncSetAttribute(spmm_rows<VT, MT, VW, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(BW * 3 * 256 * sizeof(double))));
     KNB_CUDA(cudaFuncSetAttribute(spmm_long<VT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(BW * 3 * 256 * sizeof(double))));
@@ -516,39 +516,81 @@ static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uin
   }
   int launches = 0;
   if (nchunks) {
-    spmm_chunks<VT, MT, VW><<<grid, BT, 0, s>>>(op, Zold, chunks.get(), nchunks, bs.B, scratch,
-                                                 all_frozen);
+    spmm_chunks<VT, MT, VW, U><<<grid, BT, 0, s>>>(op, Zold, chunks.get(), nchunks, bs.B, scratch,
+                                                    all_frozen);
     ++launches;
   }
-  spmm_rows<VT, MT, VW><<<grid, BT, smem, s>>>(op, Zold, ranges.get(), nranges, bs, cs, Yold, Ynew,
-                                               Znew, inv_out, P, part, all_frozen);
+  spmm_rows<VT, MT, VW, U><<<grid, BT, smem, s>>>(op, Zold, ranges.get(), nranges, bs, cs, Yold,
+                                                  Ynew, Znew, inv_out, P, part, all_frozen);
   spmm_long<VT, VW><<<grid, BT, smem, s>>>(lrow.get(), lfirst.get(), nlong, scratch, bs, cs, Yold,
                                            Ynew, Znew, inv_out, P, part + (size_t)grid * 3 * bs.B,
                                            all_frozen);
-  spmm_finish<<<1, 256, 0, s>>>(part, 2 * grid, bs, cs, all_frozen, 1);
+  if (finish) spmm_finish<<<1, 256, 0, s>>>(part, 2 * grid, bs, cs, all_frozen, 1);
   KNB_LAUNCH("batch sweep");
-  return launches + 3;
+  return launches + (finish ? 3 : 2);
 }
 
 template <class VT, class MT>
-static int batch_sweep_vw(int vw, const OpView<MT>& op, const DevBuf<RowRange>& ranges,
+static int batch_sweep_vw(int vw, int u, const OpView<MT>& op, const DevBuf<RowRange>& ranges,
                           uint32_t nranges, const DevBuf<Chunk>& chunks, uint32_t nchunks,
                           const DevBuf<uint32_t>& lrow, const DevBuf<uint32_t>& lfirst,
                           uint32_t nlong, const BatchScalars& bs, ColState* cs, const VT* Yold,
                           VT* Ynew, const VT* Zold, VT* Znew, const VT* inv_out, const PersView& P,
                           VT* scratch, double* part, int32_t* all_frozen, unsigned grid,
-                          cudaStream_t s) {
-#define KNB_SW(V)                                                                                 \
-  return batch_sweep<VT, MT, V>(op, ranges, nranges, chunks, nchunks, lrow, lfirst, nlong, bs, cs, \
-                                Yold, Ynew, Zold, Znew, inv_out, P, scratch, part, all_frozen,     \
-                                grid, s)
-  switch (vw) {
-    case 1: KNB_SW(1);
-    case 2: KNB_SW(2);
-    case 4: KNB_SW(4);
-    default: KNB_SW(8);
+                          cudaStream_t s, bool finish = true) {
+#define KNB_SW(V, UU)                                                                             \
+  return batch_sweep<VT, MT, V, UU>(op, ranges, nranges, chunks, nchunks, lrow, lfirst, nlong,    \
+                                    bs, cs, Yold, Ynew, Zold, Znew, inv_out, P, scratch, part,    \
+                                    all_frozen, grid, finish, s)
+#define KNB_SWU(V)                   \
+  switch (u) {                       \
+    case 1: KNB_SW(V, 1);            \
+    case 2: KNB_SW(V, 2);            \
+    default: KNB_SW(V, 4);           \
   }
+  switch (vw) {
+    case 1: KNB_SWU(1);
+    case 2: KNB_SWU(2);
+    case 4: KNB_SWU(4);
+    default: KNB_SWU(8);
+  }
+#undef KNB_SWU
 #undef KNB_SW
+}
+
+// Times one sweep of each arcs-in-flight candidate on the phase's starting
+// state (without the finish, so nothing but buffers the first real sweep
+// rewrites is touched) and returns the fastest.
+template <class VT, class MT>
+static int tune_arcs_in_flight(int vw, const OpView<MT>& op, const DevBuf<RowRange>& ranges,
+                               uint32_t nranges, const DevBuf<Chunk>& chunks, uint32_t nchunks,
+                               const DevBuf<uint32_t>& lrow, const DevBuf<uint32_t>& lfirst,
+                               uint32_t nlong, const BatchScalars& bs, ColState* cs,
+                               const VT* Yold, VT* Ynew, const VT* Zold, VT* Znew,
+                               const VT* inv_out, const PersView& P, VT* scratch, double* part,
+                               int32_t* all_frozen, unsigned grid, cudaStream_t s) {
+  cudaEvent_t e0, e1;
+  KNB_CUDA(cudaEventCreate(&e0));
+  KNB_CUDA(cudaEventCreate(&e1));
+  int best = U_CANDIDATES[0];
+  float best_ms = 0;
+  for (int u : U_CANDIDATES) {
+    KNB_CUDA(cudaEventRecord(e0, s));
+    batch_sweep_vw<VT, MT>(vw, u, op, ranges, nranges, chunks, nchunks, lrow, lfirst, nlong, bs,
+                           cs, Yold, Ynew, Zold, Znew, inv_out, P, scratch, part, all_frozen, grid,
+                           s, false);
+    KNB_CUDA(cudaEventRecord(e1, s));
+    KNB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    KNB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (u == U_CANDIDATES[0] || ms < best_ms) {
+      best = u;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
 }
 
 static int vw_for(uint32_t B) {
@@ -565,6 +607,16 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
   const int which = (g.directed && prm.directed) ? 1 : (g.directed ? 2 : 0);
   const double lfac = prm.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (prm.loops == 0 ? 2.0 : 1.0));
   Operator& op = g.op(which, prm.weighted, lfac, s);
+  // arcs in flight per (column width, value types), tuned on first use
+  auto tuned_u = [&](int key) {
+    std::lock_guard<std::mutex> lock(op.mu);
+    auto it = op.batch_u.find(key);
+    return it == op.batch_u.end() ? 0 : it->second;
+  };
+  auto keep_u = [&](int key, int u) {
+    std::lock_guard<std::mutex> lock(op.mu);
+    op.batch_u[key] = u;
+  };
   std::vector<uint32_t> hoff(n + 1);
   KNB_CUDA(cudaMemcpyAsync(hoff.data(), op.rows->off.get(), ((size_t)n + 1) * 4,
                            cudaMemcpyDeviceToHost, s));
@@ -658,12 +710,20 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       bs.tol = std::max(prm.tol * prm.switch_factor, prm.switch_floor);
       bs.max_iter = (int32_t)prm.max_iter;
       launches += 2;
+      int u32 = tuned_u(vw * 4 + 0);
+      if (!u32) {
+        u32 = tune_arcs_in_flight<float, float>(
+            vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
+            cs.get(), Y32[0].get(), Y32[1].get(), Z32[0].get(), Z32[1].get(), op.inv_out32.get(),
+            P, sc32.get(), part.get(), all_frozen.get(), grid, s);
+        keep_u(vw * 4 + 0, u32);
+      }
       int k = 0;
       for (;;) {
         const int b = k & 1;
         launches += batch_sweep_vw<float, float>(
-            vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
-            cs.get(), Y32[b].get(), Y32[1 - b].get(), Z32[b].get(), Z32[1 - b].get(),
+            vw, u32, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
+            bs, cs.get(), Y32[b].get(), Y32[1 - b].get(), Z32[b].get(), Z32[1 - b].get(),
             op.inv_out32.get(), P, sc32.get(), part.get(), all_frozen.get(), grid, s);
         ++k;
         if (k % 4 == 0) {
@@ -713,18 +773,32 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     bs.max_iter = (int32_t)(prm.max_iter - (mixed ? 0 : 0));
     sc64.alloc(std::max<size_t>((size_t)nchunks * B, 1));
     const bool use32v = op.has_vals && op.vals32_exact;
+    const int key64 = vw * 4 + (use32v ? 1 : 2);
+    int u64 = tuned_u(key64);
+    if (!u64) {
+      u64 = use32v
+                ? tune_arcs_in_flight<double, float>(
+                      vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst,
+                      nlong, bs, cs.get(), Y64[0].get(), Y64[1].get(), Z64[0].get(), Z64[1].get(),
+                      op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s)
+                : tune_arcs_in_flight<double, double>(
+                      vw, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst,
+                      nlong, bs, cs.get(), Y64[0].get(), Y64[1].get(), Z64[0].get(), Z64[1].get(),
+                      op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
+      keep_u(key64, u64);
+    }
     int k = 0;
     for (;;) {
       const int b = k & 1;
       if (use32v)
         launches += batch_sweep_vw<double, float>(
-            vw, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
-            cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
+            vw, u64, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
+            bs, cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
             op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
       else
         launches += batch_sweep_vw<double, double>(
-            vw, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong, bs,
-            cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
+            vw, u64, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
+            bs, cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
             op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
       ++k;
       if (k % 4 == 0) {

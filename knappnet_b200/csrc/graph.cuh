@@ -82,6 +82,7 @@ struct Operator {
   std::unique_ptr<Workspace> eig_ws;  // eigenvector centrality's (eigen.cu), created on first use
   std::unique_ptr<Workspace> hits_ws;  // hubs and authorities' (eigen.cu), created on first use
   std::unique_ptr<Workspace> series_ws;  // the Katz / Bonacich attenuation check's (katz.cu)
+  std::map<int, int> batch_u;  // batched PageRank's tuned arcs in flight (batch.cu), under mu
 
   const Relabeled& relabeled(cudaStream_t s);
   const Partition& relabeled_partition(uint32_t tile_items, cudaStream_t s);
