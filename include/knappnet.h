@@ -202,6 +202,7 @@ typedef struct NetBatchInfo {
   int64_t max_column_iterations;
   int32_t kernel_launches;
   int32_t reserved;
+  double sweep_seconds;          /* device time of the sweeps alone (no copies, set-up) */
 } NetBatchInfo;
 
 /* Personalised PageRank for `batch` teleport vectors at once (one sparse

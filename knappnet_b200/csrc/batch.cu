@@ -633,10 +633,20 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
                  nlong = (uint32_t)plan.lrow.size();
   const unsigned grid = 148 * 4;
 
-  cudaEvent_t t0, t1;
+  cudaEvent_t t0, t1, l0, l1;
   KNB_CUDA(cudaEventCreate(&t0));
   KNB_CUDA(cudaEventCreate(&t1));
+  KNB_CUDA(cudaEventCreate(&l0));
+  KNB_CUDA(cudaEventCreate(&l1));
   KNB_CUDA(cudaEventRecord(t0, s));
+  double sweep_ms = 0.0;  // device time of the sweep loops alone
+  auto loop_end = [&] {
+    KNB_CUDA(cudaEventRecord(l1, s));
+    KNB_CUDA(cudaEventSynchronize(l1));
+    float lm = 0;
+    KNB_CUDA(cudaEventElapsedTime(&lm, l0, l1));
+    sweep_ms += lm;
+  };
   int launches = 0;
   int64_t sweeps32 = 0, sweeps64 = 0;
   const bool mixed = prm.precision == PREC_MIXED;
@@ -719,6 +729,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
         keep_u(vw * 4 + 0, u32);
       }
       int k = 0;
+      KNB_CUDA(cudaEventRecord(l0, s));
       for (;;) {
         const int b = k & 1;
         launches += batch_sweep_vw<float, float>(
@@ -733,6 +744,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
           if (af) break;
         }
       }
+      loop_end();
       // every column's FP32 phase ended; hand over from its own buffer
       std::vector<ColState> h(B);
       KNB_CUDA(cudaMemcpyAsync(h.data(), cs.get(), B * sizeof(ColState), cudaMemcpyDeviceToHost, s));
@@ -788,6 +800,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       keep_u(key64, u64);
     }
     int k = 0;
+    KNB_CUDA(cudaEventRecord(l0, s));
     for (;;) {
       const int b = k & 1;
       if (use32v)
@@ -808,6 +821,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
         if (af) break;
       }
     }
+    loop_end();
     sweeps64 += k;
     std::vector<ColState> h(B);
     KNB_CUDA(cudaMemcpyAsync(h.data(), cs.get(), B * sizeof(ColState), cudaMemcpyDeviceToHost, s));
@@ -831,8 +845,11 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
   KNB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  cudaEventDestroy(l0);
+  cudaEventDestroy(l1);
   if (info) {
     info->seconds = ms * 1e-3;
+    info->sweep_seconds = sweep_ms * 1e-3;
     info->sweeps = sweeps32 + sweeps64;
     info->sweeps_fp32 = sweeps32;
     int64_t tot = 0, mx = 0;

@@ -27,6 +27,7 @@ struct BatchInfo {
   int64_t column_iterations = 0;    // sum over vectors of their own iteration counts
   int64_t max_column_iterations = 0;
   int kernel_launches = 0;
+  double sweep_seconds = 0;         // device time of the sweep loops alone
 };
 
 // personalization and out are column-major n x B (vector c at c * n).

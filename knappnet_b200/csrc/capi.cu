@@ -859,6 +859,7 @@ static int32_t batch_impl(const GraphHandle* h, double damping, int32_t directed
       info->column_iterations = bi.column_iterations;
       info->max_column_iterations = bi.max_column_iterations;
       info->kernel_launches = bi.kernel_launches;
+      info->sweep_seconds = bi.sweep_seconds;
     }
   });
 }
