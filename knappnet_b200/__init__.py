@@ -274,6 +274,8 @@ class Graph:
         P = np.ascontiguousarray(personalization, dtype=np.float64)
         if P.ndim != 2 or P.shape[1] != self.n:
             raise ValueError("personalization must have shape (batch, n)")
+        # written with zeros first: copying scores into untouched pages
+        # would fault them in during the device-to-host copy, which is slower
         out = np.zeros_like(P)
         info = NetBatchInfo()
         err = ctypes.create_string_buffer(ERR_LEN)

@@ -600,6 +600,29 @@ static int vw_for(uint32_t B) {
   return 8;
 }
 
+// What batched solves on one operator keep between calls: the row ranges
+// and chunks, and every buffer (grown when a call needs more, never shrunk;
+// freeing the tens of GB a large batch holds costs as much as a quarter of a
+// solve). A solve holds `mu` while it runs, so concurrent calls on one
+// operator take turns.
+struct BatchWorkspace : Workspace {
+  std::mutex mu;
+  bool planned = false;
+  uint32_t nranges = 0, nchunks = 0, nlong = 0;
+  DevBuf<RowRange> d_ranges;
+  DevBuf<Chunk> d_chunks;
+  DevBuf<uint32_t> d_lrow, d_lfirst, prow, pcols;
+  DevBuf<double> pin, dout, Pd, sums, pvals, part, Y64[2], Z64[2], sc64;
+  DevBuf<float> Y32[2], Z32[2], sc32;
+  DevBuf<ColState> cs;
+  DevBuf<int32_t> flags, all_frozen;
+};
+
+template <class T>
+static void grow(DevBuf<T>& b, size_t count) {
+  if (b.n < count) b.alloc(count);
+}
+
 void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pers_colmajor,
                     double* out_colmajor, BatchInfo* info, cudaStream_t s) {
   const uint32_t n = g.n;
@@ -617,20 +640,35 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     std::lock_guard<std::mutex> lock(op.mu);
     op.batch_u[key] = u;
   };
-  std::vector<uint32_t> hoff(n + 1);
-  KNB_CUDA(cudaMemcpyAsync(hoff.data(), op.rows->off.get(), ((size_t)n + 1) * 4,
-                           cudaMemcpyDeviceToHost, s));
-  KNB_CUDA(cudaStreamSynchronize(s));
-  BatchPlan plan = make_plan(hoff, n);
-  DevBuf<RowRange> d_ranges;
-  DevBuf<Chunk> d_chunks;
-  DevBuf<uint32_t> d_lrow, d_lfirst;
-  upload(d_ranges, plan.ranges, s);
-  upload(d_chunks, plan.chunks, s);
-  upload(d_lrow, plan.lrow, s);
-  upload(d_lfirst, plan.lfirst, s);
-  const uint32_t nranges = (uint32_t)plan.ranges.size(), nchunks = (uint32_t)plan.chunks.size(),
-                 nlong = (uint32_t)plan.lrow.size();
+  BatchWorkspace* wsp = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(op.mu);
+    if (!op.batch_ws) op.batch_ws = std::make_unique<BatchWorkspace>();
+    wsp = static_cast<BatchWorkspace*>(op.batch_ws.get());
+  }
+  BatchWorkspace& ws = *wsp;
+  std::lock_guard<std::mutex> ws_lock(ws.mu);
+  if (!ws.planned) {
+    std::vector<uint32_t> hoff(n + 1);
+    KNB_CUDA(cudaMemcpyAsync(hoff.data(), op.rows->off.get(), ((size_t)n + 1) * 4,
+                             cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    BatchPlan plan = make_plan(hoff, n);
+    upload(ws.d_ranges, plan.ranges, s);
+    upload(ws.d_chunks, plan.chunks, s);
+    upload(ws.d_lrow, plan.lrow, s);
+    upload(ws.d_lfirst, plan.lfirst, s);
+    ws.nranges = (uint32_t)plan.ranges.size();
+    ws.nchunks = (uint32_t)plan.chunks.size();
+    ws.nlong = (uint32_t)plan.lrow.size();
+    KNB_CUDA(cudaStreamSynchronize(s));
+    ws.planned = true;
+  }
+  const DevBuf<RowRange>& d_ranges = ws.d_ranges;
+  const DevBuf<Chunk>& d_chunks = ws.d_chunks;
+  const DevBuf<uint32_t>& d_lrow = ws.d_lrow;
+  const DevBuf<uint32_t>& d_lfirst = ws.d_lfirst;
+  const uint32_t nranges = ws.nranges, nchunks = ws.nchunks, nlong = ws.nlong;
   const unsigned grid = 148 * 4;
 
   cudaEvent_t t0, t1, l0, l1;
@@ -651,14 +689,14 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
   int64_t sweeps32 = 0, sweeps64 = 0;
   const bool mixed = prm.precision == PREC_MIXED;
   const uint32_t Btot = prm.B;
-  DevBuf<double> pin((size_t)n * Btot);
+  DevBuf<double>& pin = ws.pin;
+  grow(pin, (size_t)n * Btot);
   KNB_CUDA(cudaMemcpyAsync(pin.get(), pers_colmajor, (size_t)n * Btot * 8,
                            prm.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-  DevBuf<double> dout;
   double* outp = out_colmajor;
   if (!prm.on_device) {
-    dout.alloc((size_t)n * Btot);
-    outp = dout.get();
+    grow(ws.dout, (size_t)n * Btot);
+    outp = ws.dout.get();
   }
   std::vector<int32_t> col_iters(Btot, 0);
   std::vector<uint8_t> col_conv(Btot, 0);
@@ -666,9 +704,15 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
   for (uint32_t c0 = 0; c0 < Btot; c0 += 256) {
     const uint32_t B = std::min<uint32_t>(256, Btot - c0);
     const int vw = vw_for(B);
-    DevBuf<double> Pd, sums(B), pvals;
-    DevBuf<uint32_t> prow((size_t)n + 1), pcols;
-    DevBuf<int32_t> flags(2);
+    DevBuf<double>& Pd = ws.Pd;
+    DevBuf<double>& sums = ws.sums;
+    DevBuf<double>& pvals = ws.pvals;
+    DevBuf<uint32_t>& prow = ws.prow;
+    DevBuf<uint32_t>& pcols = ws.pcols;
+    DevBuf<int32_t>& flags = ws.flags;
+    grow(sums, B);
+    grow(prow, (size_t)n + 1);
+    grow(flags, 2);
     KNB_CUDA(cudaMemsetAsync(flags.get(), 0, 8, s));
     pers_columns<<<grid_for(B, BW, 1184), BT, 0, s>>>(pin.get() + (size_t)c0 * n, n, B, nullptr,
                                                       flags.get(), sums.get());
@@ -685,13 +729,13 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     const uint32_t pnnz = exclusive_scan<uint32_t>(prow.get(), prow.get(), (size_t)n + 1, s);
     PersView P{nullptr, nullptr, nullptr, nullptr};
     if ((uint64_t)pnnz * 16 <= (uint64_t)n * B) {
-      pcols.alloc(std::max<uint32_t>(pnnz, 1));
-      pvals.alloc(std::max<uint32_t>(pnnz, 1));
+      grow(pcols, std::max<uint32_t>(pnnz, 1));
+      grow(pvals, std::max<uint32_t>(pnnz, 1));
       pers_row_fill<<<grid_for(n, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n, sums.get(), n, B,
                                                      prow.get(), pcols.get(), pvals.get());
       P = PersView{nullptr, prow.get(), pcols.get(), pvals.get()};
     } else {
-      Pd.alloc((size_t)n * B);
+      grow(Pd, (size_t)n * B);
       pers_scatter<<<grid_for((uint64_t)n * B, 256), 256, 0, s>>>(pin.get() + (size_t)c0 * n,
                                                                    sums.get(), n, B, Pd.get());
       P = PersView{Pd.get(), nullptr, nullptr, nullptr};
@@ -699,20 +743,27 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     KNB_LAUNCH("teleport columns");
     launches += 4;
     BatchScalars bs{prm.damping, 1.0 / n, n, B, prm.dangling == 1 ? 1 : 0, 0.0, 0, 0};
-    DevBuf<ColState> cs(B);
-    DevBuf<int32_t> all_frozen(1);
-    DevBuf<double> part(std::max<size_t>((size_t)2 * grid * 3 * B, (size_t)1184 * 2 * B));
+    DevBuf<ColState>& cs = ws.cs;
+    DevBuf<int32_t>& all_frozen = ws.all_frozen;
+    DevBuf<double>& part = ws.part;
+    grow(cs, B);
+    grow(all_frozen, 1);
+    grow(part, std::max<size_t>((size_t)2 * grid * 3 * B, (size_t)1184 * 2 * B));
     const double dterm0 = (double)op.n_dangling / (double)n;
     int64_t done32 = 0;
     const size_t nb = (size_t)n * B;
-    DevBuf<float> Y32[2], Z32[2], sc32;
-    DevBuf<double> Y64[2], Z64[2], sc64;
+    DevBuf<float>(&Y32)[2] = ws.Y32;
+    DevBuf<float>(&Z32)[2] = ws.Z32;
+    DevBuf<float>& sc32 = ws.sc32;
+    DevBuf<double>(&Y64)[2] = ws.Y64;
+    DevBuf<double>(&Z64)[2] = ws.Z64;
+    DevBuf<double>& sc64 = ws.sc64;
     if (mixed) {
       for (int k = 0; k < 2; ++k) {
-        Y32[k].alloc(nb);
-        Z32[k].alloc(nb);
+        grow(Y32[k], nb);
+        grow(Z32[k], nb);
       }
-      sc32.alloc(std::max<size_t>((size_t)nchunks * B, 1));
+      grow(sc32, std::max<size_t>((size_t)nchunks * B, 1));
       spmm_init<float><<<grid_for(nb, 256), 256, 0, s>>>(Y32[0].get(), Z32[0].get(),
                                                           op.inv_out32.get(), n, B, nullptr);
       spmm_set_state<<<1, 256, 0, s>>>(cs.get(), B, dterm0, 0);
@@ -758,8 +809,8 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       sweeps32 += k;
       // columns stopped at different sweeps: each is read from its own buffer
       for (int kk = 0; kk < 2; ++kk) {
-        Y64[kk].alloc(nb);
-        Z64[kk].alloc(nb);
+        grow(Y64[kk], nb);
+        grow(Z64[kk], nb);
       }
       spmm_switch<<<grid_for(nb, 256), 256, 0, s>>>(Y32[0].get(), Y32[1].get(), cs.get(),
                                                     Y64[0].get(), Z64[0].get(),
@@ -771,8 +822,8 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       for (uint32_t c = 0; c < B; ++c) col_iters[c0 + c] = h[c].iter;
     } else {
       for (int kk = 0; kk < 2; ++kk) {
-        Y64[kk].alloc(nb);
-        Z64[kk].alloc(nb);
+        grow(Y64[kk], nb);
+        grow(Z64[kk], nb);
       }
       spmm_init<double><<<grid_for(nb, 256), 256, 0, s>>>(Y64[0].get(), Z64[0].get(),
                                                            op.inv_out64.get(), n, B, nullptr);
@@ -783,7 +834,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     KNB_CUDA(cudaMemsetAsync(all_frozen.get(), 0, 4, s));
     bs.tol = prm.tol;
     bs.max_iter = (int32_t)(prm.max_iter - (mixed ? 0 : 0));
-    sc64.alloc(std::max<size_t>((size_t)nchunks * B, 1));
+    grow(sc64, std::max<size_t>((size_t)nchunks * B, 1));
     const bool use32v = op.has_vals && op.vals32_exact;
     const int key64 = vw * 4 + (use32v ? 1 : 2);
     int u64 = tuned_u(key64);
