@@ -340,7 +340,8 @@ NET_API void net_set_sweep_timing(int32_t on);
  * CTA, 2-5 one tile per warp, 6 and 7 persistent warp tiles with the most
  * gathered nodes in shared memory, 32 or 16 warps per SM, 8 warp tiles whose
  * gathers allocate in L1 only for the most gathered columns); 5 = preferred
- * shared-memory carveout of the sweep (-1 driver default, 0..100 percent);
+ * shared-memory carveout of the sweep (-1 just what the CTAs the kernel keeps
+ * resident need, 0..100 percent);
  * 6 = threads per CTA of the packed-graph PageRank (0 tuned on first use,
  * 128, 256, 512, 1024); 7 = the most nodes kernels 6 and 7 keep in shared
  * memory (-1 as many as fit, 0 none), or the columns below which kernel 8

@@ -45,7 +45,7 @@ struct Tuning {
   int ipt = 0;            // merge-path items per thread: 4, 8 or 16
   int relabel = 1;        // 1: sweep on the operator renumbered by column count
   int variant = 0;        // sweep kernel: 1 CTA tiles, 2-5 warp tiles (see pagerank.cu)
-  int carveout = -1;      // preferred shared-memory carveout percent (-1: driver default)
+  int carveout = -1;      // preferred shared-memory carveout percent (-1: what the resident CTAs need)
   int64_t hot_nodes = -1; // hot-node sweeps: cap on the nodes kept in shared memory (-1: none)
   int persistent = 1;     // warp-tile sweeps: 1 launches only the CTAs that fit at once
   int refine = 1;         // mixed: 1 anchor + refinement sweeps, 0 plain FP64 sweeps
