@@ -199,6 +199,8 @@ void pagerank_grad(GraphHandleImpl& g, const double* d_w, const double* d_x, con
   const OpView<double> v = tr->view64();
   IterState h{};
   int k = 0;
+  fit_warp_carveout<double, double, AdjointEpi, IPT, WPB>();
+  fit_warp_carveout<double, double, RowSumEpi, IPT, WPB>();
   for (;;) {
     for (int b = 0; b < 8; ++b, ++k) {
       AdjointEpi e;

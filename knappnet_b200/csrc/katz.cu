@@ -383,6 +383,7 @@ void sweep(const OpView<double>& v, const Partition& P, const double* x, const E
            cudaStream_t s) {
   constexpr size_t smem = warp_smem_bytes<double, K_IPT, K_WPB>();
   const unsigned grid = (P.ntiles + K_WPB - 1) / K_WPB;
+  fit_warp_carveout<double, double, Epi, K_IPT, K_WPB>();
   warp_spmv<double, double, Epi, K_IPT, K_WPB><<<grid, K_WPB * 32, smem, s>>>(
       v, x, e, P.coords.get(), P.ntiles, carry, head, part1, st, 0xFFFFFFFFu);
   KNB_LAUNCH("series sweep");
