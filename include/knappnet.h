@@ -1,26 +1,32 @@
 /*
- * C interface of the knappnet B200 library: the spectral-centrality path
- * (graph build, degree, PageRank, eigenvector centrality) of the reference
- * engine's C ABI, computed on an NVIDIA B200 (sm_100a), plus additive
- * extensions.
+ * C interface of the knappnet B200 library: the reference engine's
+ * spectral-centrality entry points (graph build, degree, PageRank,
+ * eigenvector centrality and the measures built on the same products),
+ * computed on an NVIDIA B200 (sm_100a), plus additive extensions. The
+ * reference entry points keep the signatures and codes of
+ * crates/capi/include/netcapi.h, so a program built against that header
+ * links against this library unchanged.
  *
- * Conventions (as the reference's crates/capi/include/netcapi.h:1-25):
- * - Functions that take `err` return 0 on success and non-zero on failure,
- *   after writing a NUL-terminated message into `err` (at most `err_len`
- *   bytes). Accessors that return a count give -1 for a NULL handle.
- * - Node indices are 0-based. Output buffers are allocated by the caller; a
- *   node-aligned result holds n doubles.
- * - A handle belongs to the caller until released with net_graph_free,
- *   which accepts NULL. Handles are immutable: concurrent calls on one
- *   handle are safe.
- * - Codes: mode 1 = out, 2 = in, 3 = all; loops 0 = an undirected self-loop
- *   counts twice (igraph), 1 = once (NetworkX), 2 = not at all; dangling
- *   0 = jump by the personalization vector, 1 = jump uniformly; scale 0 =
- *   largest score 1, 1 = unit Euclidean norm. tol <= 0 and max_iter <= 0
- *   select the defaults (1e-12 and 10000). `threads` is accepted for
- *   compatibility; results never depend on it.
- * - The graph lives in GPU memory (the current CUDA device when it is
- *   built). Functions with `_device` in their name take device pointers.
+ * How every function behaves:
+ * - A function with an `err` buffer returns 0 when it succeeds. On failure
+ *   it returns a non-zero status and leaves a message in `err`, cut to
+ *   `err_len` bytes and NUL-terminated. Count accessors answer -1 when
+ *   given a NULL handle.
+ * - Nodes are numbered from 0. The caller owns every output buffer; a
+ *   per-node result needs room for n doubles.
+ * - The caller owns a handle until it passes it to net_graph_free (NULL is
+ *   ignored there). A handle never changes after it is built, so threads
+ *   may share it.
+ * - Codes: mode 1 follows arcs out of a node, 2 into it, 3 both ways;
+ *   loops 0 counts an undirected self-loop twice (as igraph), 1 once (as
+ *   NetworkX), 2 not at all; dangling 0 sends the mass of nodes without
+ *   out-arcs along the personalization vector, 1 spreads it uniformly;
+ *   scale 0 makes the largest score 1, 1 gives unit Euclidean length. A
+ *   tolerance or iteration cap that is not positive means the default
+ *   (1e-12, 10000). `threads` is accepted and ignored: no result depends
+ *   on it.
+ * - A graph is stored in the memory of the CUDA device that is current
+ *   when it is built. Functions named `_device` take device pointers.
  */
 #ifndef KNAPPNET_H
 #define KNAPPNET_H
@@ -42,28 +48,34 @@ typedef struct GraphHandle GraphHandle;
 
 /* ---- Reference entry points ------------------------------------------- */
 
-/* Builds a graph from m edges on n nodes; weights may be NULL; directed != 0
- * keeps arc directions. Replaces netcapi.h:46-48 (crates/capi/src/lib.rs:139-164). */
+/* Makes a handle for a graph of n nodes and m edges src[k] -> tgt[k], with
+ * one weight per edge or none (weights NULL). With directed == 0 every edge
+ * is stored both ways. Replaces netcapi.h:46-48 (crates/capi/src/lib.rs:139-164). */
 NET_API int32_t net_graph_new(int64_t n, const int64_t *src, const int64_t *tgt,
                       const double *weights, int64_t m, int32_t directed,
                       GraphHandle **out, char *err, size_t err_len);
 
-/* Releases a graph (NULL is allowed). Replaces netcapi.h:51 (lib.rs:171-175). */
+/* Frees a handle and the device memory behind it; NULL does nothing.
+ * Replaces netcapi.h:51 (lib.rs:171-175). */
 NET_API void net_graph_free(GraphHandle *h);
 
-/* Number of nodes, or -1 for NULL. Replaces netcapi.h:54 (lib.rs:182-184). */
+/* n of the handle; -1 when h is NULL. Replaces netcapi.h:54 (lib.rs:182-184). */
 NET_API int64_t net_graph_node_count(const GraphHandle *h);
 
-/* Edges as supplied, or -1 for NULL. Replaces netcapi.h:57. */
+/* m as given to net_graph_new, repeated edges and self-loops included; -1
+ * when h is NULL. Replaces netcapi.h:57. */
 NET_API int64_t net_graph_edge_count(const GraphHandle *h);
 
-/* Degree (weighted == 0) or strength; out holds n doubles. Replaces
+/* Per-node count of the arcs that mode selects, or the sum of their
+ * weights when weighted != 0; n doubles to out. Replaces
  * netcapi.h:383-384 (lib.rs:192-212). */
 NET_API int32_t net_degree(const GraphHandle *h, int32_t mode, int32_t loops,
                    int32_t weighted, double *out, char *err, size_t err_len);
 
-/* PageRank; out holds n doubles summing to 1. personalization is NULL
- * (uniform) or n nonnegative values. directed == 0 ignores directions.
+/* Stationary distribution of the damped random walk: n scores adding up
+ * to 1 go to out. The teleport vector is uniform when personalization is
+ * NULL, else n values that must not be negative (rescaled to sum 1). With
+ * directed == 0 each arc is walked both ways.
  * Replaces netcapi.h:463-467 (crates/capi/src/spectral.rs:59-97). */
 NET_API int32_t net_pagerank(const GraphHandle *h, double damping, int32_t directed,
                      int32_t weighted, const double *personalization,
@@ -71,47 +83,52 @@ NET_API int32_t net_pagerank(const GraphHandle *h, double damping, int32_t direc
                      int64_t max_iter, int32_t threads, double *out,
                      char *err, size_t err_len);
 
-/* Katz centrality x = alpha A' x + beta; beta holds 1 or n values; an alpha
- * not below 1 / lambda_max is an error; normalized != 0 scales to unit
- * Euclidean norm; mode 1 out, 2 in, 3 all. Replaces netcapi.h:472-476
+/* Katz scores: the solution x of x = alpha A' x + beta, with beta one value
+ * shared by all nodes or one per node. The call fails when alpha reaches
+ * 1 / lambda_max, where the series no longer converges; normalized != 0
+ * rescales x to Euclidean length 1. Replaces netcapi.h:472-476
  * (crates/capi/src/spectral.rs:107-140). */
 NET_API int32_t net_katz(const GraphHandle *h, double alpha, const double *beta,
                          int64_t beta_len, int32_t mode, int32_t weighted, int32_t loops,
                          int32_t normalized, double tol, int64_t max_iter, int32_t threads,
                          double *out, char *err, size_t err_len);
 
-/* Bonacich power centrality (I - exponent A)^-1 A 1, scaled so the squares
- * sum to n, or (rescale != 0) so the scores sum to 1; when |exponent|
- * lambda_max >= 1 a dense solve (at most 5,000 nodes); a singular system is
- * an error. Replaces netcapi.h:481-486 (crates/capi/src/spectral.rs:149-179). */
+/* Bonacich's power centrality c = (I - exponent A)^-1 A 1, rescaled to a sum
+ * of squares n, or to a sum of 1 when rescale != 0. When the series would
+ * not converge (|exponent| lambda_max >= 1) the system is solved densely,
+ * for at most 5,000 nodes; a singular system fails the call.
+ * Replaces netcapi.h:481-486 (crates/capi/src/spectral.rs:149-179). */
 NET_API int32_t net_bonacich_power(const GraphHandle *h, double exponent, int32_t mode,
                                    int32_t weighted, int32_t loops, int32_t rescale,
                                    double tol, int64_t max_iter, int32_t threads,
                                    double *out, char *err, size_t err_len);
 
-/* Hub and authority scores (n doubles each); *value receives the largest
- * eigenvalue of A^T A, *unique 1 if the leading singular value is simple;
- * scale 0 largest 1, 1 sum 1, 2 unit norm. Replaces netcapi.h:489-493
+/* Kleinberg's hubs and authorities: n hub scores and n authority scores.
+ * *value gets the leading eigenvalue of A^T A and *unique is 1 when the top
+ * singular value has multiplicity one; scale 0 makes the largest score 1,
+ * 1 the sum 1, 2 the Euclidean length 1. Replaces netcapi.h:489-493
  * (crates/capi/src/spectral.rs:189-230). */
 NET_API int32_t net_hits(const GraphHandle *h, int32_t weighted, int32_t loops, int32_t scale,
                          double tol, int64_t max_iter, int32_t threads, double *hubs,
                          double *authorities, double *value, int32_t *unique, char *err,
                          size_t err_len);
 
-/* Eigenvector centrality; out holds n doubles; *eigenvalue receives the
- * principal eigenvalue and *connected 1 if the graph is (strongly)
- * connected. Replaces netcapi.h:455-459 (crates/capi/src/topography.rs:208-249). */
+/* The leading eigenvector of the adjacency matrix in the direction mode
+ * picks, as n scores; *eigenvalue gets its eigenvalue and *connected is 1
+ * when the graph is connected (strongly, for directed graphs).
+ * Replaces netcapi.h:455-459 (crates/capi/src/topography.rs:208-249). */
 NET_API int32_t net_eigenvector(const GraphHandle *h, int32_t mode, int32_t weighted,
                         int32_t scale, int32_t loops, double tol,
                         int64_t max_iter, int32_t threads, double *out,
                         double *eigenvalue, int32_t *connected, char *err,
                         size_t err_len);
 
-/* The adjacency-matrix reading of a graph (sna, UCINET): parallel edges
- * collapse, keeping the largest (keep 0) or smallest (keep 1) weight, and
- * self-loops are dropped; undirected != 0 also symmetrizes a directed
- * graph. Edges come out sorted by (from, to). Release *out with
- * net_graph_free. Replaces netcapi.h:59-65 (crates/capi/src/topography.rs:42-56). */
+/* The graph as sna and UCINET read it, an adjacency matrix: one edge per
+ * pair of nodes, carrying the largest weight of its parallel edges (keep 0)
+ * or the smallest (keep 1), and no self-loops; undirected != 0 also merges
+ * the two directions of a directed graph. The new handle lists its edges in
+ * (from, to) order; free it with net_graph_free.
+ * Replaces netcapi.h:59-65 (crates/capi/src/topography.rs:42-56). */
 NET_API int32_t net_graph_simplify(const GraphHandle *h, int32_t undirected, int32_t keep,
                                    GraphHandle **out, char *err, size_t err_len);
 
@@ -135,10 +152,11 @@ NET_API int32_t net_twomode_eigenvector(const GraphHandle *h, const int32_t *typ
 NET_API int32_t net_leading_eigen(const GraphHandle *h, int32_t weighted, int64_t *membership,
                                   double *q, int64_t *splits, char *err, size_t err_len);
 
-/* Weak (kind 0) or strong (kind 1) components: membership receives n
- * labels, numbered from 0 in order of each component's lowest-numbered
- * node, count one value; strong components of an undirected graph are its
- * weak ones. Replaces netcapi.h:517-520 (crates/capi/src/topography.rs:85-106). */
+/* Component of every node, weak (kind 0) or strong (kind 1), as n labels in
+ * membership; labels count up from 0 in the order of each component's
+ * smallest node, and *count gets the number of components. An undirected
+ * graph's strong components are its weak ones.
+ * Replaces netcapi.h:517-520 (crates/capi/src/topography.rs:85-106). */
 NET_API int32_t net_components(const GraphHandle *h, int32_t kind, int32_t *membership,
                                int64_t *count, char *err, size_t err_len);
 
@@ -362,10 +380,16 @@ NET_API int32_t net_set_tuning(int32_t key, double value);
  * stall the device, which cudaMalloc and cudaFree may do): its scratch is a
  * static device array of the library holding graphs of up to 262,144 (2^18)
  * nodes (8 MiB, held on every device that loads the library); larger graphs
- * are rejected with an error. The first call on a device looks up that
- * array's address, so it should come before any stream capture. All calls
- * share the array: calls that overlap on the GPU race and must be
- * serialized by the caller. No counterpart in the reference. */
+ * are rejected with an error. The kernel checks the arrays before it uses
+ * them: offsets that decrease, a source outside [0, n) or a weight that is
+ * negative or not finite fail the call with a message naming the first such
+ * row or arc. Out-strengths are summed in a fixed order, so repeated calls
+ * give identical scores. A tolerance or iteration cap that is not positive
+ * (a NaN tolerance included) selects the defaults 1e-12 and 10000, as in
+ * net_pagerank. The first call on a device looks up the array's address,
+ * so it should come before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race and must be serialized by the caller.
+ * No counterpart in the reference. */
 NET_API int32_t net_pagerank_csr_static(int64_t n, const uint32_t *d_offsets,
                                 const uint32_t *d_sources,
                                 const double *d_weights, double damping,

@@ -506,14 +506,10 @@ static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uin
                        const VT* inv_out, const PersView& P, VT* scratch, double* part,
                        int32_t* all_frozen, unsigned grid, bool finish, cudaStream_t s) {
   const size_t smem = (size_t)BW * 3 * bs.B * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    KNB_CUDA(cudaFuncSetAttribute(spmm_rows<VT, MT, VW, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(BW * 3 * 256 * sizeof(double))));
-    KNB_CUDA(cudaFuncSetAttribute(spmm_long<VT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(BW * 3 * 256 * sizeof(double))));
-    attr = true;
-  }
+  set_func_attr((const void*)spmm_rows<VT, MT, VW, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int)(BW * 3 * 256 * sizeof(double)));
+  set_func_attr((const void*)spmm_long<VT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int)(BW * 3 * 256 * sizeof(double)));
   int launches = 0;
   if (nchunks) {
     spmm_chunks<VT, MT, VW, U><<<grid, BT, 0, s>>>(op, Zold, chunks.get(), nchunks, bs.B, scratch,

@@ -66,6 +66,12 @@ std::string fmt_g(double v) {
   return b;
 }
 
+// The tolerance a call runs with: the given value when it is positive, else
+// the default 1e-12. NaN is not positive, so it also selects the default,
+// as in the reference's wrappers (crates/capi/src/spectral.rs:36-42,
+// crates/capi/src/topography.rs:232).
+double tolerance(double tol) { return tol > 0 ? tol : 1e-12; }
+
 // ---------------------------------------------------------------- device checks
 // First invalid endpoint, as 2 * edge + (0 for source, 1 for target), so the
 // smallest value names the edge and endpoint the reference reports first
@@ -353,10 +359,9 @@ static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t direc
     p.weighted = weighted != 0;
     p.dangling = dangling;
     p.loops = loops;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
     p.precision = precision;
-    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
     if (!(damping >= 0.0 && damping <= 1.0))
       throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
     if (g.n == 0) return;
@@ -424,10 +429,9 @@ static int32_t eigen_impl(const GraphHandle* h, int32_t mode, int32_t weighted, 
     p.weighted = weighted != 0;
     p.scale = scale;
     p.loops = loops;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
     p.precision = precision;
-    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
     cudaStream_t s = knb::thread_stream();
     if (g.n > 0 && p.weighted) check_nonnegative(g, "eigenvector centrality", s);
     knb::EigenResult r;
@@ -468,9 +472,8 @@ int32_t net_katz(const GraphHandle* h, double alpha, const double* beta, int64_t
     p.mode = mode;
     p.weighted = weighted != 0;
     p.loops = loops;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
-    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
     if (!std::isfinite(alpha) || alpha < 0.0)
       throw Error("alpha is " + fmt_g(alpha) +
                   "; it must be a nonnegative number below 1 / lambda_max");
@@ -502,9 +505,8 @@ int32_t net_bonacich_power(const GraphHandle* h, double exponent, int32_t mode, 
     p.mode = mode;
     p.weighted = weighted != 0;
     p.loops = loops;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
-    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
     if (!std::isfinite(exponent)) throw Error("the exponent must be finite");
     if (g.n == 0) return;
     cudaStream_t s = knb::thread_stream();
@@ -528,9 +530,8 @@ int32_t net_hits(const GraphHandle* h, int32_t weighted, int32_t loops, int32_t 
     p.weighted = weighted != 0;
     p.loops = loops;
     p.scale = scale;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
-    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
     cudaStream_t s = knb::thread_stream();
     if (p.weighted) check_nonnegative(g, "hub and authority scores", s);
     double v = 0.0;
@@ -625,7 +626,7 @@ int32_t net_twomode_eigenvector(const GraphHandle* h, const int32_t* types, doub
                     "; use 0 for the first mode and 1 for the second");
       t[v] = (uint8_t)types[v];
     }
-    const double tl = tol > 0 ? tol : 1e-12;
+    const double tl = tolerance(tol);
     const int64_t mi = max_iter > 0 ? max_iter : 10000;
     cudaStream_t s = knb::thread_stream();
     if (g.m) {
@@ -835,7 +836,7 @@ static int32_t batch_impl(const GraphHandle* h, double damping, int32_t directed
     p.weighted = weighted != 0;
     p.dangling = dangling;
     p.loops = loops;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
     p.precision = precision;
     p.B = (uint32_t)batch;
@@ -843,7 +844,6 @@ static int32_t batch_impl(const GraphHandle* h, double damping, int32_t directed
     const knb::Tuning& tu = knb::tuning();
     p.switch_factor = tu.switch_factor;
     p.switch_floor = tu.switch_floor;
-    if (std::isnan(p.tol)) throw Error("the tolerance and the iteration cap must be positive");
     if (!(damping >= 0.0 && damping <= 1.0))
       throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
     if (g.n == 0 || batch == 0) return;
@@ -902,11 +902,10 @@ int32_t net_pagerank_graphs(const GraphHandle* h, int64_t count, const int64_t* 
     in.weighted = weighted != 0;
     in.dangling = dangling;
     in.loops = loops;
-    in.tol = tol > 0 ? tol : 1e-12;
+    in.tol = tolerance(tol);
     in.max_iter = max_iter > 0 ? max_iter : 10000;
     in.personalization = personalization;
     in.iterations_out = iterations;
-    if (std::isnan(in.tol)) throw Error("the tolerance and the iteration cap must be positive");
     if (!(damping >= 0.0 && damping <= 1.0))
       throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
     if (g.n == 0) return;
@@ -990,7 +989,7 @@ int32_t net_pagerank_weights_device(const GraphHandle* h, const double* d_weight
     p.pers_on_device = true;
     p.dangling = dangling;
     p.loops = loops;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
     p.precision = precision;
     knb::PagerankInfo pi;
@@ -1030,7 +1029,7 @@ int32_t net_pagerank_grad_device(const GraphHandle* h, const double* d_weights,
     p.dangling = dangling;
     p.loops = loops;
     p.personalization = d_personalization;
-    p.tol = tol > 0 ? tol : 1e-12;
+    p.tol = tolerance(tol);
     p.max_iter = max_iter > 0 ? max_iter : 10000;
     knb::AdjointInfo ai;
     knb::pagerank_grad(g, d_weights, d_scores, d_grad_scores, p, d_grad_weights, d_lambda, &ai, s);

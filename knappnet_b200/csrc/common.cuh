@@ -4,8 +4,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <type_traits>
 
 namespace knb {
@@ -179,6 +182,23 @@ __device__ __forceinline__ T block_max(T v, T* scratch) {
 }
 
 // ---------------------------------------------------------------- launch helpers
+// Sets a kernel attribute on the current device unless this process already
+// set it to the same value there: cudaFuncSetAttribute acts on the current
+// device only, and graph handles may live on any device, so the record is
+// kept per (kernel, device, attribute), under a lock shared by all threads.
+inline void set_func_attr(const void* fn, cudaFuncAttribute attr, int value) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, int>, int> applied;
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(fn, dev, (int)attr);
+  auto it = applied.find(key);
+  if (it != applied.end() && it->second == value) return;
+  cuda_check(cudaFuncSetAttribute(fn, attr, value), "cudaFuncSetAttribute");
+  applied[key] = value;
+}
+
 inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap = 148u * 32u) {
   uint64_t g = (work + block - 1) / block;
   if (g < 1) g = 1;

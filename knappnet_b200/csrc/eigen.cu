@@ -19,7 +19,9 @@
 // - Components: weak components by a concurrent union-find on the device
 //   whose roots are the smallest node of each component, relabelled in order
 //   of their smallest node (topography.rs:183-246); strong components (for
-//   directed matrices) by Tarjan's algorithm on the host (topography.rs:248-305).
+//   directed matrices) also on the device, by rounds of trimming, max-colour
+//   propagation and backward propagation from each colour's root, labelled
+//   in the order of Tarjan's first appearance (topography.rs:248-305).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>

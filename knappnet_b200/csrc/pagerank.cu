@@ -540,38 +540,25 @@ static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>
         part1, st);
   } else if constexpr (VAR == VAR_CTA) {
     constexpr size_t smem = tile_smem_bytes<VT, IPT>();
-    static bool attr_set = false;
-    if (!attr_set) {
-      KNB_CUDA(cudaFuncSetAttribute(tile_spmv<VT, MT, Epi, IPT>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr_set = true;
-    }
+    set_func_attr((const void*)tile_spmv<VT, MT, Epi, IPT>,
+                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     tile_spmv<VT, MT, Epi, IPT><<<P.ntiles, SPMV_THREADS, smem, s>>>(
         v, x, e, P.coords.get(), carry, head, part1, st);
   } else {
     constexpr int WPB = VAR == VAR_WARP4 ? 4 : (VAR == VAR_WARP16 || VAR == VAR_WARPL1) ? 16 : 8;
     constexpr int GNA = VAR == VAR_WARPNA ? 1 : VAR == VAR_WARPL1 ? 2 : 0;
     constexpr size_t smem = warp_smem_bytes<VT, IPT, WPB>();
-    static bool attr_set = false;
-    static int carve = -2;
     auto fnp = warp_spmv<VT, MT, Epi, IPT, WPB, GNA>;
-    if (!attr_set) {
-      KNB_CUDA(cudaFuncSetAttribute(fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr_set = true;
-    }
+    set_func_attr((const void*)fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // Shared-memory carveout: by default just enough for the CTAs the kernel
     // is built to keep resident (each with its dynamic shared memory and the
     // 1 KB the driver reserves), as a percentage of the 228 KB an SM has; the
     // driver rounds the hint up to the next configuration it supports, and
     // the rest of the SM's 256 KB stays L1. Left to itself the driver picks a
     // larger configuration (132 KB for the FP32 sweep's 78 KB), 2-3% slower.
-    if (tuning().carveout != carve) {
-      carve = tuning().carveout;
-      constexpr int resident = warp_min_blocks<VT, IPT, WPB>();
-      const int fit = (int)((resident * (smem + 1024) * 100 + 233471) / 233472) + 1;
-      KNB_CUDA(cudaFuncSetAttribute(fnp, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    carve >= 0 ? carve : std::min(fit, 100)));
-    }
+    const int carve =
+        tuning().carveout >= 0 ? tuning().carveout : warp_fit_carveout<VT, IPT, WPB>();
+    set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     unsigned grid = (P.ntiles + WPB - 1) / WPB;
     if (tuning().persistent) {
       // the CTAs that fit on the GPU at once, each warp looping over tiles

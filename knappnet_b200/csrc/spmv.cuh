@@ -581,23 +581,24 @@ constexpr size_t warp_smem_bytes() {
   return sizeof(WarpSmem<VT, IPT>) * WPB;
 }
 
-// Asks, once per process, for a shared-memory carveout of just what the
-// warp-tile kernel's resident CTAs need (their dynamic shared memory and the
-// 1 KB per CTA the driver reserves, as a percentage of an SM's 228 KB); the
-// driver rounds the hint up to the next configuration it supports and the
-// rest of the SM's 256 KB stays L1.
+// Asks for a shared-memory carveout of just what the warp-tile kernel's
+// resident CTAs need (their dynamic shared memory and the 1 KB per CTA the
+// driver reserves, as a percentage of an SM's 228 KB); the driver rounds the
+// hint up to the next configuration it supports and the rest of the SM's
+// 256 KB stays L1. Applied once per device.
+template <class VT, int IPT, int WPB>
+constexpr int warp_fit_carveout() {
+  constexpr size_t smem = warp_smem_bytes<VT, IPT, WPB>();
+  constexpr int resident = warp_min_blocks<VT, IPT, WPB>();
+  constexpr int pct = (int)((resident * (smem + 1024) * 100 + 233471) / 233472) + 1;
+  return pct < 100 ? pct : 100;
+}
+
 template <class VT, class MT, class Epi, int IPT, int WPB, int GNA = 0>
 inline void fit_warp_carveout() {
-  static const bool once = [] {
-    constexpr size_t smem = warp_smem_bytes<VT, IPT, WPB>();
-    constexpr int resident = warp_min_blocks<VT, IPT, WPB>();
-    const int pct = (int)((resident * (smem + 1024) * 100 + 233471) / 233472) + 1;
-    KNB_CUDA(cudaFuncSetAttribute(warp_spmv<VT, MT, Epi, IPT, WPB, GNA>,
-                                  cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  pct < 100 ? pct : 100));
-    return true;
-  }();
-  (void)once;
+  set_func_attr((const void*)warp_spmv<VT, MT, Epi, IPT, WPB, GNA>,
+                cudaFuncAttributePreferredSharedMemoryCarveout,
+                warp_fit_carveout<VT, IPT, WPB>());
 }
 
 template <class VT, int IPT>

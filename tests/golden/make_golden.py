@@ -12,7 +12,7 @@ validation/manifest.d/spectral.yaml (PageRank) and topography.yaml
 The GPU box has no copy of the reference, so the tests read this packed
 file. Regenerate it with
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path of the reference checkout>
 """
 from __future__ import annotations
 
@@ -72,7 +72,8 @@ def read_values(path: Path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="root of the reference checkout (holds validation/)")
     ap.add_argument("--out", default=str(HERE / "spectral_golden.json"))
     args = ap.parse_args()
     val = Path(args.reference) / "validation"
