@@ -357,7 +357,9 @@ NET_API void net_set_sweep_timing(int32_t on);
  * (default 2e-6); 4 = sweep kernel (0 automatic, 1 one merge-path tile per
  * CTA, 2-5 one tile per warp, 6 and 7 persistent warp tiles with the most
  * gathered nodes in shared memory, 32 or 16 warps per SM, 8 warp tiles whose
- * gathers allocate in L1 only for the most gathered columns); 5 = preferred
+ * gathers allocate in L1 only for the most gathered columns, 9 and 10 the
+ * sliced layout: nodes renumbered by row length, long rows by whole warps,
+ * the others one lane per row, with 48 or 64 resident warps per SM); 5 = preferred
  * shared-memory carveout of the sweep (-1 just what the CTAs the kernel keeps
  * resident need, 0..100 percent);
  * 6 = threads per CTA of the packed-graph PageRank (0 tuned on first use,
@@ -367,7 +369,8 @@ NET_API void net_set_sweep_timing(int32_t on);
  * per tile (0) or only the CTAs that fit on the GPU at once, each warp
  * looping over tiles (1, default); 9 = mixed precision ends with one FP64
  * anchor sweep and refinement sweeps that gather the FP32 correction (1,
- * default) or with FP64 sweeps (0).
+ * default) or with FP64 sweeps (0); 10 = sliced sweeps: rows of at least
+ * this many arcs (1..255) are taken by whole warps (0: automatic).
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 

@@ -1169,7 +1169,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (!(value >= 0 && value <= 8) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 10) || value != (int)value) return 1;
       t.variant = (int)value;
       return 0;
     case 5:
@@ -1191,6 +1191,10 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 9:
       if (value != 0 && value != 1) return 1;
       t.refine = (int)value;
+      return 0;
+    case 10:
+      if (!(value >= 0 && value <= 255) || value != (int)value) return 1;
+      t.long_row = (int)value;
       return 0;
     default:
       return 1;

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "slice.cuh"
 #include "spmv.cuh"
 
 namespace knb {
@@ -52,6 +53,53 @@ struct Relabeled {
   std::map<uint32_t, std::unique_ptr<Partition>> parts;
 };
 
+// An operator in the sliced layout of slice.cuh: nodes renumbered by
+// decreasing row length, ties by decreasing column count, then by node
+// (perm[k] is the node whose new number is k, iperm its inverse). Each row's
+// arcs are sorted by renamed column (parallel arcs keep their order); rows
+// of at least `lw` arcs form a row-compressed part cut into pieces of
+// `piece` arcs, the others slices of 32 rows stored arc-major. Row sums add
+// the same terms as the reference's, in column order.
+struct SlicedOp {
+  uint32_t n = 0;
+  uint64_t nnz = 0;
+  uint32_t lw = 0;
+  uint32_t n_long = 0;
+  uint32_t long_arcs = 0;
+  uint32_t piece = 0;
+  uint32_t npieces = 0;
+  uint32_t nslices = 0;
+  uint64_t slice_elems = 0;  // arc-major elements, padding included
+  DevBuf<uint32_t> perm, iperm;
+  DevBuf<uint32_t> loff, lcols, prow;
+  DevBuf<double> lvals64;
+  DevBuf<float> lvals32;
+  DevBuf<uint32_t> sbase, scols;
+  DevBuf<uint8_t> slen;
+  DevBuf<double> svals64;
+  DevBuf<float> svals32;
+  DevBuf<double> inv_out64;
+  DevBuf<float> inv_out32;
+  DevBuf<SplitRow> split;  // rows cut by piece boundaries (split_rows)
+  uint32_t nsplit = 0;
+  uint32_t nshort = 0;
+  bool has_vals = false;
+  SliceView<double> view64() const {
+    return {n, n_long, long_arcs, piece, npieces, nslices, loff.get(), lcols.get(),
+            has_vals ? lvals64.get() : nullptr, prow.get(), sbase.get(), slen.get(),
+            scols.get(), has_vals ? svals64.get() : nullptr};
+  }
+  SliceView<float> view32() const {
+    return {n, n_long, long_arcs, piece, npieces, nslices, loff.get(), lcols.get(),
+            has_vals ? lvals32.get() : nullptr, prow.get(), sbase.get(), slen.get(),
+            scols.get(), has_vals ? svals32.get() : nullptr};
+  }
+  template <class MT>
+  SliceView<MT> view() const {
+    if constexpr (sizeof(MT) == 8) return view64(); else return view32();
+  }
+};
+
 // Per-operator scratch a solver keeps between calls (iterates, partials,
 // events), so a call allocates nothing once warm.
 struct Workspace {
@@ -78,6 +126,7 @@ struct Operator {
   std::mutex mu;  // guards parts and relabel
   const DevCsr* trans = nullptr;  // adjacency whose row lengths are this operator's column counts
   std::unique_ptr<Relabeled> relabel;
+  std::map<std::pair<uint32_t, uint32_t>, std::unique_ptr<SlicedOp>> sliced_ops;  // (lw, pieces)
   std::unique_ptr<Workspace> pr_ws;  // PageRank's (pagerank.cu), created on first use
   std::unique_ptr<Workspace> eig_ws;  // eigenvector centrality's (eigen.cu), created on first use
   std::unique_ptr<Workspace> hits_ws;  // hubs and authorities' (eigen.cu), created on first use
@@ -87,6 +136,9 @@ struct Operator {
 
   const Relabeled& relabeled(cudaStream_t s);
   const Partition& relabeled_partition(uint32_t tile_items, cudaStream_t s);
+  // The sliced layout with long rows of at least lw (<= 255) arcs cut into
+  // about `pieces` pieces; built on first use and kept.
+  const SlicedOp& sliced(uint32_t lw, uint32_t pieces, cudaStream_t s);
   OpView<double> rview64() const { return {n, nnz, relabel->off.get(), relabel->cols.get(), has_vals ? relabel->vals64.get() : nullptr}; }
   OpView<float> rview32() const { return {n, nnz, relabel->off.get(), relabel->cols.get(), has_vals ? relabel->vals32.get() : nullptr}; }
   OpView<double> view64() const { return {n, nnz, rows->off.get(), rows->tgt.get(), has_vals ? vals64.get() : nullptr}; }

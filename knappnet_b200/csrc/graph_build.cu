@@ -616,6 +616,233 @@ const Partition& Operator::relabeled_partition(uint32_t tile_items, cudaStream_t
   return ref;
 }
 
+// ----------------------------------------------------------------- sliced layout
+// Node order of the sliced layout: decreasing row length, then decreasing
+// column count (how often a sweep gathers the node's value), then node.
+__global__ void slice_node_keys(const uint32_t* __restrict__ off, const uint32_t* __restrict__ toff,
+                                uint32_t n, uint64_t* __restrict__ keys, uint32_t* __restrict__ ids) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t len = off[i + 1] - off[i];
+    const uint32_t cnt = toff ? toff[i + 1] - toff[i] : 0u;
+    keys[i] = ((uint64_t)(0xFFFFFFFFu - len) << 32) | (0xFFFFFFFFu - cnt);
+    ids[i] = i;
+  }
+}
+
+// Number of rows of at least lw arcs (lengths descend).
+__global__ void slice_count_long(const uint32_t* __restrict__ len, uint32_t n, uint32_t lw,
+                                 uint32_t* __restrict__ out) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    if (len[k] >= lw && (k + 1 == n || len[k + 1] < lw)) *out = k + 1;
+}
+
+// Arc a of the operator: key (new row, new column), payload a. The old row
+// comes from a binary search over the old offsets.
+__global__ void slice_arc_keys(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cols,
+                               const uint32_t* __restrict__ iperm, uint32_t n, uint64_t nnz,
+                               int cbits, uint64_t* __restrict__ keys, uint32_t* __restrict__ ids) {
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < nnz;
+       a += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n;  // largest i with off[i] <= a
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (off[mid] <= a) lo = mid; else hi = mid;
+    }
+    keys[a] = ((uint64_t)iperm[lo] << cbits) | iperm[cols[a]];
+    ids[a] = (uint32_t)a;
+  }
+}
+
+// Elements of slice s: 32 times the length of its first row (the longest).
+__global__ void slice_widths(const uint32_t* __restrict__ len, uint32_t n_long, uint32_t nslices,
+                             uint64_t* __restrict__ w) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s <= nslices;
+       s += gridDim.x * blockDim.x)
+    w[s] = s < nslices ? 32ull * len[n_long + 32u * s] : 0ull;
+}
+
+// 32-bit slice bases and 8-bit lengths of the short rows.
+__global__ void slice_small(const uint64_t* __restrict__ base64, const uint32_t* __restrict__ len,
+                            uint32_t n_long, uint32_t n, uint32_t nslices,
+                            uint32_t* __restrict__ base, uint8_t* __restrict__ slen) {
+  const uint32_t count = max(n, nslices + 1);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    if (k <= nslices) base[k] = (uint32_t)base64[k];
+    if (k >= n_long && k < n) slen[k - n_long] = (uint8_t)len[k];
+  }
+}
+
+// Sorted arc q (key = new row << cbits | new column, payload = old arc):
+// long rows go to the row-compressed part in order, short rows to element
+// sbase[s] + 32 j + l of their slice (row n_long + 32 s + l, arc j).
+__global__ void slice_place_arcs(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ids,
+                                 uint64_t nnz, int cbits, const uint32_t* __restrict__ noff,
+                                 uint32_t n_long, uint32_t long_arcs,
+                                 const uint32_t* __restrict__ sbase, const double* __restrict__ v64,
+                                 const float* __restrict__ v32, uint32_t* __restrict__ lcols,
+                                 double* __restrict__ lv64, float* __restrict__ lv32,
+                                 uint32_t* __restrict__ scols, double* __restrict__ sv64,
+                                 float* __restrict__ sv32) {
+  const uint64_t cmask = (1ull << cbits) - 1;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < nnz;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t key = keys[q];
+    const uint32_t col = (uint32_t)(key & cmask);
+    const uint32_t a = ids[q];
+    if (q < long_arcs) {
+      lcols[q] = col;
+      if (v64) {
+        lv64[q] = v64[a];
+        lv32[q] = v32[a];
+      }
+    } else {
+      const uint32_t k = (uint32_t)(key >> cbits);
+      const uint32_t j = (uint32_t)(q - noff[k]);
+      const uint32_t rel = k - n_long;
+      const uint64_t dst = (uint64_t)sbase[rel >> 5] + 32ull * j + (rel & 31u);
+      scols[dst] = col;
+      if (v64) {
+        sv64[dst] = v64[a];
+        sv32[dst] = v32[a];
+      }
+    }
+  }
+}
+
+const SlicedOp& Operator::sliced(uint32_t lw, uint32_t pieces, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(lw, pieces);
+  auto it = sliced_ops.find(key);
+  if (it != sliced_ops.end()) return *it->second;
+  if (lw < 1 || lw > 255) throw Error("sliced layout: long-row threshold must be 1..255");
+  auto r = std::make_unique<SlicedOp>();
+  r->n = n;
+  r->nnz = nnz;
+  r->lw = lw;
+  r->has_vals = has_vals;
+  const size_t nn = std::max<uint32_t>(n, 1);
+  r->perm.alloc(nn);
+  r->iperm.alloc(nn);
+  r->inv_out64.alloc(nn);
+  r->inv_out32.alloc(nn);
+  {
+    DevBuf<uint64_t> keys(nn);
+    slice_node_keys<<<grid_for(n, 256), 256, 0, s>>>(rows->off.get(), trans ? trans->off.get() : nullptr,
+                                                      n, keys.get(), r->perm.get());
+    KNB_LAUNCH("slice_node_keys");
+    radix_sort(keys.get(), r->perm.get(), n, 64, s);
+  }
+  invert_perm<<<grid_for(n, 256), 256, 0, s>>>(r->perm.get(), n, r->iperm.get());
+  KNB_LAUNCH("invert_perm");
+  DevBuf<uint32_t> nlen((size_t)n + 1), noff((size_t)n + 1);
+  permuted_lengths<<<grid_for((uint64_t)n + 1, 256), 256, 0, s>>>(rows->off.get(), r->perm.get(), n,
+                                                                  nlen.get());
+  KNB_LAUNCH("permuted_lengths");
+  const uint64_t total = exclusive_scan<uint32_t>(nlen.get(), noff.get(), (size_t)n + 1, s);
+  if (total != nnz) throw Error("sliced layout: arc count mismatch");
+  {
+    DevBuf<uint32_t> cnt(1);
+    KNB_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, s));
+    if (n) {
+      slice_count_long<<<grid_for(n, 256), 256, 0, s>>>(nlen.get(), n, lw, cnt.get());
+      KNB_LAUNCH("slice_count_long");
+    }
+    KNB_CUDA(cudaMemcpyAsync(&r->n_long, cnt.get(), 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+  }
+  KNB_CUDA(cudaMemcpyAsync(&r->long_arcs, noff.get() + r->n_long, 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  r->nslices = (n - r->n_long + 31) / 32;
+  // slice bases
+  {
+    DevBuf<uint64_t> w((size_t)r->nslices + 1);
+    slice_widths<<<grid_for((uint64_t)r->nslices + 1, 256), 256, 0, s>>>(nlen.get(), r->n_long,
+                                                                          r->nslices, w.get());
+    KNB_LAUNCH("slice_widths");
+    r->slice_elems = exclusive_scan<uint64_t>(w.get(), w.get(), (size_t)r->nslices + 1, s);
+    if (r->slice_elems >= 0xFFFFFFFFull) throw Error("sliced layout: too many slice elements");
+    r->sbase.alloc((size_t)r->nslices + 1);
+    r->slen.alloc(std::max<size_t>((size_t)(n - r->n_long), 1));
+    slice_small<<<grid_for(std::max<uint64_t>(n, (uint64_t)r->nslices + 1), 256), 256, 0, s>>>(
+        w.get(), nlen.get(), r->n_long, n, r->nslices, r->sbase.get(), r->slen.get());
+    KNB_LAUNCH("slice_small");
+  }
+  // arcs: sorted by (new row, new column), placed
+  r->loff.alloc((size_t)r->n_long + 1);
+  KNB_CUDA(cudaMemcpyAsync(r->loff.get(), noff.get(), ((size_t)r->n_long + 1) * 4,
+                           cudaMemcpyDeviceToDevice, s));
+  r->lcols.alloc(std::max<size_t>(r->long_arcs, 1));
+  r->scols.alloc(std::max<uint64_t>(r->slice_elems, 1));
+  if (has_vals) {
+    r->lvals64.alloc(std::max<size_t>(r->long_arcs, 1));
+    r->lvals32.alloc(std::max<size_t>(r->long_arcs, 1));
+    r->svals64.alloc(std::max<uint64_t>(r->slice_elems, 1));
+    r->svals32.alloc(std::max<uint64_t>(r->slice_elems, 1));
+  }
+  if (nnz) {
+    const int cbits = std::max(1, bits_for(n));
+    DevBuf<uint64_t> keys(nnz);
+    DevBuf<uint32_t> ids(nnz);
+    slice_arc_keys<<<grid_for(nnz, 256), 256, 0, s>>>(rows->off.get(), rows->tgt.get(),
+                                                       r->iperm.get(), n, nnz, cbits, keys.get(),
+                                                       ids.get());
+    KNB_LAUNCH("slice_arc_keys");
+    radix_sort(keys.get(), ids.get(), nnz, 2 * cbits, s);
+    slice_place_arcs<<<grid_for(nnz, 256), 256, 0, s>>>(
+        keys.get(), ids.get(), nnz, cbits, noff.get(), r->n_long, r->long_arcs, r->sbase.get(),
+        has_vals ? vals64.get() : nullptr, has_vals ? vals32.get() : nullptr, r->lcols.get(),
+        has_vals ? r->lvals64.get() : nullptr, has_vals ? r->lvals32.get() : nullptr,
+        r->scols.get(), has_vals ? r->svals64.get() : nullptr,
+        has_vals ? r->svals32.get() : nullptr);
+    KNB_LAUNCH("slice_place_arcs");
+  }
+  gather_vec<double><<<grid_for(n, 256), 256, 0, s>>>(inv_out64.get(), r->perm.get(), n,
+                                                      r->inv_out64.get());
+  gather_vec<float><<<grid_for(n, 256), 256, 0, s>>>(inv_out32.get(), r->perm.get(), n,
+                                                     r->inv_out32.get());
+  KNB_LAUNCH("gather_vec");
+  // pieces of the long rows, the row holding each piece's first arc, and the
+  // rows a piece boundary cuts (their partials are added by split_rows)
+  std::vector<uint32_t> hl((size_t)r->n_long + 1);
+  KNB_CUDA(cudaMemcpyAsync(hl.data(), r->loff.get(), hl.size() * 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  const uint32_t want = std::max<uint32_t>(pieces, 1);
+  uint32_t piece = r->long_arcs ? (uint32_t)(((uint64_t)r->long_arcs + want - 1) / want) : 1;
+  piece = std::max<uint32_t>(32, (piece + 31) & ~31u);
+  r->piece = piece;
+  r->npieces = r->long_arcs ? (uint32_t)(((uint64_t)r->long_arcs + piece - 1) / piece) : 0;
+  std::vector<uint32_t> prow(std::max<uint32_t>(r->npieces, 1), 0);
+  {
+    uint32_t row = 0;
+    for (uint32_t t = 0; t < r->npieces; ++t) {
+      const uint64_t a0 = (uint64_t)t * piece;
+      while (row + 1 < r->n_long && hl[row + 1] <= a0) ++row;
+      prow[t] = row;
+    }
+  }
+  std::vector<SplitRow> sr;
+  for (uint32_t row = 0; row < r->n_long; ++row) {
+    const uint32_t first = hl[row] / piece, last = (hl[row + 1] - 1) / piece;
+    if (first != last) sr.push_back({row, first, last});
+  }
+  std::stable_partition(sr.begin(), sr.end(),
+                        [](const SplitRow& x) { return x.last - x.first <= SHORT_SPAN; });
+  r->nshort = 0;
+  while (r->nshort < sr.size() && sr[r->nshort].last - sr[r->nshort].first <= SHORT_SPAN)
+    ++r->nshort;
+  r->nsplit = (uint32_t)sr.size();
+  r->prow.alloc(prow.size());
+  KNB_CUDA(cudaMemcpyAsync(r->prow.get(), prow.data(), prow.size() * 4, cudaMemcpyHostToDevice, s));
+  r->split.alloc(std::max<size_t>(sr.size(), 1));
+  if (!sr.empty())
+    KNB_CUDA(cudaMemcpyAsync(r->split.get(), sr.data(), sr.size() * sizeof(SplitRow),
+                             cudaMemcpyHostToDevice, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  auto& ref = *r;
+  sliced_ops[key] = std::move(r);
+  return ref;
+}
+
 // Arc values from per-edge weights given by the caller (input edge order),
 // through each arc's edge index.
 __global__ void op_values_from_edges(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,

@@ -462,6 +462,7 @@ struct SweepBuffers {
   IterState* st;
   const double* y_ref = nullptr;  // refinement sweeps: the anchor iterate (FP64)
   double* s_ref = nullptr;        //   and its row sums
+  const SlicedOp* so = nullptr;   // the sliced layout (slice variants)
 };
 
 enum SweepVariant : int {
@@ -469,7 +470,10 @@ enum SweepVariant : int {
   VAR_HOT = 6,    // hot-node cache, one CTA of 32 warps per SM
   VAR_HOT16 = 7,  // hot-node cache, one CTA of 16 warps per SM
   VAR_WARPL1 = 8, // 16 warps per CTA; only gathers of the most gathered columns allocate in L1
+  VAR_SLICE = 9,    // sliced layout (slice.cuh), 48 resident warps per SM
+  VAR_SLICE64 = 10, // sliced layout, 64 resident warps per SM
 };
+static bool slice_variant(int var) { return var == VAR_SLICE || var == VAR_SLICE64; }
 
 // SM count and the largest dynamic shared memory a CTA may opt into, per
 // device (queried once).
@@ -507,14 +511,58 @@ static uint32_t hot_nodes(uint32_t n, size_t warp_bytes, int smem_optin) {
 // One merge-path sweep with epilogue `e`: the sweep kernel of variant VAR
 // gathering x, then the split-row kernel, whose CTAs also reduce the
 // epilogue's per-tile scalars and whose last CTA decides convergence.
+// CTAs of a sliced sweep that fit on the device at once (per device).
+template <class VT, class MT, class Epi, int U, int MINB, int GNA>
+static unsigned slice_grid() {
+  static std::mutex mu;
+  static std::map<int, unsigned> grids;
+  int dev = 0;
+  KNB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = grids.find(dev);
+  if (it != grids.end()) return it->second;
+  int per_sm = 0;
+  KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, slice_spmv<VT, MT, Epi, U, MINB, GNA>, SLICE_WPB * 32, 0));
+  const unsigned g = (unsigned)std::max(1, per_sm) * (unsigned)device_limits().sms;
+  grids[dev] = g;
+  return g;
+}
+
+// Sliced sweeps: a persistent grid of the CTAs that fit at once. The kernel
+// uses no shared memory, so it asks for the smallest carveout: L1 keeps the
+// SM's whole 256 KB.
+template <class VT, class MT, class Epi, int U, int MINB>
+static unsigned launch_slice(const SlicedOp& so, const VT* x, const Epi& e, VT* carry, VT* head,
+                             double* part1, IterState* st, cudaStream_t s) {
+  constexpr int GNA = sizeof(VT) == 4 ? 2 : 0;
+  auto fnp = slice_spmv<VT, MT, Epi, U, MINB, GNA>;
+  set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+  const unsigned grid = slice_grid<VT, MT, Epi, U, MINB, GNA>();
+  const uint32_t l1_hot = tuning().hot_nodes >= 0 ? (uint32_t)std::min<int64_t>(
+                                                        tuning().hot_nodes, 0xFFFFFFFFll)
+                                                  : 24576u;
+  fnp<<<grid, SLICE_WPB * 32, 0, s>>>(so.view<MT>(), x, e, carry, head, part1, st, l1_hot);
+  return grid * SLICE_WPB;
+}
+
 template <class VT, class MT, class Epi, int VAR, int IPT>
 static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>& v,
                         const VT* x, const Epi& e, VT* carry, VT* head, double* part1,
                         double* part2, IterState* st, cudaStream_t s, unsigned g2,
-                        cudaEvent_t ev0, cudaEvent_t ev1) {
+                        cudaEvent_t ev0, cudaEvent_t ev1, const SlicedOp* so = nullptr) {
   if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
   uint32_t npart = P.ntiles;  // partials the sweep leaves for split_rows
-  if constexpr (VAR == VAR_HOT || VAR == VAR_HOT16) {
+  if constexpr (VAR == VAR_SLICE || VAR == VAR_SLICE64) {
+    npart = launch_slice<VT, MT, Epi, IPT, VAR == VAR_SLICE ? 6 : 8>(*so, x, e, carry, head,
+                                                                     part1, st, s);
+    KNB_LAUNCH("slice_spmv");
+    if (ev1) KNB_CUDA(cudaEventRecord(ev1, s));
+    split_rows<VT, Epi><<<g2, SPMV_THREADS, 0, s>>>(so->split.get(), so->nsplit, so->nshort,
+                                                     carry, head, e, part1, npart, part2, st);
+    KNB_LAUNCH("split_rows");
+    return;
+  } else if constexpr (VAR == VAR_HOT || VAR == VAR_HOT16) {
     constexpr int WPB = VAR == VAR_HOT ? 32 : 16;
     constexpr size_t wbytes = hot_warp_smem_bytes<VT, IPT, WPB>();
     const DeviceLimits lim = device_limits();
@@ -613,7 +661,7 @@ static void launch_sweep(const Operator& op, const Partition& P, const SweepBuff
   OpView<MT> v;
   if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
   launch_spmv<VT, MT, Epi, VAR, IPT>(op, P, v, (const VT*)B.z[buf], e, (VT*)B.carry,
-                                     (VT*)B.head, B.part1, B.part2, B.st, s, g2, ev0, ev1);
+                                     (VT*)B.head, B.part1, B.part2, B.st, s, g2, ev0, ev1, B.so);
   if (EXACT) {
     pr_exact_change<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
         (const double*)B.y[buf], (const double*)B.y[1 - buf], op.n, B.part3, B.st);
@@ -652,6 +700,10 @@ static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
     case VAR_HOT: return pick_warp_ipt<VT, MT, EXACT, VAR_HOT>(ipt, pv, ju);
     case VAR_HOT16: return pick_warp_ipt<VT, MT, EXACT, VAR_HOT16>(ipt, pv, ju);
     case VAR_WARPL1: return pick_warp_ipt<VT, MT, EXACT, VAR_WARPL1>(ipt, pv, ju);
+    case VAR_SLICE:
+      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICE, 4>(pv, ju)
+                      : pick_pv<VT, MT, EXACT, VAR_SLICE, 8>(pv, ju);
+    case VAR_SLICE64: return pick_pv<VT, MT, EXACT, VAR_SLICE64, 4>(pv, ju);
     default: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP>(ipt, pv, ju);
   }
 }
@@ -676,7 +728,7 @@ static void launch_refine(const Operator& op, const Partition& P, const SweepBuf
   e.pu = 1.0 / (double)op.n;
   launch_spmv<float, float, Epi, VAR, IPT>(op, P, B.v32, (const float*)B.z[buf], e,
                                            (float*)B.carry, (float*)B.head, B.part1, B.part2,
-                                           B.st, s, g2, ev0, ev1);
+                                           B.st, s, g2, ev0, ev1, B.so);
   pr_exact_change_ref<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
       B.y_ref, (const float*)B.y[buf], (const float*)B.y[1 - buf], op.n, B.part3, B.st);
   KNB_LAUNCH("pr_exact_change_ref");
@@ -703,7 +755,7 @@ static void launch_anchor(const Operator& op, const Partition& P, const SweepBuf
   OpView<MT> v;
   if constexpr (sizeof(MT) == 8) v = B.v64; else v = B.v32;
   launch_spmv<double, MT, Epi, VAR, IPT>(op, P, v, z_ref, e, carry64, head64, B.part1, B.part2,
-                                         B.st, s, g2, ev0, ev1);
+                                         B.st, s, g2, ev0, ev1, B.so);
   pr_exact_change_ref<<<grid_for(op.n, VT_THREADS, 1184), VT_THREADS, 0, s>>>(
       B.y_ref, nullptr, (const float*)B.y[0], op.n, B.part3, B.st);
   KNB_LAUNCH("pr_exact_change_ref");
@@ -727,6 +779,8 @@ static SweepFn pick_refine_ipt(int ipt, bool pv, bool ju) {
 }
 static SweepFn pick_refine(int var, int ipt, bool pv, bool ju) {
   switch (var) {
+    case VAR_SLICE: return pick_refine_pv<VAR_SLICE, 4>(pv, ju);
+    case VAR_SLICE64: return pick_refine_pv<VAR_SLICE64, 4>(pv, ju);
     case VAR_WARP: return pick_refine_ipt<VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_refine_ipt<VAR_WARP4>(ipt, pv, ju);
     case VAR_WARPL1: return pick_refine_ipt<VAR_WARPL1>(ipt, pv, ju);
@@ -746,13 +800,16 @@ static AnchorFn pick_anchor_ipt(int ipt, bool pv, bool ju) {
 template <class MT>
 static AnchorFn pick_anchor(int var, int ipt, bool pv, bool ju) {
   switch (var) {
+    case VAR_SLICE: return pick_anchor_pv<MT, VAR_SLICE, 4>(pv, ju);
+    case VAR_SLICE64: return pick_anchor_pv<MT, VAR_SLICE64, 4>(pv, ju);
     case VAR_WARP: return pick_anchor_ipt<MT, VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_anchor_ipt<MT, VAR_WARP4>(ipt, pv, ju);
     default: return pick_anchor_ipt<MT, VAR_WARP16>(ipt, pv, ju);
   }
 }
 static bool refine_variant(int var) {
-  return var == VAR_WARP || var == VAR_WARP4 || var == VAR_WARP16 || var == VAR_WARPL1;
+  return var == VAR_WARP || var == VAR_WARP4 || var == VAR_WARP16 || var == VAR_WARPL1 ||
+         slice_variant(var);
 }
 
 static uint32_t tile_items(int var, int ipt) {
@@ -903,9 +960,17 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   // FP64 sweeps; FP32 sweeps let only gathers of the 24,576 most gathered
   // columns allocate in L1, 8% faster than allocating every gather, while the
   // refinement sweeps, with more registers live, keep plain gathers).
-  const bool rl = prm.relabel;
-  int var32 = prm.variant ? prm.variant : (rl ? VAR_WARPL1 : VAR_WARP16);
+  int var32 = prm.variant ? prm.variant : (prm.relabel ? VAR_WARPL1 : VAR_WARP16);
   int var64 = prm.variant ? prm.variant : VAR_WARP16;
+  // The sliced layout numbers nodes its own way, so every phase of a solve
+  // on it runs a sliced sweep; the other variants share the renumbering by
+  // column count (or none).
+  const bool sl = slice_variant(var32) || slice_variant(var64);
+  if (sl) {
+    if (!slice_variant(var32)) var32 = var64;
+    if (!slice_variant(var64)) var64 = var32;
+  }
+  const bool rl = prm.relabel && !sl;
   // The hot-node sweep needs the renumbered operator: its most gathered
   // nodes come first, and its arc arrays are padded for 16-byte loads.
   if (!rl && (var32 == VAR_HOT || var32 == VAR_HOT16)) var32 = VAR_WARP4;
@@ -915,41 +980,58 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   // Mixed precision with refinement: one FP64 anchor sweep, then refinement
   // sweeps with FP32 gathers (RefineEpi); both run on warp tiles.
   const bool refine = prm.precision == PREC_MIXED && tu.refine != 0;
-  const int var_r = prm.variant && refine_variant(var32) ? var32 : VAR_WARP16;  // refinement
-  const int ipt_r = ipt32 == 4 ? 4 : 8;
+  const int var_r =  // refinement
+      sl ? var32 : (prm.variant && refine_variant(var32) ? var32 : VAR_WARP16);
+  const int ipt_r = (ipt32 == 4 || sl) ? 4 : 8;
   if (refine) {  // the anchor sweep takes the FP64 settings
     if (!refine_variant(var64)) var64 = VAR_WARP16;
     ipt64 = ipt64 == 8 ? 8 : 4;
   }
+  // Sliced sweeps keep 4 gathers per lane in flight (8 in FP32 sweeps at 48
+  // warps per SM): wider ones spill at their register budget.
+  if (sl) {
+    ipt64 = 4;
+    if (var32 == VAR_SLICE64 || ipt32 != 4) ipt32 = var32 == VAR_SLICE64 ? 4 : 8;
+  }
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
+  // Sliced layout: pieces of long rows a multiple of the resident warps at
+  // 48 and at 64 warps per SM (192 per SM), so every warp gets as many.
+  const SlicedOp* SO =
+      sl ? &op.sliced(tu.long_row > 0 ? (uint32_t)tu.long_row : 64u,
+                      192u * (uint32_t)device_limits().sms, s)
+         : nullptr;
+  static const Partition no_partition;  // sliced sweeps cut their own work
   const bool mixed_pre = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
   const Partition* P32 = nullptr;
   const Partition* P64 = nullptr;
   if (mixed_pre) {
     const uint32_t tile = tile_items(var32, ipt32);
-    P32 = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
+    P32 = sl ? &no_partition : rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
   }
   if (prm.precision != PREC_FP32) {
     const uint32_t tile = tile_items(var64, ipt64);
-    P64 = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
+    P64 = sl ? &no_partition : rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
   }
   const Partition* PR = nullptr;
   if (refine) {
     const uint32_t tile = tile_items(var_r, ipt_r);
-    PR = rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
+    PR = sl ? &no_partition : rl ? &op.relabeled_partition(tile, s) : &op.partition(tile, s);
   }
   const OpView<double> v64 = rl ? op.rview64() : op.view64();
   const OpView<float> v32 = rl ? op.rview32() : op.view32();
-  const double* inv64 = rl ? R->inv_out64.get() : op.inv_out64.get();
-  const float* inv32 = rl ? R->inv_out32.get() : op.inv_out32.get();
-  const uint32_t* perm = rl ? R->perm.get() : nullptr;
-  const uint32_t* iperm = rl ? R->iperm.get() : nullptr;
+  const double* inv64 = sl ? SO->inv_out64.get() : rl ? R->inv_out64.get() : op.inv_out64.get();
+  const float* inv32 = sl ? SO->inv_out32.get() : rl ? R->inv_out32.get() : op.inv_out32.get();
+  const uint32_t* perm = sl ? SO->perm.get() : rl ? R->perm.get() : nullptr;
+  const uint32_t* iperm = sl ? SO->iperm.get() : rl ? R->iperm.get() : nullptr;
 
   const bool pv = prm.personalization != nullptr;
   const bool ju = !pv || prm.dangling == 1;
   const bool mixed = mixed_pre;
-  const uint32_t nt = std::max({P32 ? P32->ntiles : 0u, P64 ? P64->ntiles : 0u,
-                                PR ? PR->ntiles : 0u});
+  // carries and heads per tile or piece; partials per tile or warp (a
+  // sliced sweep leaves one per warp of its grid, at most 64 per SM)
+  const uint32_t nt =
+      sl ? std::max<uint32_t>(SO->npieces + 1, 64u * (uint32_t)device_limits().sms)
+         : std::max({P32 ? P32->ntiles : 0u, P64 ? P64->ntiles : 0u, PR ? PR->ntiles : 0u});
   const unsigned gv = grid_for(n, VT_THREADS, 1184);
 
   PrWorkspace* wsp = nullptr;
@@ -1000,6 +1082,7 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
     SweepBuffers B{v64, v32, {ws.y32[0].get(), ws.y32[1].get()},
                    {ws.z32[0].get(), ws.z32[1].get()}, inv32, pdev, ws.carry32.get(),
                    ws.head32.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st};
+    B.so = SO;
     SweepFn fn = pick_kernel<float, float, false>(var32, ipt32, pv, ju);
     r32 = run_phase(fn, op, *P32, B, prm.damping, false, s, ws, hstate, &tms32, &tn32);
     launches += r32.launches;
@@ -1031,7 +1114,7 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
       SweepBuffers R{v64, v32, {ws.y32[0].get(), ws.y32[1].get()},
                      {ws.z32[0].get(), ws.z32[1].get()}, inv32, pdev, ws.carry32.get(),
                      ws.head32.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1,
-                     ws.y64[0].get(), ws.z64[1].get()};
+                     ws.y64[0].get(), ws.z64[1].get(), SO};
       AnchorFn af = use32 ? pick_anchor<float>(var64, ipt64, pv, ju)
                           : pick_anchor<double>(var64, ipt64, pv, ju);
       af(op, *P64, R, ws.z64[0].get(), ws.carry64.get(), ws.head64.get(), prm.damping, s,
@@ -1049,6 +1132,7 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
       SweepBuffers B{v64, v32, {ws.y64[0].get(), ws.y64[1].get()},
                      {ws.z64[0].get(), ws.z64[1].get()}, inv64, pdev, ws.carry64.get(),
                      ws.head64.get(), ws.part1.get(), ws.part2.get(), ws.part3.get(), st + 1};
+      B.so = SO;
       SweepFn fn = use32 ? pick_kernel<double, float, true>(var64, ipt64, pv, ju)
                          : pick_kernel<double, double, true>(var64, ipt64, pv, ju);
       r64 = run_phase(fn, op, *P64, B, prm.damping, true, s, ws, hstate, &tms64, &tn64);

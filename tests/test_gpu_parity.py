@@ -414,6 +414,63 @@ def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot, persis
         K.set_tuning(K.TUNE_PERSISTENT, 1)
 
 
+@pytest.mark.parametrize("variant,long_row", [(9, 0), (9, 16), (9, 255), (9, 1), (10, 0),
+                                              (10, 200)])
+def test_sliced_sweep_matches_oracle(variant, long_row):
+    """The sliced layout (rows renumbered by length; long rows by whole
+    warps in pieces, the others one lane per row): FP64 and mixed (FP32
+    sweeps, FP64 anchor, refinement) solves, every option set, against
+    the oracle. Long-row thresholds from 1 (every row taken by a warp) to
+    255 (the longest rows a slice holds)."""
+    kg, og = rmat_pair(12, True, seed=23)
+    n = kg.n
+    p = np.zeros(n)
+    p[[3, 70, 900]] = 1.0
+    try:
+        K.set_tuning(K.TUNE_VARIANT, variant)
+        K.set_tuning(K.TUNE_LONG_ROW, long_row)
+        for opts in (dict(), dict(personalization=p), dict(directed=False),
+                     dict(personalization=p, dangling=1), dict(weighted=False)):
+            o = dict(weighted=True)
+            o.update(opts)
+            b = og.pagerank(**o)
+            a, ia = kg.pagerank_ex(precision=K.PREC_FP64, **o)
+            assert np.abs(a - b).sum() <= 1e-12, opts
+            assert ia.iterations == og.last_iters, opts
+            bm = og.pagerank(tol=1e-10, **o)
+            am, _ = kg.pagerank_ex(precision=K.PREC_MIXED, tol=1e-10, **o)
+            assert np.abs(am - bm).sum() <= 1e-9, opts
+            top = np.argsort(-bm, kind="stable")[:100]
+            assert np.array_equal(np.argsort(-am, kind="stable")[:100], top), opts
+        # repeated solves are bit-identical
+        x1, _ = kg.pagerank_ex(weighted=True, precision=K.PREC_MIXED, tol=1e-10)
+        x2, _ = kg.pagerank_ex(weighted=True, precision=K.PREC_MIXED, tol=1e-10)
+        assert np.array_equal(x1, x2)
+    finally:
+        K.set_tuning(K.TUNE_VARIANT, 0)
+        K.set_tuning(K.TUNE_LONG_ROW, 0)
+
+
+def test_sliced_sweep_on_fixtures_and_edge_cases():
+    """Every golden fixture (empty graph, single node, loops, parallel arcs,
+    disconnected parts) and every loop code through the sliced layout."""
+    try:
+        K.set_tuning(K.TUNE_VARIANT, 9)
+        for name in sorted(DOC["fixtures"]):
+            kg, og = both(DOC["fixtures"][name])
+            for loops in (0, 1, 2):
+                for weighted in ((False, True) if kg.weighted else (False,)):
+                    b = og.pagerank(weighted=weighted, loops=loops)
+                    a = kg.pagerank(weighted=weighted, loops=loops)
+                    assert np.abs(a - b).sum() <= 1e-12, (name, loops, weighted)
+                    am, _ = kg.pagerank_ex(weighted=weighted, loops=loops,
+                                           precision=K.PREC_MIXED, tol=1e-10)
+                    assert np.abs(am - og.pagerank(weighted=weighted, loops=loops,
+                                                   tol=1e-10)).sum() <= 1e-9, name
+    finally:
+        K.set_tuning(K.TUNE_VARIANT, 0)
+
+
 @pytest.mark.parametrize("variant", [6, 7])
 def test_hot_node_sweep_larger_than_shared_memory(variant):
     """Scale 17 (131,072 nodes): more nodes than shared memory holds, so
