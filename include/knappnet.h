@@ -370,7 +370,7 @@ NET_API void net_set_sweep_timing(int32_t on);
  * looping over tiles (1, default); 9 = mixed precision ends with one FP64
  * anchor sweep and refinement sweeps that gather the FP32 correction (1,
  * default) or with FP64 sweeps (0); 10 = sliced sweeps: rows of at least
- * this many arcs (1..255) are taken by whole warps (0: automatic).
+ * this many arcs (1..65535) are taken by whole warps (0: automatic).
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 

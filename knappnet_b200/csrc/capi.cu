@@ -1193,7 +1193,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.refine = (int)value;
       return 0;
     case 10:
-      if (!(value >= 0 && value <= 255) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 65535) || value != (int)value) return 1;
       t.long_row = (int)value;
       return 0;
     default:

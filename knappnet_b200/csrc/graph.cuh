@@ -75,7 +75,7 @@ struct SlicedOp {
   DevBuf<double> lvals64;
   DevBuf<float> lvals32;
   DevBuf<uint32_t> sbase, scols;
-  DevBuf<uint8_t> slen;
+  DevBuf<uint16_t> slen;
   DevBuf<double> svals64;
   DevBuf<float> svals32;
   DevBuf<double> inv_out64;
@@ -136,7 +136,7 @@ struct Operator {
 
   const Relabeled& relabeled(cudaStream_t s);
   const Partition& relabeled_partition(uint32_t tile_items, cudaStream_t s);
-  // The sliced layout with long rows of at least lw (<= 255) arcs cut into
+  // The sliced layout with long rows of at least lw (<= 65535) arcs cut into
   // about `pieces` pieces; built on first use and kept.
   const SlicedOp& sliced(uint32_t lw, uint32_t pieces, cudaStream_t s);
   OpView<double> rview64() const { return {n, nnz, relabel->off.get(), relabel->cols.get(), has_vals ? relabel->vals64.get() : nullptr}; }

@@ -661,14 +661,14 @@ __global__ void slice_widths(const uint32_t* __restrict__ len, uint32_t n_long, 
     w[s] = s < nslices ? 32ull * len[n_long + 32u * s] : 0ull;
 }
 
-// 32-bit slice bases and 8-bit lengths of the short rows.
+// 32-bit slice bases and 16-bit lengths of the short rows.
 __global__ void slice_small(const uint64_t* __restrict__ base64, const uint32_t* __restrict__ len,
                             uint32_t n_long, uint32_t n, uint32_t nslices,
-                            uint32_t* __restrict__ base, uint8_t* __restrict__ slen) {
+                            uint32_t* __restrict__ base, uint16_t* __restrict__ slen) {
   const uint32_t count = max(n, nslices + 1);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
     if (k <= nslices) base[k] = (uint32_t)base64[k];
-    if (k >= n_long && k < n) slen[k - n_long] = (uint8_t)len[k];
+    if (k >= n_long && k < n) slen[k - n_long] = (uint16_t)len[k];
   }
 }
 
@@ -714,7 +714,7 @@ const SlicedOp& Operator::sliced(uint32_t lw, uint32_t pieces, cudaStream_t s) {
   const auto key = std::make_pair(lw, pieces);
   auto it = sliced_ops.find(key);
   if (it != sliced_ops.end()) return *it->second;
-  if (lw < 1 || lw > 255) throw Error("sliced layout: long-row threshold must be 1..255");
+  if (lw < 1 || lw > 65535) throw Error("sliced layout: long-row threshold must be 1..65535");
   auto r = std::make_unique<SlicedOp>();
   r->n = n;
   r->nnz = nnz;

@@ -49,7 +49,7 @@ struct Tuning {
   int64_t hot_nodes = -1; // hot-node sweeps: cap on the nodes kept in shared memory (-1: none)
   int persistent = 1;     // warp-tile sweeps: 1 launches only the CTAs that fit at once
   int refine = 1;         // mixed: 1 anchor + refinement sweeps, 0 plain FP64 sweeps
-  int long_row = 0;       // sliced sweeps: rows of at least this many arcs are long (0: 64)
+  int long_row = 0;       // sliced sweeps: rows of at least this many arcs are long (0: 255)
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

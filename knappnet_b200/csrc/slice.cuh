@@ -47,7 +47,7 @@ struct SliceView {
   const MT* lvals;        // long_arcs values (nullptr: every entry is 1)
   const uint32_t* prow;   // npieces: the row holding each piece's first arc
   const uint32_t* sbase;  // nslices + 1: first element of each slice
-  const uint8_t* slen;    // n - n_long row lengths (below lw <= 255)
+  const uint16_t* slen;   // n - n_long row lengths (below lw)
   const uint32_t* scols;  // arc-major slice elements
   const MT* svals;
 };
