@@ -1169,7 +1169,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (!(value >= 0 && value <= 10) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 12) || value != (int)value) return 1;
       t.variant = (int)value;
       return 0;
     case 5:

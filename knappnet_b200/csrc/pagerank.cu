@@ -62,17 +62,28 @@ struct PagerankEpi {
   static __device__ __forceinline__ double combine(int, double a, double b) { return a + b; }
   static __device__ __forceinline__ double warp_combine(int, double v) { return warp_sum(v); }
 
-  __device__ __forceinline__ void row(uint32_t g, VT s, double* a) const {
-    const VT pg = PV ? (VT)p[g] : (VT)pu;
+  // The per-node inputs of row g's update, loaded apart from it so a sweep
+  // can issue these loads before the row sum is ready (fetch, then row_in).
+  struct In {
+    VT yo, io, pg;
+  };
+  __device__ __forceinline__ In fetch(uint32_t g) const {
+    return {y_old[g], inv_out[g], PV ? (VT)p[g] : (VT)pu};
+  }
+  __device__ __forceinline__ void row_in(uint32_t g, VT s, const In& in, double* a) const {
+    const VT pg = in.pg;
     const VT jg = JU ? (VT)pu : pg;
     const VT u = (VT)d * (s * c_it + c_dt * jg) + (VT)(1.0 - d) * pg;
-    const VT xo = y_old[g] * c_it;
-    const VT io = inv_out[g];
+    const VT xo = in.yo * c_it;
+    const VT io = in.io;
     y_new[g] = u;
     z_new[g] = u * io;
     a[0] += (double)u;
     if (io == VT(0)) a[1] += (double)u;
     a[2] += fabs((double)u - (double)xo);
+  }
+  __device__ __forceinline__ void row(uint32_t g, VT s, double* a) const {
+    row_in(g, s, fetch(g), a);
   }
 
   __device__ void finish(IterState* st, const double* tot) const {
@@ -130,27 +141,44 @@ struct RefineEpi {
   static __device__ __forceinline__ double combine(int, double a, double b) { return a + b; }
   static __device__ __forceinline__ double warp_combine(int, double v) { return warp_sum(v); }
 
-  __device__ __forceinline__ void row(uint32_t g, VT s_in, double* a) const {
+  // The per-node inputs of row g's update (see PagerankEpi::fetch).
+  struct In {
+    double sr, yr, pg;
+    float eo, io;
+  };
+  __device__ __forceinline__ In fetch(uint32_t g) const {
+    In in;
+    in.sr = ANCHOR ? 0.0 : s_ref[g];
+    in.yr = y_ref[g];
+    in.pg = PV ? p[g] : pu;
+    in.eo = ANCHOR ? 0.0f : e_old[g];
+    in.io = inv_out[g];
+    return in;
+  }
+  __device__ __forceinline__ void row_in(uint32_t g, VT s_in, const In& in, double* a) const {
     double s;
     if constexpr (ANCHOR) {
       s = (double)s_in;
       s_ref[g] = s;
     } else {
-      s = s_ref[g] + (double)s_in;
+      s = in.sr + (double)s_in;
     }
-    const double pg = PV ? p[g] : pu;
+    const double pg = in.pg;
     const double jg = JU ? pu : pg;
     const double u = d * (s * c_it + c_dt * jg) + (1.0 - d) * pg;
-    const double yr = y_ref[g];
-    const double yo = ANCHOR ? yr : yr + (double)e_old[g];
+    const double yr = in.yr;
+    const double yo = ANCHOR ? yr : yr + (double)in.eo;
     const float en = (float)(u - yr);
     const double us = yr + (double)en;  // the iterate as stored
-    const float io = inv_out[g];
+    const float io = in.io;
     e_new[g] = en;
     z_new[g] = en * io;
     a[0] += us;
     if (io == 0.0f) a[1] += us;
     a[2] += fabs(us - yo * c_it);
+  }
+  __device__ __forceinline__ void row(uint32_t g, VT s_in, double* a) const {
+    row_in(g, s_in, fetch(g), a);
   }
 
   __device__ void finish(IterState* st, const double* tot) const {
@@ -472,8 +500,11 @@ enum SweepVariant : int {
   VAR_WARPL1 = 8, // 16 warps per CTA; only gathers of the most gathered columns allocate in L1
   VAR_SLICE = 9,    // sliced layout (slice.cuh), 48 resident warps per SM
   VAR_SLICE64 = 10, // sliced layout, 64 resident warps per SM
+  VAR_SLICEP = 11,  // sliced layout, pipelined loads, 40 resident warps per SM
+  VAR_SLICEP64 = 12,  // sliced layout, pipelined loads, 32 resident warps per SM
 };
-static bool slice_variant(int var) { return var == VAR_SLICE || var == VAR_SLICE64; }
+static bool slice_variant(int var) { return var >= VAR_SLICE && var <= VAR_SLICEP64; }
+static bool slice64_variant(int var) { return var == VAR_SLICE64; }
 
 // SM count and the largest dynamic shared memory a CTA may opt into, per
 // device (queried once).
@@ -512,7 +543,7 @@ static uint32_t hot_nodes(uint32_t n, size_t warp_bytes, int smem_optin) {
 // gathering x, then the split-row kernel, whose CTAs also reduce the
 // epilogue's per-tile scalars and whose last CTA decides convergence.
 // CTAs of a sliced sweep that fit on the device at once (per device).
-template <class VT, class MT, class Epi, int U, int MINB, int GNA>
+template <class VT, class MT, class Epi, int U, int MINB, int GNA, bool PIPE>
 static unsigned slice_grid() {
   static std::mutex mu;
   static std::map<int, unsigned> grids;
@@ -522,8 +553,12 @@ static unsigned slice_grid() {
   auto it = grids.find(dev);
   if (it != grids.end()) return it->second;
   int per_sm = 0;
-  KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, slice_spmv<VT, MT, Epi, U, MINB, GNA>, SLICE_WPB * 32, 0));
+  if constexpr (PIPE)
+    KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, slice_spmv_p<VT, MT, Epi, U, MINB, GNA>, SLICE_WPB * 32, 0));
+  else
+    KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, slice_spmv<VT, MT, Epi, U, MINB, GNA>, SLICE_WPB * 32, 0));
   const unsigned g = (unsigned)std::max(1, per_sm) * (unsigned)device_limits().sms;
   grids[dev] = g;
   return g;
@@ -535,13 +570,15 @@ static unsigned slice_grid() {
 // L1: 49,152 FP32 values (192 KB) by default, as many bytes of FP64 values
 // (measured on R-MAT 24: no L1 allocation at all makes the FP32 sweep 1.36
 // ms instead of 0.83 ms; 24,576, 98,304 or every column 0.86-0.88 ms).
-template <class VT, class MT, class Epi, int U, int MINB>
+template <class VT, class MT, class Epi, int U, int MINB, bool PIPE>
 static unsigned launch_slice(const SlicedOp& so, const VT* x, const Epi& e, VT* carry, VT* head,
                              double* part1, IterState* st, cudaStream_t s) {
   constexpr int GNA = 2;
-  auto fnp = slice_spmv<VT, MT, Epi, U, MINB, GNA>;
+  void (*fnp)(SliceView<MT>, const VT*, Epi, VT*, VT*, double*, const IterState*, uint32_t);
+  if constexpr (PIPE) fnp = slice_spmv_p<VT, MT, Epi, U, MINB, GNA>;
+  else fnp = slice_spmv<VT, MT, Epi, U, MINB, GNA>;
   set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  const unsigned grid = slice_grid<VT, MT, Epi, U, MINB, GNA>();
+  const unsigned grid = slice_grid<VT, MT, Epi, U, MINB, GNA, PIPE>();
   const uint64_t hot32 = tuning().hot_nodes >= 0 ? (uint64_t)tuning().hot_nodes : 49152u;
   const uint32_t l1_hot = (uint32_t)std::min<uint64_t>(hot32 * 4 / sizeof(VT), 0xFFFFFFFFull);
   fnp<<<grid, SLICE_WPB * 32, 0, s>>>(so.view<MT>(), x, e, carry, head, part1, st, l1_hot);
@@ -555,9 +592,10 @@ static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>
                         cudaEvent_t ev0, cudaEvent_t ev1, const SlicedOp* so = nullptr) {
   if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
   uint32_t npart = P.ntiles;  // partials the sweep leaves for split_rows
-  if constexpr (VAR == VAR_SLICE || VAR == VAR_SLICE64) {
-    npart = launch_slice<VT, MT, Epi, IPT, VAR == VAR_SLICE ? 6 : 8>(*so, x, e, carry, head,
-                                                                     part1, st, s);
+  if constexpr (VAR >= VAR_SLICE && VAR <= VAR_SLICEP64) {
+    constexpr int MINB = VAR == VAR_SLICE64 ? 8 : VAR == VAR_SLICEP ? 5 : VAR == VAR_SLICEP64 ? 4 : 6;
+    constexpr bool PIPE = VAR == VAR_SLICEP || VAR == VAR_SLICEP64;
+    npart = launch_slice<VT, MT, Epi, IPT, MINB, PIPE>(*so, x, e, carry, head, part1, st, s);
     KNB_LAUNCH("slice_spmv");
     if (ev1) KNB_CUDA(cudaEventRecord(ev1, s));
     split_rows<VT, Epi><<<g2, SPMV_THREADS, 0, s>>>(so->split.get(), so->nsplit, so->nshort,
@@ -706,6 +744,12 @@ static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
       return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICE, 4>(pv, ju)
                       : pick_pv<VT, MT, EXACT, VAR_SLICE, 8>(pv, ju);
     case VAR_SLICE64: return pick_pv<VT, MT, EXACT, VAR_SLICE64, 4>(pv, ju);
+    case VAR_SLICEP:
+      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEP, 4>(pv, ju)
+                      : pick_pv<VT, MT, EXACT, VAR_SLICEP, 8>(pv, ju);
+    case VAR_SLICEP64:
+      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEP64, 4>(pv, ju)
+                      : pick_pv<VT, MT, EXACT, VAR_SLICEP64, 8>(pv, ju);
     default: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP>(ipt, pv, ju);
   }
 }
@@ -783,6 +827,8 @@ static SweepFn pick_refine(int var, int ipt, bool pv, bool ju) {
   switch (var) {
     case VAR_SLICE: return pick_refine_pv<VAR_SLICE, 4>(pv, ju);
     case VAR_SLICE64: return pick_refine_pv<VAR_SLICE64, 4>(pv, ju);
+    case VAR_SLICEP: return pick_refine_pv<VAR_SLICEP, 4>(pv, ju);
+    case VAR_SLICEP64: return pick_refine_pv<VAR_SLICEP64, 4>(pv, ju);
     case VAR_WARP: return pick_refine_ipt<VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_refine_ipt<VAR_WARP4>(ipt, pv, ju);
     case VAR_WARPL1: return pick_refine_ipt<VAR_WARPL1>(ipt, pv, ju);
@@ -804,6 +850,8 @@ static AnchorFn pick_anchor(int var, int ipt, bool pv, bool ju) {
   switch (var) {
     case VAR_SLICE: return pick_anchor_pv<MT, VAR_SLICE, 4>(pv, ju);
     case VAR_SLICE64: return pick_anchor_pv<MT, VAR_SLICE64, 4>(pv, ju);
+    case VAR_SLICEP: return pick_anchor_pv<MT, VAR_SLICEP, 4>(pv, ju);
+    case VAR_SLICEP64: return pick_anchor_pv<MT, VAR_SLICEP64, 4>(pv, ju);
     case VAR_WARP: return pick_anchor_ipt<MT, VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_anchor_ipt<MT, VAR_WARP4>(ipt, pv, ju);
     default: return pick_anchor_ipt<MT, VAR_WARP16>(ipt, pv, ju);
@@ -995,7 +1043,7 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   // warps per SM): wider ones spill at their register budget.
   if (sl) {
     ipt64 = 4;
-    if (var32 == VAR_SLICE64 || ipt32 != 4) ipt32 = var32 == VAR_SLICE64 ? 4 : 8;
+    if (slice64_variant(var32) || ipt32 != 4) ipt32 = slice64_variant(var32) ? 4 : 8;
   }
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
   // Sliced layout: pieces of long rows a multiple of the resident warps at
