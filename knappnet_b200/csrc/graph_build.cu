@@ -773,11 +773,16 @@ const SlicedOp& Operator::sliced(uint32_t lw, uint32_t pieces, cudaStream_t s) {
                            cudaMemcpyDeviceToDevice, s));
   r->lcols.alloc(std::max<size_t>(r->long_arcs, 1));
   r->scols.alloc(std::max<uint64_t>(r->slice_elems, 1));
+  // slice padding (lanes shorter than their slice's first row) holds column
+  // 0 and value 0; sweeps may load it but never gather or add it
+  KNB_CUDA(cudaMemsetAsync(r->scols.get(), 0, r->scols.bytes(), s));
   if (has_vals) {
     r->lvals64.alloc(std::max<size_t>(r->long_arcs, 1));
     r->lvals32.alloc(std::max<size_t>(r->long_arcs, 1));
     r->svals64.alloc(std::max<uint64_t>(r->slice_elems, 1));
     r->svals32.alloc(std::max<uint64_t>(r->slice_elems, 1));
+    KNB_CUDA(cudaMemsetAsync(r->svals64.get(), 0, r->svals64.bytes(), s));
+    KNB_CUDA(cudaMemsetAsync(r->svals32.get(), 0, r->svals32.bytes(), s));
   }
   if (nnz) {
     const int cbits = std::max(1, bits_for(n));
