@@ -478,11 +478,12 @@ def set_sweep_timing(on: bool) -> None:
 
 
 TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT, \
-    TUNE_EGO_THREADS, TUNE_HOT_NODES, TUNE_PERSISTENT, TUNE_REFINE, TUNE_LONG_ROW = \
-    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
+    TUNE_EGO_THREADS, TUNE_HOT_NODES, TUNE_PERSISTENT, TUNE_REFINE, TUNE_LONG_ROW, \
+    TUNE_SMEM_HOT = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
 # sweep kernels (TUNE_VARIANT): merge-path warp tiles with L1-filtered
-# gathers, and the sliced layout at 48 and 64 resident warps per SM
-VARIANT_WARP_L1, VARIANT_SLICE, VARIANT_SLICE64 = 8, 9, 10
+# gathers; the sliced layout at 48 and 64 resident warps per SM, and with the
+# most gathered values in shared memory
+VARIANT_WARP_L1, VARIANT_SLICE, VARIANT_SLICE64, VARIANT_SLICE_SMEM = 8, 9, 10, 11
 
 
 def set_tuning(key: int, value: float) -> None:

@@ -1169,7 +1169,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (!(value >= 0 && value <= 12) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 11) || value != (int)value) return 1;
       t.variant = (int)value;
       return 0;
     case 5:
@@ -1195,6 +1195,10 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 10:
       if (!(value >= 0 && value <= 65535) || value != (int)value) return 1;
       t.long_row = (int)value;
+      return 0;
+    case 11:
+      if (!(value >= -1 && value <= 1048576) || value != (int)value) return 1;
+      t.smem_hot = (int64_t)value;
       return 0;
     default:
       return 1;

@@ -500,10 +500,9 @@ enum SweepVariant : int {
   VAR_WARPL1 = 8, // 16 warps per CTA; only gathers of the most gathered columns allocate in L1
   VAR_SLICE = 9,    // sliced layout (slice.cuh), 48 resident warps per SM
   VAR_SLICE64 = 10, // sliced layout, 64 resident warps per SM
-  VAR_SLICEP = 11,  // sliced layout, pipelined loads, 40 resident warps per SM
-  VAR_SLICEP64 = 12,  // sliced layout, pipelined loads, 32 resident warps per SM
+  VAR_SLICEH = 11,  // sliced layout, one 32-warp CTA per SM, most gathered values in shared memory
 };
-static bool slice_variant(int var) { return var >= VAR_SLICE && var <= VAR_SLICEP64; }
+static bool slice_variant(int var) { return var >= VAR_SLICE && var <= VAR_SLICEH; }
 static bool slice64_variant(int var) { return var == VAR_SLICE64; }
 
 // SM count and the largest dynamic shared memory a CTA may opt into, per
@@ -542,47 +541,57 @@ static uint32_t hot_nodes(uint32_t n, size_t warp_bytes, int smem_optin) {
 // One merge-path sweep with epilogue `e`: the sweep kernel of variant VAR
 // gathering x, then the split-row kernel, whose CTAs also reduce the
 // epilogue's per-tile scalars and whose last CTA decides convergence.
-// CTAs of a sliced sweep that fit on the device at once (per device).
-template <class VT, class MT, class Epi, int U, int MINB, int GNA, bool PIPE>
-static unsigned slice_grid() {
+// CTAs of a sliced sweep that fit on the device at once (per device and
+// shared-memory size).
+template <class VT, class MT, class Epi, int U, int WPB, int MINB, int GNA>
+static unsigned slice_grid(size_t smem) {
   static std::mutex mu;
-  static std::map<int, unsigned> grids;
+  static std::map<std::pair<int, size_t>, unsigned> grids;
   int dev = 0;
   KNB_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  auto it = grids.find(dev);
+  const auto key = std::make_pair(dev, smem);
+  auto it = grids.find(key);
   if (it != grids.end()) return it->second;
   int per_sm = 0;
-  if constexpr (PIPE)
-    KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, slice_spmv_p<VT, MT, Epi, U, MINB, GNA>, SLICE_WPB * 32, 0));
-  else
-    KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, slice_spmv<VT, MT, Epi, U, MINB, GNA>, SLICE_WPB * 32, 0));
+  KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, slice_spmv<VT, MT, Epi, U, WPB, MINB, GNA>, WPB * 32, smem));
   const unsigned g = (unsigned)std::max(1, per_sm) * (unsigned)device_limits().sms;
-  grids[dev] = g;
+  grids[key] = g;
   return g;
 }
 
-// Sliced sweeps: a persistent grid of the CTAs that fit at once. The kernel
-// uses no shared memory, so it asks for the smallest carveout: L1 keeps the
-// SM's whole 256 KB. Only gathers of the most gathered columns allocate in
-// L1: 49,152 FP32 values (192 KB) by default, as many bytes of FP64 values
-// (measured on R-MAT 24: no L1 allocation at all makes the FP32 sweep 1.36
-// ms instead of 0.83 ms; 24,576, 98,304 or every column 0.86-0.88 ms).
-template <class VT, class MT, class Epi, int U, int MINB, bool PIPE>
+// Sliced sweeps: a persistent grid of the CTAs that fit at once. Only
+// gathers of the most gathered columns allocate in L1: 49,152 FP32 values
+// (192 KB) by default, as many bytes of FP64 values (measured on R-MAT 24:
+// no L1 allocation at all makes the FP32 sweep 1.36 ms instead of 0.83 ms;
+// 24,576, 98,304 or every column 0.86-0.88 ms). Without a shared-memory
+// tier the kernel asks for the smallest carveout, so L1 keeps the SM's whole
+// 256 KB; with one (HOT), one CTA per SM keeps the first smem_n values of
+// the iterate in shared memory and the carveout is what that needs.
+template <class VT, class MT, class Epi, int U, int MINB, bool HOT>
 static unsigned launch_slice(const SlicedOp& so, const VT* x, const Epi& e, VT* carry, VT* head,
                              double* part1, IterState* st, cudaStream_t s) {
   constexpr int GNA = 2;
-  void (*fnp)(SliceView<MT>, const VT*, Epi, VT*, VT*, double*, const IterState*, uint32_t);
-  if constexpr (PIPE) fnp = slice_spmv_p<VT, MT, Epi, U, MINB, GNA>;
-  else fnp = slice_spmv<VT, MT, Epi, U, MINB, GNA>;
-  set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-  const unsigned grid = slice_grid<VT, MT, Epi, U, MINB, GNA, PIPE>();
+  constexpr int WPB = HOT ? SLICE_HOT_WPB : SLICE_WPB;
+  auto fnp = slice_spmv<VT, MT, Epi, U, WPB, HOT ? 1 : MINB, GNA>;
+  uint32_t smem_n = 0;
+  if constexpr (HOT) {
+    const int64_t want = tuning().smem_hot >= 0 ? tuning().smem_hot : 32768;
+    const uint64_t cap = (uint64_t)(device_limits().smem_optin - 1024) / sizeof(VT);
+    uint64_t hn = std::min<uint64_t>({(uint64_t)want * 4 / sizeof(VT), cap, (uint64_t)so.n});
+    hn -= hn % (16 / sizeof(VT));
+    smem_n = (uint32_t)hn;
+  }
+  const size_t smem = (size_t)smem_n * sizeof(VT);
+  if (smem) set_func_attr((const void*)fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int carve = smem ? std::min(100, (int)((smem + 1024) * 100 / 233472) + 1) : 0;
+  set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  const unsigned grid = slice_grid<VT, MT, Epi, U, WPB, HOT ? 1 : MINB, GNA>(smem);
   const uint64_t hot32 = tuning().hot_nodes >= 0 ? (uint64_t)tuning().hot_nodes : 49152u;
   const uint32_t l1_hot = (uint32_t)std::min<uint64_t>(hot32 * 4 / sizeof(VT), 0xFFFFFFFFull);
-  fnp<<<grid, SLICE_WPB * 32, 0, s>>>(so.view<MT>(), x, e, carry, head, part1, st, l1_hot);
-  return grid * SLICE_WPB;
+  fnp<<<grid, WPB * 32, smem, s>>>(so.view<MT>(), x, e, carry, head, part1, st, l1_hot, smem_n);
+  return grid * WPB;
 }
 
 template <class VT, class MT, class Epi, int VAR, int IPT>
@@ -592,10 +601,10 @@ static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>
                         cudaEvent_t ev0, cudaEvent_t ev1, const SlicedOp* so = nullptr) {
   if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
   uint32_t npart = P.ntiles;  // partials the sweep leaves for split_rows
-  if constexpr (VAR >= VAR_SLICE && VAR <= VAR_SLICEP64) {
-    constexpr int MINB = VAR == VAR_SLICE64 ? 8 : VAR == VAR_SLICEP ? 5 : VAR == VAR_SLICEP64 ? 4 : 6;
-    constexpr bool PIPE = VAR == VAR_SLICEP || VAR == VAR_SLICEP64;
-    npart = launch_slice<VT, MT, Epi, IPT, MINB, PIPE>(*so, x, e, carry, head, part1, st, s);
+  if constexpr (VAR >= VAR_SLICE && VAR <= VAR_SLICEH) {
+    constexpr int MINB = VAR == VAR_SLICE64 ? 8 : 6;
+    npart = launch_slice<VT, MT, Epi, IPT, MINB, VAR == VAR_SLICEH>(*so, x, e, carry, head,
+                                                                    part1, st, s);
     KNB_LAUNCH("slice_spmv");
     if (ev1) KNB_CUDA(cudaEventRecord(ev1, s));
     split_rows<VT, Epi><<<g2, SPMV_THREADS, 0, s>>>(so->split.get(), so->nsplit, so->nshort,
@@ -744,12 +753,9 @@ static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
       return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICE, 4>(pv, ju)
                       : pick_pv<VT, MT, EXACT, VAR_SLICE, 8>(pv, ju);
     case VAR_SLICE64: return pick_pv<VT, MT, EXACT, VAR_SLICE64, 4>(pv, ju);
-    case VAR_SLICEP:
-      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEP, 4>(pv, ju)
-                      : pick_pv<VT, MT, EXACT, VAR_SLICEP, 8>(pv, ju);
-    case VAR_SLICEP64:
-      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEP64, 4>(pv, ju)
-                      : pick_pv<VT, MT, EXACT, VAR_SLICEP64, 8>(pv, ju);
+    case VAR_SLICEH:
+      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEH, 4>(pv, ju)
+                      : pick_pv<VT, MT, EXACT, VAR_SLICEH, 8>(pv, ju);
     default: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP>(ipt, pv, ju);
   }
 }
@@ -827,8 +833,7 @@ static SweepFn pick_refine(int var, int ipt, bool pv, bool ju) {
   switch (var) {
     case VAR_SLICE: return pick_refine_pv<VAR_SLICE, 4>(pv, ju);
     case VAR_SLICE64: return pick_refine_pv<VAR_SLICE64, 4>(pv, ju);
-    case VAR_SLICEP: return pick_refine_pv<VAR_SLICEP, 4>(pv, ju);
-    case VAR_SLICEP64: return pick_refine_pv<VAR_SLICEP64, 4>(pv, ju);
+    case VAR_SLICEH: return pick_refine_pv<VAR_SLICEH, 4>(pv, ju);
     case VAR_WARP: return pick_refine_ipt<VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_refine_ipt<VAR_WARP4>(ipt, pv, ju);
     case VAR_WARPL1: return pick_refine_ipt<VAR_WARPL1>(ipt, pv, ju);
@@ -850,8 +855,7 @@ static AnchorFn pick_anchor(int var, int ipt, bool pv, bool ju) {
   switch (var) {
     case VAR_SLICE: return pick_anchor_pv<MT, VAR_SLICE, 4>(pv, ju);
     case VAR_SLICE64: return pick_anchor_pv<MT, VAR_SLICE64, 4>(pv, ju);
-    case VAR_SLICEP: return pick_anchor_pv<MT, VAR_SLICEP, 4>(pv, ju);
-    case VAR_SLICEP64: return pick_anchor_pv<MT, VAR_SLICEP64, 4>(pv, ju);
+    case VAR_SLICEH: return pick_anchor_pv<MT, VAR_SLICEH, 4>(pv, ju);
     case VAR_WARP: return pick_anchor_ipt<MT, VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_anchor_ipt<MT, VAR_WARP4>(ipt, pv, ju);
     default: return pick_anchor_ipt<MT, VAR_WARP16>(ipt, pv, ju);

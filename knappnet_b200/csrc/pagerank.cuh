@@ -50,6 +50,7 @@ struct Tuning {
   int persistent = 1;     // warp-tile sweeps: 1 launches only the CTAs that fit at once
   int refine = 1;         // mixed: 1 anchor + refinement sweeps, 0 plain FP64 sweeps
   int long_row = 0;       // sliced sweeps: rows of at least this many arcs are long (0: 255)
+  int64_t smem_hot = -1;  // sliced sweeps with a shared-memory tier: FP32 values kept there (-1: 32768)
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

@@ -31,7 +31,8 @@
 
 namespace knb {
 
-constexpr int SLICE_WPB = 8;  // warps per CTA of the sliced sweep
+constexpr int SLICE_WPB = 8;  // warps per CTA of the sliced sweep (no shared-memory tier)
+constexpr int SLICE_HOT_WPB = 32;  // warps per CTA with the shared-memory tier (one CTA per SM)
 
 // Device view of a sliced operator.
 template <class MT>
@@ -54,10 +55,13 @@ struct SliceView {
 
 // Gather of the iterate with the L2 keep policy; GNA 2 lets only columns
 // below l1_hot allocate in L1 (the most gathered values stay there while
-// one-off gathers pass through), GNA 0 allocates every gather.
+// one-off gathers pass through), GNA 0 allocates every gather. With a
+// shared-memory tier (smem non-null) columns below smem_n come from there.
 template <int GNA, class VT>
 __device__ __forceinline__ VT slice_gather(const VT* xg, uint32_t c, uint32_t l1_hot,
-                                           uint64_t pol) {
+                                           uint64_t pol, const VT* smem = nullptr,
+                                           uint32_t smem_n = 0) {
+  if (smem != nullptr && c < smem_n) return smem[c];
   if constexpr (GNA == 2) return c < l1_hot ? ld_keep(xg + c, pol) : ld_keep_na(xg + c, pol);
   else return ld_keep(xg + c, pol);
 }
@@ -73,7 +77,8 @@ __device__ __forceinline__ VT slice_mul(const MT* vals, MT w, VT x) {
 template <class VT, class MT, int U, int GNA>
 __device__ __forceinline__ VT slice_long_sum(const SliceView<MT>& op, const VT* __restrict__ xg,
                                              uint32_t lo, uint32_t hi, int lane, uint32_t l1_hot,
-                                             uint64_t pol_stream, uint64_t pol_keep) {
+                                             uint64_t pol_stream, uint64_t pol_keep,
+                                             const VT* smem, uint32_t smem_n) {
   VT s = VT(0);
   for (uint32_t k0 = (lo & ~31u) + (uint32_t)lane; k0 < hi; k0 += 32u * U) {
     uint32_t c[U];
@@ -89,7 +94,8 @@ __device__ __forceinline__ VT slice_long_sum(const SliceView<MT>& op, const VT* 
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const uint32_t k = k0 + 32u * u;
-      x[u] = (k >= lo && k < hi) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep) : VT(0);
+      x[u] = (k >= lo && k < hi) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep, smem, smem_n)
+                                 : VT(0);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) s += slice_mul<VT, MT>(op.lvals, w[u], x[u]);
@@ -99,16 +105,29 @@ __device__ __forceinline__ VT slice_long_sum(const SliceView<MT>& op, const VT* 
 
 // One sweep: every warp first takes pieces t = global warp, + all warps,
 // then slices the same way, and leaves one partial of the epilogue's
-// scalars at part[global warp] (all warps of the grid write one).
-template <class VT, class MT, class Epi, int U, int MINB, int GNA>
-__global__ void __launch_bounds__(SLICE_WPB * 32, MINB)
+// scalars at part[global warp] (all warps of the grid write one). With
+// smem_n > 0 each CTA first copies x[0, smem_n) (the most gathered values;
+// smem_n a multiple of 16 / sizeof(VT)) into shared memory, and gathers of
+// those columns read it there instead of sending a request to L1 and L2.
+template <class VT, class MT, class Epi, int U, int WPB, int MINB, int GNA>
+__global__ void __launch_bounds__(WPB * 32, MINB)
 slice_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __restrict__ carry,
            VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st,
-           uint32_t l1_hot) {
+           uint32_t l1_hot, uint32_t smem_n) {
   if (st && iteration_done(st)) return;
+  extern __shared__ __align__(16) unsigned char slice_smem[];
+  const VT* hot = nullptr;
+  if (smem_n > 0) {
+    const uint4* src = reinterpret_cast<const uint4*>(xg);
+    uint4* dst = reinterpret_cast<uint4*>(slice_smem);
+    const uint32_t nvec = smem_n * (uint32_t)sizeof(VT) / 16u;
+    for (uint32_t i = threadIdx.x; i < nvec; i += WPB * 32) dst[i] = __ldg(src + i);
+    __syncthreads();
+    hot = reinterpret_cast<const VT*>(slice_smem);
+  }
   const int lane = threadIdx.x & 31;
-  const uint32_t gw = blockIdx.x * SLICE_WPB + (threadIdx.x >> 5);
-  const uint32_t nw = gridDim.x * SLICE_WPB;
+  const uint32_t gw = blockIdx.x * WPB + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * WPB;
   Epi epi = epi_in;
   epi.prepare(st);
   double acc[Epi::NACC > 0 ? Epi::NACC : 1];
@@ -124,7 +143,7 @@ slice_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __restri
     uint32_t rs = op.loff[r], re = op.loff[r + 1];
     while (true) {
       const VT sum = slice_long_sum<VT, MT, U, GNA>(op, xg, max(rs, a0), min(re, a1), lane,
-                                                    l1_hot, pol_stream, pol_keep);
+                                                    l1_hot, pol_stream, pol_keep, hot, smem_n);
       if (re > a1) {  // continues in the next piece
         if (lane == 0) carry[t] = sum;
         break;
@@ -161,173 +180,12 @@ slice_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __restri
       VT x[U];
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        x[u] = (k0 + u < len) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep) : VT(0);
+        x[u] = (k0 + u < len) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep, hot, smem_n)
+                              : VT(0);
 #pragma unroll
       for (int u = 0; u < U; ++u) s += slice_mul<VT, MT>(op.svals, w[u], x[u]);
     }
     if (r < op.n) epi.row(r, s, acc);
-  }
-  warp_store_partials<Epi>(acc, part, gw, lane);
-}
-
-// ------------------------------------------------------------- pipelined form
-// The same sweep with shorter chains of dependent loads. Measured on R-MAT
-// scale 22 the plain form waits on memory most of the time (0.8 eligible
-// warps per scheduler, no unit above 65% busy): a slice was four dependent
-// round trips (base, lengths, arcs, gathers) plus the epilogue's inputs.
-// Here a slice's width comes from its two bases, loaded one slice ahead;
-// the lane lengths, the first arcs and the epilogue's inputs are loaded
-// together; and each group of U arcs is loaded while the previous group's
-// gathers are in flight. A long row's epilogue inputs and the next row's
-// end are loaded before its sum. Arcs in a slice's padding (lanes shorter
-// than the slice's first row) are loaded but neither gathered nor added.
-
-// U arc positions k0 .. k0 + U - 1 of one slice lane; none at or past lmax.
-template <class MT, int U>
-__device__ __forceinline__ void slice_load(const SliceView<MT>& op, uint32_t base, uint32_t k0,
-                                           uint32_t lmax, uint64_t pol, uint32_t (&c)[U],
-                                           MT (&w)[U]) {
-#pragma unroll
-  for (int u = 0; u < U; ++u) {
-    const uint32_t k = k0 + u;
-    const bool ok = k < lmax;
-    c[u] = ok ? ld_stream(op.scols + base + 32u * k, pol) : 0u;
-    w[u] = (op.svals && ok) ? ld_stream(op.svals + base + 32u * k, pol) : MT(0);
-  }
-}
-
-// U arcs k0, k0 + 32, ... of a long row segment [lo, hi).
-template <class MT, int U>
-__device__ __forceinline__ void long_load(const SliceView<MT>& op, uint32_t k0, uint32_t lo,
-                                          uint32_t hi, uint64_t pol, uint32_t (&c)[U],
-                                          MT (&w)[U]) {
-#pragma unroll
-  for (int u = 0; u < U; ++u) {
-    const uint32_t k = k0 + 32u * u;
-    const bool ok = k >= lo && k < hi;
-    c[u] = ok ? ld_stream(op.lcols + k, pol) : 0u;
-    w[u] = (op.lvals && ok) ? ld_stream(op.lvals + k, pol) : MT(0);
-  }
-}
-
-template <class VT, class MT, int U, int GNA>
-__device__ __forceinline__ VT slice_long_sum_p(const SliceView<MT>& op, const VT* __restrict__ xg,
-                                               uint32_t lo, uint32_t hi, int lane,
-                                               uint32_t l1_hot, uint64_t pol_stream,
-                                               uint64_t pol_keep) {
-  VT s = VT(0);
-  uint32_t k0 = (lo & ~31u) + (uint32_t)lane;
-  uint32_t c[U];
-  MT w[U];
-  long_load<MT, U>(op, k0, lo, hi, pol_stream, c, w);
-  for (; k0 < hi; k0 += 32u * U) {
-    uint32_t cn[U];
-    MT wn[U];
-    long_load<MT, U>(op, k0 + 32u * U, lo, hi, pol_stream, cn, wn);
-    VT x[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const uint32_t k = k0 + 32u * u;
-      x[u] = (k >= lo && k < hi) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep) : VT(0);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      s += slice_mul<VT, MT>(op.lvals, w[u], x[u]);
-      c[u] = cn[u];
-      w[u] = wn[u];
-    }
-  }
-  return warp_sum(s);
-}
-
-template <class VT, class MT, class Epi, int U, int MINB, int GNA>
-__global__ void __launch_bounds__(SLICE_WPB * 32, MINB)
-slice_spmv_p(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __restrict__ carry,
-             VT* __restrict__ head, double* __restrict__ part, const IterState* __restrict__ st,
-             uint32_t l1_hot) {
-  if (st && iteration_done(st)) return;
-  const int lane = threadIdx.x & 31;
-  const uint32_t gw = blockIdx.x * SLICE_WPB + (threadIdx.x >> 5);
-  const uint32_t nw = gridDim.x * SLICE_WPB;
-  Epi epi = epi_in;
-  epi.prepare(st);
-  double acc[Epi::NACC > 0 ? Epi::NACC : 1];
-  Epi::init(acc);
-  const uint64_t pol_stream = policy_evict_first();
-  const uint64_t pol_keep = policy_evict_last();
-
-  // long rows, piece by piece
-  for (uint32_t t = gw; t < op.npieces; t += nw) {
-    const uint32_t a0 = t * op.piece;
-    const uint32_t a1 = min(a0 + op.piece, op.long_arcs);
-    uint32_t r = op.prow[t];
-    uint32_t rs = op.loff[r], re = op.loff[r + 1];
-    while (true) {
-      typename Epi::In in{};
-      if (lane == 0 && rs >= a0 && re <= a1) in = epi.fetch(r);
-      const uint32_t nre = re < a1 ? op.loff[r + 2] : 0u;  // row r + 1 exists
-      const VT sum = slice_long_sum_p<VT, MT, U, GNA>(op, xg, max(rs, a0), min(re, a1), lane,
-                                                      l1_hot, pol_stream, pol_keep);
-      if (re > a1) {  // continues in the next piece
-        if (lane == 0) carry[t] = sum;
-        break;
-      }
-      if (rs < a0) {  // began in an earlier piece, ends here
-        if (lane == 0) head[t] = sum;
-      } else if (lane == 0) {
-        epi.row_in(r, sum, in, acc);
-      }
-      if (re == a1) break;
-      ++r;
-      rs = re;
-      re = nre;
-    }
-  }
-
-  // short rows, slice by slice
-  uint32_t b0 = 0, b1 = 0;
-  if (gw < op.nslices) {
-    b0 = op.sbase[gw];
-    b1 = op.sbase[gw + 1];
-  }
-  for (uint32_t sl = gw; sl < op.nslices; sl += nw) {
-    uint32_t nb0 = 0, nb1 = 0;
-    if (sl + nw < op.nslices) {
-      nb0 = op.sbase[sl + nw];
-      nb1 = op.sbase[sl + nw + 1];
-    }
-    const uint32_t r = op.n_long + sl * 32u + (uint32_t)lane;
-    const bool valid = r < op.n;
-    const uint32_t lmax = (b1 - b0) >> 5;
-    const uint32_t base = b0 + (uint32_t)lane;
-    typename Epi::In in{};
-    uint32_t len = 0;
-    if (valid) {
-      in = epi.fetch(r);
-      len = op.slen[r - op.n_long];
-    }
-    uint32_t c[U];
-    MT w[U];
-    slice_load<MT, U>(op, base, 0, lmax, pol_stream, c, w);
-    VT s = VT(0);
-    for (uint32_t k0 = 0; k0 < lmax; k0 += U) {
-      uint32_t cn[U];
-      MT wn[U];
-      slice_load<MT, U>(op, base, k0 + U, lmax, pol_stream, cn, wn);
-      VT x[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        x[u] = (k0 + u < len) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep) : VT(0);
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (k0 + u < len) s += slice_mul<VT, MT>(op.svals, w[u], x[u]);
-        c[u] = cn[u];
-        w[u] = wn[u];
-      }
-    }
-    if (valid) epi.row_in(r, s, in, acc);
-    b0 = nb0;
-    b1 = nb1;
   }
   warp_store_partials<Epi>(acc, part, gw, lane);
 }

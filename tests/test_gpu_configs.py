@@ -12,7 +12,7 @@ the same inputs the benchmark uses:
   (plus the oracle's own normalisation residual) with the same sweep count,
   and the mixed path (FP32 sweeps, FP64 anchor, refinement sweeps) within
   1e-9 L1 with the same top-100 order; for the merge-path sweep and for the
-  sliced sweep;
+  sliced sweep (the default);
 - C4a: batched personalised PageRank on R-MAT scale 22 with 256 teleport
   vectors of 1-64 seed nodes: sampled columns within 1e-9 L1 of their own
   oracle calls.
@@ -75,7 +75,7 @@ def c3_graph():
     g.close()
 
 
-@pytest.mark.parametrize("variant", [0, K.VARIANT_SLICE])
+@pytest.mark.parametrize("variant", [K.VARIANT_WARP_L1, 0])
 def test_c3_rmat24_fp64_and_mixed_match_oracle(c3_graph, variant):
     g, ref, iters = c3_graph
     try:
