@@ -1043,11 +1043,11 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
     if (!refine_variant(var64)) var64 = VAR_WARP16;
     ipt64 = ipt64 == 8 ? 8 : 4;
   }
-  // Sliced sweeps keep 4 gathers per lane in flight (8 in FP32 sweeps at 48
-  // warps per SM): wider ones spill at their register budget.
+  // Sliced sweeps keep 4 arcs per lane in flight (8 in FP32 sweeps only when
+  // asked for: 0.83 against 0.81 ms on R-MAT 24; wider ones spill).
   if (sl) {
     ipt64 = 4;
-    if (slice64_variant(var32) || ipt32 != 4) ipt32 = slice64_variant(var32) ? 4 : 8;
+    ipt32 = (ipt32 == 8 && prm.ipt == 8 && !slice64_variant(var32)) ? 8 : 4;
   }
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
   // Sliced layout: pieces of long rows a multiple of the resident warps at
