@@ -47,6 +47,7 @@ def lib() -> ctypes.CDLL:
     L.orc_gnm.argtypes = [i64, i64, i32, i32, u64, u64, vp, vp, cp, sz]
     L.orc_gnm.restype = i32
     L.orc_rmat.argtypes = [i32, i64, f64, f64, f64, u64, vp, vp]
+    L.orc_lognormal.argtypes = [i64, u64, vp]
     L.orc_graph_new.argtypes = [i64, vp, vp, vp, i64, i32, ctypes.POINTER(vp), cp, sz]
     L.orc_graph_new.restype = i32
     L.orc_graph_free.argtypes = [vp]
@@ -126,6 +127,32 @@ def rmat_raw(scale: int, m: int, a: float, b: float, c: float, seed: int):
     t = np.zeros(m, dtype=np.uint32)
     lib().orc_rmat(scale, m, a, b, c, seed, _ptr(s), _ptr(t))
     return s, t
+
+
+def rmat(scale: int, edge_factor: int, a: float, b: float, c: float, seed: int,
+         clean: bool = True, symmetrize: bool = False):
+    """R-MAT edges as the library's generator makes them: raw draws, or with
+    self-loops and duplicate arcs removed (edges sorted by (source, target));
+    symmetrize keeps each unordered pair once as (smaller, larger)."""
+    s, t = rmat_raw(scale, edge_factor << scale, a, b, c, seed)
+    if not clean and not symmetrize:
+        return s, t
+    keep = s != t
+    s, t = s[keep].astype(np.int64), t[keep].astype(np.int64)
+    if symmetrize:
+        s, t = np.minimum(s, t), np.maximum(s, t)
+    key = np.sort(s << scale | t)
+    if len(key):
+        key = key[np.concatenate(([True], key[1:] != key[:-1]))]
+    return (key >> scale).astype(np.uint32), (key & ((1 << scale) - 1)).astype(np.uint32)
+
+
+def lognormal(m: int, seed: int) -> np.ndarray:
+    """Lognormal(0, 1) strengths of edges 0 .. m - 1 rounded to FP32, as the
+    library's generator draws them (Box-Muller on stream (seed, edge))."""
+    w = np.zeros(m, dtype=np.float32)
+    lib().orc_lognormal(m, seed, _ptr(w))
+    return w
 
 
 class Graph:

@@ -5,8 +5,11 @@
 // library with identical arguments. Status 0 is success; on failure 1 is
 // returned and a message is written to err (crates/capi/src/lib.rs:57-87).
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <exception>
+#include <thread>
+#include <vector>
 
 #include "oracle.hpp"
 
@@ -39,6 +42,19 @@ static int32_t guard(char* err, size_t len, F f) {
 static const Graph& handle(const OrcGraph* h) {
   if (!h) throw Error{"graph handle is null"};
   return h->g;
+}
+
+// Runs f(lo, hi) over [0, count) in contiguous blocks on every host core;
+// every element depends on its own index only, so results do not depend on
+// the thread count.
+template <class F>
+static void for_blocks(int64_t count, F f) {
+  const int64_t nt = std::max<int64_t>(
+      1, std::min<int64_t>(std::thread::hardware_concurrency(), (count + 65535) / 65536));
+  std::vector<std::thread> pool;
+  for (int64_t t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] { f(count * t / nt, count * (t + 1) / nt); });
+  for (auto& th : pool) th.join();
 }
 
 extern "C" {
@@ -76,19 +92,38 @@ void orc_rmat(int32_t scale, int64_t m, double a, double b, double c, uint64_t s
   const double two32 = 4294967296.0;
   uint64_t ta = (uint64_t)(a * two32), tab = (uint64_t)((a + b) * two32),
            tabc = (uint64_t)((a + b + c) * two32);
-  for (int64_t k = 0; k < m; ++k) {
-    Stream s(seed, (uint64_t)k);
-    uint32_t r = 0, q = 0;
-    for (int l = 0; l < scale; ++l) {
-      uint64_t u = s.next_u32();
-      uint32_t rb = u >= tab ? 1u : 0u;
-      uint32_t cb = (u >= ta && u < tab) || u >= tabc ? 1u : 0u;
-      r = r << 1 | rb;
-      q = q << 1 | cb;
+  for_blocks(m, [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k) {
+      Stream s(seed, (uint64_t)k);
+      uint32_t r = 0, q = 0;
+      for (int l = 0; l < scale; ++l) {
+        uint64_t u = s.next_u32();
+        uint32_t rb = u >= tab ? 1u : 0u;
+        uint32_t cb = (u >= ta && u < tab) || u >= tabc ? 1u : 0u;
+        r = r << 1 | rb;
+        q = q << 1 | cb;
+      }
+      src[k] = r;
+      tgt[k] = q;
     }
-    src[k] = r;
-    tgt[k] = q;
-  }
+  });
+}
+
+// Lognormal(0, 1) strengths rounded to FP32, as this project defines them:
+// for edge e the first four words of stream (seed, e) make two 53-bit
+// uniforms u1, u2 in [0, 1), and w = exp(sqrt(-2 ln(1 - u1)) cos(2 pi u2))
+// (Box and Muller 1958).
+void orc_lognormal(int64_t m, uint64_t seed, float* w) {
+  for_blocks(m, [&](int64_t lo, int64_t hi) {
+    for (int64_t e = lo; e < hi; ++e) {
+      Stream s(seed, (uint64_t)e);
+      uint64_t r0 = s.next_u32(), r1 = s.next_u32(), r2 = s.next_u32(), r3 = s.next_u32();
+      const uint64_t a = (r0 << 32 | r1) >> 11, b = (r2 << 32 | r3) >> 11;
+      const double u1 = (double)a / 9007199254740992.0, u2 = (double)b / 9007199254740992.0;
+      const double z = std::sqrt(-2.0 * std::log(1.0 - u1)) * std::cos(6.283185307179586 * u2);
+      w[e] = (float)std::exp(z);
+    }
+  });
 }
 
 int32_t orc_graph_new(int64_t n, const int64_t* src, const int64_t* tgt, const double* weights,

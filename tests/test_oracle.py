@@ -330,6 +330,34 @@ def test_rmat_quadrant_frequencies():
     assert np.allclose(freq, [0.57, 0.19, 0.19, 0.05], atol=0.01)
 
 
+def test_rmat_cleaning_and_lognormal_strengths():
+    """The generators the benchmark's reference arm uses: cleaned R-MAT edges
+    (self-loops and duplicates removed, sorted by (source, target); or each
+    unordered pair once) and lognormal strengths from Box-Muller on the
+    edge's Philox stream, computed here one value at a time."""
+    scale = 11
+    r, q = O.rmat_raw(scale, 16 << scale, 0.57, 0.19, 0.19, seed=77)
+    keep = r != q
+    key = np.unique(r[keep].astype(np.int64) << scale | q[keep].astype(np.int64))
+    s, t = O.rmat(scale, 16, 0.57, 0.19, 0.19, 77)
+    assert np.array_equal(s, key >> scale) and np.array_equal(t, key & ((1 << scale) - 1))
+    lo = np.minimum(r, q)[keep].astype(np.int64)
+    hi = np.maximum(r, q)[keep].astype(np.int64)
+    key = np.unique(lo << scale | hi)
+    s, t = O.rmat(scale, 16, 0.57, 0.19, 0.19, 77, symmetrize=True)
+    assert np.array_equal(s, key >> scale) and np.array_equal(t, key & ((1 << scale) - 1))
+    raw = O.rmat(scale, 16, 0.57, 0.19, 0.19, 77, clean=False)
+    assert np.array_equal(raw[0], r) and np.array_equal(raw[1], q)
+    w = O.lognormal(500, 5)
+    u = np.array([O.stream_u32(5, e, 4) for e in range(500)], dtype=np.uint64)
+    a = (u[:, 0] << np.uint64(32) | u[:, 1]) >> np.uint64(11)
+    b = (u[:, 2] << np.uint64(32) | u[:, 3]) >> np.uint64(11)
+    z = (np.sqrt(-2 * np.log(1 - a.astype(np.float64) / 2.0 ** 53))
+         * np.cos(2 * np.pi * (b.astype(np.float64) / 2.0 ** 53)))
+    want = np.exp(z).astype(np.float32).astype(np.float64)
+    assert np.abs(w / want - 1).max() <= 2 ** -23
+
+
 # ------------------------------------------------------------------ Katz, Bonacich
 def katz_bonacich_known_answers(G, err):
     """The reference's hand values (crates/engine/src/metrics/spectral.rs:
