@@ -57,6 +57,18 @@ SEED, WSEED = 20240601, 20240602
 DAMPING, TOL = 0.85, 1e-9
 
 
+# sweep kernels by their tuning code (net_set_tuning key 4)
+KERNEL_NAMES = {
+    8: "warp_spmv (merge-path warp tiles on the layout renumbered by column count, 16 warps "
+       "per CTA)",
+    9: "slice_spmv (sliced layout: long rows by whole warps, the others one lane per row in "
+       "32-row slices; 48 resident warps per SM, 4 arcs per lane in flight)",
+    10: "slice_spmv (sliced layout, 64 resident warps per SM, 4 arcs per lane in flight)",
+    11: "slice_spmv (sliced layout, one 32-warp CTA per SM, most gathered values in shared "
+        "memory)",
+}
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -273,13 +285,13 @@ def run_ours(args):
     rr = roof(swr_ms, swr_n, bytesr)
     r64 = roof(sw64[1], sw64[0], sw64[2])
     # dominant kernel of the measured path: the sweep kind with most time
-    kinds = [(sw32_ms, r32, "fp32", "warp_spmv<float> FP32 sweep (persistent merge-path warp "
-                                    "tiles, 16 warps per CTA, 8 items per lane, L1 allocation "
-                                    "only for the 24,576 most gathered columns)"),
-             (swr_ms, rr, "refine", "warp_spmv<float> refinement sweep (FP32 gathers of the "
-                                  "correction, FP64 update; 16 warps per CTA, 8 items per lane)"),
-             (sw64m_ms, r64m, "fp64", "warp_spmv<double> FP64 sweep (16 warps per CTA, "
-                                      "4 items per lane)")]
+    kname = KERNEL_NAMES.get(infom.sweep_kernel, f"sweep kernel {infom.sweep_kernel}")
+    kdesc = (f"{kname}; long rows from {infom.long_row} arcs" if infom.long_row else kname) + \
+        f"; gathers of the {infom.hot_columns:,} most gathered columns allocate in L1"
+    kinds = [(sw32_ms, r32, "fp32", "FP32 sweep: " + kdesc),
+             (swr_ms, rr, "refine", "refinement sweep (FP32 gathers of the correction, FP64 "
+                                  "update): " + kdesc),
+             (sw64m_ms, r64m, "fp64", "FP64 sweep: " + kdesc)]
     _, dom, dom_kind, dom_name = max(kinds, key=lambda k: k[0])
     traffic = None
     tfile = ROOT / "profiles" / "sweep_traffic.json"
@@ -317,6 +329,14 @@ def run_ours(args):
         "fp64_path": {"value": round(float(m) * info64.iterations / fp64_time / 1e9, 3),
                       "time_to_solution_ms": round(fp64_time * 1e3, 3),
                       "sweeps": info64.iterations},
+        "sweep_kernel": {"mixed": {"kernel": int(infom.sweep_kernel),
+                                   "long_row": int(infom.long_row),
+                                   "hot_columns": int(infom.hot_columns)},
+                         "fp64": {"kernel": int(info64.sweep_kernel),
+                                  "long_row": int(info64.long_row),
+                                  "hot_columns": int(info64.hot_columns)},
+                         "picked_by": "per-operator timing of the candidates on the first "
+                                      "solve (warm-up)"},
         "mixed_path": {"time_to_solution_ms": round(mixed_time * 1e3, 3),
                        "sweeps": infom.iterations, "fp32_sweeps": infom.iterations_fp32,
                        "speedup_vs_fp64": round(fp64_time / mixed_time, 3),

@@ -182,7 +182,10 @@ typedef struct NetSolveInfo {
   int32_t kernel_launches; /* CUDA kernels the solve launched */
   double eigenvalue;
   int32_t connected;
-  int32_t reserved;
+  int32_t sweep_kernel;    /* PageRank: the sweep kernel used (net_set_tuning key 4 codes);
+                              packed graphs: threads per CTA of the launch */
+  int32_t long_row;        /* sliced sweeps: rows of at least this many arcs are long */
+  int32_t hot_columns;     /* FP32 values of the most gathered columns kept in L1 */
 } NetSolveInfo;
 
 /* Precision codes: 0 = FP64, 1 = mixed (FP32 sweeps, then FP64 sweeps on
@@ -359,7 +362,10 @@ NET_API void net_set_sweep_timing(int32_t on);
  * gathered nodes in shared memory, 32 or 16 warps per SM, 8 warp tiles whose
  * gathers allocate in L1 only for the most gathered columns, 9 and 10 the
  * sliced layout: nodes renumbered by row length, long rows by whole warps,
- * the others one lane per row, with 48 or 64 resident warps per SM); 5 = preferred
+ * the others one lane per row, with 48 or 64 resident warps per SM, 11 the
+ * sliced layout with the most gathered values in shared memory, one CTA per
+ * SM; 0 lets the library choose: on operators of at least 2^21 arcs the
+ * first solve times the candidates and keeps the fastest); 5 = preferred
  * shared-memory carveout of the sweep (-1 just what the CTAs the kernel keeps
  * resident need, 0..100 percent);
  * 6 = threads per CTA of the packed-graph PageRank (0 tuned on first use,
@@ -370,7 +376,10 @@ NET_API void net_set_sweep_timing(int32_t on);
  * looping over tiles (1, default); 9 = mixed precision ends with one FP64
  * anchor sweep and refinement sweeps that gather the FP32 correction (1,
  * default) or with FP64 sweeps (0); 10 = sliced sweeps: rows of at least
- * this many arcs (1..65535) are taken by whole warps (0: automatic).
+ * this many arcs (1..65535) are taken by whole warps (0: automatic); 11 =
+ * FP32 values kernel 11 keeps in shared memory (-1: 32,768); 12 = pick the
+ * sweep kernel per operator by timing (1, default) or always use kernel 9
+ * (0). Setting key 0, 4, 7 or 10 also bypasses the timing.
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 

@@ -46,10 +46,11 @@ class NetSolveInfo(ctypes.Structure):
                 ("change", ctypes.c_double), ("seconds", ctypes.c_double),
                 ("converged", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
                 ("eigenvalue", ctypes.c_double), ("connected", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("sweep_kernel", ctypes.c_int32), ("long_row", ctypes.c_int32),
+                ("hot_columns", ctypes.c_int32)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 def lib() -> ctypes.CDLL:
@@ -479,7 +480,7 @@ def set_sweep_timing(on: bool) -> None:
 
 TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT, \
     TUNE_EGO_THREADS, TUNE_HOT_NODES, TUNE_PERSISTENT, TUNE_REFINE, TUNE_LONG_ROW, \
-    TUNE_SMEM_HOT = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+    TUNE_SMEM_HOT, TUNE_AUTOTUNE = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12
 # sweep kernels (TUNE_VARIANT): merge-path warp tiles with L1-filtered
 # gathers; the sliced layout at 48 and 64 resident warps per SM, and with the
 # most gathered values in shared memory

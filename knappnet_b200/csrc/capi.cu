@@ -382,6 +382,9 @@ static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t direc
       info->seconds = pi.seconds;
       info->converged = pi.converged;
       info->kernel_launches = pi.kernel_launches;
+      info->sweep_kernel = pi.sweep_kernel;
+      info->long_row = pi.long_row;
+      info->hot_columns = pi.hot_columns;
     }
   });
 }
@@ -919,7 +922,7 @@ int32_t net_pagerank_graphs(const GraphHandle* h, int64_t count, const int64_t* 
       info->seconds = r.seconds;
       info->converged = 1;
       info->kernel_launches = 1;
-      info->reserved = r.threads;
+      info->sweep_kernel = r.threads;  // threads per CTA of the packed launch
     }
   });
 }
@@ -1002,6 +1005,9 @@ int32_t net_pagerank_weights_device(const GraphHandle* h, const double* d_weight
       info->seconds = pi.seconds;
       info->converged = pi.converged;
       info->kernel_launches = pi.kernel_launches;
+      info->sweep_kernel = pi.sweep_kernel;
+      info->long_row = pi.long_row;
+      info->hot_columns = pi.hot_columns;
     }
   });
 }
@@ -1199,6 +1205,10 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 11:
       if (!(value >= -1 && value <= 1048576) || value != (int)value) return 1;
       t.smem_hot = (int64_t)value;
+      return 0;
+    case 12:
+      if (value != 0 && value != 1) return 1;
+      t.autotune = (int)value;
       return 0;
     default:
       return 1;

@@ -100,6 +100,17 @@ struct SlicedOp {
   }
 };
 
+// The PageRank sweep a tuner picked for an operator: kernel (tuning key 4
+// codes), long-row threshold of the sliced layout, columns whose gathers
+// allocate in L1 (in FP32 values), and its measured time per sweep.
+struct SweepPick {
+  int32_t variant = 0;
+  int32_t long_row = 0;
+  int32_t ipt = 0;
+  int64_t hot = -1;
+  double ms = 0;
+};
+
 // Per-operator scratch a solver keeps between calls (iterates, partials,
 // events), so a call allocates nothing once warm.
 struct Workspace {
@@ -127,6 +138,7 @@ struct Operator {
   const DevCsr* trans = nullptr;  // adjacency whose row lengths are this operator's column counts
   std::unique_ptr<Relabeled> relabel;
   std::map<std::pair<uint32_t, uint32_t>, std::unique_ptr<SlicedOp>> sliced_ops;  // (lw, pieces)
+  std::map<int, SweepPick> pr_pick;  // PageRank's tuned sweep per precision class (pagerank.cu), under mu
   std::unique_ptr<Workspace> pr_ws;  // PageRank's (pagerank.cu), created on first use
   std::unique_ptr<Workspace> eig_ws;  // eigenvector centrality's (eigen.cu), created on first use
   std::unique_ptr<Workspace> hits_ws;  // hubs and authorities' (eigen.cu), created on first use

@@ -505,6 +505,17 @@ enum SweepVariant : int {
 static bool slice_variant(int var) { return var >= VAR_SLICE && var <= VAR_SLICEH; }
 static bool slice64_variant(int var) { return var == VAR_SLICE64; }
 
+// Columns whose gathers allocate in L1 (FP32 values): the tuned choice of the
+// solve running on this thread, else the process-wide tuning (-1: each
+// kernel's default).
+static thread_local int64_t g_hot_override = -1;
+static int64_t hot_setting() { return g_hot_override >= 0 ? g_hot_override : tuning().hot_nodes; }
+struct HotOverride {
+  int64_t saved;
+  explicit HotOverride(int64_t v) : saved(g_hot_override) { g_hot_override = v; }
+  ~HotOverride() { g_hot_override = saved; }
+};
+
 // SM count and the largest dynamic shared memory a CTA may opt into, per
 // device (queried once).
 struct DeviceLimits {
@@ -588,7 +599,7 @@ static unsigned launch_slice(const SlicedOp& so, const VT* x, const Epi& e, VT* 
   const int carve = smem ? std::min(100, (int)((smem + 1024) * 100 / 233472) + 1) : 0;
   set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
   const unsigned grid = slice_grid<VT, MT, Epi, U, WPB, HOT ? 1 : MINB, GNA>(smem);
-  const uint64_t hot32 = tuning().hot_nodes >= 0 ? (uint64_t)tuning().hot_nodes : 49152u;
+  const uint64_t hot32 = hot_setting() >= 0 ? (uint64_t)hot_setting() : 49152u;
   const uint32_t l1_hot = (uint32_t)std::min<uint64_t>(hot32 * 4 / sizeof(VT), 0xFFFFFFFFull);
   fnp<<<grid, WPB * 32, smem, s>>>(so.view<MT>(), x, e, carry, head, part1, st, l1_hot, smem_n);
   return grid * WPB;
@@ -679,9 +690,9 @@ static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>
       grid = std::min(grid, cap);
     }
     // L1-allocating gathers only below this column (GNA 2)
-    const uint32_t l1_hot = tuning().hot_nodes >= 0 ? (uint32_t)std::min<int64_t>(
-                                                          tuning().hot_nodes, 0xFFFFFFFFll)
-                                                    : 24576u;
+    const uint32_t l1_hot = hot_setting() >= 0 ? (uint32_t)std::min<int64_t>(
+                                                     hot_setting(), 0xFFFFFFFFll)
+                                               : 24576u;
     npart = std::min<uint32_t>(P.ntiles, grid * WPB);
     warp_spmv<VT, MT, Epi, IPT, WPB, GNA><<<grid, WPB * 32, smem, s>>>(
         v, x, e, P.coords.get(), P.ntiles, carry, head,
@@ -998,6 +1009,126 @@ void pagerank(GraphHandleImpl& g, const PagerankParams& prm, double* out, bool o
   pagerank_op(op, prm, out, out_on_device, info, s);
 }
 
+// The operator's PageRank workspace (created on first use).
+static PrWorkspace& pr_workspace(Operator& op) {
+  std::lock_guard<std::mutex> lock(op.mu);
+  if (!op.pr_ws) op.pr_ws = std::make_unique<PrWorkspace>();
+  return *static_cast<PrWorkspace*>(op.pr_ws.get());
+}
+
+// Pieces of the sliced layout's long rows: a multiple of the resident warps
+// at 48 and at 64 warps per SM (192 per SM), so every warp gets as many.
+static uint32_t slice_pieces() { return 192u * (uint32_t)device_limits().sms; }
+
+// Milliseconds per sweep of candidate c on operator op: FP32 sweeps (class
+// 0, the FP32 phase of mixed solves) or FP64 sweeps (class 1, FP64 solves),
+// from the uniform start, the mean of two sweeps after one untimed sweep.
+// The state never converges (tolerance -1), so every sweep does its work;
+// the solve that follows starts over from its own initial state. Runs
+// under the workspace's lock.
+static double time_candidate(Operator& op, const SweepPick& c, int cls, bool use32v,
+                             PrWorkspace& ws, cudaStream_t s) {
+  HotOverride hot(c.hot);
+  const bool sl = slice_variant(c.variant);
+  const SlicedOp* SO = sl ? &op.sliced((uint32_t)c.long_row, slice_pieces(), s) : nullptr;
+  const Relabeled* R = sl ? nullptr : &op.relabeled(s);
+  const int ipt = (cls == 0 && !sl) ? 8 : 4;
+  static const Partition no_partition;
+  const Partition* P = sl ? &no_partition : &op.relabeled_partition(tile_items(c.variant, ipt), s);
+  const uint32_t nt = sl ? std::max<uint32_t>(SO->npieces + 1, 64u * (uint32_t)device_limits().sms)
+                         : P->ntiles;
+  ws.ensure(op.n, nt, cls == 0, cls == 1, false);
+  IterState* st = ws.st.get();
+  IterState init{};
+  init.tol = -1.0;
+  init.max_iter = 1 << 30;
+  KNB_CUDA(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  const unsigned gv = grid_for(op.n, VT_THREADS, 1184);
+  SweepFn fn;
+  SweepBuffers B{};
+  B.v64 = sl ? OpView<double>{} : op.rview64();
+  B.v32 = sl ? OpView<float>{} : op.rview32();
+  B.part1 = ws.part1.get();
+  B.part2 = ws.part2.get();
+  B.part3 = ws.part3.get();
+  B.st = st;
+  B.so = SO;
+  if (cls == 0) {
+    const float* inv32 = sl ? SO->inv_out32.get() : R->inv_out32.get();
+    pr_init<float><<<gv, VT_THREADS, 0, s>>>(ws.y32[0].get(), ws.z32[0].get(), inv32, op.n,
+                                              ws.part3.get(), st);
+    B.y[0] = ws.y32[0].get(); B.y[1] = ws.y32[1].get();
+    B.z[0] = ws.z32[0].get(); B.z[1] = ws.z32[1].get();
+    B.inv_out = inv32;
+    B.carry = ws.carry32.get();
+    B.head = ws.head32.get();
+    fn = pick_kernel<float, float, false>(c.variant, ipt, false, true);
+  } else {
+    const double* inv64 = sl ? SO->inv_out64.get() : R->inv_out64.get();
+    pr_init<double><<<gv, VT_THREADS, 0, s>>>(ws.y64[0].get(), ws.z64[0].get(), inv64, op.n,
+                                               ws.part3.get(), st);
+    B.y[0] = ws.y64[0].get(); B.y[1] = ws.y64[1].get();
+    B.z[0] = ws.z64[0].get(); B.z[1] = ws.z64[1].get();
+    B.inv_out = inv64;
+    B.carry = ws.carry64.get();
+    B.head = ws.head64.get();
+    fn = use32v ? pick_kernel<double, float, true>(c.variant, ipt, false, true)
+                : pick_kernel<double, double, true>(c.variant, ipt, false, true);
+  }
+  KNB_LAUNCH("pr_init");
+  fn(op, *P, B, 0, 0.85, s, SPLIT_CTAS, nullptr, nullptr);
+  KNB_CUDA(cudaEventRecord(ws.t0, s));
+  fn(op, *P, B, 1, 0.85, s, SPLIT_CTAS, nullptr, nullptr);
+  fn(op, *P, B, 0, 0.85, s, SPLIT_CTAS, nullptr, nullptr);
+  KNB_CUDA(cudaEventRecord(ws.t1, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  KNB_CUDA(cudaEventElapsedTime(&ms, ws.t0, ws.t1));
+  return ms / 2.0;
+}
+
+// Operators with fewer arcs keep the default sweep: their sweeps take a few
+// microseconds, too little to tell the candidates apart.
+constexpr uint64_t AUTOTUNE_MIN_ARCS = 1u << 21;
+
+// The sweep kernel for an operator, picked on its first large solve by
+// timing each candidate (time_candidate) and kept for the operator's life,
+// per precision class (0: solves that start with FP32 sweeps, 1: FP64
+// solves). Candidates: the sliced layout at 48 resident warps per SM with
+// 24,576, 49,152 or 98,304 FP32 values' worth of L1-allocating columns, at
+// 64 warps per SM, with long rows from 64 instead of 255 arcs, and the
+// merge-path warp tiles on the layout renumbered by column count. Every
+// candidate computes the same sums up to rounding; each meets the same
+// parity bars (tests/test_gpu_parity.py), and a pinned kernel (net_set_tuning
+// keys 4, 7, 10) or key 12 set to 0 bypasses the tuner.
+static SweepPick tuned_sweep(Operator& op, int cls, bool use32v, cudaStream_t s) {
+  {
+    std::lock_guard<std::mutex> lock(op.mu);
+    auto it = op.pr_pick.find(cls);
+    if (it != op.pr_pick.end()) return it->second;
+  }
+  PrWorkspace& ws = pr_workspace(op);
+  std::lock_guard<std::mutex> ws_lock(ws.mu);
+  {
+    std::lock_guard<std::mutex> lock(op.mu);  // another thread may have tuned meanwhile
+    auto it = op.pr_pick.find(cls);
+    if (it != op.pr_pick.end()) return it->second;
+  }
+  std::vector<SweepPick> cands = {
+      {VAR_SLICE, 255, 0, 49152, 0},   {VAR_SLICE, 255, 0, 24576, 0},
+      {VAR_SLICE, 255, 0, 98304, 0},   {VAR_SLICE64, 255, 0, 49152, 0},
+      {VAR_SLICE, 64, 0, 49152, 0},    {VAR_WARPL1, 0, 0, 24576, 0}};
+  SweepPick best = cands[0];
+  best.ms = 1e300;
+  for (SweepPick& c : cands) {
+    c.ms = time_candidate(op, c, cls, use32v, ws, s);
+    if (c.ms < best.ms) best = c;
+  }
+  std::lock_guard<std::mutex> lock(op.mu);
+  op.pr_pick[cls] = best;
+  return best;
+}
+
 void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool out_on_device,
                  PagerankInfo* info, cudaStream_t s) {
   PagerankParams prm = prm_in;
@@ -1007,6 +1138,15 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   prm.relabel = prm.relabel && tu.relabel != 0;
   prm.switch_factor = tu.switch_factor;
   prm.switch_floor = tu.switch_floor;
+  // the tuned kernel, unless one is pinned (or the operator is small)
+  SweepPick pick;
+  if (tu.autotune && prm.variant == 0 && prm.ipt == 0 && prm.relabel && tu.long_row == 0 &&
+      tu.hot_nodes < 0 && op.nnz >= AUTOTUNE_MIN_ARCS && op.n > 0) {
+    const bool use32t = op.has_vals && op.vals32_exact && !prm.fp64_values;
+    pick = tuned_sweep(op, prm.precision == PREC_FP64 ? 1 : 0, use32t, s);
+    prm.variant = pick.variant;
+  }
+  HotOverride hot_guard(pick.hot);
   const uint32_t n = op.n;
   if (n == 0) return;
   // Kernel choice (measured on R-MAT scale 24): the sliced layout, 48
@@ -1050,11 +1190,10 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
     ipt32 = (ipt32 == 8 && prm.ipt == 8 && !slice64_variant(var32)) ? 8 : 4;
   }
   const Relabeled* R = rl ? &op.relabeled(s) : nullptr;
-  // Sliced layout: pieces of long rows a multiple of the resident warps at
-  // 48 and at 64 warps per SM (192 per SM), so every warp gets as many.
   const SlicedOp* SO =
-      sl ? &op.sliced(tu.long_row > 0 ? (uint32_t)tu.long_row : 255u,
-                      192u * (uint32_t)device_limits().sms, s)
+      sl ? &op.sliced(pick.long_row > 0 ? (uint32_t)pick.long_row
+                                        : tu.long_row > 0 ? (uint32_t)tu.long_row : 255u,
+                      slice_pieces(), s)
          : nullptr;
   static const Partition no_partition;  // sliced sweeps cut their own work
   const bool mixed_pre = prm.precision == PREC_MIXED || prm.precision == PREC_FP32;
@@ -1090,13 +1229,7 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
          : std::max({P32 ? P32->ntiles : 0u, P64 ? P64->ntiles : 0u, PR ? PR->ntiles : 0u});
   const unsigned gv = grid_for(n, VT_THREADS, 1184);
 
-  PrWorkspace* wsp = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(op.mu);
-    if (!op.pr_ws) op.pr_ws = std::make_unique<PrWorkspace>();
-    wsp = static_cast<PrWorkspace*>(op.pr_ws.get());
-  }
-  PrWorkspace& ws = *wsp;
+  PrWorkspace& ws = pr_workspace(op);
   std::lock_guard<std::mutex> ws_lock(ws.mu);
   ws.ensure(n, nt, mixed, prm.precision != PREC_FP32, pv || !out_on_device);
   IterState* st = ws.st.get();
@@ -1228,6 +1361,9 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
     info->seconds = ms * 1e-3;
     info->converged = 1;
     info->kernel_launches = launches;
+    info->sweep_kernel = prm.precision == PREC_FP64 ? var64 : var32;
+    info->long_row = sl ? (int32_t)SO->lw : 0;
+    info->hot_columns = (int32_t)(hot_setting() >= 0 ? hot_setting() : sl ? 49152 : 24576);
   }
   const bool use32v = op.has_vals && op.vals32_exact && !prm.fp64_values;
   g_timing[0] = {tn32, tms32, sweep_bytes(op, 4, 4, pv)};

@@ -37,6 +37,9 @@ struct PagerankInfo {
   double seconds = 0;           // device time of the solve (events)
   int32_t converged = 0;
   int32_t kernel_launches = 0;  // kernels launched by the solve
+  int32_t sweep_kernel = 0;     // the FP32-phase (or FP64) sweep kernel, tuning key 4 codes
+  int32_t long_row = 0;         // sliced sweeps: the long-row threshold
+  int32_t hot_columns = 0;      // FP32 values of the most gathered columns kept in L1
 };
 
 // Process-wide tuning knobs (set through net_set_tuning); 0 leaves a
@@ -51,6 +54,7 @@ struct Tuning {
   int refine = 1;         // mixed: 1 anchor + refinement sweeps, 0 plain FP64 sweeps
   int long_row = 0;       // sliced sweeps: rows of at least this many arcs are long (0: 255)
   int64_t smem_hot = -1;  // sliced sweeps with a shared-memory tier: FP32 values kept there (-1: 32768)
+  int autotune = 1;       // 1: pick the sweep kernel per operator by timing candidates (large operators)
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

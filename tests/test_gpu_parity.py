@@ -451,6 +451,69 @@ def test_sliced_sweep_matches_oracle(variant, long_row):
         K.set_tuning(K.TUNE_LONG_ROW, 0)
 
 
+# The sweep kernels the tuner chooses between (pagerank.cu, tuned_sweep):
+# (kernel, long-row threshold, L1-allocating FP32 columns).
+TUNER_CANDIDATES = [(9, 255, 49152), (9, 255, 24576), (9, 255, 98304), (10, 255, 49152),
+                    (9, 64, 49152), (8, 0, 24576)]
+
+
+@pytest.mark.parametrize("variant,long_row,hot", TUNER_CANDIDATES)
+def test_tuner_candidates_match_oracle(variant, long_row, hot):
+    """Each kernel the tuner may pick, pinned, meets the oracle bars on a
+    weighted R-MAT 14: FP64 within 1e-12 L1 and the same sweep count, mixed
+    within 1e-9 with the same top-100 order."""
+    kg, og = rmat_pair(14, True, seed=27)
+    try:
+        K.set_tuning(K.TUNE_VARIANT, variant)
+        K.set_tuning(K.TUNE_LONG_ROW, long_row)
+        K.set_tuning(K.TUNE_HOT_NODES, hot)
+        b = og.pagerank(weighted=True, tol=1e-10)
+        a, ia = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_FP64)
+        assert np.abs(a - b).sum() <= 1e-12
+        assert ia.iterations == og.last_iters
+        assert ia.sweep_kernel == variant and ia.hot_columns == hot
+        am, im = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_MIXED)
+        assert np.abs(am - b).sum() <= 1e-9
+        top = np.argsort(-b, kind="stable")[:100]
+        assert np.array_equal(np.argsort(-am, kind="stable")[:100], top)
+        if variant in (9, 10):
+            assert im.long_row == long_row
+    finally:
+        K.set_tuning(K.TUNE_VARIANT, 0)
+        K.set_tuning(K.TUNE_LONG_ROW, 0)
+        K.set_tuning(K.TUNE_HOT_NODES, -1)
+
+
+def test_tuner_picks_once_per_operator_and_reports_it():
+    """On an operator of at least 2^21 arcs the first solve times the
+    candidates and keeps the fastest; later solves on the operator reuse it
+    (and give bit-identical results), the pick is one of the candidates, and
+    the results meet the oracle bars. With the tuner off, kernel 9."""
+    kg, og = rmat_pair(18, True, seed=29)
+    assert kg.csr(1)[0][-1] >= 1 << 21
+    b = og.pagerank(weighted=True, tol=1e-10)
+    x1, i1 = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_MIXED)
+    x2, i2 = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_MIXED)
+    pick = (i1.sweep_kernel, i1.long_row if i1.sweep_kernel != 8 else 0, i1.hot_columns)
+    assert pick in TUNER_CANDIDATES
+    assert (i2.sweep_kernel, i2.long_row, i2.hot_columns) == \
+        (i1.sweep_kernel, i1.long_row, i1.hot_columns)
+    assert np.array_equal(x1, x2)
+    assert np.abs(x1 - b).sum() <= 1e-9
+    x64, i64 = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_FP64)
+    assert (i64.sweep_kernel, i64.long_row if i64.sweep_kernel != 8 else 0,
+            i64.hot_columns) in TUNER_CANDIDATES
+    assert np.abs(x64 - b).sum() <= 1e-12 + abs(b.sum() - 1.0)
+    assert i64.iterations == og.last_iters
+    try:
+        K.set_tuning(K.TUNE_AUTOTUNE, 0)
+        kg2, _ = rmat_pair(18, True, seed=29)
+        _, i3 = kg2.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_MIXED)
+        assert (i3.sweep_kernel, i3.long_row, i3.hot_columns) == (9, 255, 49152)
+    finally:
+        K.set_tuning(K.TUNE_AUTOTUNE, 1)
+
+
 def test_sliced_sweep_on_fixtures_and_edge_cases():
     """Every golden fixture (empty graph, single node, loops, parallel arcs,
     disconnected parts) and every loop code through the sliced layout."""
