@@ -383,6 +383,14 @@ NET_API void net_set_sweep_timing(int32_t on);
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 
+/* Eigenvalues (ascending, n doubles) and eigenvectors (the columns of the
+ * row-major n x n `vectors`) of a symmetric n x n matrix (row-major, n at
+ * most 20), computed by the device solver that eigenvector centrality's
+ * Lanczos process runs on its projected matrices. Fails if the QL iteration
+ * does not converge. */
+NET_API int32_t net_projected_eigen(int64_t n, const double *a, double *values,
+                                    double *vectors, char *err, size_t err_len);
+
 /* PageRank (uniform teleport, weights as strengths when d_weights is not
  * NULL) of one graph given as device arrays of its in-arcs: d_offsets (n + 1)
  * and d_sources, d_weights (one per arc, or NULL), scores to d_out (n

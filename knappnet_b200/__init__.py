@@ -66,6 +66,8 @@ def lib() -> ctypes.CDLL:
     vp, cp, sz = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t
     h = ctypes.c_void_p
     info_p = ctypes.POINTER(NetSolveInfo)
+    L.net_projected_eigen.argtypes = [i64, vp, vp, vp, cp, sz]
+    L.net_projected_eigen.restype = i32
     L.net_graph_new.argtypes = [i64, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
     L.net_graph_new.restype = i32
     L.net_graph_free.argtypes = [h]
@@ -491,6 +493,19 @@ def set_tuning(key: int, value: float) -> None:
     """Process-wide PageRank tuning (net_set_tuning)."""
     if lib().net_set_tuning(key, float(value)):
         raise EngineError(f"invalid tuning key {key} or value {value}")
+
+
+def projected_eigen(a):
+    """Eigenvalues (ascending) and eigenvectors (columns) of a symmetric
+    matrix of order <= 20 by the device solver of the Lanczos process
+    (net_projected_eigen)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    vals = np.zeros(n)
+    vecs = np.zeros((n, n))
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_projected_eigen(n, _ptr(a), _ptr(vals), _ptr(vecs), err, ERR_LEN), err)
+    return vals, vecs
 
 
 def device_sync() -> None:

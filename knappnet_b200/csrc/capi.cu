@@ -1215,6 +1215,17 @@ int32_t net_set_tuning(int32_t key, double value) {
   }
 }
 
+int32_t net_projected_eigen(int64_t n, const double* a, double* values, double* vectors,
+                            char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (n < 0 || n > 20) throw Error("the matrix order must be between 0 and 20");
+    if (n == 0) return;
+    if (!a || !values || !vectors) throw Error("a buffer is null");
+    if (!knb::symmetric_eigen_device(a, (int)n, values, vectors, knb::thread_stream()))
+      throw Error("the QL iteration did not converge");
+  });
+}
+
 int32_t net_device_sync(char* err, size_t err_len) {
   return guard(err, err_len, [&] { KNB_CUDA(cudaDeviceSynchronize()); });
 }

@@ -12,8 +12,9 @@
 //   reference's constants (basis <= 20, keep 8, a convergence check every 4
 //   steps, a true-residual check of every candidate; eigenvector.rs:729-878).
 //   The basis, the products, the projections and the norms live on the
-//   device; the DGKS decision is taken on the device, and the host only runs
-//   the <= 20 x 20 projected eigenproblem at each check. Sums over vectors
+//   device; the DGKS decision is taken on the device, and so is the <= 20 x
+//   20 projected eigenproblem at each check (one warp, EISPACK order); the
+//   host reads a few scalars per check to choose the next step. Sums over vectors
 //   use fixed 4096-row blocks added in a fixed order (eigenvector.rs:913-971),
 //   so the results do not change from run to run.
 // - Components: weak components by a concurrent union-find on the device
@@ -39,154 +40,6 @@
 #include "eigen.cuh"
 
 namespace knb {
-
-// ======================================================================= dense eigensolver
-// Householder tridiagonalisation with accumulated transformations and the
-// implicit QL method (EISPACK tred2 / tql2; Martin, Reinsch and Wilkinson),
-// in EISPACK's order of operations. V is row-major n x n.
-bool symmetric_eigen(const double* a, int n, double* d, double* V) {
-  if (n == 0) return true;
-  std::vector<double> e(n, 0.0);
-  std::memcpy(V, a, sizeof(double) * n * n);
-  auto at = [&](int r, int c) -> double& { return V[r * n + c]; };
-  // tred2
-  for (int j = 0; j < n; ++j) d[j] = at(n - 1, j);
-  for (int i = n - 1; i > 0; --i) {
-    double scale = 0.0, h = 0.0;
-    for (int k = 0; k < i; ++k) scale += std::fabs(d[k]);
-    if (scale == 0.0) {
-      e[i] = d[i - 1];
-      for (int j = 0; j < i; ++j) {
-        d[j] = at(i - 1, j);
-        at(i, j) = 0.0;
-        at(j, i) = 0.0;
-      }
-    } else {
-      for (int k = 0; k < i; ++k) {
-        d[k] /= scale;
-        h += d[k] * d[k];
-      }
-      double f = d[i - 1], g = std::sqrt(h);
-      if (f > 0) g = -g;
-      e[i] = scale * g;
-      h -= f * g;
-      d[i - 1] = f - g;
-      for (int j = 0; j < i; ++j) e[j] = 0.0;
-      for (int j = 0; j < i; ++j) {
-        f = d[j];
-        at(j, i) = f;
-        g = e[j] + at(j, j) * f;
-        for (int k = j + 1; k < i; ++k) {
-          g += at(k, j) * d[k];
-          e[k] += at(k, j) * f;
-        }
-        e[j] = g;
-      }
-      f = 0.0;
-      for (int j = 0; j < i; ++j) {
-        e[j] /= h;
-        f += e[j] * d[j];
-      }
-      const double hh = f / (h + h);
-      for (int j = 0; j < i; ++j) e[j] -= hh * d[j];
-      for (int j = 0; j < i; ++j) {
-        f = d[j];
-        g = e[j];
-        for (int k = j; k < i; ++k) at(k, j) -= (f * e[k] + g * d[k]);
-        d[j] = at(i - 1, j);
-        at(i, j) = 0.0;
-      }
-    }
-    d[i] = h;
-  }
-  for (int i = 0; i < n - 1; ++i) {
-    at(n - 1, i) = at(i, i);
-    at(i, i) = 1.0;
-    const double h = d[i + 1];
-    if (h != 0.0) {
-      for (int k = 0; k <= i; ++k) d[k] = at(k, i + 1) / h;
-      for (int j = 0; j <= i; ++j) {
-        double g = 0.0;
-        for (int k = 0; k <= i; ++k) g += at(k, i + 1) * at(k, j);
-        for (int k = 0; k <= i; ++k) at(k, j) -= g * d[k];
-      }
-    }
-    for (int k = 0; k <= i; ++k) at(k, i + 1) = 0.0;
-  }
-  for (int j = 0; j < n; ++j) {
-    d[j] = at(n - 1, j);
-    at(n - 1, j) = 0.0;
-  }
-  at(n - 1, n - 1) = 1.0;
-  e[0] = 0.0;
-  // tql2
-  for (int i = 1; i < n; ++i) e[i - 1] = e[i];
-  e[n - 1] = 0.0;
-  double f = 0.0, tst1 = 0.0;
-  const double eps = DBL_EPSILON;
-  for (int l = 0; l < n; ++l) {
-    tst1 = std::max(tst1, std::fabs(d[l]) + std::fabs(e[l]));
-    int m = l;
-    while (m < n && !(std::fabs(e[m]) <= eps * tst1)) ++m;
-    if (m > l) {
-      int iter = 0;
-      do {
-        if (++iter > 60) return false;
-        double g = d[l];
-        double p = (d[l + 1] - g) / (2.0 * e[l]);
-        double r = std::hypot(p, 1.0);
-        if (p < 0) r = -r;
-        d[l] = e[l] / (p + r);
-        d[l + 1] = e[l] * (p + r);
-        const double dl1 = d[l + 1];
-        double h = g - d[l];
-        for (int i = l + 2; i < n; ++i) d[i] -= h;
-        f += h;
-        p = d[m];
-        double c = 1.0, c2 = c, c3 = c, s = 0.0, s2 = 0.0;
-        const double el1 = e[l + 1];
-        for (int i = m - 1; i >= l; --i) {
-          c3 = c2;
-          c2 = c;
-          s2 = s;
-          g = c * e[i];
-          h = c * p;
-          r = std::hypot(p, e[i]);
-          e[i + 1] = s * r;
-          s = e[i] / r;
-          c = p / r;
-          p = c * d[i] - s * g;
-          d[i + 1] = h + s * (c * g + s * d[i]);
-          for (int k = 0; k < n; ++k) {
-            h = at(k, i + 1);
-            at(k, i + 1) = s * at(k, i) + c * h;
-            at(k, i) = c * at(k, i) - s * h;
-          }
-        }
-        p = -s * s2 * c3 * el1 * e[l] / dl1;
-        e[l] = s * p;
-        d[l] = c * p;
-      } while (std::fabs(e[l]) > eps * tst1);
-    }
-    d[l] += f;
-    e[l] = 0.0;
-  }
-  for (int i = 0; i < n - 1; ++i) {
-    int k = i;
-    double p = d[i];
-    for (int j = i + 1; j < n; ++j)
-      if (d[j] < p) {
-        k = j;
-        p = d[j];
-      }
-    if (k != i) {
-      d[k] = d[i];
-      d[i] = p;
-      for (int r = 0; r < n; ++r) std::swap(at(r, i), at(r, k));
-    }
-  }
-  return true;
-}
 
 // ======================================================================= components
 constexpr int ET = 256;
@@ -689,6 +542,11 @@ struct LzState {
   int32_t bd_step;     // that step's j
   int32_t pad;
   uint32_t ticket;
+  // the projected eigenproblem of the last check (lz_eigen)
+  double theta_top;    // its largest eigenvalue
+  double estimate;     // beta |s_last| of that Ritz pair (0 after a breakdown)
+  int32_t eig_ok;      // 0 if the QL iteration did not converge
+  int32_t eig_size;    // the projected matrix's order
 };
 
 __device__ __forceinline__ double fixed_block_sum(const double* part, uint32_t nb, int stride,
@@ -880,6 +738,323 @@ __global__ void lz_rotate(const double* __restrict__ V, size_t dim, int cols,
     }
     for (int q = 0; q < p; ++q) out[(size_t)q * dim + i] = o[q];
   }
+}
+
+// ------------------------------------------------------------- projected eigenproblem
+// Symmetric eigensolver for the <= MAXB x MAXB projected matrix on the
+// device, run by one warp: Householder tridiagonalisation with accumulated
+// transformations and the implicit QL method (EISPACK tred2 / tql2; Martin,
+// Reinsch and Wilkinson), as crates/engine/src/linalg.rs:478-720 restates
+// them. Each matrix entry sees the same operations in the same order as in
+// the sequential algorithm: lane 0 runs the scalar recurrences and every sum,
+// and the warp shares only loops whose iterations touch disjoint rows or
+// columns (lane r takes row r or column r). The caller loads the matrix into
+// V; on return V holds the eigenvectors in its columns and d the eigenvalues
+// in ascending order. Returns false if the QL iteration does not converge.
+struct EigWork {
+  double V[MAXB][MAXB + 1];
+  double d[MAXB], e[MAXB], cs[MAXB], sn[MAXB];
+  double scale, h;
+  int m, done, ok, swaps[MAXB];
+};
+
+// tql2 on the tridiagonal (d, e) that tred2 leaves, rotating V's columns;
+// then the eigenpairs in ascending order (selection by swaps, as EISPACK).
+__device__ bool warp_tql2(EigWork& W, int n) {
+  const int lane = threadIdx.x & 31;
+  double (*V)[MAXB + 1] = W.V;
+  double* d = W.d;
+  double* e = W.e;
+  double f = 0.0, tst1 = 0.0;  // lane 0's
+  const double eps = DBL_EPSILON;
+  if (lane == 0) {
+    for (int i = 1; i < n; ++i) e[i - 1] = e[i];
+    e[n - 1] = 0.0;
+    W.ok = 1;
+  }
+  __syncwarp();
+  for (int l = 0; l < n; ++l) {
+    if (lane == 0) {
+      tst1 = fmax(tst1, fabs(d[l]) + fabs(e[l]));
+      int m = l;
+      while (m < n && !(fabs(e[m]) <= eps * tst1)) ++m;
+      W.m = m;
+      W.done = m > l ? 0 : 1;
+    }
+    __syncwarp();
+    const int m = W.m;
+    int iter = 0;
+    while (!W.done) {
+      if (lane == 0) {
+        if (++iter > 60) {
+          W.ok = 0;
+          W.done = 1;
+        } else {
+          double g = d[l];
+          double p = (d[l + 1] - g) / (2.0 * e[l]);
+          double r = hypot(p, 1.0);
+          if (p < 0) r = -r;
+          d[l] = e[l] / (p + r);
+          d[l + 1] = e[l] * (p + r);
+          const double dl1 = d[l + 1];
+          double h = g - d[l];
+          for (int i = l + 2; i < n; ++i) d[i] -= h;
+          f += h;
+          p = d[m];
+          double c = 1.0, c2 = c, c3 = c, s = 0.0, s2 = 0.0;
+          const double el1 = e[l + 1];
+          for (int i = m - 1; i >= l; --i) {
+            c3 = c2;
+            c2 = c;
+            s2 = s;
+            g = c * e[i];
+            h = c * p;
+            r = hypot(p, e[i]);
+            e[i + 1] = s * r;
+            s = e[i] / r;
+            c = p / r;
+            p = c * d[i] - s * g;
+            d[i + 1] = h + s * (c * g + s * d[i]);
+            W.cs[i] = c;
+            W.sn[i] = s;
+          }
+          p = -s * s2 * c3 * el1 * e[l] / dl1;
+          e[l] = s * p;
+          d[l] = c * p;
+          W.done = fabs(e[l]) > eps * tst1 ? 0 : 1;
+        }
+      }
+      __syncwarp();
+      if (!W.ok) return false;
+      // the step's rotations, in the order the scalar chain made them
+      if (lane < n)
+        for (int i = m - 1; i >= l; --i) {
+          const double c = W.cs[i], sv = W.sn[i];
+          const double h = V[lane][i + 1];
+          V[lane][i + 1] = sv * V[lane][i] + c * h;
+          V[lane][i] = c * V[lane][i] - sv * h;
+        }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      d[l] += f;
+      e[l] = 0.0;
+    }
+    __syncwarp();
+  }
+  if (lane == 0)
+    for (int i = 0; i < n - 1; ++i) {
+      int k = i;
+      double p = d[i];
+      for (int j = i + 1; j < n; ++j)
+        if (d[j] < p) {
+          k = j;
+          p = d[j];
+        }
+      if (k != i) {
+        d[k] = d[i];
+        d[i] = p;
+      }
+      W.swaps[i] = k;
+    }
+  __syncwarp();
+  if (lane < n)
+    for (int i = 0; i < n - 1; ++i) {
+      const int k = W.swaps[i];
+      if (k != i) {
+        const double t = V[lane][i];
+        V[lane][i] = V[lane][k];
+        V[lane][k] = t;
+      }
+    }
+  __syncwarp();
+  return true;
+}
+
+__device__ bool warp_symmetric_eigen(EigWork& W, int n) {
+  const int lane = threadIdx.x & 31;
+  double (*V)[MAXB + 1] = W.V;
+  double* d = W.d;
+  double* e = W.e;
+  if (lane < n) d[lane] = V[n - 1][lane];
+  __syncwarp();
+  // tred2
+  for (int i = n - 1; i > 0; --i) {
+    if (lane == 0) {
+      double scale = 0.0, h = 0.0;
+      for (int k = 0; k < i; ++k) scale += fabs(d[k]);
+      if (scale == 0.0) {
+        e[i] = d[i - 1];
+        for (int j = 0; j < i; ++j) {
+          d[j] = V[i - 1][j];
+          V[i][j] = 0.0;
+          V[j][i] = 0.0;
+        }
+      } else {
+        for (int k = 0; k < i; ++k) {
+          d[k] /= scale;
+          h += d[k] * d[k];
+        }
+        double f = d[i - 1], g = sqrt(h);
+        if (f > 0) g = -g;
+        e[i] = scale * g;
+        h -= f * g;
+        d[i - 1] = f - g;
+        for (int j = 0; j < i; ++j) e[j] = 0.0;
+        for (int j = 0; j < i; ++j) {
+          f = d[j];
+          V[j][i] = f;
+          g = e[j] + V[j][j] * f;
+          for (int k = j + 1; k < i; ++k) {
+            g += V[k][j] * d[k];
+            e[k] += V[k][j] * f;
+          }
+          e[j] = g;
+        }
+        f = 0.0;
+        for (int j = 0; j < i; ++j) {
+          e[j] /= h;
+          f += e[j] * d[j];
+        }
+        const double hh = f / (h + h);
+        for (int j = 0; j < i; ++j) e[j] -= hh * d[j];
+      }
+      W.scale = scale;
+      W.h = h;
+    }
+    __syncwarp();
+    if (W.scale != 0.0) {
+      // column j of the update belongs to lane j; d[j] is refreshed once
+      // every column is done (the sequential loop reads d[k], k > j, before
+      // iteration k rewrites it)
+      if (lane < i) {
+        const double f = d[lane], g = e[lane];
+        for (int k = lane; k < i; ++k) V[k][lane] -= (f * e[k] + g * d[k]);
+      }
+      __syncwarp();
+      if (lane < i) {
+        d[lane] = V[i - 1][lane];
+        V[i][lane] = 0.0;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) d[i] = W.h;
+    __syncwarp();
+  }
+  for (int i = 0; i < n - 1; ++i) {
+    if (lane == 0) {
+      V[n - 1][i] = V[i][i];
+      V[i][i] = 1.0;
+    }
+    __syncwarp();
+    const double h = d[i + 1];
+    if (h != 0.0) {
+      if (lane <= i) d[lane] = V[lane][i + 1] / h;
+      __syncwarp();
+      if (lane <= i) {
+        double g = 0.0;
+        for (int k = 0; k <= i; ++k) g += V[k][i + 1] * V[k][lane];
+        for (int k = 0; k <= i; ++k) V[k][lane] -= g * d[k];
+      }
+      __syncwarp();
+    }
+    if (lane <= i) V[lane][i + 1] = 0.0;
+    __syncwarp();
+  }
+  if (lane < n) {
+    d[lane] = V[n - 1][lane];
+    V[n - 1][lane] = 0.0;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    V[n - 1][n - 1] = 1.0;
+    e[0] = 0.0;
+  }
+  __syncwarp();
+  return warp_tql2(W, n);
+}
+
+// The projected eigenproblem of a check (eigenvector.rs:1128-1137), on the
+// device: the symmetrised matrix of the steps done (its order follows from
+// the step jc the host enqueued up to, or the breakdown step), its
+// eigenpairs (warp_symmetric_eigen), and what the host's decisions and the
+// kernels after them need: the largest eigenvalue and the residual estimate
+// beta |s_last| (into st), the top Ritz vector's coefficients (svec, for
+// lz_combine), and for a thick restart (eigenvector.rs:846-868) the
+// coefficients of the `keep` leading Ritz vectors (srot, row-major size x p,
+// for lz_rotate) and the arrowhead matrix that replaces the projected one
+// (hm_next). One warp.
+__global__ void __launch_bounds__(32)
+lz_eigen(const double* __restrict__ hm, int m, int jc, int keep, double* __restrict__ svec,
+         double* __restrict__ srot, double* __restrict__ hm_next, LzState* st) {
+  __shared__ EigWork W;
+  __shared__ int order[MAXB];
+  const int lane = threadIdx.x;
+  const int size = (st->breakdown ? st->bd_step : jc) + 1;
+  for (int k = lane; k < size * size; k += 32) {
+    const int r = k / size, c = k % size;
+    W.V[r][c] = 0.5 * (hm[r * m + c] + hm[c * m + r]);
+  }
+  __syncwarp();
+  if (!warp_symmetric_eigen(W, size)) {
+    if (lane == 0) {
+      st->eig_ok = 0;
+      st->eig_size = size;
+    }
+    return;
+  }
+  int top = 0;
+  for (int i = 0; i < size; ++i)
+    if (W.d[i] > W.d[top]) top = i;
+  const double beta = st->beta;
+  if (lane < size) svec[lane] = W.V[lane][top];
+  if (lane == 0) {
+    st->theta_top = W.d[top];
+    st->estimate = st->breakdown ? 0.0 : beta * fabs(W.V[size - 1][top]);
+    st->eig_ok = 1;
+    st->eig_size = size;
+    // decreasing eigenvalue, ties in index order (a stable sort)
+    for (int i = 0; i < size; ++i) {
+      const int key = i;
+      int j = i - 1;
+      while (j >= 0 && W.d[order[j]] < W.d[key]) {
+        order[j + 1] = order[j];
+        --j;
+      }
+      order[j + 1] = key;
+    }
+  }
+  __syncwarp();
+  const int p = min(keep, size - 1);
+  for (int l = lane; l < size; l += 32)
+    for (int q = 0; q < p; ++q) srot[l * p + q] = W.V[l][order[q]];
+  for (int k = lane; k < m * m; k += 32) hm_next[k] = 0.0;
+  __threadfence_block();
+  __syncwarp();
+  if (lane < p) {
+    const int q = lane;
+    const double c = beta * W.V[size - 1][order[q]];
+    hm_next[q * m + q] = W.d[order[q]];
+    hm_next[q * m + p] = c;
+    hm_next[p * m + q] = c;
+  }
+}
+
+// A symmetric n x n matrix a (row-major, n <= MAXB) through the same warp
+// solver: eigenvalues ascending into d, eigenvectors in the columns of V
+// (row-major); *ok 0 if the QL iteration did not converge.
+__global__ void __launch_bounds__(32)
+small_eigen(const double* __restrict__ a, int n, double* __restrict__ d, double* __restrict__ V,
+            int* ok) {
+  __shared__ EigWork W;
+  const int lane = threadIdx.x;
+  for (int k = lane; k < n * n; k += 32) W.V[k / n][k % n] = a[k];
+  __syncwarp();
+  const bool good = warp_symmetric_eigen(W, n);
+  if (lane == 0) *ok = good ? 1 : 0;
+  if (!good) return;
+  for (int k = lane; k < n; k += 32) d[k] = W.d[k];
+  for (int k = lane; k < n * n; k += 32) V[k] = W.V[k / n][k % n];
 }
 
 // xx = x.x, xy = x.y, sum = sum(x); the last CTA sets value = xy / xx.
@@ -1168,7 +1343,7 @@ struct Leading {
 // Buffers of the Lanczos process, kept between calls by callers that solve
 // repeatedly (they only grow).
 struct LzBuffers {
-  DevBuf<double> tmp, V, w, y, x, rot, hm, svec, part;
+  DevBuf<double> tmp, V, w, y, x, rot, hm, svec, part, srot, hm_next;
   DevBuf<float> v32;
   DevBuf<LzState> st;
   DevBuf<IterState> ist;
@@ -1193,6 +1368,8 @@ struct LzBuffers {
     grow(x, dim);
     grow(hm, (size_t)MAXB * MAXB);
     grow(svec, (size_t)MAXB * MAXB);
+    grow(srot, (size_t)MAXB * MAXB);
+    grow(hm_next, (size_t)MAXB * MAXB);
     grow(part, part_n);
     if (mixed) grow(v32, dim);
     grow(st, 1);
@@ -1263,7 +1440,6 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
   if (mixed) to_float<<<gv, 256, 0, s>>>(x.get(), dim, v32.get());
   *launches += 4;
 
-  std::vector<double> hm((size_t)m * m, 0.0), theta, S;
   int64_t matvecs = 0, matvecs32 = 0;
   int j0 = 0;
   bool use32 = mixed;
@@ -1302,6 +1478,12 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
       }
       KNB_LAUNCH("lanczos step");
       if (jc < j) return false;  // matvec cap
+      // The projected eigenproblem on the device; the host reads its
+      // scalars with the step state, in one round trip per group of steps.
+      lz_eigen<<<1, 32, 0, s>>>(hm_d.get(), m, jc, keep, svec.get(), L.srot.get(),
+                                L.hm_next.get(), st.get());
+      KNB_LAUNCH("lz_eigen");
+      ++*launches;
       read_state();
       int jdone = hst->breakdown ? hst->bd_step : jc;
       int64_t done_now = jdone - j + 1;
@@ -1310,33 +1492,19 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
       j = jdone;
       const int size = j + 1;
       const bool breakdown = hst->breakdown != 0;
-      const double beta = hst->beta;
       const bool end = breakdown || size == m;
       const bool check = end || (size - j0) % 4 == 0;
-      KNB_CUDA(cudaMemcpyAsync(hm.data(), hm_d.get(), (size_t)m * m * 8, cudaMemcpyDeviceToHost, s));
-      KNB_CUDA(cudaStreamSynchronize(s));
       if (!check) {
         if (matvecs >= max_matvecs) return false;
         continue;  // cap reached mid-cycle; loop will return at next enqueue
       }
-      // projected eigenproblem (eigenvector.rs:1128-1137)
-      std::vector<double> b((size_t)size * size);
-      for (int r = 0; r < size; ++r)
-        for (int c = 0; c < size; ++c) b[r * size + c] = 0.5 * (hm[r * m + c] + hm[c * m + r]);
-      theta.assign(size, 0.0);
-      S.assign((size_t)size * size, 0.0);
-      if (!symmetric_eigen(b.data(), size, theta.data(), S.data())) return false;
-      int top = 0;
-      for (int i = 0; i < size; ++i)
-        if (theta[i] > theta[top]) top = i;
-      const double estimate = breakdown ? 0.0 : beta * std::fabs(S[(size - 1) * size + top]);
-      const double limit = tol * (std::max(theta[top], 0.0) + shift);
-      if (use32 && estimate <= std::max(limit, FP32_FLOOR * (std::max(theta[top], 0.0) + shift))) {
+      if (!hst->eig_ok || hst->eig_size != size) return false;
+      const double theta_top = hst->theta_top;
+      const double estimate = hst->estimate;
+      const double limit = tol * (std::max(theta_top, 0.0) + shift);
+      if (use32 && estimate <= std::max(limit, FP32_FLOOR * (std::max(theta_top, 0.0) + shift))) {
         // FP32 products cannot resolve the residual further: restart the
         // Lanczos process with FP64 products from the current Ritz vector.
-        std::vector<double> cf(size);
-        for (int l = 0; l < size; ++l) cf[l] = S[l * size + top];
-        KNB_CUDA(cudaMemcpyAsync(svec.get(), cf.data(), size * 8, cudaMemcpyHostToDevice, s));
         lz_combine<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), x.get());
         lz_dots<<<nb, VB_T, 0, s>>>(x.get(), nullptr, dim, part.get(), st.get());
         read_state();
@@ -1352,9 +1520,6 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
         continue;
       }
       if (estimate <= std::min(limit, threshold)) {
-        std::vector<double> cf(size);
-        for (int l = 0; l < size; ++l) cf[l] = S[l * size + top];
-        KNB_CUDA(cudaMemcpyAsync(svec.get(), cf.data(), size * 8, cudaMemcpyHostToDevice, s));
         lz_combine<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), x.get());
         if (matvecs >= max_matvecs) return false;
         *launches += 1 + apply(x.get(), nullptr, y.get(), nullptr);
@@ -1404,28 +1569,15 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
       }
       if (end) {
         if (breakdown) return false;
-        std::vector<int> idx(size);
-        std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b2) { return theta[a] > theta[b2]; });
+        // thick restart from the coefficients lz_eigen left on the device
         const int p = std::min(keep, size - 1);
-        std::vector<double> sv((size_t)size * p);
-        for (int q = 0; q < p; ++q)
-          for (int l = 0; l < size; ++l) sv[l * p + q] = S[l * size + idx[q]];
-        KNB_CUDA(cudaMemcpyAsync(svec.get(), sv.data(), sv.size() * 8, cudaMemcpyHostToDevice, s));
-        lz_rotate<<<gv, 256, 0, s>>>(V.get(), dim, size, svec.get(), p, rot.get());
+        lz_rotate<<<gv, 256, 0, s>>>(V.get(), dim, size, L.srot.get(), p, rot.get());
         KNB_CUDA(cudaMemcpyAsync(V.get(), rot.get(), (size_t)p * dim * 8, cudaMemcpyDeviceToDevice, s));
-        std::fill(hm.begin(), hm.end(), 0.0);
-        for (int q = 0; q < p; ++q) {
-          hm[q * m + q] = theta[idx[q]];
-          double c = beta * S[(size - 1) * size + idx[q]];
-          hm[q * m + p] = c;
-          hm[p * m + q] = c;
-        }
-        KNB_CUDA(cudaMemcpyAsync(hm_d.get(), hm.data(), hm.size() * 8, cudaMemcpyHostToDevice, s));
+        KNB_CUDA(cudaMemcpyAsync(hm_d.get(), L.hm_next.get(), (size_t)m * m * 8,
+                                 cudaMemcpyDeviceToDevice, s));
         KNB_CUDA(cudaMemsetAsync(&ist.get()->stopped, 0, 4, s));
         lz_next<<<gv, 256, 0, s>>>(V.get(), dim, p, w.get(), use32 ? v32.get() : nullptr,
                                    hm_d.get(), m, st.get(), ist.get(), 0);
-        KNB_CUDA(cudaStreamSynchronize(s));
         *launches += 2;
         j0 = p;
         restart = true;
@@ -2412,6 +2564,23 @@ void leading_eigen(GraphHandleImpl& g, bool weighted, int64_t* membership, doubl
   *q = qv;
   *splits_out = (int64_t)splits;
   if (launches_out) *launches_out = launches;
+}
+
+bool symmetric_eigen_device(const double* a, int n, double* d, double* V, cudaStream_t s) {
+  if (n < 0 || n > MAXB) throw Error("the projected eigensolver takes matrices of order 0.." +
+                                     std::to_string(MAXB));
+  if (n == 0) return true;
+  DevBuf<double> ad((size_t)n * n), dd(n), vd((size_t)n * n);
+  DevBuf<int> ok(1);
+  KNB_CUDA(cudaMemcpyAsync(ad.get(), a, (size_t)n * n * 8, cudaMemcpyHostToDevice, s));
+  small_eigen<<<1, 32, 0, s>>>(ad.get(), n, dd.get(), vd.get(), ok.get());
+  KNB_LAUNCH("small_eigen");
+  int good = 0;
+  KNB_CUDA(cudaMemcpyAsync(&good, ok.get(), 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaMemcpyAsync(d, dd.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaMemcpyAsync(V, vd.get(), (size_t)n * n * 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
+  return good != 0;
 }
 
 }  // namespace knb

@@ -62,11 +62,12 @@ struct HitsParams {
 void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs, double* auths, double* value,
           int* unique, cudaStream_t s);
 
-// Dense symmetric eigensolver for the projected Lanczos problems: EISPACK
-// tred2 + tql2 order (reference: crates/engine/src/linalg.rs:478-720).
-// a is row-major n x n; eigenvalues ascending, eigenvectors in the columns of
-// vecs. Returns false if the QL iteration does not converge.
-bool symmetric_eigen(const double* a, int n, double* vals, double* vecs);
+// The device solver of the projected Lanczos problems (one warp, EISPACK
+// tred2 + tql2 order; reference: crates/engine/src/linalg.rs:478-720) on a
+// host matrix: a is row-major symmetric n x n (n <= 20); eigenvalues
+// ascending, eigenvectors in the columns of vecs (row-major). Returns false
+// if the QL iteration does not converge.
+bool symmetric_eigen_device(const double* a, int n, double* vals, double* vecs, cudaStream_t s);
 
 // Newman's leading eigenvector communities of an undirected graph with at
 // most 3000 nodes (crates/engine/src/metrics/partition/leading_eigen.rs):

@@ -91,3 +91,15 @@ def test_power_law_sizes(so):
     # mean of the truncated continuous law, floored: about 275 - 0.5
     assert 240 < x.mean() < 310
     assert np.array_equal(x, K.power_law_sizes(20000, 2.1, 50, 50000, 3))
+
+
+def test_projected_eigen_rejects_orders_beyond_twenty(so):
+    """Checked before any device work: orders outside 0..20 fail, order 0
+    succeeds with nothing to do."""
+    import knappnet_b200 as K
+    import numpy as np
+    err = ctypes.create_string_buffer(K.ERR_LEN)
+    a = np.zeros(441)
+    assert K.lib().net_projected_eigen(21, K._ptr(a), K._ptr(a), K._ptr(a), err, K.ERR_LEN) != 0
+    assert b"between 0 and 20" in err.value
+    assert K.lib().net_projected_eigen(0, None, None, None, err, K.ERR_LEN) == 0

@@ -327,6 +327,44 @@ def test_lanczos_symmetric_rmat_matches_oracle(precision):
     assert bool(info.connected) == cb
 
 
+def projected_cases():
+    """Symmetric matrices like the Lanczos process's projected ones: random,
+    tridiagonal, arrowhead (after a thick restart), with a cluster of close
+    eigenvalues, diagonal, of every order from 1 to 20."""
+    rng = np.random.default_rng(11)
+    for n in range(1, 21):
+        a = rng.standard_normal((n, n))
+        yield "random", (a + a.T) / 2
+        t = np.diag(rng.random(n) * 10) + np.diag(rng.random(n - 1), 1) + np.diag(
+            rng.random(n - 1), -1) if n > 1 else np.array([[3.0]])
+        yield "tridiagonal", t
+        h = np.diag(np.sort(rng.random(n))[::-1] * 50)
+        if n > 2:
+            p = min(8, n - 1)
+            h[:p, p] = h[p, :p] = rng.standard_normal(p)
+        yield "arrowhead", h
+    q, _ = np.linalg.qr(rng.standard_normal((12, 12)))
+    yield "cluster", q @ np.diag([5.0, 5.0 + 1e-12, 5.0 + 2e-12] + list(range(9))) @ q.T
+    yield "diagonal", np.diag([3.0, 1.0, 2.0, 1.0])
+
+
+def test_projected_eigensolver_on_device_matches_eispack():
+    """The warp solver Lanczos uses for its projected matrices against the
+    oracle's EISPACK restatement (crates/engine/src/linalg.rs:478-720):
+    eigenvalues within 1e-13 of the largest, eigenvectors the same up to
+    rounding where eigenvalues are apart, and A V = V diag(d) for all."""
+    for kind, a in projected_cases():
+        d, v = K.projected_eigen(a)
+        od, ov = O.symmetric_eigen(a)
+        scale = max(1.0, np.abs(od).max())
+        assert np.abs(d - od).max() <= 1e-13 * scale, kind
+        assert np.abs(a @ v - v * d).max() <= 1e-12 * scale, kind
+        assert np.abs(v.T @ v - np.eye(len(d))).max() <= 1e-12, kind
+        gaps = np.diff(od)
+        if kind != "cluster" and (len(od) < 2 or gaps.min() > 1e-6 * scale):
+            assert np.abs(v - ov).max() <= 1e-10, kind
+
+
 def test_power_iteration_directed_rmat_matches_oracle():
     kg, og = rmat_pair(11, True, seed=9)
     for mode in (1, 2):
