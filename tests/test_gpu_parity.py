@@ -335,9 +335,8 @@ def projected_cases():
     for n in range(1, 21):
         a = rng.standard_normal((n, n))
         yield "random", (a + a.T) / 2
-        t = np.diag(rng.random(n) * 10) + np.diag(rng.random(n - 1), 1) + np.diag(
-            rng.random(n - 1), -1) if n > 1 else np.array([[3.0]])
-        yield "tridiagonal", t
+        off = rng.random(n - 1)
+        yield "tridiagonal", np.diag(rng.random(n) * 10) + np.diag(off, 1) + np.diag(off, -1)
         h = np.diag(np.sort(rng.random(n))[::-1] * 50)
         if n > 2:
             p = min(8, n - 1)
