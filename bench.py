@@ -515,6 +515,22 @@ def run_c4a(args):
         return info.seconds
     sec = _median_device(gpu, args.steps, args.warmup)
     info = keep["info"]
+    # the same solve with teleport vectors and scores in device memory: the
+    # device time of the solve and of its sweeps alone
+    import torch
+    dP = torch.from_numpy(P).cuda()
+    dX = torch.empty_like(dP)
+    dev = {}
+
+    def gpu_dev():
+        i = g.pagerank_batch_device(dP.data_ptr(), B, dX.data_ptr(), precision=K.PREC_MIXED,
+                                    tol=1e-10)
+        dev["info"] = i
+        return i.seconds
+    dsec = _median_device(gpu_dev, args.steps, args.warmup)
+    dinfo = dev["info"]
+    same = bool(np.array_equal(dX.cpu().numpy(), keep["x"]))
+    del dP, dX
     s, t, _ = g.edges()
     og = O.Graph(n, s, t, None, True)
     errs, cpu = [], 0.0
@@ -524,8 +540,29 @@ def run_c4a(args):
         cpu += time.perf_counter() - t0
         errs.append(float(np.abs(keep["x"][b] - ref).sum()))
     arcs = int(g.csr(1)[0][-1])
+    hbm, peak_kind = peaks()
+    # bytes every sweep moves whatever columns are still active: row offsets,
+    # column indices and one read of the gathered n x B block (4 or 8 bytes a
+    # value); the active columns' own reads and writes come on top, so this
+    # is a lower bound of the algorithmic bytes
+    s32, s64 = int(dinfo.sweeps_fp32), int(dinfo.sweeps - dinfo.sweeps_fp32)
+    lb = s32 * (4.0 * (n + 1) + 4.0 * arcs + 4.0 * n * B) + \
+        s64 * (4.0 * (n + 1) + 4.0 * arcs + 8.0 * n * B)
+    ach = lb / dinfo.sweep_seconds / 1e9
     return {"workload": f"c4a: R-MAT {scale} directed, 256 personalisation vectors (uniform over "
                         "1-64 seed nodes), batched SpMM PageRank, mixed precision, tol 1e-10",
+            "device_pointers": {"solve_ms": round(dsec * 1e3, 2),
+                                "sweeps_ms": round(dinfo.sweep_seconds * 1e3, 2),
+                                "gteps_b_per_sweep": round(arcs * B * dinfo.sweeps /
+                                                           dinfo.sweep_seconds / 1e9, 2),
+                                "same_scores_as_host_call": same,
+                                "roofline_lower_bound": {
+                                    "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
+                                    "peak_kind": peak_kind, "unit": "GB/s",
+                                    "frac": round(ach / hbm, 4),
+                                    "bytes": "per sweep: offsets, indices and one read of the "
+                                             "gathered n x B block; the active columns' updates "
+                                             "are not counted"}},
             "metric": "GTEPS*B per sweep", "unit": "GTEPS*B/sweep", "higher_is_better": True,
             "value": round(arcs * B * info.sweeps / sec / 1e9, 2),
             "solve_ms": round(sec * 1e3, 2),
@@ -576,6 +613,8 @@ def run_c4b(args):
             "metric": "batch ms", "value": round(sec * 1e3, 3), "unit": "ms",
             "higher_is_better": False, "nodes": int(off[-1]), "edges": int(m.sum()),
             "kernel_launches": int(keep["info"].kernel_launches),
+            "launch_graph_instantiations": int(keep["info"].long_row),
+            "threads_per_cta": int(keep["info"].sweep_kernel),
             "max_iterations": int(keep["its"].max()),
             "l1_vs_oracle_worst_of_200": worst,
             "cpu_restatement_ms_estimated": round(cpu * total_work / work * 1e3, 1),

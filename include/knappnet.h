@@ -184,7 +184,9 @@ typedef struct NetSolveInfo {
   int32_t connected;
   int32_t sweep_kernel;    /* PageRank: the sweep kernel used (net_set_tuning key 4 codes);
                               packed graphs: threads per CTA of the launch */
-  int32_t long_row;        /* sliced sweeps: rows of at least this many arcs are long */
+  int32_t long_row;        /* sliced sweeps: rows of at least this many arcs are long;
+                              packed graphs: how many times the operator's launch graph
+                              has been instantiated (a repeated batch replays it) */
   int32_t hot_columns;     /* FP32 values of the most gathered columns kept in L1 */
 } NetSolveInfo;
 

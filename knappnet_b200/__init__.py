@@ -287,6 +287,20 @@ class Graph:
                                         _ptr(out), ctypes.byref(info), err, ERR_LEN), err)
         return out, info
 
+    def pagerank_batch_device(self, p_ptr: int, batch: int, out_ptr: int, damping=0.85,
+                              directed=True, weighted=False, dangling=0, loops=0, tol=0.0,
+                              max_iter=0, precision=PREC_FP64):
+        """net_pagerank_batch_device: teleport vectors and scores in device
+        memory (batch x n, vector c at offset c * n); returns NetBatchInfo."""
+        info = NetBatchInfo()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_pagerank_batch_device(self.h, damping, int(directed), int(weighted),
+                                               ctypes.c_void_p(p_ptr), batch, dangling, loops,
+                                               tol, max_iter, precision,
+                                               ctypes.c_void_p(out_ptr), ctypes.byref(info), err,
+                                               ERR_LEN), err)
+        return info
+
     def pagerank_graphs(self, node_offsets, damping=0.85, directed=True, weighted=False,
                         personalization=None, dangling=0, loops=0, tol=0.0, max_iter=0):
         """PageRank of every graph packed in this handle (graph k on nodes

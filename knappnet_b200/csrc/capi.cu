@@ -923,6 +923,7 @@ int32_t net_pagerank_graphs(const GraphHandle* h, int64_t count, const int64_t* 
       info->converged = 1;
       info->kernel_launches = 1;
       info->sweep_kernel = r.threads;  // threads per CTA of the packed launch
+      info->long_row = r.instantiations;  // instantiations of the operator's launch graph
     }
   });
 }

@@ -12,7 +12,9 @@
 // The vectors of the graph being solved stay in L2 (a graph's nodes are
 // contiguous in the packed numbering).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -145,6 +147,44 @@ static int g_ego_threads = 0;  // 0: tuned on first use (per process)
 
 void set_ego_threads(int t) { g_ego_threads = t; }
 
+// A packed batch kept per operator between calls: the graph offsets and the
+// largest-first order, every buffer, and the launch (queue reset and kernel)
+// instantiated as a CUDA graph, which later calls with the same offsets,
+// parameters and threads replay instead of capturing it again. Teleport
+// values are copied in on every call. A call with other offsets rebuilds
+// the plan; solves on one operator take turns on its mutex.
+struct EgoPlan : Workspace {
+  std::mutex mu;
+  std::vector<uint32_t> hoff;  // the batch the buffers are laid out for
+  bool pers = false;
+  EgoParams prm{};
+  int threads = 0;             // of the instantiated launch
+  DevBuf<uint32_t> doff, dorder;
+  DevBuf<double> dpers, dpsum, xa, xb, zb, dout;
+  DevBuf<int32_t> iters, status;
+  DevBuf<unsigned int> queue;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  int instantiations = 0;
+  ~EgoPlan() override {
+    drop_graph();
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+  }
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+};
+
+static bool same_params(const EgoParams& a, const EgoParams& b) {
+  return a.d == b.d && a.tol == b.tol && a.max_iter == b.max_iter &&
+         a.jump_uniform == b.jump_uniform;
+}
+
 void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoResult* res,
                      cudaStream_t s) {
   const uint32_t n = g.n;
@@ -157,36 +197,10 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
       throw Error("graph offsets must be nondecreasing");
   std::vector<uint32_t> hoff(count + 1);
   for (uint32_t k = 0; k <= count; ++k) hoff[k] = (uint32_t)in.node_offsets[k];
-  DevBuf<uint32_t> doff(count + 1), dorder(std::max<uint32_t>(count, 1));
-  KNB_CUDA(cudaMemcpyAsync(doff.get(), hoff.data(), (count + 1) * 4, cudaMemcpyHostToDevice, s));
-  if (g.m) {
-    DevBuf<unsigned long long> bad(1);
-    KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
-    ego_check_blocks<<<grid_for(g.m, 256), 256, 0, s>>>(g.src.get(), g.tgt.get(), g.m, doff.get(),
-                                                        count, bad.get());
-    KNB_LAUNCH("ego_check_blocks");
-    unsigned long long hb = 0;
-    KNB_CUDA(cudaMemcpyAsync(&hb, bad.get(), 8, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaStreamSynchronize(s));
-    if (hb != ~0ull)
-      throw Error("edge " + std::to_string(hb) + " joins two different graphs of the batch");
-  }
-  // largest graphs first
-  std::vector<uint32_t> order(count);
-  std::iota(order.begin(), order.end(), 0u);
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-    return hoff[a + 1] - hoff[a] > hoff[b + 1] - hoff[b];
-  });
-  KNB_CUDA(cudaMemcpyAsync(dorder.get(), order.data(), (size_t)count * 4, cudaMemcpyHostToDevice, s));
-
-  const int which = (g.directed && in.directed) ? 1 : (g.directed ? 2 : 0);
-  const double lfac = in.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (in.loops == 0 ? 2.0 : 1.0));
-  Operator& op = g.op(which, in.weighted, lfac, s);
-
   // personalization: per-graph sums (host, in node order within each graph)
-  DevBuf<double> dpers, dpsum;
+  std::vector<double> ps;
   if (in.personalization) {
-    std::vector<double> ps(count, 0.0);
+    ps.assign(count, 0.0);
     for (uint32_t k = 0; k < count; ++k) {
       double t = 0;
       for (uint32_t i = hoff[k]; i < hoff[k + 1]; ++i) {
@@ -199,102 +213,145 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
         throw Error("the personalization vector must have a positive sum");
       ps[k] = t;
     }
-    dpers.alloc(n);
-    dpsum.alloc(count);
-    KNB_CUDA(cudaMemcpyAsync(dpers.get(), in.personalization, (size_t)n * 8, cudaMemcpyHostToDevice, s));
-    KNB_CUDA(cudaMemcpyAsync(dpsum.get(), ps.data(), (size_t)count * 8, cudaMemcpyHostToDevice, s));
   }
-  DevBuf<double> xa(n), xb(n), zb(n), dout(n);
-  DevBuf<int32_t> iters(count), status(count);
-  DevBuf<unsigned int> queue(1);
-  EgoParams prm{in.damping, in.tol, (int32_t)std::min<int64_t>(in.max_iter, INT32_MAX),
-                in.dangling == 1 ? 1 : 0};
+  const int which = (g.directed && in.directed) ? 1 : (g.directed ? 2 : 0);
+  const double lfac = in.loops == 2 ? 0.0 : (which == 1 ? 1.0 : (in.loops == 0 ? 2.0 : 1.0));
+  Operator& op = g.op(which, in.weighted, lfac, s);
+  EgoPlan* pp = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(op.mu);
+    if (!op.ego_ws) op.ego_ws = std::make_unique<EgoPlan>();
+    pp = static_cast<EgoPlan*>(op.ego_ws.get());
+  }
+  EgoPlan& P = *pp;
+  std::lock_guard<std::mutex> plan_lock(P.mu);
+  const bool pers = in.personalization != nullptr;
+  if (P.hoff != hoff) {
+    // a new batch: check that no edge joins two graphs, order, buffers
+    P.drop_graph();
+    P.hoff.clear();
+    P.doff.alloc(count + 1);
+    P.dorder.alloc(std::max<uint32_t>(count, 1));
+    KNB_CUDA(cudaMemcpyAsync(P.doff.get(), hoff.data(), (count + 1) * 4, cudaMemcpyHostToDevice, s));
+    if (g.m) {
+      DevBuf<unsigned long long> bad(1);
+      KNB_CUDA(cudaMemsetAsync(bad.get(), 0xFF, 8, s));
+      ego_check_blocks<<<grid_for(g.m, 256), 256, 0, s>>>(g.src.get(), g.tgt.get(), g.m,
+                                                          P.doff.get(), count, bad.get());
+      KNB_LAUNCH("ego_check_blocks");
+      unsigned long long hb = 0;
+      KNB_CUDA(cudaMemcpyAsync(&hb, bad.get(), 8, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      if (hb != ~0ull)
+        throw Error("edge " + std::to_string(hb) + " joins two different graphs of the batch");
+    }
+    // largest graphs first
+    std::vector<uint32_t> order(count);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+      return hoff[a + 1] - hoff[a] > hoff[b + 1] - hoff[b];
+    });
+    KNB_CUDA(cudaMemcpyAsync(P.dorder.get(), order.data(), (size_t)count * 4,
+                             cudaMemcpyHostToDevice, s));
+    P.xa.alloc(n);
+    P.xb.alloc(n);
+    P.zb.alloc(n);
+    P.dout.alloc(n);
+    P.iters.alloc(count);
+    P.status.alloc(count);
+    P.queue.alloc(1);
+    P.dpers.release();
+    P.dpsum.release();
+    KNB_CUDA(cudaStreamSynchronize(s));
+    P.hoff = hoff;
+  }
+  if (pers && !P.dpers.get()) {
+    P.dpers.alloc(n);
+    P.dpsum.alloc(count);
+  }
+  if (pers) {
+    KNB_CUDA(cudaMemcpyAsync(P.dpers.get(), in.personalization, (size_t)n * 8,
+                             cudaMemcpyHostToDevice, s));
+    KNB_CUDA(cudaMemcpyAsync(P.dpsum.get(), ps.data(), (size_t)count * 8, cudaMemcpyHostToDevice, s));
+  }
+  const EgoParams prm{in.damping, in.tol, (int32_t)std::min<int64_t>(in.max_iter, INT32_MAX),
+                      in.dangling == 1 ? 1 : 0};
   int dev = 0, sms = 148;
   KNB_CUDA(cudaGetDevice(&dev));
   KNB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-
-  auto launch = [&](int threads) {
-    KNB_CUDA(cudaMemsetAsync(queue.get(), 0, 4, s));
+  auto launch = [&](int threads, cudaStream_t st) {
+    KNB_CUDA(cudaMemsetAsync(P.queue.get(), 0, 4, st));
     const unsigned grid = (unsigned)std::min<uint64_t>(count, (uint64_t)sms * (2048 / threads));
-    ego_pagerank<<<grid, threads, 0, s>>>(op.view64(), op.colsum.get(), doff.get(), dorder.get(),
-                                          count, queue.get(), prm, dpers.get(), dpsum.get(),
-                                          xa.get(), xb.get(), zb.get(), dout.get(), iters.get(),
-                                          status.get());
+    ego_pagerank<<<grid, threads, 0, st>>>(op.view64(), op.colsum.get(), P.doff.get(),
+                                           P.dorder.get(), count, P.queue.get(), prm,
+                                           pers ? P.dpers.get() : nullptr,
+                                           pers ? P.dpsum.get() : nullptr, P.xa.get(), P.xb.get(),
+                                           P.zb.get(), P.dout.get(), P.iters.get(),
+                                           P.status.get());
     KNB_LAUNCH("ego_pagerank");
   };
+  if (!P.t0) {
+    KNB_CUDA(cudaEventCreate(&P.t0));
+    KNB_CUDA(cudaEventCreate(&P.t1));
+  }
   // Threads per CTA: tuned once per process by timing each candidate on
   // this batch (the results do not depend on the choice).
   if (g_ego_threads == 0) {
     float best = 1e30f;
     int pick = 256;
-    cudaEvent_t a, b;
-    KNB_CUDA(cudaEventCreate(&a));
-    KNB_CUDA(cudaEventCreate(&b));
     for (int t : {128, 256, 512, 1024}) {
-      KNB_CUDA(cudaEventRecord(a, s));
-      launch(t);
-      KNB_CUDA(cudaEventRecord(b, s));
-      KNB_CUDA(cudaEventSynchronize(b));
+      KNB_CUDA(cudaEventRecord(P.t0, s));
+      launch(t, s);
+      KNB_CUDA(cudaEventRecord(P.t1, s));
+      KNB_CUDA(cudaEventSynchronize(P.t1));
       float ms = 0;
-      KNB_CUDA(cudaEventElapsedTime(&ms, a, b));
+      KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
       if (ms < best) {
         best = ms;
         pick = t;
       }
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     g_ego_threads = pick;
   }
   const int threads = g_ego_threads;
-
-  // The launch sequence (queue reset + kernel) as a CUDA graph.
-  cudaGraph_t graph;
-  cudaGraphExec_t exec;
-  cudaStream_t cs;
-  KNB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-  KNB_CUDA(cudaStreamSynchronize(s));
-  KNB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-  {
-    cudaStream_t keep = s;
-    s = cs;
-    launch(threads);
-    s = keep;
+  if (!P.exec || P.threads != threads || P.pers != pers || !same_params(P.prm, prm)) {
+    P.drop_graph();
+    cudaStream_t cs;
+    KNB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    KNB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    launch(threads, cs);
+    KNB_CUDA(cudaStreamEndCapture(cs, &P.graph));
+    KNB_CUDA(cudaGraphInstantiate(&P.exec, P.graph, 0));
+    KNB_CUDA(cudaStreamDestroy(cs));
+    P.threads = threads;
+    P.pers = pers;
+    P.prm = prm;
+    ++P.instantiations;
   }
-  KNB_CUDA(cudaStreamEndCapture(cs, &graph));
-  KNB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-  cudaEvent_t t0, t1;
-  KNB_CUDA(cudaEventCreate(&t0));
-  KNB_CUDA(cudaEventCreate(&t1));
-  KNB_CUDA(cudaEventRecord(t0, cs));
-  KNB_CUDA(cudaGraphLaunch(exec, cs));
-  KNB_CUDA(cudaEventRecord(t1, cs));
-  KNB_CUDA(cudaStreamSynchronize(cs));
-  float ms = 0;
-  KNB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
-  cudaStreamDestroy(cs);
-
+  KNB_CUDA(cudaEventRecord(P.t0, s));
+  KNB_CUDA(cudaGraphLaunch(P.exec, s));
+  KNB_CUDA(cudaEventRecord(P.t1, s));
   std::vector<int32_t> hst(count), hit(count);
-  KNB_CUDA(cudaMemcpyAsync(hst.data(), status.get(), (size_t)count * 4, cudaMemcpyDeviceToHost, s));
-  KNB_CUDA(cudaMemcpyAsync(hit.data(), iters.get(), (size_t)count * 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaMemcpyAsync(hst.data(), P.status.get(), (size_t)count * 4, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaMemcpyAsync(hit.data(), P.iters.get(), (size_t)count * 4, cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
   for (uint32_t k = 0; k < count; ++k)
     if (hst[k])
       throw Error("PageRank did not converge to tolerance " + std::to_string(in.tol) +
                   " within " + std::to_string(in.max_iter) + " iterations (graph " +
                   std::to_string(k) + " of the batch)");
   if (in.out_on_device)
-    KNB_CUDA(cudaMemcpyAsync(out, dout.get(), (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    KNB_CUDA(cudaMemcpyAsync(out, P.dout.get(), (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
   else
-    KNB_CUDA(cudaMemcpyAsync(out, dout.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(out, P.dout.get(), (size_t)n * 8, cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
   if (res) {
     res->seconds = ms * 1e-3;
     res->threads = threads;
+    res->instantiations = P.instantiations;
     int64_t tot = 0, mx = 0;
     for (uint32_t k = 0; k < count; ++k) {
       tot += hit[k];

@@ -25,6 +25,7 @@ struct EgoResult {
   int threads = 0;
   int64_t total_iterations = 0;
   int64_t max_iterations = 0;
+  int instantiations = 0;  // times the operator's launch graph has been instantiated
 };
 
 void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoResult* res,

@@ -145,6 +145,7 @@ struct Operator {
   std::unique_ptr<Workspace> series_ws;  // the Katz / Bonacich attenuation check's (katz.cu)
   std::map<int, int> batch_u;  // batched PageRank's tuned arcs in flight (batch.cu), under mu
   std::unique_ptr<Workspace> batch_ws;  // batched PageRank's plan and buffers (batch.cu)
+  std::unique_ptr<Workspace> ego_ws;  // packed-graph PageRank's plan and launch graph (ego.cu)
 
   const Relabeled& relabeled(cudaStream_t s);
   const Partition& relabeled_partition(uint32_t tile_items, cudaStream_t s);

@@ -680,6 +680,46 @@ def test_pagerank_graphs_matches_each_graph(directed, weighted):
     assert info.kernel_launches == 1
 
 
+def test_pagerank_graphs_replays_its_launch_graph():
+    """A repeated batch replays the instantiated launch graph (no new
+    instantiation) with the same results; new teleport values are copied in
+    and honoured without one; other parameters or another batch on the same
+    handle instantiate again; every answer still matches the oracle."""
+    sizes = np.array([40, 3, 120, 17, 64])
+    src, tgt = K.generate_gnm(sizes, np.minimum(5 * sizes, sizes * (sizes - 1) // 2), False,
+                              False, seed=31)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    g = K.Graph(int(off[-1]), src, tgt, None, False)
+
+    def oracle(p=None, damping=0.85, offs=off):
+        ref = np.zeros(int(offs[-1]))
+        for k in range(len(offs) - 1):
+            lo, hi = offs[k], offs[k + 1]
+            sel = (src >= lo) & (src < hi)
+            og = O.Graph(hi - lo, src[sel] - lo, tgt[sel] - lo, None, False)
+            ref[lo:hi] = og.pagerank(personalization=None if p is None else p[lo:hi],
+                                     damping=damping)
+        return ref
+
+    a, _, i1 = g.pagerank_graphs(off)
+    b, _, i2 = g.pagerank_graphs(off)
+    assert np.array_equal(a, b)
+    assert i2.long_row == i1.long_row  # replayed, not instantiated again
+    assert np.abs(a - oracle()).sum() <= 1e-12 * len(sizes)
+    p = np.arange(off[-1], dtype=float) % 4 + 1
+    c, _, i3 = g.pagerank_graphs(off, personalization=p)
+    c2, _, i4 = g.pagerank_graphs(off, personalization=p[::-1].copy())
+    assert i4.long_row == i3.long_row
+    assert np.abs(c - oracle(p)).sum() <= 1e-12 * len(sizes)
+    assert np.abs(c2 - oracle(p[::-1].copy())).sum() <= 1e-12 * len(sizes)
+    d, _, i5 = g.pagerank_graphs(off, damping=0.6)
+    assert i5.long_row == i4.long_row + 1
+    assert np.abs(d - oracle(damping=0.6)).sum() <= 1e-12 * len(sizes)
+    off2 = np.array([0, 43, off[-1]])  # graphs 0-1 and 2-4 taken together
+    e, _, _ = g.pagerank_graphs(off2)
+    assert np.abs(e - oracle(offs=off2)).sum() <= 1e-12 * 2
+
+
 def test_pagerank_graphs_options_and_errors():
     sizes = np.array([7, 1, 30, 12])
     src, tgt = K.generate_gnm(sizes, np.minimum(2 * sizes, sizes * (sizes - 1) // 2), False,
