@@ -6,9 +6,10 @@ shard, so the benchmark runs independent replicas, one per GPU, and reports
 the arcs all ranks processed over the slowest rank's time. The batched and
 packed-graph workloads split with no exchange at all: teleport vectors by
 contiguous column ranges, packed graphs by contiguous graph ranges balanced
-by their nodes plus arcs. Reductions run on the process group's own device
-(CUDA tensors for NCCL, CPU tensors for gloo), so the same code serves the
-GPU runs and the CPU tests.
+by their nodes plus arcs; each rank solves its part alone, and the parts
+are assembled on rank 0 afterwards (gather_rows). Reductions and gathers run
+on the process group's own device (CUDA tensors for NCCL, CPU tensors for
+gloo), so the same code serves the GPU runs and the CPU tests.
 """
 from __future__ import annotations
 
@@ -92,3 +93,28 @@ def split_graphs(node_offsets, arc_counts, world: int, rank: int):
     for k in range(1, world + 1):
         cuts[k] = max(cuts[k], cuts[k - 1])
     return cuts[rank], cuts[rank + 1]
+
+
+def gather_rows(dist, local, ranges):
+    """Assembles on rank 0 the rows every rank computed: rank r holds rows
+    ranges[r] = (lo, hi) of a result whose rows follow the ranges in rank
+    order, as `local` (a tensor of shape (hi - lo, ...) on the group's
+    device). Parts are padded to the longest for the collective and cut
+    back. Returns the whole result as a numpy array on rank 0 and None on
+    the other ranks (the local part itself, as numpy, for a single
+    process)."""
+    if dist is None:
+        return local.cpu().numpy()
+    import torch
+    world = dist.get_world_size()
+    if len(ranges) != world:
+        raise ValueError("one row range per rank")
+    longest = max(hi - lo for lo, hi in ranges)
+    shape = (longest,) + tuple(local.shape[1:])
+    pad = torch.zeros(shape, dtype=local.dtype, device=local.device)
+    pad[: local.shape[0]] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad)
+    if dist.get_rank() != 0:
+        return None
+    return torch.cat([parts[r][: hi - lo] for r, (lo, hi) in enumerate(ranges)]).cpu().numpy()

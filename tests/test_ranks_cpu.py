@@ -51,6 +51,49 @@ def test_two_gloo_ranks_reduce_and_split():
     assert all(r[6] == 256 for r in res)
 
 
+def _gather_worker(rank, world, port, queue):
+    import torch
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    r, w, _, dist = ranks.init("gloo", timeout_s=60.0)
+    # 7 teleport vectors of 5 scores: rank r holds its column range
+    ranges = [ranks.split_columns(7, w, k) for k in range(w)]
+    lo, hi = ranges[r]
+    full = np.arange(35, dtype=np.float64).reshape(7, 5)
+    got = ranks.gather_rows(dist, torch.from_numpy(full[lo:hi].copy()), ranges)
+    # packed graphs: per-node scores of the graphs each rank solved
+    sizes = np.array([3, 1, 4, 1, 5, 9, 2, 6])
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    cuts = [ranks.split_graphs(off, 2 * sizes, w, k) for k in range(w)]
+    nodes = [(int(off[a]), int(off[b])) for a, b in cuts]
+    a, b = nodes[r]
+    scores = np.linspace(0.0, 1.0, int(off[-1]))
+    got2 = ranks.gather_rows(dist, torch.from_numpy(scores[a:b].copy()), nodes)
+    queue.put((r, None if got is None else got.tolist(), None if got2 is None else got2.tolist()))
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_gather_their_parts_in_order():
+    """Rank 0 reassembles teleport columns and packed-graph scores in the
+    original order from parts of different lengths; the other rank gets
+    nothing back."""
+    mp = pytest.importorskip("torch.multiprocessing")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((x for x in (q.get(timeout=120) for _ in procs)), key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    full = np.arange(35, dtype=np.float64).reshape(7, 5)
+    assert np.array_equal(np.array(res[0][1]), full)
+    assert np.array_equal(np.array(res[0][2]), np.linspace(0.0, 1.0, 31))
+    assert res[1][1] is None and res[1][2] is None
+
+
 def test_single_process_reductions_are_identities():
     assert ranks.max_over_ranks(None, 3.0) == 3.0
     assert ranks.sum_over_ranks(None, 3.0) == 3.0
