@@ -226,6 +226,7 @@ typedef struct NetBatchInfo {
   int32_t kernel_launches;
   int32_t reserved;
   double sweep_seconds;          /* device time of the sweeps alone (no copies, set-up) */
+  int64_t column_iterations_fp32; /* of column_iterations, those in FP32 sweeps */
 } NetBatchInfo;
 
 /* Personalised PageRank for `batch` teleport vectors at once (one sparse

@@ -682,7 +682,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     sweep_ms += lm;
   };
   int launches = 0;
-  int64_t sweeps32 = 0, sweeps64 = 0;
+  int64_t sweeps32 = 0, sweeps64 = 0, colits32 = 0;
   const bool mixed = prm.precision == PREC_MIXED;
   const uint32_t Btot = prm.B;
   DevBuf<double>& pin = ws.pin;
@@ -815,7 +815,10 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       column_sums_finish<<<1, 256, 0, s>>>(part.get(), 1184, B, cs.get());
       KNB_LAUNCH("batch hand-over");
       launches += 3;
-      for (uint32_t c = 0; c < B; ++c) col_iters[c0 + c] = h[c].iter;
+      for (uint32_t c = 0; c < B; ++c) {
+        col_iters[c0 + c] = h[c].iter;
+        colits32 += h[c].iter;
+      }
     } else {
       for (int kk = 0; kk < 2; ++kk) {
         grow(Y64[kk], nb);
@@ -905,6 +908,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       mx = std::max<int64_t>(mx, col_iters[c]);
     }
     info->column_iterations = tot;
+    info->column_iterations_fp32 = colits32;
     info->max_column_iterations = mx;
     info->kernel_launches = launches;
   }
