@@ -303,6 +303,41 @@ NET_API int32_t net_graph_new_device(int64_t n, const uint32_t *d_src,
                              const double *d_w64, int64_t m, int32_t directed,
                              GraphHandle **out, char *err, size_t err_len);
 
+/* The graph of a frame's observed edge rows, as the reference's frame builder
+ * makes it from a validated frame (graph_of, crates/engine/src/frame/
+ * build.rs:106-121), built on the device from the resolved edge table:
+ * endpoint node indices src[e], tgt[e] of every row over n nodes, weights
+ * (NULL: none) and missing flags (NULL: every row observed; rows flagged 1
+ * are left out). Edges keep row order; edge_rows (NULL or m values) receives
+ * each graph edge's table row and *edge_count (NULL allowed) the number of
+ * edges. The reference reaches this step through net_frame_build
+ * (crates/capi/src/frame.rs:651), which takes a typed frame handle; this
+ * entry point starts from the resolved indices. */
+NET_API int32_t net_frame_graph(int64_t n, const int64_t *src, const int64_t *tgt,
+                                const double *weights, const uint8_t *missing, int64_t m,
+                                int32_t directed, GraphHandle **out, int64_t *edge_rows,
+                                int64_t *edge_count, char *err, size_t err_len);
+
+/* Every ego network of a frame at once (the reference's ego_subgraph,
+ * crates/engine/src/frame/build.rs:153-194 and 220-238, reached one ego at
+ * a time through net_frame_subgraph, crates/capi/src/frame.rs:952): ego k
+ * has the nodes i with node_ego[i] == k, ascending, and the observed rows e
+ * with edge_ego[e] == k whose endpoints are both in ego k, in row order
+ * (labels outside 0..egos-1 mark a node or row of no ego; edge_ego NULL:
+ * every row takes its source's ego, as the reference's resolved ego codes
+ * do, crates/engine/src/frame/validate.rs:115-117). The egos are
+ * packed back to back into one graph, ego k on nodes node_offsets[k] ..
+ * node_offsets[k + 1] - 1 (egos + 1 values written), ready for
+ * net_pagerank_graphs; node_ids (NULL or n values) receives the table's
+ * node index of each packed node, edge_rows (NULL or m values) the table
+ * row of each packed edge, *edge_count the number of edges. */
+NET_API int32_t net_frame_egos(int64_t n, const int64_t *src, const int64_t *tgt,
+                               const double *weights, const uint8_t *missing, int64_t m,
+                               int32_t directed, const int64_t *node_ego, const int64_t *edge_ego,
+                               int64_t egos, GraphHandle **out, int64_t *node_offsets,
+                               int64_t *node_ids, int64_t *edge_rows, int64_t *edge_count,
+                               char *err, size_t err_len);
+
 /* Number of arcs of the out (which = 0), in (1) or undirected (2) CSR. */
 NET_API int64_t net_graph_arc_count(const GraphHandle *h, int32_t which);
 

@@ -67,6 +67,12 @@ def lib() -> ctypes.CDLL:
     vp, cp, sz = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t
     h = ctypes.c_void_p
     info_p = ctypes.POINTER(NetSolveInfo)
+    L.net_frame_graph.argtypes = [i64, vp, vp, vp, vp, i64, i32, ctypes.POINTER(h), vp,
+                                  ctypes.POINTER(i64), cp, sz]
+    L.net_frame_graph.restype = i32
+    L.net_frame_egos.argtypes = [i64, vp, vp, vp, vp, i64, i32, vp, vp, i64, ctypes.POINTER(h),
+                                 vp, vp, vp, ctypes.POINTER(i64), cp, sz]
+    L.net_frame_egos.restype = i32
     L.net_projected_eigen.argtypes = [i64, vp, vp, vp, cp, sz]
     L.net_projected_eigen.restype = i32
     L.net_graph_new.argtypes = [i64, vp, vp, vp, i64, i32, ctypes.POINTER(h), cp, sz]
@@ -457,6 +463,50 @@ def generate_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, clean=T
                                    int(lognormal), wseed, ctypes.byref(h), ctypes.byref(m), err,
                                    ERR_LEN), err)
     return Graph(1 << scale, directed=not symmetrize, _handle=h, _m=m.value, _weighted=lognormal)
+
+
+def frame_graph(n, src, tgt, weights=None, missing=None, directed=True):
+    """The graph of a resolved edge table's observed rows (net_frame_graph):
+    returns (Graph, table row of each graph edge)."""
+    s = np.ascontiguousarray(src, dtype=np.int64)
+    t = np.ascontiguousarray(tgt, dtype=np.int64)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    miss = None if missing is None else np.ascontiguousarray(missing, dtype=np.uint8)
+    m = len(s)
+    rows = np.zeros(max(m, 1), dtype=np.int64)
+    cnt = ctypes.c_int64()
+    h = ctypes.c_void_p()
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_frame_graph(int(n), _ptr(s), _ptr(t), _ptr(w), _ptr(miss), m, int(directed),
+                                 ctypes.byref(h), _ptr(rows), ctypes.byref(cnt), err, ERR_LEN), err)
+    return (Graph(int(n), directed=directed, _handle=h, _m=cnt.value, _weighted=w is not None),
+            rows[: cnt.value])
+
+
+def frame_egos(n, src, tgt, node_ego, edge_ego, egos, weights=None, missing=None, directed=True):
+    """Every ego network of a resolved table packed into one graph
+    (net_frame_egos): returns (Graph, node_offsets, table node of each packed
+    node, table row of each packed edge). edge_ego None: every row takes its
+    source's ego."""
+    s = np.ascontiguousarray(src, dtype=np.int64)
+    t = np.ascontiguousarray(tgt, dtype=np.int64)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    miss = None if missing is None else np.ascontiguousarray(missing, dtype=np.uint8)
+    ne = np.ascontiguousarray(node_ego, dtype=np.int64)
+    ee = None if edge_ego is None else np.ascontiguousarray(edge_ego, dtype=np.int64)
+    m = len(s)
+    off = np.zeros(int(egos) + 1, dtype=np.int64)
+    ids = np.zeros(max(int(n), 1), dtype=np.int64)
+    rows = np.zeros(max(m, 1), dtype=np.int64)
+    cnt = ctypes.c_int64()
+    h = ctypes.c_void_p()
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_frame_egos(int(n), _ptr(s), _ptr(t), _ptr(w), _ptr(miss), m, int(directed),
+                                _ptr(ne), _ptr(ee), int(egos), ctypes.byref(h), _ptr(off),
+                                _ptr(ids), _ptr(rows), ctypes.byref(cnt), err, ERR_LEN), err)
+    members = int(off[-1])
+    g = Graph(members, directed=directed, _handle=h, _m=cnt.value, _weighted=w is not None)
+    return g, off, ids[:members], rows[: cnt.value]
 
 
 def generate_gnm(n, m, directed=False, loops=False, seed=1):

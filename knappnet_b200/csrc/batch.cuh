@@ -25,6 +25,7 @@ struct BatchInfo {
   int64_t sweeps = 0;               // batch sweeps (SpMM launches)
   int64_t sweeps_fp32 = 0;
   int64_t column_iterations = 0;    // sum over vectors of their own iteration counts
+  int64_t column_iterations_fp32 = 0;  // of which in FP32 sweeps
   int64_t max_column_iterations = 0;
   int kernel_launches = 0;
   double sweep_seconds = 0;         // device time of the sweep loops alone

@@ -18,6 +18,7 @@
 #include "batch.cuh"
 #include "ego.cuh"
 #include "eigen.cuh"
+#include "frame.cuh"
 #include "katz.cuh"
 #include "generate.cuh"
 #include "graph.cuh"
@@ -863,6 +864,7 @@ static int32_t batch_impl(const GraphHandle* h, double damping, int32_t directed
       info->max_column_iterations = bi.max_column_iterations;
       info->kernel_launches = bi.kernel_launches;
       info->sweep_seconds = bi.sweep_seconds;
+      info->column_iterations_fp32 = bi.column_iterations_fp32;
     }
   });
 }
@@ -1124,6 +1126,72 @@ int32_t net_graph_new_device(int64_t n, const uint32_t* d_src, const uint32_t* d
     }
     finish_build(g, s);
     *out = h.release();
+  });
+}
+
+// A graph handle over the edges frame_observed / frame_egos laid out.
+static GraphHandle* frame_handle(knb::FrameEdges& fe, bool directed, bool weighted,
+                                 int64_t* edge_rows, int64_t* edge_count, cudaStream_t s) {
+  auto h = std::make_unique<GraphHandle>();
+  knb::GraphHandleImpl& g = h->g;
+  g.n = fe.n;
+  g.m = fe.m;
+  g.directed = directed;
+  g.weighted = weighted;
+  KNB_CUDA(cudaGetDevice(&g.device));
+  g.src = std::move(fe.src);
+  g.tgt = std::move(fe.tgt);
+  if (weighted) g.w = std::move(fe.w);
+  finish_build(g, s);
+  if (edge_rows && fe.m) {
+    std::vector<uint32_t> r(fe.m);
+    KNB_CUDA(cudaMemcpyAsync(r.data(), fe.rows.get(), fe.m * 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+    for (uint64_t e = 0; e < fe.m; ++e) edge_rows[e] = r[e];
+  }
+  if (edge_count) *edge_count = (int64_t)fe.m;
+  KNB_CUDA(cudaStreamSynchronize(s));
+  return h.release();
+}
+
+int32_t net_frame_graph(int64_t n, const int64_t* src, const int64_t* tgt, const double* weights,
+                        const uint8_t* missing, int64_t m, int32_t directed, GraphHandle** out,
+                        int64_t* edge_rows, int64_t* edge_count, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (!out) throw Error("out is null");
+    *out = nullptr;
+    if (m > 0 && (!src || !tgt)) throw Error("an endpoint array is null");
+    cudaStream_t s = knb::thread_stream();
+    knb::FrameTable t{n, m, src, tgt, weights, missing};
+    knb::FrameEdges fe;
+    knb::frame_observed(t, &fe, s);
+    *out = frame_handle(fe, directed != 0, weights != nullptr, edge_rows, edge_count, s);
+  });
+}
+
+int32_t net_frame_egos(int64_t n, const int64_t* src, const int64_t* tgt, const double* weights,
+                       const uint8_t* missing, int64_t m, int32_t directed,
+                       const int64_t* node_ego, const int64_t* edge_ego, int64_t egos,
+                       GraphHandle** out, int64_t* node_offsets, int64_t* node_ids,
+                       int64_t* edge_rows, int64_t* edge_count, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (!out || !node_offsets) throw Error("out or node_offsets is null");
+    *out = nullptr;
+    if (m > 0 && (!src || !tgt)) throw Error("an endpoint array is null");
+    if (n > 0 && !node_ego) throw Error("node_ego is null");
+    cudaStream_t s = knb::thread_stream();
+    knb::FrameTable t{n, m, src, tgt, weights, missing};
+    knb::FrameEdges fe;
+    knb::frame_egos(t, node_ego, edge_ego, egos, &fe, s);
+    for (size_t k = 0; k < fe.node_offsets.size(); ++k) node_offsets[k] = fe.node_offsets[k];
+    if (node_ids && fe.n) {
+      std::vector<uint32_t> ids(fe.n);
+      KNB_CUDA(cudaMemcpyAsync(ids.data(), fe.node_ids.get(), (size_t)fe.n * 4,
+                               cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      for (uint32_t i = 0; i < fe.n; ++i) node_ids[i] = ids[i];
+    }
+    *out = frame_handle(fe, directed != 0, weights != nullptr, edge_rows, edge_count, s);
   });
 }
 

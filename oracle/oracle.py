@@ -479,6 +479,87 @@ def pagerank_time_op(off, cols, vals, out_strength, damping, iters, threads):
     return secs, out
 
 
+# --------------------------------------------------------------- frame graphs
+# The last steps of the reference's frame builder, restated in Python loops
+# for the small tables the tests use. A table is the resolved edge table:
+# endpoint node indices src[e], tgt[e] over n nodes, optional weights, and
+# optional missing flags (True: the row is unobserved).
+
+NO_NODE = 0xFFFFFFFF
+
+
+def _from_edges_checks(n, src, tgt, weights):
+    """The checks of Graph::from_edges (crates/engine/src/graph.rs:149-192):
+    the node count, every weight before any endpoint, then each edge's
+    source and target in edge order. Edges are numbered as given."""
+    if n > 0xFFFFFFFF:
+        raise OracleError(f"node count ({n}) exceeds the supported maximum")
+    if weights is not None:
+        for e, x in enumerate(weights):
+            if not math.isfinite(x):
+                raise OracleError(f"edge {e} has a missing, NaN, or infinite weight")
+    if len(src) > 0xFFFFFFFF // 2:
+        raise OracleError(f"edge count ({len(src)}) exceeds the supported maximum")
+    for e in range(len(src)):
+        for v in (int(src[e]), int(tgt[e])):
+            if v < 0 or v >= n:
+                raise OracleError(
+                    f"edge {e} refers to node index {v}, but valid indices are 0..{n}")
+
+
+def frame_graph_of(n, src, tgt, weights=None, missing=None):
+    """build_validated's observed-row pick and graph_of
+    (crates/engine/src/frame/build.rs:84-88 and 106-121): the graph over all n
+    nodes of the observed rows in row order. Returns (src, tgt, weights, rows)
+    with rows the table row of each graph edge."""
+    m = len(src)
+    rows = [e for e in range(m) if missing is None or not missing[e]]
+    s = [int(src[e]) for e in rows]
+    t = [int(tgt[e]) for e in rows]
+    w = None if weights is None else [float(weights[e]) for e in rows]
+    _from_edges_checks(n, s, t, w)
+    return (np.array(s, dtype=np.int64), np.array(t, dtype=np.int64),
+            None if w is None else np.array(w, dtype=np.float64), np.array(rows, dtype=np.int64))
+
+
+def frame_subgraph(n, src, tgt, weights, missing, keep_node, keep_edge):
+    """subgraph (crates/engine/src/frame/build.rs:153-194): the nodes for which
+    keep_node holds, renumbered in ascending order, and the observed rows for
+    which keep_edge holds whose endpoints are both kept, in row order.
+    Returns (nodes, edges, src, tgt, weights) with src/tgt renumbered."""
+    index = [NO_NODE] * n
+    nodes = []
+    for i in range(n):
+        if keep_node(i):
+            index[i] = len(nodes)
+            nodes.append(i)
+    edges = [e for e in range(len(src))
+             if (missing is None or not missing[e]) and keep_edge(e)
+             and index[int(src[e])] != NO_NODE and index[int(tgt[e])] != NO_NODE]
+    s = [index[int(src[e])] for e in edges]
+    t = [index[int(tgt[e])] for e in edges]
+    w = None if weights is None else [float(weights[e]) for e in edges]
+    return (np.array(nodes, dtype=np.int64), np.array(edges, dtype=np.int64),
+            np.array(s, dtype=np.int64), np.array(t, dtype=np.int64),
+            None if w is None else np.array(w, dtype=np.float64))
+
+
+def frame_ego_subgraph(n, src, tgt, weights, missing, node_ego, edge_ego, egos, ego):
+    """ego_subgraph (crates/engine/src/frame/build.rs:220-238) on a built frame:
+    the table is first checked as build does (graph_of over the observed rows).
+    node_ego None: the frame has no ego role. edge_ego None: every row takes
+    its source's ego (crates/engine/src/frame/validate.rs:115-117)."""
+    frame_graph_of(n, src, tgt, weights, missing)
+    if node_ego is None:
+        raise OracleError("the frame has no ego role")
+    if ego >= egos:
+        raise OracleError(f"ego index {ego} is out of range; the network has {egos} ego(s)")
+    if edge_ego is None:
+        edge_ego = [node_ego[int(src[e])] for e in range(len(src))]
+    return frame_subgraph(n, src, tgt, weights, missing,
+                          lambda i: node_ego[i] == ego, lambda e: edge_ego[e] == ego)
+
+
 def threads_for(requested: int, items: int, work: int) -> int:
     return int(lib().orc_threads_for(requested, items, work))
 
