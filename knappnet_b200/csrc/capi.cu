@@ -1244,7 +1244,7 @@ int32_t net_set_tuning(int32_t key, double value) {
       t.switch_floor = value;
       return 0;
     case 4:
-      if (!(value >= 0 && value <= 11) || value != (int)value) return 1;
+      if (!(value >= 0 && value <= 12) || value != (int)value) return 1;
       t.variant = (int)value;
       return 0;
     case 5:
@@ -1278,6 +1278,10 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 12:
       if (value != 0 && value != 1) return 1;
       t.autotune = (int)value;
+      return 0;
+    case 13:
+      if (!(value >= 0 && value <= 8) || value != (int)value) return 1;
+      t.bulk_ctas = (int)value;
       return 0;
     default:
       return 1;

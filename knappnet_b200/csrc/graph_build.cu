@@ -771,14 +771,22 @@ const SlicedOp& Operator::sliced(uint32_t lw, uint32_t pieces, cudaStream_t s) {
   r->loff.alloc((size_t)r->n_long + 1);
   KNB_CUDA(cudaMemcpyAsync(r->loff.get(), noff.get(), ((size_t)r->n_long + 1) * 4,
                            cudaMemcpyDeviceToDevice, s));
-  r->lcols.alloc(std::max<size_t>(r->long_arcs, 1));
+  // long-row arrays end on a whole 32-arc block: bulk-staged sweeps copy
+  // whole blocks (the tail past long_arcs is never added)
+  const size_t long_alloc = ((size_t)r->long_arcs + 31) / 32 * 32 + 32;
+  r->lcols.alloc(long_alloc);
+  KNB_CUDA(cudaMemsetAsync(r->lcols.get() + r->long_arcs, 0, (long_alloc - r->long_arcs) * 4, s));
   r->scols.alloc(std::max<uint64_t>(r->slice_elems, 1));
   // slice padding (lanes shorter than their slice's first row) holds column
   // 0 and value 0; sweeps may load it but never gather or add it
   KNB_CUDA(cudaMemsetAsync(r->scols.get(), 0, r->scols.bytes(), s));
   if (has_vals) {
-    r->lvals64.alloc(std::max<size_t>(r->long_arcs, 1));
-    r->lvals32.alloc(std::max<size_t>(r->long_arcs, 1));
+    r->lvals64.alloc(long_alloc);
+    r->lvals32.alloc(long_alloc);
+    KNB_CUDA(cudaMemsetAsync(r->lvals64.get() + r->long_arcs, 0,
+                             (long_alloc - r->long_arcs) * sizeof(double), s));
+    KNB_CUDA(cudaMemsetAsync(r->lvals32.get() + r->long_arcs, 0,
+                             (long_alloc - r->long_arcs) * sizeof(float), s));
     r->svals64.alloc(std::max<uint64_t>(r->slice_elems, 1));
     r->svals32.alloc(std::max<uint64_t>(r->slice_elems, 1));
     KNB_CUDA(cudaMemsetAsync(r->svals64.get(), 0, r->svals64.bytes(), s));

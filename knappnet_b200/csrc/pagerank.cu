@@ -35,6 +35,7 @@
 #include <string>
 #include <vector>
 
+#include "bulk.cuh"
 #include "pagerank.cuh"
 
 namespace knb {
@@ -501,8 +502,9 @@ enum SweepVariant : int {
   VAR_SLICE = 9,    // sliced layout (slice.cuh), 48 resident warps per SM
   VAR_SLICE64 = 10, // sliced layout, 64 resident warps per SM
   VAR_SLICEH = 11,  // sliced layout, one 32-warp CTA per SM, most gathered values in shared memory
+  VAR_SLICEB = 12,  // sliced layout, arc streams staged in shared memory by bulk copies
 };
-static bool slice_variant(int var) { return var >= VAR_SLICE && var <= VAR_SLICEH; }
+static bool slice_variant(int var) { return var >= VAR_SLICE && var <= VAR_SLICEB; }
 static bool slice64_variant(int var) { return var == VAR_SLICE64; }
 
 // Columns whose gathers allocate in L1 (FP32 values): the tuned choice of the
@@ -605,6 +607,46 @@ static unsigned launch_slice(const SlicedOp& so, const VT* x, const Epi& e, VT* 
   return grid * WPB;
 }
 
+// Bulk-staged sliced sweeps (bulk.cuh): U arc positions per chunk, S stages
+// per warp (4 for U = 4, 3 for U = 8), 8 warps per CTA. The carveout asks
+// for the shared memory of `ctas` CTAs per SM (default 4: 32 warps and 135
+// KB of rings for FP32 values, the rest of the SM's 256 KB left to L1); the
+// grid is every CTA that fits at once.
+constexpr int BULK_WPB = 8;
+template <class VT, class MT, class Epi, int U>
+static unsigned launch_slice_bulk(const SlicedOp& so, const VT* x, const Epi& e, VT* carry,
+                                  VT* head, double* part1, IterState* st, cudaStream_t s) {
+  constexpr int GNA = 2;
+  constexpr int S = U >= 8 ? 3 : 4;
+  auto fnp = slice_bulk_spmv<VT, MT, Epi, U, S, BULK_WPB, 4, GNA>;
+  const size_t smem = (size_t)BULK_WPB * bulk_ring_bytes<MT, U, S>();
+  const int ctas = tuning().bulk_ctas > 0 ? tuning().bulk_ctas : 4;
+  set_func_attr((const void*)fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int carve = std::min(100, (int)(((smem + 1024) * ctas * 100 + 233471) / 233472));
+  set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int>, unsigned> grids;
+  int dev = 0;
+  KNB_CUDA(cudaGetDevice(&dev));
+  unsigned grid = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_tuple(dev, (const void*)fnp, ctas);
+    auto it = grids.find(key);
+    if (it == grids.end()) {
+      int per_sm = 0;
+      KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fnp, BULK_WPB * 32, smem));
+      per_sm = std::max(1, std::min(per_sm, ctas));
+      it = grids.emplace(key, (unsigned)per_sm * (unsigned)device_limits().sms).first;
+    }
+    grid = it->second;
+  }
+  const uint64_t hot32 = hot_setting() >= 0 ? (uint64_t)hot_setting() : 49152u;
+  const uint32_t l1_hot = (uint32_t)std::min<uint64_t>(hot32 * 4 / sizeof(VT), 0xFFFFFFFFull);
+  fnp<<<grid, BULK_WPB * 32, smem, s>>>(so.view<MT>(), x, e, carry, head, part1, st, l1_hot);
+  return grid * BULK_WPB;
+}
+
 template <class VT, class MT, class Epi, int VAR, int IPT>
 static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>& v,
                         const VT* x, const Epi& e, VT* carry, VT* head, double* part1,
@@ -612,11 +654,16 @@ static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>
                         cudaEvent_t ev0, cudaEvent_t ev1, const SlicedOp* so = nullptr) {
   if (ev0) KNB_CUDA(cudaEventRecord(ev0, s));
   uint32_t npart = P.ntiles;  // partials the sweep leaves for split_rows
-  if constexpr (VAR >= VAR_SLICE && VAR <= VAR_SLICEH) {
-    constexpr int MINB = VAR == VAR_SLICE64 ? 8 : 6;
-    npart = launch_slice<VT, MT, Epi, IPT, MINB, VAR == VAR_SLICEH>(*so, x, e, carry, head,
-                                                                    part1, st, s);
-    KNB_LAUNCH("slice_spmv");
+  if constexpr (VAR >= VAR_SLICE && VAR <= VAR_SLICEB) {
+    if constexpr (VAR == VAR_SLICEB) {
+      npart = launch_slice_bulk<VT, MT, Epi, IPT>(*so, x, e, carry, head, part1, st, s);
+      KNB_LAUNCH("slice_bulk_spmv");
+    } else {
+      constexpr int MINB = VAR == VAR_SLICE64 ? 8 : 6;
+      npart = launch_slice<VT, MT, Epi, IPT, MINB, VAR == VAR_SLICEH>(*so, x, e, carry, head,
+                                                                      part1, st, s);
+      KNB_LAUNCH("slice_spmv");
+    }
     if (ev1) KNB_CUDA(cudaEventRecord(ev1, s));
     split_rows<VT, Epi><<<g2, SPMV_THREADS, 0, s>>>(so->split.get(), so->nsplit, so->nshort,
                                                      carry, head, e, part1, npart, part2, st);
@@ -767,6 +814,9 @@ static SweepFn pick_kernel(int var, int ipt, bool pv, bool ju) {
     case VAR_SLICEH:
       return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEH, 4>(pv, ju)
                       : pick_pv<VT, MT, EXACT, VAR_SLICEH, 8>(pv, ju);
+    case VAR_SLICEB:
+      return ipt == 4 ? pick_pv<VT, MT, EXACT, VAR_SLICEB, 4>(pv, ju)
+                      : pick_pv<VT, MT, EXACT, VAR_SLICEB, 8>(pv, ju);
     default: return pick_warp_ipt<VT, MT, EXACT, VAR_WARP>(ipt, pv, ju);
   }
 }
@@ -845,6 +895,7 @@ static SweepFn pick_refine(int var, int ipt, bool pv, bool ju) {
     case VAR_SLICE: return pick_refine_pv<VAR_SLICE, 4>(pv, ju);
     case VAR_SLICE64: return pick_refine_pv<VAR_SLICE64, 4>(pv, ju);
     case VAR_SLICEH: return pick_refine_pv<VAR_SLICEH, 4>(pv, ju);
+    case VAR_SLICEB: return pick_refine_ipt<VAR_SLICEB>(ipt, pv, ju);
     case VAR_WARP: return pick_refine_ipt<VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_refine_ipt<VAR_WARP4>(ipt, pv, ju);
     case VAR_WARPL1: return pick_refine_ipt<VAR_WARPL1>(ipt, pv, ju);
@@ -867,6 +918,7 @@ static AnchorFn pick_anchor(int var, int ipt, bool pv, bool ju) {
     case VAR_SLICE: return pick_anchor_pv<MT, VAR_SLICE, 4>(pv, ju);
     case VAR_SLICE64: return pick_anchor_pv<MT, VAR_SLICE64, 4>(pv, ju);
     case VAR_SLICEH: return pick_anchor_pv<MT, VAR_SLICEH, 4>(pv, ju);
+    case VAR_SLICEB: return pick_anchor_ipt<MT, VAR_SLICEB>(ipt, pv, ju);
     case VAR_WARP: return pick_anchor_ipt<MT, VAR_WARP>(ipt, pv, ju);
     case VAR_WARP4: return pick_anchor_ipt<MT, VAR_WARP4>(ipt, pv, ju);
     default: return pick_anchor_ipt<MT, VAR_WARP16>(ipt, pv, ju);
@@ -962,6 +1014,7 @@ static PhaseResult run_phase(SweepFn fn, const Operator& op, const Partition& P,
   KNB_CUDA(cudaMemcpyAsync(&h_state[0], B.st, sizeof(IterState), cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
   const IterState fin = h_state[0];
+  if (fin.fault) throw Error("a sweep gave up waiting for its staged arc copies");
   r.iter = fin.iter;
   r.converged = fin.converged;
   r.stopped = fin.stopped;
@@ -1081,7 +1134,10 @@ static double time_candidate(Operator& op, const SweepPick& c, int cls, bool use
   fn(op, *P, B, 1, 0.85, s, SPLIT_CTAS, nullptr, nullptr);
   fn(op, *P, B, 0, 0.85, s, SPLIT_CTAS, nullptr, nullptr);
   KNB_CUDA(cudaEventRecord(ws.t1, s));
+  int32_t fault = 0;
+  KNB_CUDA(cudaMemcpyAsync(&fault, &st->fault, sizeof(fault), cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
+  if (fault) throw Error("a sweep gave up waiting for its staged arc copies");
   float ms = 0;
   KNB_CUDA(cudaEventElapsedTime(&ms, ws.t0, ws.t1));
   return ms / 2.0;

@@ -55,6 +55,7 @@ struct Tuning {
   int long_row = 0;       // sliced sweeps: rows of at least this many arcs are long (0: 255)
   int64_t smem_hot = -1;  // sliced sweeps with a shared-memory tier: FP32 values kept there (-1: 32768)
   int autotune = 1;       // 1: pick the sweep kernel per operator by timing candidates (large operators)
+  int bulk_ctas = 0;      // bulk-staged sliced sweeps: CTAs per SM the carveout is sized for (0: 4)
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

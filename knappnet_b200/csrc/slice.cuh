@@ -66,9 +66,14 @@ __device__ __forceinline__ VT slice_gather(const VT* xg, uint32_t c, uint32_t l1
   else return ld_keep(xg + c, pol);
 }
 
+// s + w x with one rounding (s + x without values): spelled out so that every
+// sliced kernel rounds each arc's term the same way, whatever the compiler
+// would contract.
 template <class VT, class MT>
-__device__ __forceinline__ VT slice_mul(const MT* vals, MT w, VT x) {
-  return vals ? (VT)w * x : x;
+__device__ __forceinline__ VT slice_fma(const MT* vals, MT w, VT x, VT s) {
+  if (!vals) return s + x;
+  if constexpr (sizeof(VT) == 4) return __fmaf_rn((VT)w, x, s);
+  else return __fma_rn((VT)w, x, s);
 }
 
 // Sum over arcs [lo, hi) of one long row, lanes striding by 32 from the
@@ -98,7 +103,7 @@ __device__ __forceinline__ VT slice_long_sum(const SliceView<MT>& op, const VT* 
                                  : VT(0);
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) s += slice_mul<VT, MT>(op.lvals, w[u], x[u]);
+    for (int u = 0; u < U; ++u) s = slice_fma<VT, MT>(op.lvals, w[u], x[u], s);
   }
   return warp_sum(s);
 }
@@ -191,7 +196,7 @@ slice_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __restri
         x[u] = (k0 + u < len) ? slice_gather<GNA>(xg, c[u], l1_hot, pol_keep, hot, smem_n)
                               : VT(0);
 #pragma unroll
-      for (int u = 0; u < U; ++u) s += slice_mul<VT, MT>(op.svals, w[u], x[u]);
+      for (int u = 0; u < U; ++u) s = slice_fma<VT, MT>(op.svals, w[u], x[u], s);
     }
     if (r < op.n) {
       if (EARLY) epi.row_in(r, s, ein, acc);

@@ -74,7 +74,7 @@ struct IterState {
   int32_t ambiguous;      // 1 when the exact change must decide
   uint32_t ticket;        // CTA counter of the last-CTA reductions
   uint32_t ticket2;
-  int32_t pad;
+  int32_t fault;          // 1 when a sweep gave up waiting for its staged copies
 };
 
 __device__ __forceinline__ bool iteration_done(const IterState* st) {

@@ -555,7 +555,9 @@ def frame_ego_subgraph(n, src, tgt, weights, missing, node_ego, edge_ego, egos, 
     if ego >= egos:
         raise OracleError(f"ego index {ego} is out of range; the network has {egos} ego(s)")
     if edge_ego is None:
-        edge_ego = [node_ego[int(src[e])] for e in range(len(src))]
+        # unobserved rows never become edges and may hold any endpoint
+        edge_ego = [node_ego[int(src[e])] if 0 <= int(src[e]) < n else -1
+                    for e in range(len(src))]
     return frame_subgraph(n, src, tgt, weights, missing,
                           lambda i: node_ego[i] == ego, lambda e: edge_ego[e] == ego)
 

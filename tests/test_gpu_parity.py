@@ -452,7 +452,7 @@ def test_pagerank_sweep_variants_match_oracle(variant, ipt, relabel, hot, persis
 
 
 @pytest.mark.parametrize("variant,long_row", [(9, 0), (9, 16), (9, 255), (9, 1), (10, 0),
-                                              (10, 200)])
+                                              (10, 200), (12, 0), (12, 16), (12, 1), (12, 200)])
 def test_sliced_sweep_matches_oracle(variant, long_row):
     """The sliced layout (rows renumbered by length; long rows by whole
     warps in pieces, the others one lane per row): FP64 and mixed (FP32
@@ -486,6 +486,49 @@ def test_sliced_sweep_matches_oracle(variant, long_row):
     finally:
         K.set_tuning(K.TUNE_VARIANT, 0)
         K.set_tuning(K.TUNE_LONG_ROW, 0)
+
+
+@pytest.mark.parametrize("long_row", [0, 1, 16, 200])
+def test_bulk_staged_sweep_matches_sliced_sweep(long_row):
+    """Kernel 12 stages the arc streams in shared memory by bulk copies and
+    adds every row's arcs in kernel 9's order; only the per-warp partials of
+    the epilogue's scalars (iterate sum, dangling mass, change) associate
+    differently, because the two kernels keep different numbers of warps
+    resident. Every solve, in every precision, with 4 or 8 arc positions per
+    chunk and 1 to 4 CTAs per SM, agrees with kernel 9 to rounding and takes
+    the same number of sweeps (one more or fewer at most); repeated solves
+    are bit-identical."""
+    kg, _ = rmat_pair(16, True, seed=29)
+    p = np.zeros(kg.n)
+    p[[5, 600, 7000]] = 1.0
+    runs = [(dict(precision=K.PREC_FP64), 1e-13), (dict(precision=K.PREC_MIXED, tol=1e-10), 1e-10),
+            (dict(precision=K.PREC_FP32, tol=1e-6), 1e-5),
+            (dict(precision=K.PREC_MIXED, tol=1e-10, personalization=p, dangling=1), 1e-10),
+            (dict(precision=K.PREC_FP64, directed=False), 1e-13),
+            (dict(precision=K.PREC_MIXED, weighted=False), 1e-10)]
+    try:
+        K.set_tuning(K.TUNE_LONG_ROW, long_row)
+        for ipt in (0, 8):
+            K.set_tuning(K.TUNE_IPT, ipt)
+            for o, bar in runs:
+                o = dict(o)
+                o.setdefault("weighted", True)
+                K.set_tuning(K.TUNE_VARIANT, 9)
+                ref, ri = kg.pagerank_ex(**o)
+                for ctas in (0, 1, 3):
+                    K.set_tuning(K.TUNE_VARIANT, 12)
+                    K.set_tuning(K.TUNE_BULK_CTAS, ctas)
+                    got, gi = kg.pagerank_ex(**o)
+                    again, _ = kg.pagerank_ex(**o)
+                    assert gi.sweep_kernel == 12
+                    assert np.array_equal(got, again), (ipt, o, ctas)
+                    assert np.abs(got - ref).sum() <= bar, (ipt, o, ctas)
+                    assert abs(gi.iterations - ri.iterations) <= 1, (ipt, o, ctas)
+    finally:
+        K.set_tuning(K.TUNE_VARIANT, 0)
+        K.set_tuning(K.TUNE_LONG_ROW, 0)
+        K.set_tuning(K.TUNE_IPT, 0)
+        K.set_tuning(K.TUNE_BULK_CTAS, 0)
 
 
 # The sweep kernels the tuner chooses between (pagerank.cu, tuned_sweep):
