@@ -17,9 +17,10 @@ Metric: GTEPS per iteration = arcs / (solve time / sweeps) / 1e9.
 - `e2e`: the same call through the C ABI with host buffers: the teleport
   vector is copied from pinned host memory and the scores back to pinned
   host memory inside the timed region.
-- `roofline`: the dominant kernel (the merge-path sweep; FP32 and FP64 sweeps
-  reported separately), its algorithmic bytes per launch over its average
-  CUDA-event duration, against the measured HBM copy bandwidth.
+- `roofline`: the dominant kernel (the sweep kernel the per-operator tuner
+  picked, normally the sliced sweep; FP32, anchor, refinement and FP64
+  sweeps reported separately), its algorithmic bytes per launch over its
+  average CUDA-event duration, against the measured HBM copy bandwidth.
 - `cpu_baseline`: the oracle's restatement of the reference's multithreaded
   CPU PageRank iteration (oracle/), timed on this host's cores on a bounded
   sample of the same workload.
@@ -69,6 +70,8 @@ KERNEL_NAMES = {
     10: "slice_spmv (sliced layout, 64 resident warps per SM, 4 arcs per lane in flight)",
     11: "slice_spmv (sliced layout, one 32-warp CTA per SM, most gathered values in shared "
         "memory)",
+    12: "slice_bulk_spmv (sliced layout, arc streams staged in shared memory by bulk copies, "
+        "32 resident warps per SM)",
 }
 
 

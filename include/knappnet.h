@@ -402,8 +402,10 @@ NET_API void net_set_sweep_timing(int32_t on);
  * sliced layout: nodes renumbered by row length, long rows by whole warps,
  * the others one lane per row, with 48 or 64 resident warps per SM, 11 the
  * sliced layout with the most gathered values in shared memory, one CTA per
- * SM; 0 lets the library choose: on operators of at least 2^21 arcs the
- * first solve times the candidates and keeps the fastest); 5 = preferred
+ * SM, 12 the sliced layout with its column and value streams staged in
+ * shared memory by bulk copies; 0 lets the library choose: on operators of
+ * at least 2^21 arcs the first solve times the candidates and keeps the
+ * fastest); 5 = preferred
  * shared-memory carveout of the sweep (-1 just what the CTAs the kernel keeps
  * resident need, 0..100 percent);
  * 6 = threads per CTA of the packed-graph PageRank (0 tuned on first use,
@@ -417,7 +419,11 @@ NET_API void net_set_sweep_timing(int32_t on);
  * this many arcs (1..65535) are taken by whole warps (0: automatic); 11 =
  * FP32 values kernel 11 keeps in shared memory (-1: 32,768); 12 = pick the
  * sweep kernel per operator by timing (1, default) or always use kernel 9
- * (0). Setting key 0, 4, 7 or 10 also bypasses the timing.
+ * (0); 13 = CTAs per SM kernel 12 sizes its shared memory for (0: 4, 1..8);
+ * 14 = for testing kernel 12's bounded waits: the chunk of the grid's first
+ * warp whose copies are never issued, so that its wait runs out after about
+ * one second and the solve fails with an error (-1, default: none).
+ * Setting key 0, 4, 7 or 10 also bypasses the timing.
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);
 

@@ -15,10 +15,12 @@
 // their gathers at once: the stream latency leaves the warp's critical path
 // and the registers stay free for gathers in flight.
 //
-// Every wait is bounded (about two seconds of SM clock). A wait that runs out
+// Every wait is bounded (about one second of SM clock). A wait that runs out
 // marks the sweep's state (fault, stopped) and the warp stops taking work
 // after a bounded wait for the copies it still has in flight; the host turns
-// the mark into an error.
+// the mark into an error. For the test of that path the host can name one
+// chunk of the grid's first warp whose copies are never issued (skip_chunk),
+// so its wait runs out.
 #pragma once
 
 #include "slice.cuh"
@@ -36,10 +38,6 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 // Makes barrier initialisation visible to the copy engine.
 __device__ __forceinline__ void mbar_fence_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_inval(uint32_t bar) {
-  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 }
 
 // Arrives on the barrier and expects `bytes` of copies to complete on it.
@@ -81,8 +79,9 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
       : "memory");
 }
 
-constexpr long long BULK_WAIT_CYCLES = 4000000000ll;  // about two seconds
-constexpr long long BULK_DRAIN_CYCLES = 400000000ll;  // after a fault, per stage
+constexpr long long BULK_WAIT_CYCLES = 2000000000ll;  // about one second
+constexpr long long BULK_DRAIN_CYCLES = 200000000ll;  // after a fault, per stage
+constexpr uint32_t BULK_NO_SKIP = 0xFFFFFFFFu;
 
 // Bytes of one warp's ring: S stages of 32 U columns and 32 U values, then S
 // barriers, rounded to 128 bytes.
@@ -188,10 +187,13 @@ struct BulkPipe {
 
   __device__ __forceinline__ BulkPipe(unsigned char* base) : ring(base) {}
 
+  uint32_t skip = BULK_NO_SKIP;  // a chunk never issued (the wait-limit test)
+
   __device__ __forceinline__ void issue_one(const SliceView<MT>& op, int lane, uint32_t gw,
                                             uint32_t nw, uint64_t pol) {
     const uint32_t j = issued % S;
-    if (lane == 0) prod.issue(op, ring.cols_at(j), ring.vals_at(j), ring.bar(j), pol);
+    if (lane == 0 && issued != skip)
+      prod.issue(op, ring.cols_at(j), ring.vals_at(j), ring.bar(j), pol);
     ++issued;
     prod.next(op, gw, nw);
   }
@@ -227,7 +229,7 @@ template <class VT, class MT, class Epi, int U, int S, int WPB, int MINB, int GN
 __global__ void __launch_bounds__(WPB * 32, MINB)
 slice_bulk_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __restrict__ carry,
                 VT* __restrict__ head, double* __restrict__ part, IterState* __restrict__ st,
-                uint32_t l1_hot) {
+                uint32_t l1_hot, uint32_t skip_chunk) {
   if (st && iteration_done(st)) return;
   extern __shared__ __align__(128) unsigned char bulk_smem[];
   constexpr bool EARLY = sizeof(VT) == 4;
@@ -243,6 +245,7 @@ slice_bulk_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __r
   const uint64_t pol_keep = policy_evict_last();
 
   BulkPipe<MT, U, S> pipe(bulk_smem + (size_t)wib * bulk_ring_bytes<MT, U, S>());
+  if (gw == 0) pipe.skip = skip_chunk;
   if (lane == 0) {
 #pragma unroll
     for (int j = 0; j < S; ++j) mbar_init(pipe.ring.bar(j), 1);
@@ -349,10 +352,6 @@ slice_bulk_spmv(SliceView<MT> op, const VT* __restrict__ xg, Epi epi_in, VT* __r
     }
   }
   __syncwarp();
-  if (lane == 0) {
-#pragma unroll
-    for (int j = 0; j < S; ++j) mbar_inval(pipe.ring.bar(j));
-  }
   warp_store_partials<Epi>(acc, part, gw, lane);
 }
 

@@ -1283,6 +1283,10 @@ int32_t net_set_tuning(int32_t key, double value) {
       if (!(value >= 0 && value <= 8) || value != (int)value) return 1;
       t.bulk_ctas = (int)value;
       return 0;
+    case 14:
+      if (!(value >= -1 && value <= 2147483647.0) || value != (double)(int64_t)value) return 1;
+      t.bulk_skip_chunk = (int64_t)value;
+      return 0;
     default:
       return 1;
   }

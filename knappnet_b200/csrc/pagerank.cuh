@@ -56,6 +56,7 @@ struct Tuning {
   int64_t smem_hot = -1;  // sliced sweeps with a shared-memory tier: FP32 values kept there (-1: 32768)
   int autotune = 1;       // 1: pick the sweep kernel per operator by timing candidates (large operators)
   int bulk_ctas = 0;      // bulk-staged sliced sweeps: CTAs per SM the carveout is sized for (0: 4)
+  int64_t bulk_skip_chunk = -1;  // test of the bounded waits: a chunk of the first warp never copied
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

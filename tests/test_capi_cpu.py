@@ -103,3 +103,16 @@ def test_projected_eigen_rejects_orders_beyond_twenty(so):
     assert K.lib().net_projected_eigen(21, K._ptr(a), K._ptr(a), K._ptr(a), err, K.ERR_LEN) != 0
     assert b"between 0 and 20" in err.value
     assert K.lib().net_projected_eigen(0, None, None, None, err, K.ERR_LEN) == 0
+
+
+def test_tuning_keys_reject_bad_values(so):
+    """Checked on the host: unknown keys and out-of-range values fail."""
+    import knappnet_b200 as K
+    L = K.lib()
+    assert L.net_set_tuning(4, 13.0) != 0
+    assert L.net_set_tuning(13, 9.0) != 0
+    assert L.net_set_tuning(14, -2.0) != 0
+    assert L.net_set_tuning(14, 0.5) != 0
+    assert L.net_set_tuning(15, 0.0) != 0
+    assert L.net_set_tuning(13, 0.0) == 0
+    assert L.net_set_tuning(14, -1.0) == 0

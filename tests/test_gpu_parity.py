@@ -531,6 +531,29 @@ def test_bulk_staged_sweep_matches_sliced_sweep(long_row):
         K.set_tuning(K.TUNE_BULK_CTAS, 0)
 
 
+def test_bulk_staged_wait_runs_out_and_the_context_stays_usable():
+    """Kernel 12's waits on its staged copies are bounded. With tuning key 14
+    the grid's first warp never issues the copies of its first chunk, so its
+    wait on that chunk's barrier runs out after about a second: the sweep
+    marks its state, the solve fails with an error instead of hanging, and
+    the next solve on the same handle is correct."""
+    kg, og = rmat_pair(12, True, seed=31)
+    ref = og.pagerank(weighted=True)
+    try:
+        K.set_tuning(K.TUNE_VARIANT, 12)
+        K.set_tuning(K.TUNE_BULK_SKIP_CHUNK, 0)
+        with pytest.raises(K.EngineError, match="gave up waiting for its staged arc copies"):
+            kg.pagerank_ex(weighted=True, precision=K.PREC_FP64)
+        K.set_tuning(K.TUNE_BULK_SKIP_CHUNK, -1)
+        a, info = kg.pagerank_ex(weighted=True, precision=K.PREC_FP64)
+        assert info.sweep_kernel == 12
+        assert np.abs(a - ref).sum() <= 1e-12
+        assert info.iterations == og.last_iters
+    finally:
+        K.set_tuning(K.TUNE_BULK_SKIP_CHUNK, -1)
+        K.set_tuning(K.TUNE_VARIANT, 0)
+
+
 # The sweep kernels the tuner chooses between (pagerank.cu, tuned_sweep):
 # (kernel, long-row threshold, L1-allocating FP32 columns).
 TUNER_CANDIDATES = [(9, 255, 49152), (9, 255, 24576), (9, 255, 98304), (10, 255, 49152),
@@ -575,7 +598,8 @@ def test_tuner_picks_once_per_operator_and_reports_it():
     x1, i1 = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_MIXED)
     x2, i2 = kg.pagerank_ex(weighted=True, tol=1e-10, precision=K.PREC_MIXED)
     pick = (i1.sweep_kernel, i1.long_row if i1.sweep_kernel != 8 else 0, i1.hot_columns)
-    assert pick in TUNER_CANDIDATES
+    # 64 warps per SM is a candidate for FP64 solves only
+    assert pick in TUNER_CANDIDATES and pick[0] != 10
     assert (i2.sweep_kernel, i2.long_row, i2.hot_columns) == \
         (i1.sweep_kernel, i1.long_row, i1.hot_columns)
     assert np.array_equal(x1, x2)
