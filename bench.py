@@ -306,6 +306,21 @@ def run_ours(args):
         if dom_kind in tdoc:
             traffic = tdoc[dom_kind].get("bytes_per_launch_full_scale")
 
+    # The gather bound: random 4-byte loads per second from an array the size
+    # of the FP32 iterate (L2-resident), measured on this GPU after the timed
+    # region. Gathers that miss L1 (the ncu capture's hit rate) go to L2.
+    gather_rate = K.measure_gather(0, n)
+    hit = None
+    if tfile.exists():
+        hit = json.loads(tfile.read_text()).get("fp32", {}).get("l1_sector_hit_rate_scale22")
+    gather = {"l2_gathers_per_s": round(gather_rate, 0), "gathers_per_sweep": m,
+              "array": f"{n:,} FP32 values, the size of the FP32 iterate",
+              "all_from_l2_ms": round(m / gather_rate * 1e3, 4)}
+    if hit is not None and r32:
+        l2_ms = m * (1.0 - hit) / gather_rate * 1e3
+        gather.update({"l1_hit_rate_ncu": hit, "l1_misses_from_l2_ms": round(l2_ms, 4),
+                       "fp32_sweep_frac_of_gather_bound": round(l2_ms / r32["duration_ms"], 4)})
+
     clock = clocks.summary()
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
@@ -330,7 +345,7 @@ def run_ours(args):
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": dom["frac"] if dom else None, "traffic": traffic,
                      "fp32_sweep": r32, "fp64_sweep_in_mixed": r64m, "refine_sweep": rr,
-                     "fp64_path_sweep": r64},
+                     "fp64_path_sweep": r64, "gather_bound": gather},
         "clocks": clock,
         "fp64_path": {"value": round(float(m) * info64.iterations / fp64_time / 1e9, 3),
                       "time_to_solution_ms": round(fp64_time * 1e3, 3),

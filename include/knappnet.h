@@ -461,6 +461,15 @@ NET_API int32_t net_pagerank_csr_static(int64_t n, const uint32_t *d_offsets,
                                 int64_t *iterations, void *stream, char *err,
                                 size_t err_len);
 
+/* Calibration: random 4-byte gathers per second the whole GPU sustains,
+ * from a device array of `words` FP32 values (source 0; an array that fits
+ * in L2 gives the rate a sparse sweep's gathers of its iterate run into),
+ * from each SM's own shared memory (source 1), or from the shared memory of
+ * a thread-block cluster of 2, 4 or 8 CTAs (source 2, 4, 8). Takes tens of
+ * milliseconds. */
+NET_API int32_t net_measure_gather(int32_t source, int64_t words, double *gathers_per_second,
+                                   char *err, size_t err_len);
+
 /* Waits for the device; reports an asynchronous CUDA error if one occurred. */
 NET_API int32_t net_device_sync(char *err, size_t err_len);
 

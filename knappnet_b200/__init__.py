@@ -153,6 +153,8 @@ def lib() -> ctypes.CDLL:
     L.net_sweep_timing.restype = i32
     L.net_set_sweep_timing.argtypes = [i32]
     L.net_set_sweep_timing.restype = None
+    L.net_measure_gather.argtypes = [i32, i64, ctypes.POINTER(f64), cp, sz]
+    L.net_measure_gather.restype = i32
     L.net_set_tuning.argtypes = [i32, f64]
     L.net_set_tuning.restype = i32
     L.net_device_sync.argtypes = [cp, sz]
@@ -555,6 +557,16 @@ TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUN
 # shared memory by bulk copies
 VARIANT_WARP_L1, VARIANT_SLICE, VARIANT_SLICE64, VARIANT_SLICE_SMEM, VARIANT_SLICE_BULK = \
     8, 9, 10, 11, 12
+
+
+def measure_gather(source: int = 0, words: int = 1 << 24) -> float:
+    """Random 4-byte gathers per second over the GPU (net_measure_gather):
+    source 0 from a device array of `words` FP32 values, 1 from each SM's
+    shared memory, 2, 4 or 8 from a cluster's shared memory."""
+    r = ctypes.c_double()
+    err = ctypes.create_string_buffer(ERR_LEN)
+    _check(lib().net_measure_gather(int(source), int(words), ctypes.byref(r), err, ERR_LEN), err)
+    return r.value
 
 
 def set_tuning(key: int, value: float) -> None:

@@ -19,6 +19,7 @@
 #include "ego.cuh"
 #include "eigen.cuh"
 #include "frame.cuh"
+#include "calibrate.cuh"
 #include "katz.cuh"
 #include "generate.cuh"
 #include "graph.cuh"
@@ -1300,6 +1301,18 @@ int32_t net_projected_eigen(int64_t n, const double* a, double* values, double* 
     if (!a || !values || !vectors) throw Error("a buffer is null");
     if (!knb::symmetric_eigen_device(a, (int)n, values, vectors, knb::thread_stream()))
       throw Error("the QL iteration did not converge");
+  });
+}
+
+int32_t net_measure_gather(int32_t source, int64_t words, double* gathers_per_second, char* err,
+                           size_t err_len) {
+  return guard(err, err_len, [&] {
+    if (!gathers_per_second) throw Error("gathers_per_second is null");
+    if (source != 0 && source != 1 && source != 2 && source != 4 && source != 8)
+      throw Error("gather source must be 0 (device array), 1 (shared memory) or 2, 4, 8 (cluster)");
+    if (source == 0 && (words < 1024 || words > (int64_t(1) << 31)))
+      throw Error("the array must hold between 1024 and 2^31 values");
+    *gathers_per_second = knb::measure_gather_rate(source, (uint64_t)words, knb::thread_stream());
   });
 }
 

@@ -116,3 +116,16 @@ def test_tuning_keys_reject_bad_values(so):
     assert L.net_set_tuning(15, 0.0) != 0
     assert L.net_set_tuning(13, 0.0) == 0
     assert L.net_set_tuning(14, -1.0) == 0
+
+
+def test_gather_calibration_checks_arguments_before_device_work(so):
+    import knappnet_b200 as K
+    L = K.lib()
+    err = ctypes.create_string_buffer(K.ERR_LEN)
+    r = ctypes.c_double()
+    assert L.net_measure_gather(3, 1 << 20, ctypes.byref(r), err, K.ERR_LEN) != 0
+    assert b"gather source" in err.value
+    assert L.net_measure_gather(0, 100, ctypes.byref(r), err, K.ERR_LEN) != 0
+    assert b"between 1024 and 2^31" in err.value
+    assert L.net_measure_gather(0, 1 << 20, None, err, K.ERR_LEN) != 0
+    assert b"null" in err.value
