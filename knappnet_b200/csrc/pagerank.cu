@@ -1,10 +1,11 @@
 // PageRank power iteration on the device (reference: the loop of
 // crates/engine/src/metrics/spectral.rs:211-281).
 //
-// One sweep is two kernels: the merge-path SpMV with the PageRank update
-// fused into its epilogue (tile_spmv + PagerankEpi) and the split-row /
-// reduction kernel (split_rows). A third, normally idle, kernel computes the
-// exact L1 change when the fused estimate is too close to the tolerance.
+// One sweep is two kernels: the sparse product with the PageRank update
+// fused into its epilogue (by default the sliced sweep slice_spmv, else a
+// merge-path kernel, with PagerankEpi) and the split-row / reduction kernel
+// (split_rows). A third, normally idle, kernel computes the exact L1 change
+// when the fused estimate is too close to the tolerance.
 //
 // Normalisation is folded into the next sweep. The device stores the
 // unnormalised iterate y_k and z_k = y_k / out (0 for dangling nodes); with
@@ -20,12 +21,12 @@
 // exact change is computed by pr_exact_change before deciding.
 //
 // Mixed precision runs the same trajectory: FP32 sweeps (FP32 arc values,
-// iterate and row sums; FP64 reductions) from the uniform start, then FP64
-// sweeps from the FP32 iterate until the reference's stopping rule holds in
-// FP64. The FP32 phase ends when its change falls below
-// max(tol * switch_factor, switch_floor): the FP32 perturbation of the
-// trajectory (about 1e-7 in L1) then decays over the remaining FP64 sweeps by
-// the same factor as the change, to well below the tolerance.
+// iterate and row sums; FP64 reductions) from the uniform start, then one
+// FP64 anchor sweep and refinement sweeps (RefineEpi) until the reference's
+// stopping rule holds in FP64. The FP32 phase ends when its change falls
+// below max(tol * switch_factor, switch_floor): the FP32 perturbation of the
+// trajectory (about 1e-7 in L1) then decays over the remaining sweeps by the
+// same factor as the change, to well below the tolerance.
 #include <algorithm>
 #include <cfloat>
 #include <map>
@@ -551,9 +552,6 @@ static uint32_t hot_nodes(uint32_t n, size_t warp_bytes, int smem_optin) {
   return (uint32_t)hn;
 }
 
-// One merge-path sweep with epilogue `e`: the sweep kernel of variant VAR
-// gathering x, then the split-row kernel, whose CTAs also reduce the
-// epilogue's per-tile scalars and whose last CTA decides convergence.
 // CTAs of a sliced sweep that fit on the device at once (per device and
 // shared-memory size).
 template <class VT, class MT, class Epi, int U, int WPB, int MINB, int GNA>
@@ -650,6 +648,10 @@ static unsigned launch_slice_bulk(const SlicedOp& so, const VT* x, const Epi& e,
   return grid * BULK_WPB;
 }
 
+// One sweep with epilogue `e`: the sweep kernel of variant VAR gathering x
+// (sliced, bulk-staged or merge-path), then the split-row kernel, whose CTAs
+// also reduce the epilogue's per-tile or per-warp scalars and whose last CTA
+// decides convergence.
 template <class VT, class MT, class Epi, int VAR, int IPT>
 static void launch_spmv(const Operator& op, const Partition& P, const OpView<MT>& v,
                         const VT* x, const Epi& e, VT* carry, VT* head, double* part1,
@@ -1230,8 +1232,8 @@ void pagerank_op(Operator& op, const PagerankParams& prm_in, double* out, bool o
   const uint32_t n = op.n;
   if (n == 0) return;
   // Kernel choice (measured on R-MAT scale 24): the sliced layout, 48
-  // resident warps per SM, 8 gathers in flight per lane in FP32 sweeps and 4
-  // in the others; long rows from 255 arcs. Against the merge-path warp
+  // resident warps per SM, 4 gathers in flight per lane; long rows from 255
+  // arcs (the tuner may pick another candidate). Against the merge-path warp
   // tiles on the layout renumbered by column count (kernel 8) it takes the
   // FP32 sweep from 1.20 to 0.85 ms and the FP64 sweep from 1.56 to 0.99 ms.
   // Without renumbering (tuning key 1 set to 0) the merge-path warp tiles
