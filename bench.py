@@ -642,6 +642,8 @@ def run_c4b(args):
             "kernel_launches": int(keep["info"].kernel_launches),
             "launch_graph_instantiations": int(keep["info"].long_row),
             "threads_per_cta": int(keep["info"].sweep_kernel),
+            "ctas_per_cluster": int(keep["info"].hot_columns),
+            "graphs_split_over_clusters": int(keep["info"].iterations_fp32),
             "max_iterations": int(keep["its"].max()),
             "l1_vs_oracle_worst_of_200": worst,
             "cpu_restatement_ms_estimated": round(cpu * total_work / work * 1e3, 1),

@@ -187,7 +187,10 @@ typedef struct NetSolveInfo {
   int32_t long_row;        /* sliced sweeps: rows of at least this many arcs are long;
                               packed graphs: how many times the operator's launch graph
                               has been instantiated (a repeated batch replays it) */
-  int32_t hot_columns;     /* FP32 values of the most gathered columns kept in L1 */
+  int32_t hot_columns;     /* FP32 values of the most gathered columns kept in L1;
+                              packed graphs: CTAs per thread-block cluster that split
+                              each large graph (1: no graph split; iterations_fp32
+                              then counts the graphs split) */
 } NetSolveInfo;
 
 /* Precision codes: 0 = FP64, 1 = mixed (FP32 sweeps, then FP64 sweeps on
@@ -422,7 +425,11 @@ NET_API void net_set_sweep_timing(int32_t on);
  * (0); 13 = CTAs per SM kernel 12 sizes its shared memory for (0: 4, 1..8);
  * 14 = for testing kernel 12's bounded waits: the chunk of the grid's first
  * warp whose copies are never issued, so that its wait runs out after about
- * one second and the solve fails with an error (-1, default: none).
+ * one second and the solve fails with an error (-1, default: none);
+ * 15 = packed graphs: graphs of at least this many nodes are each split
+ * over a thread-block cluster (0, default: the larger of 4096 and the node
+ * count over the launch's CTAs); 16 = packed graphs: CTAs per cluster for
+ * those graphs (0 tuned with key 6 on first use, 1 none, 4, 8).
  * Setting key 0, 4, 7 or 10 also bypasses the timing.
  * Returns 1 for an unknown key or value. */
 NET_API int32_t net_set_tuning(int32_t key, double value);

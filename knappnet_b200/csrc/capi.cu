@@ -927,6 +927,8 @@ int32_t net_pagerank_graphs(const GraphHandle* h, int64_t count, const int64_t* 
       info->kernel_launches = 1;
       info->sweep_kernel = r.threads;  // threads per CTA of the packed launch
       info->long_row = r.instantiations;  // instantiations of the operator's launch graph
+      info->hot_columns = r.cluster;      // CTAs per cluster that split the large graphs
+      info->iterations_fp32 = r.split_graphs;  // graphs split over a cluster
     }
   });
 }
@@ -1287,6 +1289,14 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 14:
       if (!(value >= -1 && value <= 2147483647.0) || value != (double)(int64_t)value) return 1;
       t.bulk_skip_chunk = (int64_t)value;
+      return 0;
+    case 15:
+      if (!(value >= 0 && value <= 4294967295.0) || value != (double)(int64_t)value) return 1;
+      knb::set_ego_big_nodes((int64_t)value);
+      return 0;
+    case 16:
+      if (value != 0 && value != 1 && value != 4 && value != 8) return 1;
+      knb::set_ego_cluster((int)value);
       return 0;
     default:
       return 1;

@@ -14,11 +14,16 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "ego.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace knb {
 
@@ -41,83 +46,160 @@ __device__ __forceinline__ double cta_sum(double v, double* sh) {
   return t;
 }
 
+// Sum over the rows of one graph split across the CTAs of a cluster: each
+// CTA's fixed-order sum goes to its slot, and every thread adds the slots in
+// rank order through distributed shared memory, so all CTAs hold the same
+// bits. The cluster barrier also publishes every global write made before
+// it to the whole cluster (the z a product gathers from other CTAs' rows).
+template <int C>
+__device__ __forceinline__ double cluster_sum(double v, double* sh, double* slot,
+                                              cg::cluster_group& cl) {
+  const double t = cta_sum(v, sh);
+  if (threadIdx.x == 0) *slot = t;
+  cl.sync();
+  double s = 0;
+#pragma unroll
+  for (int r = 0; r < C; ++r) s += *cl.map_shared_rank(slot, (unsigned)r);
+  return s;
+}
+
+// One graph's iteration over rows [lo, hi) of nodes [g_lo, g_hi): the whole
+// graph when C is 1 (one CTA), this CTA's share of it otherwise. Slots (C >
+// 1): 2 x 3 doubles of this CTA's shared memory, by iteration parity and
+// reduction, so a slot is written again only after every CTA has read it.
+template <int C>
+__device__ void ego_solve(const OpView<double>& op, const double* __restrict__ outstr,
+                          uint32_t g_lo, uint32_t g_hi, uint32_t lo, uint32_t hi,
+                          const EgoParams& prm, const double* __restrict__ pers, double ps,
+                          double* __restrict__ xa, double* __restrict__ xb,
+                          double* __restrict__ zb, double* __restrict__ out, int32_t* it_out,
+                          int32_t* done_out, double* sh, double* slots) {
+  auto reduce = [&](double v, int which, int parity) -> double {
+    if constexpr (C == 1) {
+      (void)which;
+      (void)parity;
+      return cta_sum(v, sh);
+    } else {
+      cg::cluster_group cl = cg::this_cluster();
+      return cluster_sum<C>(v, sh, slots + parity * 3 + which, cl);
+    }
+  };
+  const uint32_t nk = g_hi - g_lo;
+  const double inv_n = 1.0 / (double)nk;
+  double* x = xa;
+  double* y = xb;
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) x[i] = inv_n;
+  __syncthreads();
+  int32_t it = 0, done = 0;
+  while (it < prm.max_iter) {
+    const int par = it & 1;
+    // z = x / out; stuck = dangling mass
+    double stuck = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      const double o = outstr[i];
+      if (o > 0.0) {
+        zb[i] = x[i] / o;
+      } else {
+        zb[i] = 0.0;
+        stuck += x[i];
+      }
+    }
+    stuck = reduce(stuck, 0, par);  // includes the barrier before z is read
+    // y = d (A z + stuck jump) + (1 - d) p
+    double total = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      double s = 0;
+      for (uint32_t k = op.off[i]; k < op.off[i + 1]; ++k) {
+        const double w = op.vals ? op.vals[k] : 1.0;
+        s += w * zb[op.cols[k]];
+      }
+      const double p = pers ? pers[i] / ps : inv_n;
+      const double jmp = prm.jump_uniform ? inv_n : p;
+      const double v = prm.d * (s + stuck * jmp) + (1.0 - prm.d) * p;
+      y[i] = v;
+      total += v;
+    }
+    total = reduce(total, 1, par);
+    double change = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      const double v = y[i] / total;
+      y[i] = v;
+      change += fabs(v - x[i]);
+    }
+    change = reduce(change, 2, par);
+    double* t = x;
+    x = y;
+    y = t;
+    ++it;
+    if (change <= prm.tol) {  // the same bits in every CTA of a cluster
+      done = 1;
+      break;
+    }
+  }
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) out[i] = x[i];
+  *it_out = it;
+  *done_out = done;
+}
+
+// The persistent launch. With clusters of C > 1 CTAs, each cluster first
+// takes the large graphs (order[0, nbig), largest first) off queue[0], its
+// CTAs splitting each graph's rows; once those are gone every CTA takes the
+// other graphs (order[nbig, count)) off queue[1] alone. Cluster barriers
+// are hardware barriers every CTA of the cluster executes the same number of
+// times: the graph index comes from rank 0's shared memory, and every CTA
+// stops a graph's iteration on the same bits.
+template <int C>
 __global__ void ego_pagerank(OpView<double> op, const double* __restrict__ outstr,
                              const uint32_t* __restrict__ node_off, const uint32_t* __restrict__ order,
-                             uint32_t count, unsigned int* __restrict__ queue, EgoParams prm,
-                             const double* __restrict__ pers, const double* __restrict__ psum,
-                             double* __restrict__ xa, double* __restrict__ xb,
-                             double* __restrict__ zb, double* __restrict__ out,
-                             int32_t* __restrict__ iters, int32_t* __restrict__ status) {
+                             uint32_t count, uint32_t nbig, unsigned int* __restrict__ queue,
+                             EgoParams prm, const double* __restrict__ pers,
+                             const double* __restrict__ psum, double* __restrict__ xa,
+                             double* __restrict__ xb, double* __restrict__ zb,
+                             double* __restrict__ out, int32_t* __restrict__ iters,
+                             int32_t* __restrict__ status) {
   __shared__ double sh[32];
+  __shared__ double slots[6];
   __shared__ uint32_t g_sh;
+  if constexpr (C > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    for (;;) {
+      if (rank == 0 && threadIdx.x == 0) g_sh = atomicAdd(queue, 1u);
+      cl.sync();  // rank 0's pick is visible
+      const uint32_t gi = *cl.map_shared_rank(&g_sh, 0u);
+      cl.sync();  // every CTA has read it before rank 0 picks again or leaves
+      if (gi >= nbig) break;
+      const uint32_t graph = order[gi];
+      const uint32_t g_lo = node_off[graph], g_hi = node_off[graph + 1];
+      const uint32_t per = (g_hi - g_lo + C - 1) / C;
+      const uint32_t lo = min(g_hi, g_lo + rank * per), hi = min(g_hi, lo + per);
+      int32_t it = 0, done = 0;
+      ego_solve<C>(op, outstr, g_lo, g_hi, lo, hi, prm, pers, pers ? psum[graph] : 1.0, xa, xb,
+                   zb, out, &it, &done, sh, slots);
+      if (rank == 0 && threadIdx.x == 0) {
+        iters[graph] = it;
+        status[graph] = done ? 0 : 1;
+      }
+    }
+  }
   for (;;) {
-    if (threadIdx.x == 0) g_sh = atomicAdd(queue, 1u);
+    if (threadIdx.x == 0) g_sh = atomicAdd(queue + 1, 1u);
     __syncthreads();
-    const uint32_t gi = g_sh;
+    const uint32_t gi = nbig + g_sh;
     __syncthreads();
     if (gi >= count) return;
     const uint32_t graph = order[gi];
-    const uint32_t lo = node_off[graph], hi = node_off[graph + 1];
-    const uint32_t nk = hi - lo;
-    if (nk == 0) {
+    const uint32_t g_lo = node_off[graph], g_hi = node_off[graph + 1];
+    if (g_hi == g_lo) {
       if (threadIdx.x == 0) {
         iters[graph] = 0;
         status[graph] = 0;
       }
       continue;
     }
-    const double inv_n = 1.0 / (double)nk;
-    const double ps = pers ? psum[graph] : 1.0;
-    double* x = xa;
-    double* y = xb;
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) x[i] = inv_n;
-    __syncthreads();
     int32_t it = 0, done = 0;
-    while (it < prm.max_iter) {
-      // z = x / out; stuck = dangling mass
-      double stuck = 0;
-      for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-        const double o = outstr[i];
-        if (o > 0.0) {
-          zb[i] = x[i] / o;
-        } else {
-          zb[i] = 0.0;
-          stuck += x[i];
-        }
-      }
-      stuck = cta_sum(stuck, sh);  // includes the barrier before z is read
-      // y = d (A z + stuck jump) + (1 - d) p
-      double total = 0;
-      for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-        double s = 0;
-        for (uint32_t k = op.off[i]; k < op.off[i + 1]; ++k) {
-          const double w = op.vals ? op.vals[k] : 1.0;
-          s += w * zb[op.cols[k]];
-        }
-        const double p = pers ? pers[i] / ps : inv_n;
-        const double jmp = prm.jump_uniform ? inv_n : p;
-        const double v = prm.d * (s + stuck * jmp) + (1.0 - prm.d) * p;
-        y[i] = v;
-        total += v;
-      }
-      total = cta_sum(total, sh);
-      double change = 0;
-      for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-        const double v = y[i] / total;
-        y[i] = v;
-        change += fabs(v - x[i]);
-      }
-      change = cta_sum(change, sh);
-      double* t = x;
-      x = y;
-      y = t;
-      ++it;
-      if (change <= prm.tol) {
-        done = 1;
-        break;
-      }
-    }
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) out[i] = x[i];
+    ego_solve<1>(op, outstr, g_lo, g_hi, g_lo, g_hi, prm, pers, pers ? psum[graph] : 1.0, xa, xb,
+                 zb, out, &it, &done, sh, slots);
     if (threadIdx.x == 0) {
       iters[graph] = it;
       status[graph] = done ? 0 : 1;
@@ -144,8 +226,43 @@ __global__ void ego_check_blocks(const uint32_t* __restrict__ src, const uint32_
 }
 
 static int g_ego_threads = 0;  // 0: tuned on first use (per process)
+static int g_ego_cluster = 0;  // CTAs per cluster for the large graphs; 0: tuned with the threads
+static int64_t g_ego_big = 0;  // nodes from which a graph is large; 0: automatic
 
 void set_ego_threads(int t) { g_ego_threads = t; }
+void set_ego_cluster(int c) { g_ego_cluster = c; }
+void set_ego_big_nodes(int64_t v) { g_ego_big = v; }
+
+// Clusters of C CTAs of `threads` that fit on the device at once (0 if none),
+// per device and shape.
+template <int C>
+static int ego_clusters(int threads) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> cache;
+  int dev = 0;
+  KNB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({dev, threads});
+  if (it != cache.end()) return it->second;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(threads);
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)ego_pagerank<C>, &cfg) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    clusters = 0;
+  }
+  cache[{dev, threads}] = clusters;
+  return clusters;
+}
 
 // A packed batch kept per operator between calls: the graph offsets and the
 // largest-first order, every buffer, and the launch (queue reset and kernel)
@@ -158,7 +275,10 @@ struct EgoPlan : Workspace {
   std::vector<uint32_t> hoff;  // the batch the buffers are laid out for
   bool pers = false;
   EgoParams prm{};
+  std::vector<uint32_t> sizes;  // node counts of the graphs, largest first
   int threads = 0;             // of the instantiated launch
+  int cluster = 1;             // CTAs per cluster of the instantiated launch
+  uint32_t nbig = 0;           // graphs it gives to clusters
   DevBuf<uint32_t> doff, dorder;
   DevBuf<double> dpers, dpsum, xa, xb, zb, dout;
   DevBuf<int32_t> iters, status;
@@ -253,13 +373,15 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
     });
     KNB_CUDA(cudaMemcpyAsync(P.dorder.get(), order.data(), (size_t)count * 4,
                              cudaMemcpyHostToDevice, s));
+    P.sizes.resize(count);
+    for (uint32_t k = 0; k < count; ++k) P.sizes[k] = hoff[order[k] + 1] - hoff[order[k]];
     P.xa.alloc(n);
     P.xb.alloc(n);
     P.zb.alloc(n);
     P.dout.alloc(n);
     P.iters.alloc(count);
     P.status.alloc(count);
-    P.queue.alloc(1);
+    P.queue.alloc(2);
     P.dpers.release();
     P.dpsum.release();
     KNB_CUDA(cudaStreamSynchronize(s));
@@ -279,52 +401,103 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
   int dev = 0, sms = 148;
   KNB_CUDA(cudaGetDevice(&dev));
   KNB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  auto launch = [&](int threads, cudaStream_t st) {
-    KNB_CUDA(cudaMemsetAsync(P.queue.get(), 0, 4, st));
-    const unsigned grid = (unsigned)std::min<uint64_t>(count, (uint64_t)sms * (2048 / threads));
-    ego_pagerank<<<grid, threads, 0, st>>>(op.view64(), op.colsum.get(), P.doff.get(),
-                                           P.dorder.get(), count, P.queue.get(), prm,
-                                           pers ? P.dpers.get() : nullptr,
-                                           pers ? P.dpsum.get() : nullptr, P.xa.get(), P.xb.get(),
-                                           P.zb.get(), P.dout.get(), P.iters.get(),
-                                           P.status.get());
+  // The launch: with clusters of C > 1 CTAs the graphs of at least `big`
+  // nodes (by default max(4096, n / CTAs of the grid), so no graph holds
+  // much more than a CTA's share of the batch) are each split over a
+  // cluster; the others go one per CTA. Returns the graphs given to clusters.
+  auto big_count = [&](uint64_t ctas) {
+    const uint64_t big = g_ego_big > 0 ? (uint64_t)g_ego_big
+                                       : std::max<uint64_t>(4096, (uint64_t)n / std::max<uint64_t>(ctas, 1));
+    uint32_t nb = 0;
+    while (nb < count && P.sizes[nb] >= big) ++nb;
+    return nb;
+  };
+  auto launch = [&](int threads, int C, cudaStream_t st) -> uint32_t {
+    KNB_CUDA(cudaMemsetAsync(P.queue.get(), 0, 8, st));
+    const uint64_t fit = (uint64_t)sms * (2048 / threads);
+    int clusters = 0;
+    if (C == 4) clusters = ego_clusters<4>(threads);
+    if (C == 8) clusters = ego_clusters<8>(threads);
+    const uint32_t nbig = clusters > 0 ? big_count((uint64_t)clusters * C) : 0;
+    if (nbig == 0) {
+      const unsigned grid = (unsigned)std::min<uint64_t>(count, fit);
+      ego_pagerank<1><<<grid, threads, 0, st>>>(
+          op.view64(), op.colsum.get(), P.doff.get(), P.dorder.get(), count, 0u, P.queue.get(),
+          prm, pers ? P.dpers.get() : nullptr, pers ? P.dpsum.get() : nullptr, P.xa.get(),
+          P.xb.get(), P.zb.get(), P.dout.get(), P.iters.get(), P.status.get());
+      KNB_LAUNCH("ego_pagerank");
+      return 0;
+    }
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(clusters * C));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    auto args = [&](auto fn) {
+      KNB_CUDA(cudaLaunchKernelEx(&cfg, fn, op.view64(), (const double*)op.colsum.get(),
+                                  (const uint32_t*)P.doff.get(), (const uint32_t*)P.dorder.get(),
+                                  count, nbig, P.queue.get(), prm,
+                                  (const double*)(pers ? P.dpers.get() : nullptr),
+                                  (const double*)(pers ? P.dpsum.get() : nullptr), P.xa.get(),
+                                  P.xb.get(), P.zb.get(), P.dout.get(), P.iters.get(),
+                                  P.status.get()));
+    };
+    if (C == 4) args(ego_pagerank<4>);
+    else args(ego_pagerank<8>);
     KNB_LAUNCH("ego_pagerank");
+    return nbig;
   };
   if (!P.t0) {
     KNB_CUDA(cudaEventCreate(&P.t0));
     KNB_CUDA(cudaEventCreate(&P.t1));
   }
-  // Threads per CTA: tuned once per process by timing each candidate on
-  // this batch (the results do not depend on the choice).
-  if (g_ego_threads == 0) {
+  // Threads per CTA and CTAs per cluster: tuned once per process by timing
+  // each candidate on this batch (the results do not depend on the choice
+  // beyond the association of a split graph's sums).
+  if (g_ego_threads == 0 || g_ego_cluster == 0) {
     float best = 1e30f;
-    int pick = 256;
+    int pick_t = 256, pick_c = 1;
     for (int t : {128, 256, 512, 1024}) {
-      KNB_CUDA(cudaEventRecord(P.t0, s));
-      launch(t, s);
-      KNB_CUDA(cudaEventRecord(P.t1, s));
-      KNB_CUDA(cudaEventSynchronize(P.t1));
-      float ms = 0;
-      KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
-      if (ms < best) {
-        best = ms;
-        pick = t;
+      if (g_ego_threads != 0 && t != g_ego_threads) continue;
+      for (int c : {1, 4, 8}) {
+        if (g_ego_cluster != 0 && c != g_ego_cluster) continue;
+        KNB_CUDA(cudaEventRecord(P.t0, s));
+        launch(t, c, s);
+        KNB_CUDA(cudaEventRecord(P.t1, s));
+        KNB_CUDA(cudaEventSynchronize(P.t1));
+        float ms = 0;
+        KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
+        if (ms < best) {
+          best = ms;
+          pick_t = t;
+          pick_c = c;
+        }
       }
     }
-    g_ego_threads = pick;
+    g_ego_threads = pick_t;
+    g_ego_cluster = pick_c;
   }
   const int threads = g_ego_threads;
-  if (!P.exec || P.threads != threads || P.pers != pers || !same_params(P.prm, prm)) {
+  const int cluster = g_ego_cluster;
+  if (!P.exec || P.threads != threads || P.cluster != cluster || P.pers != pers ||
+      !same_params(P.prm, prm)) {
     P.drop_graph();
     cudaStream_t cs;
     KNB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     KNB_CUDA(cudaStreamSynchronize(s));
     KNB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    launch(threads, cs);
+    P.nbig = launch(threads, cluster, cs);
     KNB_CUDA(cudaStreamEndCapture(cs, &P.graph));
     KNB_CUDA(cudaGraphInstantiate(&P.exec, P.graph, 0));
     KNB_CUDA(cudaStreamDestroy(cs));
     P.threads = threads;
+    P.cluster = cluster;
     P.pers = pers;
     P.prm = prm;
     ++P.instantiations;
@@ -351,6 +524,8 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
   if (res) {
     res->seconds = ms * 1e-3;
     res->threads = threads;
+    res->cluster = P.nbig ? cluster : 1;
+    res->split_graphs = (int32_t)P.nbig;
     res->instantiations = P.instantiations;
     int64_t tot = 0, mx = 0;
     for (uint32_t k = 0; k < count; ++k) {

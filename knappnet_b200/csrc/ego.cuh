@@ -26,10 +26,14 @@ struct EgoResult {
   int64_t total_iterations = 0;
   int64_t max_iterations = 0;
   int instantiations = 0;  // times the operator's launch graph has been instantiated
+  int cluster = 1;         // CTAs per cluster that split the large graphs (1: none split)
+  int32_t split_graphs = 0;  // graphs split over a cluster
 };
 
 void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoResult* res,
                      cudaStream_t s);
 void set_ego_threads(int threads);
+void set_ego_cluster(int ctas);           // 0: tuned with the threads; 1, 4 or 8
+void set_ego_big_nodes(int64_t nodes);    // 0: automatic
 
 }  // namespace knb

@@ -113,9 +113,13 @@ def test_tuning_keys_reject_bad_values(so):
     assert L.net_set_tuning(13, 9.0) != 0
     assert L.net_set_tuning(14, -2.0) != 0
     assert L.net_set_tuning(14, 0.5) != 0
-    assert L.net_set_tuning(15, 0.0) != 0
+    assert L.net_set_tuning(15, -1.0) != 0
+    assert L.net_set_tuning(16, 2.0) != 0
+    assert L.net_set_tuning(17, 0.0) != 0
     assert L.net_set_tuning(13, 0.0) == 0
     assert L.net_set_tuning(14, -1.0) == 0
+    assert L.net_set_tuning(15, 0.0) == 0
+    assert L.net_set_tuning(16, 0.0) == 0
 
 
 def test_gather_calibration_checks_arguments_before_device_work(so):

@@ -747,6 +747,40 @@ def test_pagerank_graphs_matches_each_graph(directed, weighted):
     assert info.kernel_launches == 1
 
 
+@pytest.mark.parametrize("cluster", [4, 8])
+def test_pagerank_graphs_splits_large_graphs_over_clusters(cluster):
+    """Graphs of at least 50 nodes (tuning key 15) are each split over a
+    thread-block cluster of 4 or 8 CTAs (key 16) that exchange their
+    partial sums through distributed shared memory; every graph still
+    matches its own oracle call, with the same iteration count, and repeated
+    calls give the same bits."""
+    sizes = K.power_law_sizes(80, 2.1, 5, 3000, seed=14)
+    m = np.minimum(6 * sizes, sizes * (sizes - 1) // 2)
+    src, tgt = K.generate_gnm(sizes, m, False, False, seed=15)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    rng = np.random.default_rng(2)
+    w = rng.lognormal(size=len(src))
+    g = K.Graph(int(off[-1]), src, tgt, w, False)
+    try:
+        K.set_tuning(K.TUNE_EGO_BIG_NODES, 50)
+        K.set_tuning(K.TUNE_EGO_CLUSTER, cluster)
+        out, its, info = g.pagerank_graphs(off, weighted=True, tol=1e-11)
+        again, _, _ = g.pagerank_graphs(off, weighted=True, tol=1e-11)
+        assert np.array_equal(out, again)
+        assert info.hot_columns == cluster
+        assert info.iterations_fp32 == int((sizes >= 50).sum()) > 0
+        for k in range(len(sizes)):
+            lo, hi = off[k], off[k + 1]
+            sel = (src >= lo) & (src < hi)
+            og = O.Graph(hi - lo, src[sel] - lo, tgt[sel] - lo, w[sel], False)
+            ref = og.pagerank(weighted=True, tol=1e-11)
+            assert np.abs(out[lo:hi] - ref).sum() <= 1e-12, k
+            assert its[k] == og.last_iters, k
+    finally:
+        K.set_tuning(K.TUNE_EGO_BIG_NODES, 0)
+        K.set_tuning(K.TUNE_EGO_CLUSTER, 0)
+
+
 def test_pagerank_graphs_replays_its_launch_graph():
     """A repeated batch replays the instantiated launch graph (no new
     instantiation) with the same results; new teleport values are copied in
