@@ -550,7 +550,7 @@ def set_sweep_timing(on: bool) -> None:
 TUNE_IPT, TUNE_RELABEL, TUNE_SWITCH_FACTOR, TUNE_SWITCH_FLOOR, TUNE_VARIANT, TUNE_CARVEOUT, \
     TUNE_EGO_THREADS, TUNE_HOT_NODES, TUNE_PERSISTENT, TUNE_REFINE, TUNE_LONG_ROW, \
     TUNE_SMEM_HOT, TUNE_AUTOTUNE, TUNE_BULK_CTAS, TUNE_BULK_SKIP_CHUNK, TUNE_EGO_BIG_NODES, \
-    TUNE_EGO_CLUSTER = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16
+    TUNE_EGO_CLUSTER, TUNE_SMALL_EDGES = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17
 # sweep kernels (TUNE_VARIANT): merge-path warp tiles with L1-filtered
 # gathers; the sliced layout at 48 and 64 resident warps per SM, with the
 # most gathered values in shared memory, and with the arc streams staged in

@@ -374,6 +374,41 @@ static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t direc
       p.personalization = personalization;
       p.pers_on_device = pers_dev != 0;
     }
+    // A small graph's FP64 solve with a uniform teleport runs as a packed
+    // batch of one graph: one launch does every iteration on the device (a
+    // cluster of CTAs splits it from 4096 nodes), where the sweep path would
+    // launch a few kernels per iteration that each take microseconds.
+    const knb::Tuning& tu = knb::tuning();
+    if (precision == 0 && !personalization && tu.variant == 0 && tu.small_edges > 0 &&
+        (int64_t)g.m <= tu.small_edges) {
+      const int64_t off[2] = {0, (int64_t)g.n};
+      int64_t iters = 0;
+      knb::EgoInput in;
+      in.count = 1;
+      in.node_offsets = off;
+      in.damping = p.damping;
+      in.directed = p.directed;
+      in.weighted = p.weighted;
+      in.dangling = dangling;
+      in.loops = loops;
+      in.tol = p.tol;
+      in.max_iter = p.max_iter;
+      in.out_on_device = out_dev != 0;
+      in.iterations_out = &iters;
+      knb::EgoResult r;
+      knb::pagerank_graphs(g, in, out, &r, s);
+      if (info) {
+        memset(info, 0, sizeof(*info));
+        info->iterations = iters;
+        info->seconds = r.seconds;
+        info->converged = 1;
+        info->kernel_launches = 1;
+        info->sweep_kernel = 0;  // no sweep kernel: the packed-graph launch
+        info->long_row = r.instantiations;
+        info->hot_columns = r.cluster;
+      }
+      return;
+    }
     knb::PagerankInfo pi;
     knb::pagerank(g, p, out, out_dev != 0, &pi, s);
     if (info) {
@@ -1297,6 +1332,10 @@ int32_t net_set_tuning(int32_t key, double value) {
     case 16:
       if (value != 0 && value != 1 && value != 4 && value != 8) return 1;
       knb::set_ego_cluster((int)value);
+      return 0;
+    case 17:
+      if (!(value >= 0 && value <= 4294967295.0) || value != (double)(int64_t)value) return 1;
+      t.small_edges = (int64_t)value;
       return 0;
     default:
       return 1;

@@ -46,27 +46,52 @@ __device__ __forceinline__ double cta_sum(double v, double* sh) {
   return t;
 }
 
-// Sum over the rows of one graph split across the CTAs of a cluster: each
-// CTA's fixed-order sum goes to its slot, and every thread adds the slots in
+// Sums over the rows of one graph split across the CTAs of a cluster: each
+// CTA's fixed-order sums go to its slots, and every thread adds the slots in
 // rank order through distributed shared memory, so all CTAs hold the same
 // bits. The cluster barrier also publishes every global write made before
 // it to the whole cluster (the z a product gathers from other CTAs' rows).
-template <int C>
-__device__ __forceinline__ double cluster_sum(double v, double* sh, double* slot,
-                                              cg::cluster_group& cl) {
-  const double t = cta_sum(v, sh);
-  if (threadIdx.x == 0) *slot = t;
-  cl.sync();
-  double s = 0;
+template <int C, int K>
+__device__ __forceinline__ void cluster_sums(double (&v)[K], double* sh, double* slot,
+                                             cg::cluster_group& cl) {
 #pragma unroll
-  for (int r = 0; r < C; ++r) s += *cl.map_shared_rank(slot, (unsigned)r);
-  return s;
+  for (int j = 0; j < K; ++j) {
+    const double t = cta_sum(v[j], sh);
+    if (threadIdx.x == 0) slot[j] = t;
+  }
+  cl.sync();
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double s = 0;
+#pragma unroll
+    for (int r = 0; r < C; ++r) s += cl.map_shared_rank(slot, (unsigned)r)[j];
+    v[j] = s;
+  }
+}
+
+// Fixed-order sums of K values over the rows of a graph: one CTA (C == 1)
+// or a cluster. Slots (C > 1): two sets of 4 doubles of this CTA's shared
+// memory, taken by turns, so a slot is written again only after every CTA
+// has passed the next cluster barrier and so has read it.
+template <int C, int K>
+__device__ __forceinline__ void graph_sums(double (&v)[K], double* sh, double* slots, int turn) {
+  if constexpr (C == 1) {
+    (void)slots;
+    (void)turn;
+#pragma unroll
+    for (int j = 0; j < K; ++j) v[j] = cta_sum(v[j], sh);
+  } else {
+    cg::cluster_group cl = cg::this_cluster();
+    cluster_sums<C, K>(v, sh, slots + 4 * (turn & 1), cl);
+  }
 }
 
 // One graph's iteration over rows [lo, hi) of nodes [g_lo, g_hi): the whole
-// graph when C is 1 (one CTA), this CTA's share of it otherwise. Slots (C >
-// 1): 2 x 3 doubles of this CTA's shared memory, by iteration parity and
-// reduction, so a slot is written again only after every CTA has read it.
+// graph when C is 1 (one CTA), this CTA's share of it otherwise. The
+// reference's steps (z = x / out with the dangling mass, y = A z, the
+// update, the division by the total, the L1 change) with the next z and
+// dangling mass formed in the same pass as the division and the change, so
+// an iteration has two reductions (each a cluster barrier when C > 1).
 template <int C>
 __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ outstr,
                           uint32_t g_lo, uint32_t g_hi, uint32_t lo, uint32_t hi,
@@ -74,42 +99,46 @@ __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ o
                           double* __restrict__ xa, double* __restrict__ xb,
                           double* __restrict__ zb, double* __restrict__ out, int32_t* it_out,
                           int32_t* done_out, double* sh, double* slots) {
-  auto reduce = [&](double v, int which, int parity) -> double {
-    if constexpr (C == 1) {
-      (void)which;
-      (void)parity;
-      return cta_sum(v, sh);
-    } else {
-      cg::cluster_group cl = cg::this_cluster();
-      return cluster_sum<C>(v, sh, slots + parity * 3 + which, cl);
-    }
-  };
   const uint32_t nk = g_hi - g_lo;
   const double inv_n = 1.0 / (double)nk;
   double* x = xa;
   double* y = xb;
-  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) x[i] = inv_n;
-  __syncthreads();
+  int turn = 0;
+  // x = 1 / n; z = x / out; stuck = dangling mass
+  double st[1] = {0.0};
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    x[i] = inv_n;
+    const double o = outstr[i];
+    if (o > 0.0) {
+      zb[i] = inv_n / o;
+    } else {
+      zb[i] = 0.0;
+      st[0] += inv_n;
+    }
+  }
+  graph_sums<C, 1>(st, sh, slots, turn++);  // includes the barrier before z is read
+  double stuck = st[0];
   int32_t it = 0, done = 0;
   while (it < prm.max_iter) {
-    const int par = it & 1;
-    // z = x / out; stuck = dangling mass
-    double stuck = 0;
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      const double o = outstr[i];
-      if (o > 0.0) {
-        zb[i] = x[i] / o;
-      } else {
-        zb[i] = 0.0;
-        stuck += x[i];
-      }
-    }
-    stuck = reduce(stuck, 0, par);  // includes the barrier before z is read
     // y = d (A z + stuck jump) + (1 - d) p
-    double total = 0;
+    double tot[1] = {0.0};
     for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      // arcs in CSR order; four gathers in flight before their products
+      // are added in that order
       double s = 0;
-      for (uint32_t k = op.off[i]; k < op.off[i + 1]; ++k) {
+      uint32_t k = op.off[i];
+      const uint32_t ke = op.off[i + 1];
+      for (; k + 4 <= ke; k += 4) {
+        double zk[4], wk[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          zk[u] = zb[op.cols[k + u]];
+          wk[u] = op.vals ? op.vals[k + u] : 1.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s += wk[u] * zk[u];
+      }
+      for (; k < ke; ++k) {
         const double w = op.vals ? op.vals[k] : 1.0;
         s += w * zb[op.cols[k]];
       }
@@ -117,16 +146,27 @@ __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ o
       const double jmp = prm.jump_uniform ? inv_n : p;
       const double v = prm.d * (s + stuck * jmp) + (1.0 - prm.d) * p;
       y[i] = v;
-      total += v;
+      tot[0] += v;
     }
-    total = reduce(total, 1, par);
-    double change = 0;
+    graph_sums<C, 1>(tot, sh, slots, turn++);  // every product has read z
+    const double total = tot[0];
+    // the division, the change, and the next z and dangling mass
+    double cs[2] = {0.0, 0.0};
     for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
       const double v = y[i] / total;
       y[i] = v;
-      change += fabs(v - x[i]);
+      cs[0] += fabs(v - x[i]);
+      const double o = outstr[i];
+      if (o > 0.0) {
+        zb[i] = v / o;
+      } else {
+        zb[i] = 0.0;
+        cs[1] += v;
+      }
     }
-    change = reduce(change, 2, par);
+    graph_sums<C, 2>(cs, sh, slots, turn++);  // publishes the next z
+    const double change = cs[0];
+    stuck = cs[1];
     double* t = x;
     x = y;
     y = t;
@@ -158,7 +198,7 @@ __global__ void ego_pagerank(OpView<double> op, const double* __restrict__ outst
                              double* __restrict__ out, int32_t* __restrict__ iters,
                              int32_t* __restrict__ status) {
   __shared__ double sh[32];
-  __shared__ double slots[6];
+  __shared__ double slots[8];
   __shared__ uint32_t g_sh;
   if constexpr (C > 1) {
     cg::cluster_group cl = cg::this_cluster();
@@ -225,8 +265,8 @@ __global__ void ego_check_blocks(const uint32_t* __restrict__ src, const uint32_
   }
 }
 
-static int g_ego_threads = 0;  // 0: tuned on first use (per process)
-static int g_ego_cluster = 0;  // CTAs per cluster for the large graphs; 0: tuned with the threads
+static int g_ego_threads = 0;  // 0: chosen per batch (tuned for large batches)
+static int g_ego_cluster = 0;  // CTAs per cluster for the large graphs; 0: chosen with the threads
 static int64_t g_ego_big = 0;  // nodes from which a graph is large; 0: automatic
 
 void set_ego_threads(int t) { g_ego_threads = t; }
@@ -276,6 +316,8 @@ struct EgoPlan : Workspace {
   bool pers = false;
   EgoParams prm{};
   std::vector<uint32_t> sizes;  // node counts of the graphs, largest first
+  int tuned_threads = 0;       // this batch's choice (0: not chosen yet)
+  int tuned_cluster = 0;
   int threads = 0;             // of the instantiated launch
   int cluster = 1;             // CTAs per cluster of the instantiated launch
   uint32_t nbig = 0;           // graphs it gives to clusters
@@ -373,6 +415,8 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
     });
     KNB_CUDA(cudaMemcpyAsync(P.dorder.get(), order.data(), (size_t)count * 4,
                              cudaMemcpyHostToDevice, s));
+    P.tuned_threads = 0;
+    P.tuned_cluster = 0;
     P.sizes.resize(count);
     for (uint32_t k = 0; k < count; ++k) P.sizes[k] = hoff[order[k] + 1] - hoff[order[k]];
     P.xa.alloc(n);
@@ -457,34 +501,41 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
     KNB_CUDA(cudaEventCreate(&P.t0));
     KNB_CUDA(cudaEventCreate(&P.t1));
   }
-  // Threads per CTA and CTAs per cluster: tuned once per process by timing
-  // each candidate on this batch (the results do not depend on the choice
-  // beyond the association of a split graph's sums).
-  if (g_ego_threads == 0 || g_ego_cluster == 0) {
-    float best = 1e30f;
-    int pick_t = 256, pick_c = 1;
-    for (int t : {128, 256, 512, 1024}) {
-      if (g_ego_threads != 0 && t != g_ego_threads) continue;
-      for (int c : {1, 4, 8}) {
-        if (g_ego_cluster != 0 && c != g_ego_cluster) continue;
-        KNB_CUDA(cudaEventRecord(P.t0, s));
-        launch(t, c, s);
-        KNB_CUDA(cudaEventRecord(P.t1, s));
-        KNB_CUDA(cudaEventSynchronize(P.t1));
-        float ms = 0;
-        KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
-        if (ms < best) {
-          best = ms;
-          pick_t = t;
-          pick_c = c;
+  // Threads per CTA and CTAs per cluster, unless pinned (tuning keys 6 and
+  // 16): for a batch of at least 2^20 arcs, timed once per batch layout on
+  // the batch itself; smaller batches, whose launch takes microseconds, take
+  // clusters of 8 and 1024 threads when they have fewer graphs than the GPU
+  // has SMs (a single graph: 0.54 ms for C1 against 0.77 ms at 256), else
+  // 256. Results do not depend on the choice beyond the association of a
+  // split graph's sums.
+  if (P.tuned_threads == 0) {
+    int pick_t = g_ego_threads ? g_ego_threads : ((int)count < sms ? 1024 : 256);
+    int pick_c = g_ego_cluster ? g_ego_cluster : 8;
+    if ((g_ego_threads == 0 || g_ego_cluster == 0) && op.nnz >= (1u << 20)) {
+      float best = 1e30f;
+      for (int t : {128, 256, 512, 1024}) {
+        if (g_ego_threads != 0 && t != g_ego_threads) continue;
+        for (int c : {1, 4, 8}) {
+          if (g_ego_cluster != 0 && c != g_ego_cluster) continue;
+          KNB_CUDA(cudaEventRecord(P.t0, s));
+          launch(t, c, s);
+          KNB_CUDA(cudaEventRecord(P.t1, s));
+          KNB_CUDA(cudaEventSynchronize(P.t1));
+          float ms = 0;
+          KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
+          if (ms < best) {
+            best = ms;
+            pick_t = t;
+            pick_c = c;
+          }
         }
       }
     }
-    g_ego_threads = pick_t;
-    g_ego_cluster = pick_c;
+    P.tuned_threads = pick_t;
+    P.tuned_cluster = pick_c;
   }
-  const int threads = g_ego_threads;
-  const int cluster = g_ego_cluster;
+  const int threads = g_ego_threads ? g_ego_threads : P.tuned_threads;
+  const int cluster = g_ego_cluster ? g_ego_cluster : P.tuned_cluster;
   if (!P.exec || P.threads != threads || P.cluster != cluster || P.pers != pers ||
       !same_params(P.prm, prm)) {
     P.drop_graph();
@@ -514,8 +565,8 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
   for (uint32_t k = 0; k < count; ++k)
     if (hst[k])
       throw Error("PageRank did not converge to tolerance " + std::to_string(in.tol) +
-                  " within " + std::to_string(in.max_iter) + " iterations (graph " +
-                  std::to_string(k) + " of the batch)");
+                  " within " + std::to_string(in.max_iter) + " iterations" +
+                  (count > 1 ? " (graph " + std::to_string(k) + " of the batch)" : ""));
   if (in.out_on_device)
     KNB_CUDA(cudaMemcpyAsync(out, P.dout.get(), (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
   else

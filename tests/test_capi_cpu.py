@@ -115,7 +115,8 @@ def test_tuning_keys_reject_bad_values(so):
     assert L.net_set_tuning(14, 0.5) != 0
     assert L.net_set_tuning(15, -1.0) != 0
     assert L.net_set_tuning(16, 2.0) != 0
-    assert L.net_set_tuning(17, 0.0) != 0
+    assert L.net_set_tuning(17, -1.0) != 0
+    assert L.net_set_tuning(18, 0.0) != 0
     assert L.net_set_tuning(13, 0.0) == 0
     assert L.net_set_tuning(14, -1.0) == 0
     assert L.net_set_tuning(15, 0.0) == 0

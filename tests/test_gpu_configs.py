@@ -32,14 +32,24 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def test_c1_er_10k_fp64_matches_oracle():
+@pytest.mark.parametrize("small_edges", [-1, 0])
+def test_c1_er_10k_fp64_matches_oracle(small_edges):
+    """C1 on both paths: the default one launch of the packed-graph kernel
+    (the graph split over a cluster) and, with tuning key 17 at 0, the sweep
+    kernels."""
     s, t = K.generate_gnm(10_000, 50_000, False, False, seed=20240701)
     g = K.Graph(10_000, s, t, None, False)
     og = O.Graph(10_000, s, t, None, False)
     ref = og.pagerank(tol=1e-12)
-    x, info = g.pagerank_ex(tol=1e-12, precision=K.PREC_FP64)
+    try:
+        if small_edges >= 0:
+            K.set_tuning(K.TUNE_SMALL_EDGES, small_edges)
+        x, info = g.pagerank_ex(tol=1e-12, precision=K.PREC_FP64)
+    finally:
+        K.set_tuning(K.TUNE_SMALL_EDGES, 1 << 18)
     assert np.abs(x - ref).sum() <= 1e-12
     assert info.iterations == og.last_iters
+    assert (info.sweep_kernel == 0) == (small_edges < 0)
     g.close()
 
 

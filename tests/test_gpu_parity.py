@@ -36,6 +36,24 @@ def test_golden(fx_name, variant, orc):
     assert ok, msg
 
 
+PAGERANK_CASES = [c for c in goldens.cases() if c[1].startswith("pagerank")]
+
+
+@pytest.mark.parametrize("fx_name,variant,orc", PAGERANK_CASES)
+def test_golden_pagerank_on_the_sweep_path(fx_name, variant, orc):
+    """The PageRank golden vectors again with small graphs kept on the sweep
+    kernels (tuning key 17 at 0) instead of the one-launch packed path."""
+    fx = DOC["fixtures"][fx_name]
+    g = goldens.make_graph(K.Graph, fx)
+    try:
+        K.set_tuning(K.TUNE_SMALL_EDGES, 0)
+        got = goldens.run_variant(g, fx, variant)
+    finally:
+        K.set_tuning(K.TUNE_SMALL_EDGES, 1 << 18)
+    ok, msg = goldens.agree_variant(got, DOC["golden"][fx_name][variant][orc], variant)
+    assert ok, msg
+
+
 # ------------------------------------------------------------------ CSR and degree
 def random_graphs(seed, count, max_n):
     rng = SplitMix64(seed)
@@ -117,18 +135,26 @@ PR_OPTIONS = [
 ]
 
 
+@pytest.mark.parametrize("small_edges", [1 << 18, 0])
 @pytest.mark.parametrize("fx_name", sorted(DOC["fixtures"]))
-def test_pagerank_fp64_within_1e12_of_oracle(fx_name):
+def test_pagerank_fp64_within_1e12_of_oracle(fx_name, small_edges):
+    """Every fixture and option set, with uniform-teleport solves as one
+    packed launch (the default) and on the sweep kernels (key 17 at 0)."""
     fx = DOC["fixtures"][fx_name]
     kg, og = both(fx)
     n = fx["n"]
-    for opt in PR_OPTIONS + ([dict(weighted=True)] if fx["weighted"] else []):
-        o = dict(opt)
-        pers = o.pop("pers", None)
-        p = np.asarray(goldens.node_rule(pers, n)) if pers else None
-        a = kg.pagerank(personalization=p, **o)
-        b = og.pagerank(personalization=p, **o)
-        assert np.abs(a - b).sum() <= 1e-12, (opt, np.abs(a - b).sum())
+    try:
+        K.set_tuning(K.TUNE_SMALL_EDGES, small_edges)
+        for opt in PR_OPTIONS + ([dict(weighted=True)] if fx["weighted"] else []):
+            o = dict(opt)
+            pers = o.pop("pers", None)
+            p = np.asarray(goldens.node_rule(pers, n)) if pers else None
+            a, ia = kg.pagerank_ex(personalization=p, **o)
+            b = og.pagerank(personalization=p, **o)
+            assert np.abs(a - b).sum() <= 1e-12, (opt, np.abs(a - b).sum())
+            assert ia.iterations == og.last_iters, opt
+    finally:
+        K.set_tuning(K.TUNE_SMALL_EDGES, 1 << 18)
 
 
 def test_pagerank_reference_signature_call():
@@ -183,6 +209,14 @@ def test_pagerank_rmat_fp64_and_mixed(weighted, refine):
     x64, i64 = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_FP64)
     assert np.abs(x64 - ref).sum() <= 1e-12
     assert i64.iterations == og.last_iters
+    try:  # the same FP64 solve on the sweep kernels rather than one packed launch
+        K.set_tuning(K.TUNE_SMALL_EDGES, 0)
+        s64, j64 = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_FP64)
+    finally:
+        K.set_tuning(K.TUNE_SMALL_EDGES, 1 << 18)
+    assert j64.sweep_kernel != 0
+    assert np.abs(s64 - ref).sum() <= 1e-12
+    assert j64.iterations == og.last_iters
     try:
         K.set_tuning(K.TUNE_REFINE, refine)
         xm, im = kg.pagerank_ex(weighted=weighted, tol=1e-9, precision=K.PREC_MIXED)
