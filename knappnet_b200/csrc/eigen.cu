@@ -1300,6 +1300,45 @@ struct SpmvScratch {
 };
 
 constexpr int EIG_IPT = 8;
+constexpr int EIG_WPB = 16;                      // warps per CTA of the product
+constexpr uint32_t EIG_TILE = 32u * EIG_IPT;     // merge items per warp tile
+
+// One product with epilogue e: merge-path warp tiles (warp_spmv) on a
+// persistent grid of the CTAs that fit at once, then split_rows for the rows
+// that cross tiles (and the epilogue's scalars, if any).
+template <class VT, class MT, class Epi>
+static void eig_product(const OpView<MT>& v, const VT* x, const Epi& e, const Partition& P,
+                        VT* carry, VT* head, double* part1, double* part2, const IterState* st,
+                        cudaStream_t s) {
+  constexpr size_t smem = warp_smem_bytes<VT, EIG_IPT, EIG_WPB>();
+  auto fnp = warp_spmv<VT, MT, Epi, EIG_IPT, EIG_WPB, 0>;
+  set_func_attr((const void*)fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout,
+                warp_fit_carveout<VT, EIG_IPT, EIG_WPB>());
+  static std::mutex mu;
+  static std::map<int, unsigned> cap_by_dev;  // CTAs that fit at once, per device
+  int dev = 0;
+  KNB_CUDA(cudaGetDevice(&dev));
+  unsigned cap = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cap_by_dev.find(dev);
+    if (it == cap_by_dev.end()) {
+      int per_sm = 0, sms = 0;
+      KNB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fnp, EIG_WPB * 32, smem));
+      KNB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      it = cap_by_dev.emplace(dev, (unsigned)std::max(1, per_sm) * (unsigned)sms).first;
+    }
+    cap = it->second;
+  }
+  const unsigned grid = std::max(1u, std::min((P.ntiles + EIG_WPB - 1) / EIG_WPB, cap));
+  const uint32_t npart = std::min<uint32_t>(P.ntiles, grid * EIG_WPB);
+  fnp<<<grid, EIG_WPB * 32, smem, s>>>(v, x, e, P.coords.get(), P.ntiles, carry, head, part1, st,
+                                      0u);
+  split_rows<VT, Epi><<<SPLIT_CTAS, SPMV_THREADS, 0, s>>>(P.split.get(), P.nsplit, P.nshort,
+                                                          carry, head, e, part1, npart, part2,
+                                                          const_cast<IterState*>(st));
+}
 // Relative residual below which FP32 products stop helping the Lanczos
 // process (FP32 rounding of the products is about 1e-7 relative).
 constexpr double FP32_FLOOR = 1e-5;
@@ -1309,23 +1348,14 @@ static int spmv(const DevOp& A, const double* x, const float* x32, double* y, Sp
                 const IterState* ist, cudaStream_t s) {
   const Partition& P = *A.part;
   sc.ensure(P.ntiles);
-  const unsigned g2 = SPLIT_CTAS;
   if (x32) {
     PlainEpi<float> e{y};
-    constexpr size_t sm = tile_smem_bytes<float, EIG_IPT>();
-    tile_spmv<float, float, PlainEpi<float>, EIG_IPT><<<P.ntiles, SPMV_THREADS, sm, s>>>(
-        A.view32(), x32, e, P.coords.get(), sc.carry32.get(), sc.head32.get(), sc.part1.get(), ist);
-    split_rows<float, PlainEpi<float>><<<g2, SPMV_THREADS, 0, s>>>(
-        P.split.get(), P.nsplit, P.nshort, sc.carry32.get(), sc.head32.get(), e, sc.part1.get(), P.ntiles,
-        sc.part2.get(), const_cast<IterState*>(ist));
+    eig_product<float, float>(A.view32(), x32, e, P, sc.carry32.get(), sc.head32.get(),
+                              sc.part1.get(), sc.part2.get(), ist, s);
   } else {
     PlainEpi<double> e{y};
-    constexpr size_t sm = tile_smem_bytes<double, EIG_IPT>();
-    tile_spmv<double, double, PlainEpi<double>, EIG_IPT><<<P.ntiles, SPMV_THREADS, sm, s>>>(
-        A.view64(), x, e, P.coords.get(), sc.carry64.get(), sc.head64.get(), sc.part1.get(), ist);
-    split_rows<double, PlainEpi<double>><<<g2, SPMV_THREADS, 0, s>>>(
-        P.split.get(), P.nsplit, P.nshort, sc.carry64.get(), sc.head64.get(), e, sc.part1.get(), P.ntiles,
-        sc.part2.get(), const_cast<IterState*>(ist));
+    eig_product<double, double>(A.view64(), x, e, P, sc.carry64.get(), sc.head64.get(),
+                                sc.part1.get(), sc.part2.get(), ist, s);
   }
   KNB_LAUNCH("spmv");
   return 2;
@@ -1623,7 +1653,7 @@ void mapped_submatrix(const OpView<double>& op, const std::vector<uint32_t>& nod
   A.cols = A.own_cols.get();
   A.v64 = A.own_v64.get();
   A.v32 = nullptr;
-  A.own_part = build_partition(kn, nnz, A.off, SPMV_THREADS * EIG_IPT, s);
+  A.own_part = build_partition(kn, nnz, A.off, EIG_TILE, s);
   A.part = A.own_part.get();
 }
 
@@ -1943,7 +1973,7 @@ void hits(GraphHandleImpl& g, const HitsParams& p, double* hubs_out, double* aut
   full.off = A.rows->off.get();
   full.cols = A.rows->tgt.get();
   full.v64 = A.has_vals ? A.vals64.get() : nullptr;
-  full.part = &A.partition(SPMV_THREADS * EIG_IPT, s);
+  full.part = &A.partition(EIG_TILE, s);
   SpmvScratch sc;
   spmv(full, ad.get(), nullptr, hd.get(), sc, nullptr, s);
   std::vector<double> hubs(n);
@@ -2063,7 +2093,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
     r->matvecs = 0;
   } else if (hdir) {
     // power iteration on A' + I (eigenvector.rs:330-374)
-    const Partition& P = op.partition(SPMV_THREADS * EIG_IPT, s);
+    const Partition& P = op.partition(EIG_TILE, s);
     DevBuf<double> xb[2] = {DevBuf<double>(n), DevBuf<double>(n)}, y(n);
     DevBuf<double> carry(P.ntiles + 1), head(P.ntiles + 1), part1((size_t)P.ntiles + 2),
         part2(SPLIT_CTAS + 2), part3(gv + 2);
@@ -2074,19 +2104,14 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
     KNB_CUDA(cudaMemcpyAsync(st.get(), &is, sizeof(is), cudaMemcpyHostToDevice, s));
     fill_value<<<gv, 256, 0, s>>>(xb[0].get(), n, 1.0);
     ++launches;
-    const unsigned g2 = SPLIT_CTAS;
-    constexpr size_t sm = tile_smem_bytes<double, EIG_IPT>();
     IterState hs{};
     int batch = 0;
     for (;;) {
       for (int k = 0; k < 8; ++k) {
         int b = k & 1;
         PowerEpi e{xb[b].get(), y.get()};
-        tile_spmv<double, double, PowerEpi, EIG_IPT><<<P.ntiles, SPMV_THREADS, sm, s>>>(
-            v64, xb[b].get(), e, P.coords.get(), carry.get(), head.get(), part1.get(), st.get());
-        split_rows<double, PowerEpi><<<g2, SPMV_THREADS, 0, s>>>(
-            P.split.get(), P.nsplit, P.nshort, carry.get(), head.get(), e, part1.get(), P.ntiles,
-            part2.get(), st.get());
+        eig_product<double, double>(v64, xb[b].get(), e, P, carry.get(), head.get(), part1.get(),
+                                    part2.get(), st.get(), s);
         power_vertex<<<gv, 256, 0, s>>>(xb[b].get(), y.get(), xb[1 - b].get(), n, part3.get(), st.get());
         launches += 3;
       }
@@ -2199,7 +2224,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
         A.cols = op.rows->tgt.get();
         A.v64 = op.has_vals ? op.vals64.get() : nullptr;
         A.v32 = op.has_vals ? op.vals32.get() : nullptr;
-        A.part = &op.partition(SPMV_THREADS * EIG_IPT, s);
+        A.part = &op.partition(EIG_TILE, s);
       } else if (build_sub) {
         const uint32_t* nodes_d = plan.members_d.get() + start[c];
         scatter_local<<<grid_for(kn, 256), 256, 0, s>>>(nodes_d, kn, local.get());
@@ -2224,7 +2249,7 @@ void eigenvector(GraphHandleImpl& g, const EigenParams& p, double* out, EigenRes
         A.cols = A.own_cols.get();
         A.v64 = op.has_vals ? A.own_v64.get() : nullptr;
         A.v32 = op.has_vals ? A.own_v32.get() : nullptr;
-        A.own_part = build_partition(kn, nnz, A.off, SPMV_THREADS * EIG_IPT, s);
+        A.own_part = build_partition(kn, nnz, A.off, EIG_TILE, s);
         A.part = A.own_part.get();
       }
       Solved sv;
@@ -2479,7 +2504,7 @@ void leading_eigen(GraphHandleImpl& g, bool weighted, int64_t* membership, doubl
         A.off = off.get();
         A.cols = cols.get();
         A.v64 = vals.get();
-        A.own_part = build_partition(dim, nnz, A.off, SPMV_THREADS * EIG_IPT, s);
+        A.own_part = build_partition(dim, nnz, A.off, EIG_TILE, s);
         A.part = A.own_part.get();
         Leading res;
         if (!symmetric_leading(A, 1e-12, maxrow, 200000, false, x.get(), &res, &launches, s,
