@@ -400,6 +400,7 @@ static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t direc
       if (info) {
         memset(info, 0, sizeof(*info));
         info->iterations = iters;
+        info->change = r.change;
         info->seconds = r.seconds;
         info->converged = 1;
         info->kernel_launches = 1;

@@ -98,7 +98,7 @@ __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ o
                           const EgoParams& prm, const double* __restrict__ pers, double ps,
                           double* __restrict__ xa, double* __restrict__ xb,
                           double* __restrict__ zb, double* __restrict__ out, int32_t* it_out,
-                          int32_t* done_out, double* sh, double* slots) {
+                          int32_t* done_out, double* change_out, double* sh, double* slots) {
   const uint32_t nk = g_hi - g_lo;
   const double inv_n = 1.0 / (double)nk;
   double* x = xa;
@@ -119,6 +119,7 @@ __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ o
   graph_sums<C, 1>(st, sh, slots, turn++);  // includes the barrier before z is read
   double stuck = st[0];
   int32_t it = 0, done = 0;
+  double change = 0.0;
   while (it < prm.max_iter) {
     // y = d (A z + stuck jump) + (1 - d) p
     double tot[1] = {0.0};
@@ -165,7 +166,7 @@ __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ o
       }
     }
     graph_sums<C, 2>(cs, sh, slots, turn++);  // publishes the next z
-    const double change = cs[0];
+    change = cs[0];
     stuck = cs[1];
     double* t = x;
     x = y;
@@ -179,6 +180,7 @@ __device__ void ego_solve(const OpView<double>& op, const double* __restrict__ o
   for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) out[i] = x[i];
   *it_out = it;
   *done_out = done;
+  *change_out = change;
 }
 
 // The persistent launch. With clusters of C > 1 CTAs, each cluster first
@@ -196,7 +198,7 @@ __global__ void ego_pagerank(OpView<double> op, const double* __restrict__ outst
                              const double* __restrict__ psum, double* __restrict__ xa,
                              double* __restrict__ xb, double* __restrict__ zb,
                              double* __restrict__ out, int32_t* __restrict__ iters,
-                             int32_t* __restrict__ status) {
+                             int32_t* __restrict__ status, double* __restrict__ changes) {
   __shared__ double sh[32];
   __shared__ double slots[8];
   __shared__ uint32_t g_sh;
@@ -214,11 +216,13 @@ __global__ void ego_pagerank(OpView<double> op, const double* __restrict__ outst
       const uint32_t per = (g_hi - g_lo + C - 1) / C;
       const uint32_t lo = min(g_hi, g_lo + rank * per), hi = min(g_hi, lo + per);
       int32_t it = 0, done = 0;
+      double ch = 0.0;
       ego_solve<C>(op, outstr, g_lo, g_hi, lo, hi, prm, pers, pers ? psum[graph] : 1.0, xa, xb,
-                   zb, out, &it, &done, sh, slots);
+                   zb, out, &it, &done, &ch, sh, slots);
       if (rank == 0 && threadIdx.x == 0) {
         iters[graph] = it;
         status[graph] = done ? 0 : 1;
+        changes[graph] = ch;
       }
     }
   }
@@ -234,15 +238,18 @@ __global__ void ego_pagerank(OpView<double> op, const double* __restrict__ outst
       if (threadIdx.x == 0) {
         iters[graph] = 0;
         status[graph] = 0;
+        changes[graph] = 0.0;
       }
       continue;
     }
     int32_t it = 0, done = 0;
+    double ch = 0.0;
     ego_solve<1>(op, outstr, g_lo, g_hi, g_lo, g_hi, prm, pers, pers ? psum[graph] : 1.0, xa, xb,
-                 zb, out, &it, &done, sh, slots);
+                 zb, out, &it, &done, &ch, sh, slots);
     if (threadIdx.x == 0) {
       iters[graph] = it;
       status[graph] = done ? 0 : 1;
+      changes[graph] = ch;
     }
     __syncthreads();
   }
@@ -324,6 +331,7 @@ struct EgoPlan : Workspace {
   DevBuf<uint32_t> doff, dorder;
   DevBuf<double> dpers, dpsum, xa, xb, zb, dout;
   DevBuf<int32_t> iters, status;
+  DevBuf<double> changes;
   DevBuf<unsigned int> queue;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -425,6 +433,7 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
     P.dout.alloc(n);
     P.iters.alloc(count);
     P.status.alloc(count);
+    P.changes.alloc(count);
     P.queue.alloc(2);
     P.dpers.release();
     P.dpsum.release();
@@ -468,7 +477,7 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
       ego_pagerank<1><<<grid, threads, 0, st>>>(
           op.view64(), op.colsum.get(), P.doff.get(), P.dorder.get(), count, 0u, P.queue.get(),
           prm, pers ? P.dpers.get() : nullptr, pers ? P.dpsum.get() : nullptr, P.xa.get(),
-          P.xb.get(), P.zb.get(), P.dout.get(), P.iters.get(), P.status.get());
+          P.xb.get(), P.zb.get(), P.dout.get(), P.iters.get(), P.status.get(), P.changes.get());
       KNB_LAUNCH("ego_pagerank");
       return 0;
     }
@@ -490,7 +499,7 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
                                   (const double*)(pers ? P.dpers.get() : nullptr),
                                   (const double*)(pers ? P.dpsum.get() : nullptr), P.xa.get(),
                                   P.xb.get(), P.zb.get(), P.dout.get(), P.iters.get(),
-                                  P.status.get()));
+                                  P.status.get(), P.changes.get()));
     };
     if (C == 4) args(ego_pagerank<4>);
     else args(ego_pagerank<8>);
@@ -557,8 +566,11 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
   KNB_CUDA(cudaGraphLaunch(P.exec, s));
   KNB_CUDA(cudaEventRecord(P.t1, s));
   std::vector<int32_t> hst(count), hit(count);
+  double change0 = 0.0;
   KNB_CUDA(cudaMemcpyAsync(hst.data(), P.status.get(), (size_t)count * 4, cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaMemcpyAsync(hit.data(), P.iters.get(), (size_t)count * 4, cudaMemcpyDeviceToHost, s));
+  if (count == 1)
+    KNB_CUDA(cudaMemcpyAsync(&change0, P.changes.get(), 8, cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
   float ms = 0;
   KNB_CUDA(cudaEventElapsedTime(&ms, P.t0, P.t1));
@@ -584,6 +596,7 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
       mx = std::max<int64_t>(mx, hit[k]);
     }
     res->total_iterations = tot;
+    res->change = change0;
     res->max_iterations = mx;
     if (in.iterations_out)
       for (uint32_t k = 0; k < count; ++k) in.iterations_out[k] = hit[k];

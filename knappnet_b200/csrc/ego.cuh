@@ -28,6 +28,7 @@ struct EgoResult {
   int instantiations = 0;  // times the operator's launch graph has been instantiated
   int cluster = 1;         // CTAs per cluster that split the large graphs (1: none split)
   int32_t split_graphs = 0;  // graphs split over a cluster
+  double change = 0;         // a batch of one graph: its last L1 change
 };
 
 void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoResult* res,

@@ -49,6 +49,7 @@ def test_c1_er_10k_fp64_matches_oracle(small_edges):
         K.set_tuning(K.TUNE_SMALL_EDGES, 1 << 18)
     assert np.abs(x - ref).sum() <= 1e-12
     assert info.iterations == og.last_iters
+    assert 0 < info.change <= 1e-12
     assert (info.sweep_kernel == 0) == (small_edges < 0)
     g.close()
 
