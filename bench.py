@@ -575,6 +575,12 @@ def run_c4a(args):
     alg = (s32 * (4.0 * (n + 1) + 4.0 * arcs + 4.0 * n * B) + c32 * 12.0 * n +
            s64 * (4.0 * (n + 1) + 4.0 * arcs + 8.0 * n * B) + c64 * 24.0 * n)
     ach = alg / dinfo.sweep_seconds / 1e9
+    # The same sweeps if every arc's gathered row (B values) came from DRAM,
+    # as it must when the n x B iterate (4.3 GB in FP32) cannot stay in L2:
+    # what the kernel moves, against the bandwidth.
+    rows = (s32 * (4.0 * (n + 1) + 4.0 * arcs + 4.0 * arcs * B) + c32 * 12.0 * n +
+            s64 * (4.0 * (n + 1) + 4.0 * arcs + 8.0 * arcs * B) + c64 * 24.0 * n)
+    ach_rows = rows / dinfo.sweep_seconds / 1e9
     return {"workload": f"c4a: R-MAT {scale} directed, 256 personalisation vectors (uniform over "
                         "1-64 seed nodes), batched SpMM PageRank, mixed precision, tol 1e-10",
             "device_pointers": {"solve_ms": round(dsec * 1e3, 2),
@@ -589,7 +595,12 @@ def run_c4a(args):
                                     "bytes_per_sweep_avg": round(alg / max(dinfo.sweeps, 1)),
                                     "bytes": "offsets, indices and the gathered n x B block per "
                                              "sweep; previous, new and scaled iterate of each "
-                                             "active column"}},
+                                             "active column",
+                                    "with_row_gathers": {
+                                        "achieved": round(ach_rows, 1),
+                                        "frac": round(ach_rows / hbm, 4),
+                                        "bytes": "as above, but one gathered row of B values per "
+                                                 "arc instead of the n x B block once"}}},
             "metric": "GTEPS*B per sweep", "unit": "GTEPS*B/sweep", "higher_is_better": True,
             "value": round(arcs * B * info.sweeps / sec / 1e9, 2),
             "solve_ms": round(sec * 1e3, 2),
