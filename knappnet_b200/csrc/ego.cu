@@ -2,15 +2,19 @@
 // graph (ego networks, layers, subgraphs packed into one handle), in one
 // persistent launch.
 //
-// Each CTA takes whole graphs off a queue, largest first (so the last graphs
-// to start are the small ones), and runs the reference's iteration on that
-// graph alone (crates/engine/src/metrics/spectral.rs:247-280): z = x / out
-// with the dangling mass `stuck`, y = A z, y = d (y + stuck jump) + (1 - d) p,
-// the division by the total and the L1 change, every step with CTA-wide
-// reductions in a fixed order. Each graph therefore gets exactly what a
-// separate net_pagerank call on it returns, up to the association of sums.
-// The vectors of the graph being solved stay in L2 (a graph's nodes are
-// contiguous in the packed numbering).
+// Graphs are taken off queues largest first (so the last graphs to start are
+// the small ones) and each runs the reference's iteration on its own
+// (crates/engine/src/metrics/spectral.rs:247-280): z = x / out with the
+// dangling mass `stuck`, y = A z, y = d (y + stuck jump) + (1 - d) p, the
+// division by the total and the L1 change, every sum in a fixed order. Each
+// graph therefore gets what a separate net_pagerank call on it returns, up to
+// the association of sums. A large graph would keep one CTA busy long after
+// the rest of the batch is done, so the launch runs in thread-block clusters:
+// each cluster first splits the large graphs' rows over its CTAs, which add
+// their sums through distributed shared memory, then every CTA takes small
+// graphs alone. The vectors of the graph being solved stay in L2 (a graph's
+// nodes are contiguous in the packed numbering). A single small graph's
+// solve runs here too, as a batch of one.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
