@@ -38,16 +38,25 @@ struct EgoParams {
   int32_t jump_uniform;  // dangling nodes jump uniformly (1) or by p (0)
 };
 
-// Fixed-order CTA sum (warp butterflies, then warp 0).
-__device__ __forceinline__ double cta_sum(double v, double* sh) {
+// Fixed-order CTA sums of K values at once (warp butterflies, then the warps
+// in order): two CTA barriers for all K. sh holds 32 K doubles.
+template <int K>
+__device__ __forceinline__ void cta_sums(double (&v)[K], double* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  v = warp_sum(v);
+#pragma unroll
+  for (int j = 0; j < K; ++j) v[j] = warp_sum(v[j]);
+  __syncthreads();  // the previous sums' reads of sh are done
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) sh[32 * j + w] = v[j];
+  }
   __syncthreads();
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  double t = 0;
-  for (int k = 0; k < nw; ++k) t += sh[k];  // same order in every thread
-  return t;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double t = 0;
+    for (int k = 0; k < nw; ++k) t += sh[32 * j + k];  // same order in every thread
+    v[j] = t;
+  }
 }
 
 // Sums over the rows of one graph split across the CTAs of a cluster: each
@@ -58,10 +67,10 @@ __device__ __forceinline__ double cta_sum(double v, double* sh) {
 template <int C, int K>
 __device__ __forceinline__ void cluster_sums(double (&v)[K], double* sh, double* slot,
                                              cg::cluster_group& cl) {
+  cta_sums<K>(v, sh);
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
-    const double t = cta_sum(v[j], sh);
-    if (threadIdx.x == 0) slot[j] = t;
+    for (int j = 0; j < K; ++j) slot[j] = v[j];
   }
   cl.sync();
 #pragma unroll
@@ -82,8 +91,7 @@ __device__ __forceinline__ void graph_sums(double (&v)[K], double* sh, double* s
   if constexpr (C == 1) {
     (void)slots;
     (void)turn;
-#pragma unroll
-    for (int j = 0; j < K; ++j) v[j] = cta_sum(v[j], sh);
+    cta_sums<K>(v, sh);
   } else {
     cg::cluster_group cl = cg::this_cluster();
     cluster_sums<C, K>(v, sh, slots + 4 * (turn & 1), cl);
@@ -203,7 +211,7 @@ __global__ void ego_pagerank(OpView<double> op, const double* __restrict__ outst
                              double* __restrict__ xb, double* __restrict__ zb,
                              double* __restrict__ out, int32_t* __restrict__ iters,
                              int32_t* __restrict__ status, double* __restrict__ changes) {
-  __shared__ double sh[32];
+  __shared__ double sh[64];
   __shared__ double slots[8];
   __shared__ uint32_t g_sh;
   if constexpr (C > 1) {
