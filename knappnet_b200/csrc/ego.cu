@@ -16,6 +16,7 @@
 // nodes are contiguous in the packed numbering). A single small graph's
 // solve runs here too, as a batch of one.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -284,9 +285,11 @@ __global__ void ego_check_blocks(const uint32_t* __restrict__ src, const uint32_
   }
 }
 
-static int g_ego_threads = 0;  // 0: chosen per batch (tuned for large batches)
-static int g_ego_cluster = 0;  // CTAs per cluster for the large graphs; 0: chosen with the threads
-static int64_t g_ego_big = 0;  // nodes from which a graph is large; 0: automatic
+// Process-wide settings (net_set_tuning keys 6, 16, 15), read by solves that
+// may run on other threads.
+static std::atomic<int> g_ego_threads{0};  // 0: chosen per batch (tuned for large batches)
+static std::atomic<int> g_ego_cluster{0};  // CTAs per cluster for the large graphs; 0: chosen
+static std::atomic<int64_t> g_ego_big{0};  // nodes from which a graph is large; 0: automatic
 
 void set_ego_threads(int t) { g_ego_threads = t; }
 void set_ego_cluster(int c) { g_ego_cluster = c; }
@@ -471,7 +474,8 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
   // much more than a CTA's share of the batch) are each split over a
   // cluster; the others go one per CTA. Returns the graphs given to clusters.
   auto big_count = [&](uint64_t ctas) {
-    const uint64_t big = g_ego_big > 0 ? (uint64_t)g_ego_big
+    const int64_t pin_big = g_ego_big.load();
+    const uint64_t big = pin_big > 0 ? (uint64_t)pin_big
                                        : std::max<uint64_t>(4096, (uint64_t)n / std::max<uint64_t>(ctas, 1));
     uint32_t nb = 0;
     while (nb < count && P.sizes[nb] >= big) ++nb;
@@ -529,15 +533,16 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
   // has SMs (a single graph: 0.54 ms for C1 against 0.77 ms at 256), else
   // 256. Results do not depend on the choice beyond the association of a
   // split graph's sums.
+  const int pin_t = g_ego_threads.load(), pin_c = g_ego_cluster.load();
   if (P.tuned_threads == 0) {
-    int pick_t = g_ego_threads ? g_ego_threads : ((int)count < sms ? 1024 : 256);
-    int pick_c = g_ego_cluster ? g_ego_cluster : 8;
-    if ((g_ego_threads == 0 || g_ego_cluster == 0) && op.nnz >= (1u << 20)) {
+    int pick_t = pin_t ? pin_t : ((int)count < sms ? 1024 : 256);
+    int pick_c = pin_c ? pin_c : 8;
+    if ((pin_t == 0 || pin_c == 0) && op.nnz >= (1u << 20)) {
       float best = 1e30f;
       for (int t : {128, 256, 512, 1024}) {
-        if (g_ego_threads != 0 && t != g_ego_threads) continue;
+        if (pin_t != 0 && t != pin_t) continue;
         for (int c : {1, 4, 8}) {
-          if (g_ego_cluster != 0 && c != g_ego_cluster) continue;
+          if (pin_c != 0 && c != pin_c) continue;
           KNB_CUDA(cudaEventRecord(P.t0, s));
           launch(t, c, s);
           KNB_CUDA(cudaEventRecord(P.t1, s));
@@ -555,8 +560,8 @@ void pagerank_graphs(GraphHandleImpl& g, const EgoInput& in, double* out, EgoRes
     P.tuned_threads = pick_t;
     P.tuned_cluster = pick_c;
   }
-  const int threads = g_ego_threads ? g_ego_threads : P.tuned_threads;
-  const int cluster = g_ego_cluster ? g_ego_cluster : P.tuned_cluster;
+  const int threads = pin_t ? pin_t : P.tuned_threads;
+  const int cluster = pin_c ? pin_c : P.tuned_cluster;
   if (!P.exec || P.threads != threads || P.cluster != cluster || P.pers != pers ||
       !same_params(P.prm, prm)) {
     P.drop_graph();
