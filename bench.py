@@ -572,14 +572,25 @@ def run_c4a(args):
     s32, s64 = int(dinfo.sweeps_fp32), int(dinfo.sweeps - dinfo.sweeps_fp32)
     c32 = int(dinfo.column_iterations_fp32)
     c64 = int(dinfo.column_iterations) - c32
-    alg = (s32 * (4.0 * (n + 1) + 4.0 * arcs + 4.0 * n * B) + c32 * 12.0 * n +
-           s64 * (4.0 * (n + 1) + 4.0 * arcs + 8.0 * n * B) + c64 * 24.0 * n)
+    refined = bool(dinfo.refined)
+    base = 4.0 * (n + 1) + 4.0 * arcs  # row offsets and column indices, every sweep
+    if refined:
+        # the FP64 phase: one anchor sweep (FP64 gathers; y_ref read, s_ref,
+        # e and z_e written: 24 bytes a node and column) and refinement sweeps
+        # (FP32 gathers; y_ref, s_ref and e read, e and z_e written: 28 bytes)
+        alg64 = (base + 8.0 * n * B + B * 24.0 * n +
+                 (s64 - 1) * (base + 4.0 * n * B) + (c64 - B) * 28.0 * n)
+        rows64 = (base + 8.0 * arcs * B + B * 24.0 * n +
+                  (s64 - 1) * (base + 4.0 * arcs * B) + (c64 - B) * 28.0 * n)
+    else:
+        alg64 = s64 * (base + 8.0 * n * B) + c64 * 24.0 * n
+        rows64 = s64 * (base + 8.0 * arcs * B) + c64 * 24.0 * n
+    alg = s32 * (base + 4.0 * n * B) + c32 * 12.0 * n + alg64
     ach = alg / dinfo.sweep_seconds / 1e9
     # The same sweeps if every arc's gathered row (B values) came from DRAM,
     # as it must when the n x B iterate (4.3 GB in FP32) cannot stay in L2:
     # what the kernel moves, against the bandwidth.
-    rows = (s32 * (4.0 * (n + 1) + 4.0 * arcs + 4.0 * arcs * B) + c32 * 12.0 * n +
-            s64 * (4.0 * (n + 1) + 4.0 * arcs + 8.0 * arcs * B) + c64 * 24.0 * n)
+    rows = s32 * (base + 4.0 * arcs * B) + c32 * 12.0 * n + rows64
     ach_rows = rows / dinfo.sweep_seconds / 1e9
     return {"workload": f"c4a: R-MAT {scale} directed, 256 personalisation vectors (uniform over "
                         "1-64 seed nodes), batched SpMM PageRank, mixed precision, tol 1e-10",
@@ -588,6 +599,9 @@ def run_c4a(args):
                                 "gteps_b_per_sweep": round(arcs * B * dinfo.sweeps /
                                                            dinfo.sweep_seconds / 1e9, 2),
                                 "same_scores_as_host_call": same,
+                                "fp64_phase": ("one anchor sweep, then refinement sweeps gathering "
+                                               "the FP32 correction" if refined else
+                                               "FP64 sweeps"),
                                 "roofline": {
                                     "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
                                     "peak_kind": peak_kind, "unit": "GB/s",

@@ -227,7 +227,8 @@ typedef struct NetBatchInfo {
   int64_t column_iterations;     /* sum over vectors of their own iteration counts */
   int64_t max_column_iterations;
   int32_t kernel_launches;
-  int32_t reserved;
+  int32_t refined;               /* mixed: 1 when the FP64 phase ran as one anchor sweep and
+                                    refinement sweeps gathering the FP32 correction */
   double sweep_seconds;          /* device time of the sweeps alone (no copies, set-up) */
   int64_t column_iterations_fp32; /* of column_iterations, those in FP32 sweeps */
 } NetBatchInfo;

@@ -35,11 +35,11 @@ class NetBatchInfo(ctypes.Structure):
     _fields_ = [("seconds", ctypes.c_double), ("sweeps", ctypes.c_int64),
                 ("sweeps_fp32", ctypes.c_int64), ("column_iterations", ctypes.c_int64),
                 ("max_column_iterations", ctypes.c_int64), ("kernel_launches", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("sweep_seconds", ctypes.c_double),
+                ("refined", ctypes.c_int32), ("sweep_seconds", ctypes.c_double),
                 ("column_iterations_fp32", ctypes.c_int64)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class NetSolveInfo(ctypes.Structure):

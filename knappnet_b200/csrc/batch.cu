@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "batch.cuh"
@@ -123,45 +124,99 @@ __device__ __forceinline__ void row_product(const OpView<MT>& op, const VT* __re
   }
 }
 
+// Epilogue modes: the plain update (VT iterate), the anchor sweep and the
+// refinement sweeps of the mixed path's FP64 phase. As in the single-vector
+// path (RefineEpi, pagerank.cu) each column's iterate is held from the
+// anchor on as y = y_ref + e with e in FP32: the anchor sweep gathers the
+// FP64 z_ref = y_ref / out and keeps s_ref = A z_ref; a refinement sweep
+// gathers z_e = e / out in FP32 and forms s = s_ref + A z_e, the update, the
+// sums and the change in FP64. A refinement sweep gathers B FP32 values per
+// arc where an FP64 sweep gathers B FP64 values.
+enum { EPI_PLAIN = 0, EPI_ANCHOR = 1, EPI_REFINE = 2 };
+struct RefineBufs {
+  const double* yref;  // n x B: the iterate the anchor sweep starts from
+  double* sref;        // n x B: A z_ref, written by the anchor sweep
+  const float* eold;   // refinement sweeps: e of the input iterate
+  float* enew;         // e of the new iterate
+  float* zenew;        // enew / out
+  const float* io32;   // 1 / out in FP32 (0 for dangling nodes)
+};
+
 // The PageRank update of row i for this lane's columns, and its per-column
 // sums (mass, dangling mass, L1 change) into the warp's slice red[3][B] of
 // shared memory (column c belongs to lane c mod 32, so every slot has one
 // writer and takes its rows in order).
-template <class VT, int VW>
+template <class VT, int VW, int MODE>
 __device__ __forceinline__ void row_update(uint32_t i, const VT (&s)[VW], int lane,
                                            const BatchScalars& bs, const ColState* cs,
                                            const VT* __restrict__ Yold, VT* __restrict__ Ynew,
                                            VT* __restrict__ Znew, const VT* __restrict__ inv_out,
-                                           const PersView& pv, double* red) {
-  const VT io = inv_out[i];
-  VT psp[VW];  // this lane's teleport values of row i (sparse teleport)
+                                           const PersView& pv, const RefineBufs& rb,
+                                           double* red) {
+  using PT = std::conditional_t<MODE == EPI_PLAIN, VT, double>;
+  PT psp[VW];  // this lane's teleport values of row i (sparse teleport)
 #pragma unroll
-  for (int v = 0; v < VW; ++v) psp[v] = VT(0);
+  for (int v = 0; v < VW; ++v) psp[v] = PT(0);
   if (!pv.dense) {
     for (uint32_t e = pv.rowptr[i]; e < pv.rowptr[i + 1]; ++e) {
       const uint32_t c = pv.cols[e];
       if ((c & 31u) != (uint32_t)lane) continue;
-      const VT x = (VT)pv.vals[e];
+      const PT x = (PT)pv.vals[e];
 #pragma unroll
       for (int v = 0; v < VW; ++v)
         if ((c >> 5) == (uint32_t)v) psp[v] = x;
     }
   }
+  if constexpr (MODE == EPI_PLAIN) {
+    const VT io = inv_out[i];
 #pragma unroll
-  for (int v = 0; v < VW; ++v) {
-    const uint32_t c = lane + 32 * v;
-    if (c >= bs.B || cs[c].frozen) continue;
-    const VT it = (VT)cs[c].inv_total, dt = (VT)cs[c].dterm;
-    const size_t q = (size_t)i * bs.B + c;
-    const VT pg = pv.dense ? (VT)pv.dense[q] : psp[v];
-    const VT jg = bs.jump_uniform ? (VT)bs.pu : pg;
-    const VT u = (VT)bs.d * (s[v] * it + dt * jg) + (VT)(1.0 - bs.d) * pg;
-    const VT xo = Yold[q] * it;
-    Ynew[q] = u;
-    Znew[q] = u * io;
-    red[c] += (double)u;
-    if (io == VT(0)) red[bs.B + c] += (double)u;
-    red[2 * bs.B + c] += fabs((double)u - (double)xo);
+    for (int v = 0; v < VW; ++v) {
+      const uint32_t c = lane + 32 * v;
+      if (c >= bs.B || cs[c].frozen) continue;
+      const VT it = (VT)cs[c].inv_total, dt = (VT)cs[c].dterm;
+      const size_t q = (size_t)i * bs.B + c;
+      const VT pg = pv.dense ? (VT)pv.dense[q] : psp[v];
+      const VT jg = bs.jump_uniform ? (VT)bs.pu : pg;
+      const VT u = (VT)bs.d * (s[v] * it + dt * jg) + (VT)(1.0 - bs.d) * pg;
+      const VT xo = Yold[q] * it;
+      Ynew[q] = u;
+      Znew[q] = u * io;
+      red[c] += (double)u;
+      if (io == VT(0)) red[bs.B + c] += (double)u;
+      red[2 * bs.B + c] += fabs((double)u - (double)xo);
+    }
+  } else {
+    (void)Yold;
+    (void)Ynew;
+    (void)Znew;
+    (void)inv_out;
+    const float io = rb.io32[i];
+#pragma unroll
+    for (int v = 0; v < VW; ++v) {
+      const uint32_t c = lane + 32 * v;
+      if (c >= bs.B || cs[c].frozen) continue;
+      const double it = cs[c].inv_total, dt = cs[c].dterm;
+      const size_t q = (size_t)i * bs.B + c;
+      double sum;
+      if constexpr (MODE == EPI_ANCHOR) {
+        sum = (double)s[v];
+        rb.sref[q] = sum;
+      } else {
+        sum = rb.sref[q] + (double)s[v];
+      }
+      const double pg = pv.dense ? pv.dense[q] : psp[v];
+      const double jg = bs.jump_uniform ? bs.pu : pg;
+      const double u = bs.d * (sum * it + dt * jg) + (1.0 - bs.d) * pg;
+      const double yr = rb.yref[q];
+      const double yo = MODE == EPI_ANCHOR ? yr : yr + (double)rb.eold[q];
+      const float en = (float)(u - yr);
+      const double us = yr + (double)en;  // the iterate as stored
+      rb.enew[q] = en;
+      rb.zenew[q] = en * io;
+      red[c] += us;
+      if (io == 0.0f) red[bs.B + c] += us;
+      red[2 * bs.B + c] += fabs(us - yo * it);
+    }
   }
 }
 
@@ -186,12 +241,12 @@ __device__ __forceinline__ void cta_column_sums(uint32_t B, double* __restrict__
   }
 }
 
-template <class VT, class MT, int VW, int U>
+template <class VT, class MT, int VW, int U, int MODE>
 __global__ void __launch_bounds__(BT)
 spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ ranges,
           uint32_t nranges, BatchScalars bs, const ColState* __restrict__ cs,
           const VT* __restrict__ Yold, VT* __restrict__ Ynew, VT* __restrict__ Znew,
-          const VT* __restrict__ inv_out, PersView P,
+          const VT* __restrict__ inv_out, PersView P, RefineBufs rb,
           double* __restrict__ part, const int32_t* __restrict__ all_frozen) {
   if (*all_frozen) return;
   extern __shared__ double smem_b[];
@@ -205,7 +260,7 @@ spmm_rows(OpView<MT> op, const VT* __restrict__ Z, const RowRange* __restrict__ 
       if (a1 - a0 > LONG_ROW) continue;  // long rows: spmm_chunks / spmm_long
       VT acc[VW];
       row_product<VT, MT, VW, U>(op, Z, bs.B, a0, a1, lane, acc);
-      row_update<VT, VW>(i, acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
+      row_update<VT, VW, MODE>(i, acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, rb, red);
     }
   }
   cta_column_sums(bs.B, part, smem_b);
@@ -233,12 +288,12 @@ spmm_chunks(OpView<MT> op, const VT* __restrict__ Z, const Chunk* __restrict__ c
 }
 
 // Long rows: chunk partials added in chunk order, then the update.
-template <class VT, int VW>
+template <class VT, int VW, int MODE>
 __global__ void __launch_bounds__(BT)
 spmm_long(const uint32_t* __restrict__ lrow, const uint32_t* __restrict__ lfirst, uint32_t nlong,
           const VT* __restrict__ scratch, BatchScalars bs, const ColState* __restrict__ cs,
           const VT* __restrict__ Yold, VT* __restrict__ Ynew, VT* __restrict__ Znew,
-          const VT* __restrict__ inv_out, PersView P,
+          const VT* __restrict__ inv_out, PersView P, RefineBufs rb,
           double* __restrict__ part, const int32_t* __restrict__ all_frozen) {
   if (*all_frozen) return;
   extern __shared__ double smem_b[];
@@ -255,7 +310,7 @@ spmm_long(const uint32_t* __restrict__ lrow, const uint32_t* __restrict__ lfirst
         const uint32_t c = lane + 32 * v;
         if (c < bs.B) acc[v] += scratch[(size_t)k * bs.B + c];
       }
-    row_update<VT, VW>(lrow[q], acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, red);
+    row_update<VT, VW, MODE>(lrow[q], acc, lane, bs, cs, Yold, Ynew, Znew, inv_out, P, rb, red);
   }
   cta_column_sums(bs.B, part, smem_b);
 }
@@ -457,6 +512,22 @@ __global__ void spmm_output(const VT* __restrict__ Y0, const VT* __restrict__ Y1
   }
 }
 
+// Output of a refined phase: (y_ref + e) / total per column, e read from the
+// buffer of the column's last sweep.
+__global__ void spmm_output_ref(const double* __restrict__ Yref, const float* __restrict__ E0,
+                                const float* __restrict__ E1, const ColState* __restrict__ cs,
+                                uint32_t n, uint32_t B, double* __restrict__ out) {
+  const uint64_t total = (uint64_t)n * B;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(q % n), c = (uint32_t)(q / n);
+    const ColState s = cs[c];
+    const float* E = (s.iter & 1) ? E1 : E0;
+    const size_t r = (size_t)i * B + c;
+    out[q] = (Yref[r] + (double)E[r]) / s.total;
+  }
+}
+
 // ----------------------------------------------------------------------- host
 struct BatchPlan {
   std::vector<RowRange> ranges;
@@ -498,17 +569,18 @@ static void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
 // One sweep: the row products and updates, then (finish) the per-column
 // sums, stopping rule and next sweep's scalars. Without finish the sweep
 // only rewrites Ynew, Znew, the chunk scratch and the partials.
-template <class VT, class MT, int VW, int U>
+template <class VT, class MT, int VW, int U, int MODE>
 static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uint32_t nranges,
                        const DevBuf<Chunk>& chunks, uint32_t nchunks, const DevBuf<uint32_t>& lrow,
                        const DevBuf<uint32_t>& lfirst, uint32_t nlong, const BatchScalars& bs,
                        ColState* cs, const VT* Yold, VT* Ynew, const VT* Zold, VT* Znew,
-                       const VT* inv_out, const PersView& P, VT* scratch, double* part,
-                       int32_t* all_frozen, unsigned grid, bool finish, cudaStream_t s) {
+                       const VT* inv_out, const PersView& P, const RefineBufs& rb, VT* scratch,
+                       double* part, int32_t* all_frozen, unsigned grid, bool finish,
+                       cudaStream_t s) {
   const size_t smem = (size_t)BW * 3 * bs.B * sizeof(double);
-  set_func_attr((const void*)spmm_rows<VT, MT, VW, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int)(BW * 3 * 256 * sizeof(double)));
-  set_func_attr((const void*)spmm_long<VT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  set_func_attr((const void*)spmm_rows<VT, MT, VW, U, MODE>,
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(BW * 3 * 256 * sizeof(double)));
+  set_func_attr((const void*)spmm_long<VT, VW, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                 (int)(BW * 3 * 256 * sizeof(double)));
   int launches = 0;
   if (nchunks) {
@@ -516,28 +588,29 @@ static int batch_sweep(const OpView<MT>& op, const DevBuf<RowRange>& ranges, uin
                                                     all_frozen);
     ++launches;
   }
-  spmm_rows<VT, MT, VW, U><<<grid, BT, smem, s>>>(op, Zold, ranges.get(), nranges, bs, cs, Yold,
-                                                  Ynew, Znew, inv_out, P, part, all_frozen);
-  spmm_long<VT, VW><<<grid, BT, smem, s>>>(lrow.get(), lfirst.get(), nlong, scratch, bs, cs, Yold,
-                                           Ynew, Znew, inv_out, P, part + (size_t)grid * 3 * bs.B,
-                                           all_frozen);
+  spmm_rows<VT, MT, VW, U, MODE><<<grid, BT, smem, s>>>(op, Zold, ranges.get(), nranges, bs, cs,
+                                                        Yold, Ynew, Znew, inv_out, P, rb, part,
+                                                        all_frozen);
+  spmm_long<VT, VW, MODE><<<grid, BT, smem, s>>>(lrow.get(), lfirst.get(), nlong, scratch, bs, cs,
+                                                 Yold, Ynew, Znew, inv_out, P, rb,
+                                                 part + (size_t)grid * 3 * bs.B, all_frozen);
   if (finish) spmm_finish<<<1, 256, 0, s>>>(part, 2 * grid, bs, cs, all_frozen, 1);
   KNB_LAUNCH("batch sweep");
   return launches + (finish ? 3 : 2);
 }
 
-template <class VT, class MT>
+template <class VT, class MT, int MODE = EPI_PLAIN>
 static int batch_sweep_vw(int vw, int u, const OpView<MT>& op, const DevBuf<RowRange>& ranges,
                           uint32_t nranges, const DevBuf<Chunk>& chunks, uint32_t nchunks,
                           const DevBuf<uint32_t>& lrow, const DevBuf<uint32_t>& lfirst,
                           uint32_t nlong, const BatchScalars& bs, ColState* cs, const VT* Yold,
                           VT* Ynew, const VT* Zold, VT* Znew, const VT* inv_out, const PersView& P,
                           VT* scratch, double* part, int32_t* all_frozen, unsigned grid,
-                          cudaStream_t s, bool finish = true) {
+                          cudaStream_t s, bool finish = true, const RefineBufs& rb = RefineBufs{}) {
 #define KNB_SW(V, UU)                                                                             \
-  return batch_sweep<VT, MT, V, UU>(op, ranges, nranges, chunks, nchunks, lrow, lfirst, nlong,    \
-                                    bs, cs, Yold, Ynew, Zold, Znew, inv_out, P, scratch, part,    \
-                                    all_frozen, grid, finish, s)
+  return batch_sweep<VT, MT, V, UU, MODE>(op, ranges, nranges, chunks, nchunks, lrow, lfirst,     \
+                                          nlong, bs, cs, Yold, Ynew, Zold, Znew, inv_out, P, rb,  \
+                                          scratch, part, all_frozen, grid, finish, s)
 #define KNB_SWU(V)                   \
   switch (u) {                       \
     case 1: KNB_SW(V, 1);            \
@@ -684,6 +757,9 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
   int launches = 0;
   int64_t sweeps32 = 0, sweeps64 = 0, colits32 = 0;
   const bool mixed = prm.precision == PREC_MIXED;
+  // mixed: the FP64 phase as one anchor sweep and refinement sweeps (tuning
+  // key 9 at 0: plain FP64 sweeps)
+  const bool refine = mixed && tuning().refine != 0;
   const uint32_t Btot = prm.B;
   DevBuf<double>& pin = ws.pin;
   grow(pin, (size_t)n * Btot);
@@ -851,24 +927,58 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     }
     int k = 0;
     KNB_CUDA(cudaEventRecord(l0, s));
-    for (;;) {
-      const int b = k & 1;
+    auto all_done = [&] {
+      int32_t af = 0;
+      KNB_CUDA(cudaMemcpyAsync(&af, all_frozen.get(), 4, cudaMemcpyDeviceToHost, s));
+      KNB_CUDA(cudaStreamSynchronize(s));
+      return af != 0;
+    };
+    if (refine) {
+      // the anchor sweep: FP64 gathers of z_ref = Y64[0] / out; s_ref into
+      // Y64[1], the correction e and z_e into Y32[1] and Z32[1]
+      const RefineBufs rb0{Y64[0].get(), Y64[1].get(), nullptr, Y32[1].get(), Z32[1].get(),
+                           op.inv_out32.get()};
       if (use32v)
-        launches += batch_sweep_vw<double, float>(
+        launches += batch_sweep_vw<double, float, EPI_ANCHOR>(
             vw, u64, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
-            bs, cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
-            op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
+            bs, cs.get(), Y64[0].get(), Y64[1].get(), Z64[0].get(), Z64[1].get(),
+            op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s, true, rb0);
       else
-        launches += batch_sweep_vw<double, double>(
+        launches += batch_sweep_vw<double, double, EPI_ANCHOR>(
             vw, u64, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
-            bs, cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
-            op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
-      ++k;
-      if (k % 4 == 0) {
-        int32_t af = 0;
-        KNB_CUDA(cudaMemcpyAsync(&af, all_frozen.get(), 4, cudaMemcpyDeviceToHost, s));
-        KNB_CUDA(cudaStreamSynchronize(s));
-        if (af) break;
+            bs, cs.get(), Y64[0].get(), Y64[1].get(), Z64[0].get(), Z64[1].get(),
+            op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s, true, rb0);
+      k = 1;
+      // refinement sweeps: FP32 gathers of z_e, FP32 arc values (the FP32
+      // phase's arcs in flight)
+      int ur = tuned_u(vw * 4 + 0);
+      if (!ur) ur = 4;
+      for (;;) {
+        const int b = k & 1;
+        const RefineBufs rb{Y64[0].get(), Y64[1].get(), Y32[b].get(), Y32[1 - b].get(),
+                            Z32[1 - b].get(), op.inv_out32.get()};
+        launches += batch_sweep_vw<float, float, EPI_REFINE>(
+            vw, ur, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
+            bs, cs.get(), Y32[b].get(), Y32[1 - b].get(), Z32[b].get(), Z32[1 - b].get(),
+            op.inv_out32.get(), P, sc32.get(), part.get(), all_frozen.get(), grid, s, true, rb);
+        ++k;
+        if (k % 4 == 0 && all_done()) break;
+      }
+    } else {
+      for (;;) {
+        const int b = k & 1;
+        if (use32v)
+          launches += batch_sweep_vw<double, float>(
+              vw, u64, op.view32(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
+              bs, cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
+              op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
+        else
+          launches += batch_sweep_vw<double, double>(
+              vw, u64, op.view64(), d_ranges, nranges, d_chunks, nchunks, d_lrow, d_lfirst, nlong,
+              bs, cs.get(), Y64[b].get(), Y64[1 - b].get(), Z64[b].get(), Z64[1 - b].get(),
+              op.inv_out64.get(), P, sc64.get(), part.get(), all_frozen.get(), grid, s);
+        ++k;
+        if (k % 4 == 0 && all_done()) break;
       }
     }
     loop_end();
@@ -883,8 +993,12 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
       col_iters[c0 + c] += h[c].iter;
       col_conv[c0 + c] = 1;
     }
-    spmm_output<double><<<grid_for(nb, 256), 256, 0, s>>>(Y64[0].get(), Y64[1].get(), cs.get(), n,
-                                                          B, outp + (size_t)c0 * n);
+    if (refine)
+      spmm_output_ref<<<grid_for(nb, 256), 256, 0, s>>>(Y64[0].get(), Y32[0].get(), Y32[1].get(),
+                                                        cs.get(), n, B, outp + (size_t)c0 * n);
+    else
+      spmm_output<double><<<grid_for(nb, 256), 256, 0, s>>>(Y64[0].get(), Y64[1].get(), cs.get(),
+                                                            n, B, outp + (size_t)c0 * n);
     ++launches;
   }
   if (!prm.on_device)
@@ -910,6 +1024,7 @@ void pagerank_batch(GraphHandleImpl& g, const BatchParams& prm, const double* pe
     info->column_iterations = tot;
     info->column_iterations_fp32 = colits32;
     info->max_column_iterations = mx;
+    info->refined = refine ? 1 : 0;
     info->kernel_launches = launches;
   }
 }

@@ -28,6 +28,7 @@ struct BatchInfo {
   int64_t column_iterations_fp32 = 0;  // of which in FP32 sweeps
   int64_t max_column_iterations = 0;
   int kernel_launches = 0;
+  int refined = 0;                  // 1: the FP64 phase was an anchor and refinement sweeps
   double sweep_seconds = 0;         // device time of the sweep loops alone
 };
 

@@ -902,6 +902,7 @@ static int32_t batch_impl(const GraphHandle* h, double damping, int32_t directed
       info->kernel_launches = bi.kernel_launches;
       info->sweep_seconds = bi.sweep_seconds;
       info->column_iterations_fp32 = bi.column_iterations_fp32;
+      info->refined = bi.refined;
     }
   });
 }

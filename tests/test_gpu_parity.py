@@ -711,7 +711,7 @@ def seed_vectors(n, B, seed):
     return P
 
 
-@pytest.mark.parametrize("precision,B", [(0, 40), (1, 40), (0, 300)])
+@pytest.mark.parametrize("precision,B", [(0, 40), (1, 40), (0, 300), (1, 300)])
 def test_pagerank_batch_matches_per_vector_oracle(precision, B):
     kg, og = rmat_pair(11 if B > 100 else 12, True, seed=31)
     P = seed_vectors(kg.n, B, 7)
@@ -724,6 +724,31 @@ def test_pagerank_batch_matches_per_vector_oracle(precision, B):
         worst = max(worst, err)
         assert err <= (1e-12 if precision == 0 else 1e-9), (b, err)
     assert info.max_column_iterations >= 1
+
+
+@pytest.mark.parametrize("refine", [1, 0])
+def test_pagerank_batch_refinement_follows_the_fp64_trajectory(refine):
+    """Mixed batches end with one FP64 anchor sweep and refinement sweeps
+    gathering the FP32 correction (tuning key 9 at 1, the default) or with
+    plain FP64 sweeps (0): every column within 1e-9 of its oracle solve,
+    and within 5e-10 of the all-FP64 batch (a column may stop one sweep
+    apart, whose change is below the 1e-10 tolerance)."""
+    kg, og = rmat_pair(12, True, seed=37)
+    P = seed_vectors(kg.n, 72, 11)
+    x64, i64 = kg.pagerank_batch(P, weighted=True, precision=0, tol=1e-10)
+    try:
+        K.set_tuning(K.TUNE_REFINE, refine)
+        xm, im = kg.pagerank_batch(P, weighted=True, precision=1, tol=1e-10)
+        again, _ = kg.pagerank_batch(P, weighted=True, precision=1, tol=1e-10)
+    finally:
+        K.set_tuning(K.TUNE_REFINE, 1)
+    assert im.refined == refine and i64.refined == 0
+    assert im.sweeps_fp32 > 0
+    assert np.array_equal(xm, again)
+    for b in range(P.shape[0]):
+        ref = og.pagerank(weighted=True, personalization=P[b], tol=1e-10)
+        assert np.abs(xm[b] - ref).sum() <= 1e-9, b
+        assert np.abs(xm[b] - x64[b]).sum() <= 5e-10, b
 
 
 @pytest.mark.parametrize("precision", [0, 1])
