@@ -193,9 +193,10 @@ typedef struct NetSolveInfo {
                               then counts the graphs split) */
 } NetSolveInfo;
 
-/* Precision codes: 0 = FP64, 1 = mixed (FP32 sweeps, then FP64 sweeps on
- * the same trajectory until the reference's stopping rule holds in FP64),
- * 2 = FP32 only. */
+/* Precision codes: 0 = FP64, 1 = mixed (FP32 sweeps, then on the same
+ * trajectory one FP64 anchor sweep and refinement sweeps that gather the
+ * FP32 correction, or plain FP64 sweeps with tuning key 9 at 0, until the
+ * reference's stopping rule holds in FP64), 2 = FP32 only. */
 NET_API int32_t net_pagerank_ex(const GraphHandle *h, double damping, int32_t directed,
                         int32_t weighted, const double *personalization,
                         int32_t dangling, int32_t loops, double tol,

@@ -14,8 +14,9 @@
 // order, so the results do not change from run to run.
 //
 // Precision: FP64, or mixed (FP32 sweeps until every column's change is below
-// max(tol * switch_factor, switch_floor), then FP64 sweeps on the same
-// trajectories until each column meets tol).
+// max(tol * switch_factor, switch_floor), then, on the same trajectories, one
+// FP64 anchor sweep and refinement sweeps gathering the FP32 correction (or
+// plain FP64 sweeps) until each column meets tol).
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
