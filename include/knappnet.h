@@ -432,7 +432,8 @@ NET_API void net_set_sweep_timing(int32_t on);
  * over a thread-block cluster (0, default: the larger of 4096 and the node
  * count over the launch's CTAs); 16 = packed graphs: CTAs per cluster for
  * those graphs (0 tuned with key 6 per batch, 1 none, 4, 8); 17 = FP64
- * PageRank with a uniform teleport on at most this many edges runs as one
+ * PageRank (teleport vector, if any, in host memory) on at most this many
+ * edges runs as one
  * packed-graph launch (default 262,144; 0 never; NetSolveInfo.sweep_kernel is
  * then 0). Setting key 0, 4, 7 or 10 also bypasses the timing.
  * Returns 1 for an unknown key or value. */

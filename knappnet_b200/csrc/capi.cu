@@ -374,13 +374,15 @@ static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t direc
       p.personalization = personalization;
       p.pers_on_device = pers_dev != 0;
     }
-    // A small graph's FP64 solve with a uniform teleport runs as a packed
-    // batch of one graph: one launch does every iteration on the device (a
-    // cluster of CTAs splits it from 4096 nodes), where the sweep path would
-    // launch a few kernels per iteration that each take microseconds.
+    // A small graph's FP64 solve (teleport vector, if any, in host memory)
+    // runs as a packed batch of one graph: one launch does every iteration
+    // on the device (a cluster of CTAs splits it from 4096 nodes), where the
+    // sweep path would launch a few kernels per iteration that each take
+    // microseconds. The packed path checks a teleport vector with the same
+    // messages.
     const knb::Tuning& tu = knb::tuning();
-    if (precision == 0 && !personalization && tu.variant == 0 && tu.small_edges > 0 &&
-        (int64_t)g.m <= tu.small_edges) {
+    if (precision == 0 && (!personalization || !pers_dev) && tu.variant == 0 &&
+        tu.small_edges > 0 && (int64_t)g.m <= tu.small_edges) {
       const int64_t off[2] = {0, (int64_t)g.n};
       int64_t iters = 0;
       knb::EgoInput in;
@@ -393,6 +395,7 @@ static int32_t pagerank_impl(const GraphHandle* h, double damping, int32_t direc
       in.loops = loops;
       in.tol = p.tol;
       in.max_iter = p.max_iter;
+      in.personalization = personalization;
       in.out_on_device = out_dev != 0;
       in.iterations_out = &iters;
       knb::EgoResult r;

@@ -57,8 +57,8 @@ struct Tuning {
   int autotune = 1;       // 1: pick the sweep kernel per operator by timing candidates (large operators)
   int bulk_ctas = 0;      // bulk-staged sliced sweeps: CTAs per SM the carveout is sized for (0: 4)
   int64_t bulk_skip_chunk = -1;  // test of the bounded waits: a chunk of the first warp never copied
-  int64_t small_edges = 1 << 18;  // FP64 solves with a uniform teleport on at most this many
-                                  // edges run as one packed-graph launch (0: never)
+  int64_t small_edges = 1 << 18;  // FP64 solves (host teleport vector, if any) on at most
+                                  // this many edges run as one packed-graph launch (0: never)
   double switch_factor = 8192;
   double switch_floor = 2e-6;
 };

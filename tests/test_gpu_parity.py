@@ -138,8 +138,8 @@ PR_OPTIONS = [
 @pytest.mark.parametrize("small_edges", [1 << 18, 0])
 @pytest.mark.parametrize("fx_name", sorted(DOC["fixtures"]))
 def test_pagerank_fp64_within_1e12_of_oracle(fx_name, small_edges):
-    """Every fixture and option set, with uniform-teleport solves as one
-    packed launch (the default) and on the sweep kernels (key 17 at 0)."""
+    """Every fixture and option set, with FP64 solves as one packed launch
+    (the default for small graphs) and on the sweep kernels (key 17 at 0)."""
     fx = DOC["fixtures"][fx_name]
     kg, og = both(fx)
     n = fx["n"]
