@@ -109,6 +109,32 @@ static int run_cpu(void) {
         "net_twomode_eigenvector on NULL");
   check(leading(NULL, 0, lmemb, &value, &splits, err, sizeof err) != 0,
         "net_leading_eigen on NULL");
+  /* the extensions check their arguments before any device work */
+  const int64_t ends[2] = {0, 1};
+  int64_t offs[3];
+  GraphHandle *fg = NULL;
+  err[0] = 0;
+  check(net_frame_graph(2, ends, ends, NULL, NULL, 2, 1, NULL, NULL, NULL, err, sizeof err) != 0 &&
+            strstr(err, "out is null") != NULL,
+        "net_frame_graph without an output handle");
+  check(net_frame_egos(2, ends, ends, NULL, NULL, 2, 1, ends, NULL, 2, &fg, NULL, NULL, NULL,
+                       NULL, err, sizeof err) != 0 &&
+            strstr(err, "node_offsets is null") != NULL && fg == NULL,
+        "net_frame_egos without node offsets");
+  check(net_frame_egos(2, ends, ends, NULL, NULL, 2, 1, NULL, NULL, 2, &fg, offs, NULL, NULL,
+                       NULL, err, sizeof err) != 0 &&
+            strstr(err, "node_ego is null") != NULL,
+        "net_frame_egos without node ego labels");
+  check(net_measure_gather(3, 1 << 20, &value, err, sizeof err) != 0 &&
+            strstr(err, "gather source") != NULL,
+        "net_measure_gather with an unknown source");
+  check(net_projected_eigen(21, out, out, out, err, sizeof err) != 0 &&
+            strstr(err, "between 0 and 20") != NULL,
+        "net_projected_eigen beyond order 20");
+  check(net_projected_eigen(0, NULL, NULL, NULL, err, sizeof err) == 0,
+        "net_projected_eigen of order 0 does nothing");
+  check(net_set_tuning(99, 0.0) != 0 && net_set_tuning(17, -1.0) != 0,
+        "net_set_tuning rejects unknown keys and values");
   /* a message is cut to the buffer and NUL-terminated */
   char tiny[5];
   memset(tiny, 'x', sizeof tiny);
