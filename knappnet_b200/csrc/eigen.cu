@@ -563,7 +563,7 @@ __device__ __forceinline__ bool lz_last(unsigned int* ticket) {
   __shared__ bool last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x * gridDim.y - 1;
   __syncthreads();
   if (last) __threadfence();
   return last;
@@ -588,35 +588,76 @@ __device__ __forceinline__ void block_partials(double (&a)[K], double* part, int
   }
 }
 
+// Rows of a 4096-row block held by one thread (rows t, t + 256, ...).
+constexpr int VR = VB / VB_T;
+// Projections per CTA of lz_project: blockIdx.y takes basis vectors
+// [4y, 4y + 4), so a full pass over 20 vectors runs 5 CTAs per row block.
+constexpr int LZ_PG = 4;
+
+__host__ __device__ constexpr int lz_project_slots(int k, int mode) { return k + (mode == 0 ? 1 : 0); }
+inline unsigned project_groups(int k, int mode) {
+  return (unsigned)((lz_project_slots(k, mode) + LZ_PG - 1) / LZ_PG);
+}
+
 // mode 0: local pass (also computes ||w||^2 -> before); 1: full pass; 2: full
-// pass 2 (skipped unless need2). Projects w on V[lo..hi).
+// pass 2 (skipped unless need2). Projects w on V[lo..hi). Each thread keeps its
+// 16 values of w in registers and loads its 16 values of one basis vector at
+// once; every dot product is summed per thread in row order, then per warp and
+// CTA and over the row blocks in fixed order, as in a one-dimensional sweep.
 __global__ void __launch_bounds__(VB_T)
 lz_project(const double* __restrict__ V, size_t dim, int lo, int hi, const double* __restrict__ w,
            int mode, double* __restrict__ part, LzState* st, const IterState* ist) {
   if (ist && iteration_done(ist)) return;
   if (mode == 2 && !st->need2) return;
-  const int K = hi - lo;
-  double a[MAXB + 1];
+  const int K = hi - lo, slots = lz_project_slots(K, mode);
+  const int s0 = blockIdx.y * LZ_PG, s1 = min(slots, s0 + LZ_PG);
+  __shared__ double sh[VB_T / 32][LZ_PG];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const size_t b0 = (size_t)blockIdx.x * VB, r1 = min(dim, b0 + VB);
+  const size_t i0 = b0 + threadIdx.x;
+  double wr[VR];
 #pragma unroll
-  for (int s = 0; s <= MAXB; ++s) a[s] = 0.0;
-  size_t r0 = (size_t)blockIdx.x * VB, r1 = min(dim, r0 + VB);
-  for (size_t i = r0 + threadIdx.x; i < r1; i += VB_T) {
-    double wi = w[i];
-#pragma unroll
-    for (int s = 0; s < MAXB; ++s)
-      if (s < K) a[s] += V[(size_t)(lo + s) * dim + i] * wi;
-    a[MAXB] += wi * wi;
+  for (int r = 0; r < VR; ++r) {
+    const size_t i = i0 + (size_t)r * VB_T;
+    wr[r] = i < r1 ? w[i] : 0.0;
   }
-  // pack the norm after the K coefficients
-  a[K] = a[MAXB];
-  block_partials<MAXB + 1>(a, part, MAXB + 1, K + 1);
+#pragma unroll 1
+  for (int s = s0; s < s1; ++s) {
+    double a = 0.0;
+    if (s < K) {
+      const double* vs = V + (size_t)(lo + s) * dim;
+      double v[VR];
+#pragma unroll
+      for (int r = 0; r < VR; ++r) {
+        const size_t i = i0 + (size_t)r * VB_T;
+        v[r] = i < r1 ? vs[i] : 0.0;
+      }
+#pragma unroll
+      for (int r = 0; r < VR; ++r)
+        if (i0 + (size_t)r * VB_T < r1) a = fma(v[r], wr[r], a);
+    } else {
+#pragma unroll
+      for (int r = 0; r < VR; ++r)
+        if (i0 + (size_t)r * VB_T < r1) a = fma(wr[r], wr[r], a);
+    }
+    a = warp_sum(a);
+    if (lane == 0) sh[wp][s - s0] = a;
+  }
+  __syncthreads();
+  if (wp == 0) {
+    for (int s = s0; s < s1; ++s) {
+      double v = lane < VB_T / 32 ? sh[lane][s - s0] : 0.0;
+      v = warp_sum(v);
+      if (lane == 0) part[(size_t)blockIdx.x * (MAXB + 1) + s] = v;
+    }
+  }
   if (!lz_last(&st->ticket)) return;
   if (threadIdx.x < 32) {
-    for (int s = 0; s <= K; ++s) {
+    for (int s = 0; s < slots; ++s) {
       double v = fixed_block_sum(part, gridDim.x, MAXB + 1, s);
       if (threadIdx.x == 0) {
         if (s < K) st->tmp[s] = v;
-        else if (mode == 0) st->before = sqrt(v);
+        else st->before = sqrt(v);
       }
     }
   }
@@ -625,6 +666,8 @@ lz_project(const double* __restrict__ V, size_t dim, int lo, int hi, const doubl
 
 // w -= V[lo..hi) tmp, ||w|| into mid (mode 0) or after; coefficients added
 // into coef; the DGKS decision after full passes (eigenvector.rs:997-1021).
+// Each thread keeps its 16 values of w in registers and subtracts one basis
+// vector at a time from all of them, in basis order.
 __global__ void __launch_bounds__(VB_T)
 lz_subtract(const double* __restrict__ V, size_t dim, int lo, int hi, double* __restrict__ w,
             int mode, double* __restrict__ part, LzState* st, const IterState* ist) {
@@ -634,13 +677,45 @@ lz_subtract(const double* __restrict__ V, size_t dim, int lo, int hi, double* __
   __shared__ double c[MAXB];
   if (threadIdx.x < K) c[threadIdx.x] = st->tmp[threadIdx.x];
   __syncthreads();
+  const size_t b0 = (size_t)blockIdx.x * VB, r1 = min(dim, b0 + VB);
+  const size_t i0 = b0 + threadIdx.x;
+  double x[VR];
+#pragma unroll
+  for (int r = 0; r < VR; ++r) {
+    const size_t i = i0 + (size_t)r * VB_T;
+    x[r] = i < r1 ? w[i] : 0.0;
+  }
+  if (b0 + VB <= dim) {
+#pragma unroll 1
+    for (int s = 0; s < K; ++s) {
+      const double* vs = V + (size_t)(lo + s) * dim + i0;
+      const double cs = c[s];
+      double v[VR];
+#pragma unroll
+      for (int r = 0; r < VR; ++r) v[r] = vs[(size_t)r * VB_T];
+#pragma unroll
+      for (int r = 0; r < VR; ++r) x[r] = fma(-cs, v[r], x[r]);
+    }
+  } else {
+#pragma unroll 1
+    for (int s = 0; s < K; ++s) {
+      const double* vs = V + (size_t)(lo + s) * dim;
+      const double cs = c[s];
+#pragma unroll
+      for (int r = 0; r < VR; ++r) {
+        const size_t i = i0 + (size_t)r * VB_T;
+        if (i < r1) x[r] = fma(-cs, vs[i], x[r]);
+      }
+    }
+  }
   double a[1] = {0.0};
-  size_t r0 = (size_t)blockIdx.x * VB, r1 = min(dim, r0 + VB);
-  for (size_t i = r0 + threadIdx.x; i < r1; i += VB_T) {
-    double x = w[i];
-    for (int s = 0; s < K; ++s) x -= c[s] * V[(size_t)(lo + s) * dim + i];
-    w[i] = x;
-    a[0] += x * x;
+#pragma unroll
+  for (int r = 0; r < VR; ++r) {
+    const size_t i = i0 + (size_t)r * VB_T;
+    if (i < r1) {
+      w[i] = x[r];
+      a[0] = fma(x[r], x[r], a[0]);
+    }
   }
   block_partials<1>(a, part, 1, 1);
   if (!lz_last(&st->ticket)) return;
@@ -1492,11 +1567,12 @@ static bool symmetric_leading(const DevOp& A, double tol, double shift, int64_t 
         lz_begin<<<1, 32, 0, s>>>(st.get(), ist.get());
         *launches += 1 + apply(vj, use32 ? v32.get() : nullptr, w.get(), ist.get());
         const int cols = jj + 1, lo = cols >= 2 ? cols - 2 : 0;
-        lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
+        const dim3 local(nb, project_groups(cols - lo, 0)), full(nb, project_groups(cols, 1));
+        lz_project<<<local, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
         lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, lo, cols, w.get(), 0, part.get(), st.get(), ist.get());
-        lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 1, part.get(), st.get(), ist.get());
+        lz_project<<<full, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 1, part.get(), st.get(), ist.get());
         lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 1, part.get(), st.get(), ist.get());
-        lz_project<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 2, part.get(), st.get(), ist.get());
+        lz_project<<<full, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 2, part.get(), st.get(), ist.get());
         lz_subtract<<<nb, VB_T, 0, s>>>(V.get(), dim, 0, cols, w.get(), 2, part.get(), st.get(), ist.get());
         lz_end<<<1, 32, 0, s>>>(st.get(), ist.get(), hm_d.get(), m, jj);
         *launches += 7;
