@@ -787,6 +787,62 @@ def run_c4b_ranks(args):
     return line
 
 
+def run_rows(args):
+    """PageRank of the benchmark line's graph (R-MAT 24, lognormal weights,
+    FP64) split by rows over N GPUs (torchrun, one process per GPU): each
+    rank's shard holds rows of nearly equal rows plus arcs (net_shard_bounds),
+    sweeps them into its payload, the ranks all-gather the payloads over
+    NCCL (one collective per sweep, also for one rank under torchrun), and
+    every rank finishes the sweep over all nodes. Total work is fixed (strong
+    scaling). Rank 0 checks the scores against the single-GPU FP64 solve."""
+    import torch
+    import knappnet_b200 as K
+    from knappnet_b200 import ranks
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    g = make_graph(args.scale)
+    b = g.shard_bounds(world, directed=True, weighted=True)
+    sh = K.Shard(g, b, rank, damping=0.85, directed=True, weighted=True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    keep = {}
+
+    def solve():
+        sh.restart(torch.empty(1, device=dev))
+        ev0.record()
+        keep["sweeps"] = ranks.pagerank_rows(dist, sh, device=dev, tol=1e-9)
+        ev1.record()
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / 1e3
+    for _ in range(args.warmup):
+        solve()
+    ranks.barrier(dist)
+    times = [solve() for _ in range(max(args.steps, 1))]
+    sec = max_over_ranks(dist, statistics.median(times))
+    sweeps = keep["sweeps"]
+    line = None
+    if rank == 0:
+        x = sh.scores()
+        ref, info = g.pagerank_ex(directed=True, weighted=True, tol=1e-9, precision=K.PREC_FP64)
+        arcs = int(g.m)  # a directed graph without loops: one pull arc per edge
+        line = {"workload": f"rows on {world} GPUs: R-MAT {args.scale} directed, lognormal "
+                            "weights, PageRank FP64, tol 1e-9, split by rows of the pull "
+                            "operator; one all-gather of the payloads per sweep over NCCL",
+                "metric": "GTEPS per iteration (whole job)",
+                "value": round(arcs * sweeps / sec / 1e9, 3), "unit": "GTEPS",
+                "higher_is_better": True, "n_gpus": world, "scaling": "strong",
+                "ms_per_solve": round(sec * 1e3, 3), "sweeps": sweeps,
+                "rows_per_rank": [int(b[k + 1] - b[k]) for k in range(world)],
+                "payload_bytes_per_rank_per_sweep": sh.payload_len * 8,
+                "exchange": "nccl all_gather_into_tensor" if dist is not None else "none",
+                "l1_vs_single_gpu_fp64": float(np.abs(x - ref).sum()),
+                "single_gpu_fp64_iterations": int(info.iterations)}
+    sh.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return line
+
+
 def run_c5(args):
     """Differentiable PageRank on directed R-MAT 20 with lognormal weights:
     forward solve, adjoint solve and edge-gradient scatter through
@@ -957,9 +1013,9 @@ def run_next(args):
     return lines
 
 
-SHARDED = {"c4a": run_c4a_ranks, "c4b": run_c4b_ranks}
+SHARDED = {"c4a": run_c4a_ranks, "c4b": run_c4b_ranks, "rows": run_rows}
 WORKLOADS = {"c1": run_c1, "c2": run_c2, "c4a": run_c4a, "c4b": run_c4b, "c5": run_c5,
-             "next": run_next}
+             "next": run_next, "rows": run_rows}
 
 
 def main():
@@ -971,7 +1027,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of CPU work for the cpu_baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["c3", "c1", "c2", "c4a", "c4b", "c5", "next"],
+    ap.add_argument("--workload", choices=["c3", "c1", "c2", "c4a", "c4b", "c5", "next", "rows"],
                     default="c3",
                     help="c3 (default) is the benchmark line; the others print one JSON line "
                          "each for the other configurations (next: one per measure beyond "

@@ -473,6 +473,56 @@ NET_API int32_t net_pagerank_csr_static(int64_t n, const uint32_t *d_offsets,
                                 int64_t *iterations, void *stream, char *err,
                                 size_t err_len);
 
+/* PageRank of one graph split over several GPUs by rows of its pull
+ * operator (in-arcs with directed set on a directed graph, else all arcs),
+ * one process per GPU. No counterpart in the reference, whose loop
+ * (crates/engine/src/metrics/spectral.rs:247-280) runs in one process.
+ *
+ * net_shard_bounds writes parts + 1 row boundaries (0 first, n last) that
+ * give each of `parts` ranks about an equal share of rows plus arcs. Each
+ * rank then builds its shard with the same graph, options and boundaries
+ * (net_shard_new; the options and their checks are net_pagerank's, with the
+ * personalization vector, if any, given as n device doubles) and starts
+ * from the uniform iterate. A sweep is: net_shard_sweep on every rank,
+ * writing *payload_len doubles (device) -- the unnormalised scores of its
+ * rows and their sum; an all-gather of the ranks' payloads in rank order
+ * (parts * payload_len doubles, e.g. ncclAllGather); net_shard_finish on
+ * every rank with the gathered payloads, which normalises the new iterate
+ * over all nodes, returns its L1 change from the previous one in *change
+ * (host; waits for the stream) and readies the next sweep. Every rank
+ * computes the same iterate bit for bit, so all ranks stop on the same
+ * sweep when the change reaches the tolerance, as net_pagerank does; the
+ * caller runs that loop (and its iteration cap). net_shard_scores copies
+ * the current iterate (n doubles) to host or device memory;
+ * net_shard_restart returns the shard to the uniform iterate. The shard
+ * lives on the current device; its calls run on `stream` (NULL: the
+ * default stream) and one shard must not be used by two threads at once.
+ * The boundaries must not decrease and parts is at most 1024. */
+typedef struct NetShard NetShard;
+NET_API int32_t net_shard_bounds(const GraphHandle *h, int32_t directed,
+                                 int32_t weighted, int32_t loops,
+                                 int32_t parts, int64_t *bounds, char *err,
+                                 size_t err_len);
+NET_API int32_t net_shard_new(const GraphHandle *h, double damping,
+                              int32_t directed, int32_t weighted,
+                              const double *d_personalization,
+                              int32_t dangling, int32_t loops,
+                              const int64_t *bounds, int32_t parts,
+                              int32_t rank, NetShard **shard,
+                              int64_t *payload_len, char *err,
+                              size_t err_len);
+NET_API int32_t net_shard_sweep(NetShard *shard, double *d_payload,
+                                void *stream, char *err, size_t err_len);
+NET_API int32_t net_shard_finish(NetShard *shard, const double *d_gathered,
+                                 double *change, void *stream, char *err,
+                                 size_t err_len);
+NET_API int32_t net_shard_scores(const NetShard *shard, double *out,
+                                 int32_t out_on_device, void *stream,
+                                 char *err, size_t err_len);
+NET_API int32_t net_shard_restart(NetShard *shard, void *stream, char *err,
+                                  size_t err_len);
+NET_API void net_shard_free(NetShard *shard);
+
 /* Calibration: random 4-byte gathers per second the whole GPU sustains,
  * from a device array of `words` FP32 values (source 0; an array that fits
  * in L2 gives the rate a sparse sweep's gathers of its iterate run into),

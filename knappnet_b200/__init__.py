@@ -159,6 +159,21 @@ def lib() -> ctypes.CDLL:
     L.net_set_tuning.restype = i32
     L.net_device_sync.argtypes = [cp, sz]
     L.net_device_sync.restype = i32
+    L.net_shard_bounds.argtypes = [h, i32, i32, i32, i32, vp, cp, sz]
+    L.net_shard_bounds.restype = i32
+    L.net_shard_new.argtypes = [h, f64, i32, i32, vp, i32, i32, vp, i32, i32, ctypes.POINTER(h),
+                                ctypes.POINTER(i64), cp, sz]
+    L.net_shard_new.restype = i32
+    L.net_shard_sweep.argtypes = [h, vp, vp, cp, sz]
+    L.net_shard_sweep.restype = i32
+    L.net_shard_finish.argtypes = [h, vp, ctypes.POINTER(f64), vp, cp, sz]
+    L.net_shard_finish.restype = i32
+    L.net_shard_scores.argtypes = [h, vp, i32, vp, cp, sz]
+    L.net_shard_scores.restype = i32
+    L.net_shard_restart.argtypes = [h, vp, cp, sz]
+    L.net_shard_restart.restype = i32
+    L.net_shard_free.argtypes = [h]
+    L.net_shard_free.restype = None
     _lib = L
     return L
 
@@ -278,6 +293,15 @@ class Graph:
                                          precision, ctypes.c_void_p(out_ptr), ctypes.byref(info),
                                          err, ERR_LEN), err)
         return info
+
+    def shard_bounds(self, parts, directed=True, weighted=False, loops=0):
+        """net_shard_bounds: parts + 1 row boundaries of PageRank's pull
+        operator giving each part about an equal share of rows plus arcs."""
+        b = np.zeros(int(parts) + 1, dtype=np.int64)
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_shard_bounds(self.h, int(directed), int(weighted), loops, int(parts),
+                                      _ptr(b), err, ERR_LEN), err)
+        return b
 
     def pagerank_batch(self, personalization, damping=0.85, directed=True, weighted=False,
                        dangling=0, loops=0, tol=0.0, max_iter=0, precision=PREC_FP64):
@@ -453,6 +477,82 @@ class Graph:
         info.eigenvalue = val.value
         info.connected = conn.value
         return out[: self.n], info
+
+
+def _stream_ptr(t):
+    """The CUDA stream handle of torch's current stream on t's device (None
+    for a CPU tensor or a plain pointer)."""
+    if hasattr(t, "is_cuda") and t.is_cuda:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+    return None
+
+
+def _dev_ptr(t):
+    return ctypes.c_void_p(t if isinstance(t, int) else t.data_ptr())
+
+
+class Shard:
+    """One rank's row shard of a graph's PageRank split over several GPUs by
+    rows (net_shard_new): `sweep` writes this rank's payload, `finish` takes
+    the payloads of all ranks gathered in rank order and returns the L1
+    change, `scores` reads the iterate. Buffers are CUDA tensors (or device
+    pointers); calls run on torch's current stream of the tensor's device."""
+
+    def __init__(self, graph, bounds, rank, damping=0.85, directed=True, weighted=False,
+                 personalization_ptr=None, dangling=0, loops=0):
+        b = np.ascontiguousarray(bounds, dtype=np.int64)
+        self.parts = len(b) - 1
+        self.rank = int(rank)
+        self.n = graph.n
+        self.bounds = b
+        self._graph = graph  # the shard reads the graph's operator
+        h = ctypes.c_void_p()
+        plen = ctypes.c_int64()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        pp = None if personalization_ptr is None else ctypes.c_void_p(personalization_ptr)
+        _check(lib().net_shard_new(graph.h, damping, int(directed), int(weighted), pp, dangling,
+                                   loops, _ptr(b), self.parts, self.rank, ctypes.byref(h),
+                                   ctypes.byref(plen), err, ERR_LEN), err)
+        self.h = h
+        self.payload_len = int(plen.value)
+
+    def sweep(self, payload):
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_shard_sweep(self.h, _dev_ptr(payload), _stream_ptr(payload), err,
+                                     ERR_LEN), err)
+
+    def finish(self, gathered) -> float:
+        change = ctypes.c_double()
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_shard_finish(self.h, _dev_ptr(gathered), ctypes.byref(change),
+                                      _stream_ptr(gathered), err, ERR_LEN), err)
+        return change.value
+
+    def restart(self, like=None):
+        """Back to the uniform iterate (on torch's current stream of `like`'s
+        device, if given)."""
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_shard_restart(self.h, _stream_ptr(like), err, ERR_LEN), err)
+
+    def scores(self):
+        out = np.zeros(self.n)
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_shard_scores(self.h, _ptr(out), 0, None, err, ERR_LEN), err)
+        return out
+
+    def scores_device(self, out):
+        err = ctypes.create_string_buffer(ERR_LEN)
+        _check(lib().net_shard_scores(self.h, _dev_ptr(out), 1, _stream_ptr(out), err, ERR_LEN),
+               err)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.net_shard_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def generate_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, clean=True,

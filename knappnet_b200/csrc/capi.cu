@@ -24,11 +24,16 @@
 #include "generate.cuh"
 #include "graph.cuh"
 #include "pagerank.cuh"
+#include "shard.cuh"
 
 using knb::Error;
 
 struct GraphHandle {
   knb::GraphHandleImpl g;
+};
+
+struct NetShard {
+  std::unique_ptr<knb::Shard> s;
 };
 
 namespace {
@@ -1369,6 +1374,107 @@ int32_t net_measure_gather(int32_t source, int64_t words, double* gathers_per_se
     *gathers_per_second = knb::measure_gather_rate(source, (uint64_t)words, knb::thread_stream());
   });
 }
+
+// Row shards of one graph's PageRank (shard.cuh): the operator and the
+// option checks of net_pagerank, then the split sweep.
+static knb::Operator& shard_operator(knb::GraphHandleImpl& g, int32_t directed, int32_t weighted,
+                                     int32_t loops, cudaStream_t s) {
+  if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+  const int which = knb::pagerank_rows(g, directed != 0);
+  return g.op(which, weighted != 0, knb::pagerank_loop_factor(which, loops), s);
+}
+
+static cudaStream_t shard_stream(void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : cudaStream_t(0);
+}
+
+static knb::Shard& shard_of(const NetShard* sh) {
+  if (!sh || !sh->s) throw Error("shard handle is null");
+  return *sh->s;
+}
+
+int32_t net_shard_bounds(const GraphHandle* h, int32_t directed, int32_t weighted, int32_t loops,
+                         int32_t parts, int64_t* bounds, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (!bounds) throw Error("bounds is null");
+    cudaStream_t s = knb::thread_stream();
+    knb::Operator& op = shard_operator(g, directed, weighted, loops, s);
+    const std::vector<int64_t> b = knb::shard_bounds(op, parts, s);
+    memcpy(bounds, b.data(), b.size() * 8);
+  });
+}
+
+int32_t net_shard_new(const GraphHandle* h, double damping, int32_t directed, int32_t weighted,
+                      const double* d_personalization, int32_t dangling, int32_t loops,
+                      const int64_t* bounds, int32_t parts, int32_t rank, NetShard** shard,
+                      int64_t* payload_len, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::GraphHandleImpl& g = handle(h);
+    if (!shard || !bounds) throw Error("a buffer is null");
+    *shard = nullptr;
+    if (dangling != 0 && dangling != 1)
+      throw Error("unknown dangling-node code " + std::to_string(dangling));
+    if (loops < 0 || loops > 2) throw Error("unknown self-loop weight code " + std::to_string(loops));
+    if (!(damping >= 0.0 && damping <= 1.0))
+      throw Error("damping is " + fmt_g(damping) + "; it must be between 0 and 1");
+    if (parts < 1 || parts > 1024) throw Error("the number of shards must be between 1 and 1024");
+    cudaStream_t s = knb::thread_stream();
+    if (weighted && g.n > 0) check_nonnegative(g, "PageRank", s);
+    knb::Operator& op = shard_operator(g, directed, weighted, loops, s);
+    knb::DevBuf<double> p;
+    if (d_personalization && g.n > 0) {
+      p.alloc(g.n);
+      KNB_CUDA(cudaMemcpyAsync(p.get(), d_personalization, (size_t)g.n * 8,
+                               cudaMemcpyDeviceToDevice, s));
+      knb::normalize_personalization_device(p.get(), g.n, s);
+    }
+    const std::vector<int64_t> b(bounds, bounds + parts + 1);
+    const bool uniform = !d_personalization || dangling == 1;
+    auto out = std::make_unique<NetShard>();
+    out->s = knb::shard_new(op, damping, p.get(), uniform, b, rank, s);
+    if (payload_len) *payload_len = (int64_t)out->s->payload_len;
+    *shard = out.release();
+  });
+}
+
+int32_t net_shard_sweep(NetShard* shard, double* d_payload, void* stream, char* err,
+                        size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::Shard& sh = shard_of(shard);
+    if (!d_payload) throw Error("the payload buffer is null");
+    knb::shard_sweep(sh, d_payload, shard_stream(stream));
+  });
+}
+
+int32_t net_shard_restart(NetShard* shard, void* stream, char* err, size_t err_len) {
+  return guard(err, err_len,
+               [&] { knb::shard_restart(shard_of(shard), shard_stream(stream)); });
+}
+
+int32_t net_shard_finish(NetShard* shard, const double* d_gathered, double* change, void* stream,
+                         char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    knb::Shard& sh = shard_of(shard);
+    if (!d_gathered || !change) throw Error("a buffer is null");
+    *change = knb::shard_finish(sh, d_gathered, shard_stream(stream));
+  });
+}
+
+int32_t net_shard_scores(const NetShard* shard, double* out, int32_t out_on_device, void* stream,
+                         char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    const knb::Shard& sh = shard_of(shard);
+    if (sh.n == 0) return;
+    if (!out) throw Error("the output buffer is null");
+    cudaStream_t s = shard_stream(stream);
+    KNB_CUDA(cudaMemcpyAsync(out, sh.x.get(), (size_t)sh.n * 8,
+                             out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+void net_shard_free(NetShard* shard) { delete shard; }
 
 int32_t net_device_sync(char* err, size_t err_len) {
   return guard(err, err_len, [&] { KNB_CUDA(cudaDeviceSynchronize()); });

@@ -1414,6 +1414,24 @@ static void eig_product(const OpView<MT>& v, const VT* x, const Epi& e, const Pa
                                                           carry, head, e, part1, npart, part2,
                                                           const_cast<IterState*>(st));
 }
+// FP64 products for row shards of PageRank (shard.cu): the same warp tiles
+// and split-row pass over a view whose offsets start at 0.
+uint32_t product_tile() { return EIG_TILE; }
+
+void product64(const OpView<double>& v, const Partition& P, const double* x, double* y,
+               ProductScratch& sc, cudaStream_t s) {
+  if (sc.carry.n < (size_t)P.ntiles + 1) {
+    sc.carry.alloc((size_t)P.ntiles + 1);
+    sc.head.alloc((size_t)P.ntiles + 1);
+    sc.part1.alloc((size_t)P.ntiles * 2 + 2);
+    sc.part2.alloc(SPLIT_CTAS * 2 + 2);
+  }
+  PlainEpi<double> e{y};
+  eig_product<double, double>(v, x, e, P, sc.carry.get(), sc.head.get(), sc.part1.get(),
+                              sc.part2.get(), nullptr, s);
+  KNB_LAUNCH("shard product");
+}
+
 // Relative residual below which FP32 products stop helping the Lanczos
 // process (FP32 rounding of the products is about 1e-7 relative).
 constexpr double FP32_FLOOR = 1e-5;

@@ -76,4 +76,14 @@ bool symmetric_eigen_device(const double* a, int n, double* vals, double* vecs, 
 void leading_eigen(GraphHandleImpl& g, bool weighted, int64_t* membership, double* q,
                    int64_t* splits, int* launches, cudaStream_t s);
 
+// FP64 products y = A x on merge-path warp tiles over the rows of `v`
+// (offsets from 0) with the partition build_partition makes for
+// product_tile() items per tile; the scratch grows on first use.
+struct ProductScratch {
+  DevBuf<double> carry, head, part1, part2;
+};
+uint32_t product_tile();
+void product64(const OpView<double>& v, const Partition& P, const double* x, double* y,
+               ProductScratch& sc, cudaStream_t s);
+
 }  // namespace knb

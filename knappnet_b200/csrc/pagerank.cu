@@ -409,6 +409,21 @@ static void normalize_personalization(double* p, uint32_t n, double* part, IterS
   KNB_LAUNCH("pers_scale");
 }
 
+void normalize_personalization_device(double* p, uint32_t n, cudaStream_t s) {
+  const unsigned gv = grid_for(n, VT_THREADS, 1184);
+  DevBuf<double> part((size_t)gv * 2 + 8);
+  DevBuf<IterState> st(1);
+  IterState* hst = nullptr;
+  KNB_CUDA(cudaMallocHost(&hst, sizeof(IterState)));
+  try {
+    normalize_personalization(p, n, part.get(), st.get(), hst, s);
+  } catch (...) {
+    cudaFreeHost(hst);
+    throw;
+  }
+  KNB_CUDA(cudaFreeHost(hst));
+}
+
 // Scratch of PageRank solves on one operator, kept between calls: iterates,
 // per-tile partials, carries, states, pinned host state slots and events.
 // A solve holds `mu` while it runs, so concurrent calls on one operator take

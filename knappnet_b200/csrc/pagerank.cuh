@@ -74,6 +74,10 @@ void pagerank_op(Operator& op, const PagerankParams& prm, double* out, bool out_
 // Which rows PageRank pulls along (1 in-CSR, 2 directions ignored, 0 the
 // undirected CSR) and the diagonal factor of a self-loop in them.
 int pagerank_rows(const GraphHandleImpl& g, bool directed);
+// Checks a device personalization vector of n values (finite, nonnegative,
+// positive sum) and rescales it to sum 1 in place, as the reference's
+// `probabilities` (crates/engine/src/metrics/spectral.rs:284-305).
+void normalize_personalization_device(double* p, uint32_t n, cudaStream_t s);
 double pagerank_loop_factor(int which, int loops);
 
 // Device time of the dominant kernel (the merge-path sweep) of the last solve

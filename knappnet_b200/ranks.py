@@ -1,15 +1,17 @@
-"""One process per GPU: rank set-up, reductions over ranks, and the splits of
-the workloads that shard with no exchange.
+"""One process per GPU: rank set-up, reductions over ranks, the splits of
+the workloads that shard with no exchange, and the row split of one graph's
+PageRank.
 
-PageRank on one graph needs an exchange of the iterate every sweep to
-shard, so the benchmark runs independent replicas, one per GPU, and reports
-the arcs all ranks processed over the slowest rank's time. The batched and
-packed-graph workloads split with no exchange at all: teleport vectors by
-contiguous column ranges, packed graphs by contiguous graph ranges balanced
-by their nodes plus arcs; each rank solves its part alone, and the parts
-are assembled on rank 0 afterwards (gather_rows). Reductions and gathers run
-on the process group's own device (CUDA tensors for NCCL, CPU tensors for
-gloo), so the same code serves the GPU runs and the CPU tests.
+The batched and packed-graph workloads split with no exchange at all:
+teleport vectors by contiguous column ranges, packed graphs by contiguous
+graph ranges balanced by their nodes plus arcs; each rank solves its part
+alone, and the parts are assembled on rank 0 afterwards (gather_rows).
+PageRank on one graph splits by rows of its pull operator with one exchange
+per sweep (pagerank_rows): every rank sweeps its rows, the ranks all-gather
+their payloads, and every rank finishes the sweep over all nodes. Reductions
+and gathers run on the process group's own device (CUDA tensors for NCCL,
+CPU tensors for gloo), so the same code serves the GPU runs and the CPU
+tests.
 """
 from __future__ import annotations
 
@@ -118,3 +120,47 @@ def gather_rows(dist, local, ranges):
     if dist.get_rank() != 0:
         return None
     return torch.cat([parts[r][: hi - lo] for r, (lo, hi) in enumerate(ranges)]).cpu().numpy()
+
+
+def all_gather_flat(dist, out, local) -> None:
+    """out (world * len(local) values) <- every rank's `local`, in rank
+    order: one all_gather_into_tensor where the backend has it (NCCL), else
+    the list form."""
+    world = dist.get_world_size()
+    if dist.get_backend() == "nccl":
+        dist.all_gather_into_tensor(out, local)
+        return
+    parts = list(out.view(world, -1).unbind(0))
+    dist.all_gather(parts, local)
+
+
+def pagerank_rows(dist, shard, device=None, tol=0.0, max_iter=0):
+    """PageRank of one graph split over the ranks by rows; returns the number
+    of sweeps (the scores stay in the shard). `shard` is this rank's row
+    shard (knappnet_b200.Shard): a sweep writes its payload_len-value
+    payload, the ranks all-gather the payloads (one collective per sweep,
+    also for a group of one; none without a group, `dist` None), and the
+    shard finishes the sweep over all nodes from them, returning the L1
+    change. Every rank
+    computes the same change, so all ranks stop on the same sweep, at the
+    first change <= tol, as net_pagerank (a tolerance that is not positive
+    selects 1e-12, an iteration cap that is not positive 10000); at the cap
+    it raises EngineError with net_pagerank's message."""
+    import torch
+    from . import EngineError
+    tol = tol if tol > 0 else 1e-12
+    max_iter = int(max_iter) if max_iter > 0 else 10000
+    if shard.n == 0:
+        return 0
+    world = dist.get_world_size() if dist is not None else 1
+    L = shard.payload_len
+    send = torch.empty(L, dtype=torch.float64, device=device)
+    recv = send if dist is None else torch.empty(world * L, dtype=torch.float64, device=device)
+    for sweep in range(1, max_iter + 1):
+        shard.sweep(send)
+        if dist is not None:
+            all_gather_flat(dist, recv, send)
+        if shard.finish(recv) <= tol:
+            return sweep
+    raise EngineError(f"PageRank did not converge to tolerance {tol:f} within {max_iter} "
+                      "iterations")

@@ -135,6 +135,22 @@ static int run_cpu(void) {
         "net_projected_eigen of order 0 does nothing");
   check(net_set_tuning(99, 0.0) != 0 && net_set_tuning(17, -1.0) != 0,
         "net_set_tuning rejects unknown keys and values");
+  int64_t bounds[3] = {0, 1, 2}, plen = 0;
+  NetShard *sh = NULL;
+  check(net_shard_bounds(NULL, 1, 0, 0, 2, bounds, err, sizeof err) != 0 &&
+            strstr(err, "graph handle is null") != NULL,
+        "net_shard_bounds on NULL");
+  check(net_shard_new(NULL, 0.85, 1, 0, NULL, 0, 0, bounds, 2, 0, &sh, &plen, err,
+                      sizeof err) != 0 && sh == NULL,
+        "net_shard_new on NULL");
+  check(net_shard_sweep(NULL, out, NULL, err, sizeof err) != 0 &&
+            strstr(err, "shard handle is null") != NULL,
+        "net_shard_sweep on NULL");
+  check(net_shard_finish(NULL, out, &value, NULL, err, sizeof err) != 0,
+        "net_shard_finish on NULL");
+  check(net_shard_scores(NULL, out, 0, NULL, err, sizeof err) != 0, "net_shard_scores on NULL");
+  check(net_shard_restart(NULL, NULL, err, sizeof err) != 0, "net_shard_restart on NULL");
+  net_shard_free(NULL);
   /* a message is cut to the buffer and NUL-terminated */
   char tiny[5];
   memset(tiny, 'x', sizeof tiny);
