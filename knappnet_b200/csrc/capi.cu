@@ -1464,13 +1464,10 @@ int32_t net_shard_finish(NetShard* shard, const double* d_gathered, double* chan
 int32_t net_shard_scores(const NetShard* shard, double* out, int32_t out_on_device, void* stream,
                          char* err, size_t err_len) {
   return guard(err, err_len, [&] {
-    const knb::Shard& sh = shard_of(shard);
+    knb::Shard& sh = shard_of(shard);
     if (sh.n == 0) return;
     if (!out) throw Error("the output buffer is null");
-    cudaStream_t s = shard_stream(stream);
-    KNB_CUDA(cudaMemcpyAsync(out, sh.x.get(), (size_t)sh.n * 8,
-                             out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaStreamSynchronize(s));
+    knb::shard_scores(sh, out, out_on_device != 0, shard_stream(stream));
   });
 }
 

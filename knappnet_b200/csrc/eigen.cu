@@ -1381,15 +1381,15 @@ constexpr uint32_t EIG_TILE = 32u * EIG_IPT;     // merge items per warp tile
 // One product with epilogue e: merge-path warp tiles (warp_spmv) on a
 // persistent grid of the CTAs that fit at once, then split_rows for the rows
 // that cross tiles (and the epilogue's scalars, if any).
-template <class VT, class MT, class Epi>
+template <class VT, class MT, class Epi, int IPT = EIG_IPT>
 static void eig_product(const OpView<MT>& v, const VT* x, const Epi& e, const Partition& P,
                         VT* carry, VT* head, double* part1, double* part2, const IterState* st,
                         cudaStream_t s) {
-  constexpr size_t smem = warp_smem_bytes<VT, EIG_IPT, EIG_WPB>();
-  auto fnp = warp_spmv<VT, MT, Epi, EIG_IPT, EIG_WPB, 0>;
+  constexpr size_t smem = warp_smem_bytes<VT, IPT, EIG_WPB>();
+  auto fnp = warp_spmv<VT, MT, Epi, IPT, EIG_WPB, 0>;
   set_func_attr((const void*)fnp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   set_func_attr((const void*)fnp, cudaFuncAttributePreferredSharedMemoryCarveout,
-                warp_fit_carveout<VT, EIG_IPT, EIG_WPB>());
+                warp_fit_carveout<VT, IPT, EIG_WPB>());
   static std::mutex mu;
   static std::map<int, unsigned> cap_by_dev;  // CTAs that fit at once, per device
   int dev = 0;
@@ -1415,8 +1415,11 @@ static void eig_product(const OpView<MT>& v, const VT* x, const Epi& e, const Pa
                                                           const_cast<IterState*>(st));
 }
 // FP64 products for row shards of PageRank (shard.cu): the same warp tiles
-// and split-row pass over a view whose offsets start at 0.
-uint32_t product_tile() { return EIG_TILE; }
+// and split-row pass over a view whose offsets start at 0, with 4 items per
+// lane (3 CTAs of 16 warps fit on an SM; 1 with 8 FP64 items), as the
+// single-graph FP64 sweeps.
+constexpr int SHARD_IPT = 4;
+uint32_t product_tile() { return 32u * SHARD_IPT; }
 
 void product64(const OpView<double>& v, const Partition& P, const double* x, double* y,
                ProductScratch& sc, cudaStream_t s) {
@@ -1427,8 +1430,8 @@ void product64(const OpView<double>& v, const Partition& P, const double* x, dou
     sc.part2.alloc(SPLIT_CTAS * 2 + 2);
   }
   PlainEpi<double> e{y};
-  eig_product<double, double>(v, x, e, P, sc.carry.get(), sc.head.get(), sc.part1.get(),
-                              sc.part2.get(), nullptr, s);
+  eig_product<double, double, PlainEpi<double>, SHARD_IPT>(
+      v, x, e, P, sc.carry.get(), sc.head.get(), sc.part1.get(), sc.part2.get(), nullptr, s);
   KNB_LAUNCH("shard product");
 }
 

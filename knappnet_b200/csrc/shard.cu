@@ -10,6 +10,7 @@ namespace {
 constexpr int SH_THREADS = 256;
 constexpr unsigned SH_GRID_CAP = 1184;  // 8 CTAs of 256 per SM
 constexpr int SH_MAX_PARTS = 1024;
+constexpr uint32_t SH_UNROLL = 4;  // elements a thread loads at once in shard_finish
 
 // One thread per boundary: the first row r with r + off[r] >= k (n + nnz) /
 // parts (r + off[r] grows strictly with r, and is n + nnz at r = n).
@@ -33,6 +34,21 @@ __global__ void shard_rebase(const uint32_t* __restrict__ off, uint32_t r0, uint
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= rows;
        i += gridDim.x * blockDim.x)
     out[i] = off[r0 + i] - base;
+}
+
+// dst[i] = src[perm[base + i]] for i < count.
+__global__ void shard_gather(const double* __restrict__ src, const uint32_t* __restrict__ perm,
+                             uint32_t base, uint32_t count, double* __restrict__ dst) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += gridDim.x * blockDim.x)
+    dst[i] = src[perm[base + i]];
+}
+
+// dst[perm[k]] = src[k] for k < n (back to node order).
+__global__ void shard_scatter(const double* __restrict__ src, const uint32_t* __restrict__ perm,
+                              uint32_t n, double* __restrict__ dst) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    dst[perm[k]] = src[k];
 }
 
 __device__ __forceinline__ bool shard_last(unsigned int* ticket) {
@@ -104,27 +120,50 @@ shard_finish_kernel(const double* __restrict__ g, size_t L, const int64_t* __res
     total = t;
   }
   __syncthreads();
+  // A thread visits i = t, t + stride, ... in that order, SH_UNROLL at a
+  // time: all their loads first, so that the divisions (whose rare slow path
+  // is a branch) do not hold each load back behind the previous one.
+  const uint32_t stride = gridDim.x * blockDim.x;
   double ch = 0, dg = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double xn = inv_n;
-    if (g) {
-      // the last rank whose range starts at or before i owns it (ranges
-      // are contiguous and may be empty)
-      int lo = 0, hi = parts - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (sb[mid] <= (int64_t)i) lo = mid; else hi = mid - 1;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += SH_UNROLL * stride) {
+    double gv[SH_UNROLL], xv[SH_UNROLL], ov[SH_UNROLL];
+#pragma unroll
+    for (int u = 0; u < SH_UNROLL; ++u) {
+      const uint32_t i = i0 + u * stride;
+      gv[u] = inv_n;
+      xv[u] = 0.0;
+      ov[u] = 0.0;
+      if (i < n) {
+        if (g) {
+          // the last rank whose range starts at or before i owns it
+          // (ranges are contiguous and may be empty)
+          int lo = 0, hi = parts - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (sb[mid] <= (int64_t)i) lo = mid; else hi = mid - 1;
+          }
+          gv[u] = g[(size_t)lo * L + (size_t)((int64_t)i - sb[lo])];
+          xv[u] = x[i];
+        }
+        ov[u] = out[i];
       }
-      xn = g[(size_t)lo * L + (size_t)((int64_t)i - sb[lo])] / total;
-      ch += fabs(xn - x[i]);
     }
-    x[i] = xn;
-    const double o = out[i];
-    if (o > 0.0) {
-      z[i] = xn / o;
-    } else {
-      z[i] = 0.0;
-      dg += xn;
+#pragma unroll
+    for (int u = 0; u < SH_UNROLL; ++u) {
+      const uint32_t i = i0 + u * stride;
+      if (i >= n) break;
+      double xn = inv_n;
+      if (g) {
+        xn = gv[u] / total;
+        ch += fabs(xn - xv[u]);
+      }
+      x[i] = xn;
+      if (ov[u] > 0.0) {
+        z[i] = xn / ov[u];
+      } else {
+        z[i] = 0.0;
+        dg += xn;
+      }
     }
   }
   ch = block_sum(ch, sh);
@@ -146,7 +185,7 @@ shard_finish_kernel(const double* __restrict__ g, size_t L, const int64_t* __res
 void launch_finish(Shard& sh, const double* g, cudaStream_t s) {
   const unsigned gv = grid_for(sh.n, SH_THREADS, SH_GRID_CAP);
   shard_finish_kernel<<<gv, SH_THREADS, 0, s>>>(g, sh.payload_len, sh.dbounds.get(), sh.parts,
-                                               sh.n, sh.x.get(), sh.z.get(), sh.op->colsum.get(),
+                                               sh.n, sh.x.get(), sh.z.get(), sh.out.get(),
                                                1.0 / (double)sh.n, sh.part_all.get(),
                                                sh.st.get());
   KNB_LAUNCH("shard_finish");
@@ -158,14 +197,15 @@ Shard::~Shard() {
   if (hst) cudaFreeHost(hst);
 }
 
-std::vector<int64_t> shard_bounds(const Operator& op, int parts, cudaStream_t s) {
+std::vector<int64_t> shard_bounds(Operator& op, int parts, cudaStream_t s) {
   if (parts < 1 || parts > SH_MAX_PARTS)
     throw Error("the number of shards must be between 1 and " + std::to_string(SH_MAX_PARTS));
   std::vector<int64_t> h((size_t)parts + 1, 0);
   if (op.n == 0) return h;
+  const Relabeled& R = op.relabeled(s);
   DevBuf<int64_t> d((size_t)parts + 1);
   shard_bounds_kernel<<<grid_for((uint64_t)parts + 1, 256), 256, 0, s>>>(
-      op.rows->off.get(), op.n, op.nnz, parts, d.get());
+      R.off.get(), op.n, op.nnz, parts, d.get());
   KNB_LAUNCH("shard_bounds");
   KNB_CUDA(cudaMemcpyAsync(h.data(), d.get(), h.size() * 8, cudaMemcpyDeviceToHost, s));
   KNB_CUDA(cudaStreamSynchronize(s));
@@ -208,12 +248,20 @@ std::unique_ptr<Shard> shard_new(Operator& op, double damping, const double* d_p
                            cudaMemcpyHostToDevice, s));
   sh->off.alloc((size_t)rows + 1);
   uint32_t o[2] = {0, 0};
+  sh->x.alloc(std::max<uint32_t>(sh->n, 1));
+  sh->z.alloc(std::max<uint32_t>(sh->n, 1));
+  sh->out.alloc(std::max<uint32_t>(sh->n, 1));
   if (sh->n > 0) {
-    shard_rebase<<<grid_for((uint64_t)rows + 1, 256), 256, 0, s>>>(op.rows->off.get(), sh->r0,
-                                                                 rows, sh->off.get());
+    sh->rl = &op.relabeled(s);
+    const uint32_t* roff = sh->rl->off.get();
+    shard_rebase<<<grid_for((uint64_t)rows + 1, 256), 256, 0, s>>>(roff, sh->r0, rows,
+                                                                 sh->off.get());
     KNB_LAUNCH("shard_rebase");
-    KNB_CUDA(cudaMemcpyAsync(&o[0], op.rows->off.get() + sh->r0, 4, cudaMemcpyDeviceToHost, s));
-    KNB_CUDA(cudaMemcpyAsync(&o[1], op.rows->off.get() + sh->r1, 4, cudaMemcpyDeviceToHost, s));
+    shard_gather<<<grid_for(sh->n, 256), 256, 0, s>>>(op.colsum.get(), sh->rl->perm.get(), 0,
+                                                      sh->n, sh->out.get());
+    KNB_LAUNCH("shard_gather");
+    KNB_CUDA(cudaMemcpyAsync(&o[0], roff + sh->r0, 4, cudaMemcpyDeviceToHost, s));
+    KNB_CUDA(cudaMemcpyAsync(&o[1], roff + sh->r1, 4, cudaMemcpyDeviceToHost, s));
   }
   KNB_CUDA(cudaStreamSynchronize(s));
   sh->arc0 = o[0];
@@ -221,12 +269,12 @@ std::unique_ptr<Shard> shard_new(Operator& op, double damping, const double* d_p
   if (rows > 0) sh->part = build_partition(rows, sh->arcs, sh->off.get(), product_tile(), s);
   if (d_pers) {
     sh->p.alloc(std::max<uint32_t>(rows, 1));
-    if (rows > 0)
-      KNB_CUDA(cudaMemcpyAsync(sh->p.get(), d_pers + sh->r0, (size_t)rows * 8,
-                               cudaMemcpyDeviceToDevice, s));
+    if (rows > 0) {
+      shard_gather<<<grid_for(rows, 256), 256, 0, s>>>(d_pers, sh->rl->perm.get(), sh->r0, rows,
+                                                       sh->p.get());
+      KNB_LAUNCH("shard_gather");
+    }
   }
-  sh->x.alloc(std::max<uint32_t>(sh->n, 1));
-  sh->z.alloc(std::max<uint32_t>(sh->n, 1));
   sh->part_rows.alloc((size_t)grid_for(std::max<uint32_t>(rows, 1), SH_THREADS, SH_GRID_CAP) + 8);
   sh->part_all.alloc((size_t)grid_for(std::max<uint32_t>(sh->n, 1), SH_THREADS, SH_GRID_CAP) * 2 +
                      8);
@@ -242,8 +290,8 @@ void shard_sweep(Shard& sh, double* d_payload, cudaStream_t s) {
   const uint32_t rows = sh.r1 - sh.r0;
   if (rows > 0) {
     const Operator& op = *sh.op;
-    const OpView<double> v{rows, sh.arcs, sh.off.get(), op.rows->tgt.get() + sh.arc0,
-                           op.has_vals ? op.vals64.get() + sh.arc0 : nullptr};
+    const OpView<double> v{rows, sh.arcs, sh.off.get(), sh.rl->cols.get() + sh.arc0,
+                           op.has_vals ? sh.rl->vals64.get() + sh.arc0 : nullptr};
     product64(v, *sh.part, sh.z.get(), d_payload, sh.scratch, s);
   }
   const unsigned gr = grid_for(std::max<uint32_t>(rows, 1), SH_THREADS, SH_GRID_CAP);
@@ -252,6 +300,20 @@ void shard_sweep(Shard& sh, double* d_payload, cudaStream_t s) {
                                          1.0 / (double)std::max<uint32_t>(sh.n, 1),
                                          sh.part_rows.get(), sh.st.get());
   KNB_LAUNCH("shard_update");
+}
+
+void shard_scores(Shard& sh, double* out, bool out_on_device, cudaStream_t s) {
+  if (sh.n == 0) return;
+  double* dst = out;
+  if (!out_on_device) {
+    if (!sh.scores.p) sh.scores.alloc(sh.n);
+    dst = sh.scores.get();
+  }
+  shard_scatter<<<grid_for(sh.n, 256), 256, 0, s>>>(sh.x.get(), sh.rl->perm.get(), sh.n, dst);
+  KNB_LAUNCH("shard_scatter");
+  if (!out_on_device)
+    KNB_CUDA(cudaMemcpyAsync(out, dst, (size_t)sh.n * 8, cudaMemcpyDeviceToHost, s));
+  KNB_CUDA(cudaStreamSynchronize(s));
 }
 
 void shard_restart(Shard& sh, cudaStream_t s) {

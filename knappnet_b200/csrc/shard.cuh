@@ -29,13 +29,19 @@ struct ShardState {
   unsigned int pad;
 };
 
-// parts + 1 row boundaries 0 = b_0 <= ... <= b_parts = n of operator `op`:
-// b_k is the first row r with r + off[r] >= k (n + nnz) / parts, so each
-// range holds about an equal share of rows plus arcs.
-std::vector<int64_t> shard_bounds(const Operator& op, int parts, cudaStream_t s);
+// Shards hold ranges of the operator's rows renumbered by column count
+// (Operator::relabeled: the values a sweep gathers most sit together, and
+// each row keeps its arcs in order, so its sum is the same); iterates are in
+// that numbering, and scores go back to node order when read.
+//
+// parts + 1 boundaries 0 = b_0 <= ... <= b_parts = n of those rows: b_k is
+// the first row r with r + off[r] >= k (n + nnz) / parts, so each range
+// holds about an equal share of rows plus arcs.
+std::vector<int64_t> shard_bounds(Operator& op, int parts, cudaStream_t s);
 
 struct Shard {
   Operator* op = nullptr;
+  const Relabeled* rl = nullptr;  // the renumbered rows (null for n = 0)
   uint32_t n = 0, r0 = 0, r1 = 0;
   uint64_t arc0 = 0;        // the first row's first arc
   uint64_t arcs = 0;        // arcs of the shard's rows
@@ -51,6 +57,8 @@ struct Shard {
   ProductScratch scratch;
   DevBuf<double> p;         // personalization of the shard's rows
   DevBuf<double> x, z;      // current iterate and x / out, all n nodes
+  DevBuf<double> out;       // out-strengths in the renumbered order
+  DevBuf<double> scores;    // the iterate in node order (shard_scores)
   DevBuf<double> part_rows, part_all;  // block partials
   DevBuf<ShardState> st;
   ShardState* hst = nullptr;  // pinned
@@ -67,6 +75,8 @@ std::unique_ptr<Shard> shard_new(Operator& op, double damping, const double* d_p
 void shard_sweep(Shard& sh, double* d_payload, cudaStream_t s);
 // Back to the uniform iterate (x = 1/n), as after shard_new.
 void shard_restart(Shard& sh, cudaStream_t s);
+// The current iterate in node order into out (n doubles, device or host).
+void shard_scores(Shard& sh, double* out, bool out_on_device, cudaStream_t s);
 // Step 3 from d_gathered (parts * payload_len doubles, rank order); returns
 // the change (waits for the stream).
 double shard_finish(Shard& sh, const double* d_gathered, cudaStream_t s);
