@@ -29,13 +29,15 @@ With --impl reference the reference arm runs instead: the CPU restatement
 reference's net_pagerank (per-call set-up and every iteration) on the same
 graph, generated by the oracle's own generators.
 
-Multi-GPU (torchrun, one process per GPU): independent replicas of the same
-solve (PageRank on one graph does not shard without an all-gather of the
-iterate every iteration); value is the arcs all ranks processed per
-iteration-second, timed as the maximum over ranks. The batched (c4a) and
-packed-graph (c4b) workloads shard with no exchange: under torchrun each
-rank solves its contiguous share of teleport vectors or graphs, the slowest
-rank's device time is reported, and the scores are gathered on rank 0.
+Multi-GPU (torchrun, one process per GPU): this line runs independent
+replicas of the same solve; value is the arcs all ranks processed per
+iteration-second, timed as the maximum over ranks. `--workload rows` splits
+one solve of the same graph by rows instead (net_shard_*: each rank sweeps
+its rows, one NCCL all-gather of the payloads per sweep, every rank finishes
+the sweep over all nodes). The batched (c4a) and packed-graph (c4b)
+workloads shard with no exchange: under torchrun each rank solves its
+contiguous share of teleport vectors or graphs, the slowest rank's device
+time is reported, and the scores are gathered on rank 0.
 """
 from __future__ import annotations
 

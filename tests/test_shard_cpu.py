@@ -1,8 +1,8 @@
-"""The row split of one graph's PageRank on CPU: two gloo ranks run
+"""The row split of one graph's PageRank on CPU: two and three gloo ranks run
 ranks.pagerank_rows, the driver every GPU rank runs, with a numpy shard that
 keeps the C ABI's payload contract (net_shard_sweep / net_shard_finish: the
 rank's unnormalised rows, zero padding, its partial sum in the last slot;
-the finish over all nodes from the payloads gathered in rank order). Both
+the finish over all nodes from the payloads gathered in rank order). All
 ranks must end with the same scores on the same sweep, and those must be
 the oracle's PageRank (crates/engine/src/metrics/spectral.rs:247-280)."""
 from __future__ import annotations
@@ -98,20 +98,22 @@ def _worker(rank, world, port, queue):
     dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_split_pagerank_by_rows():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_split_pagerank_by_rows(world):
     mp = pytest.importorskip("torch.multiprocessing")
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     res = sorted((q.get(timeout=120) for _ in procs), key=lambda x: x[0])
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (_, s0, x0), (_, s1, x1) = res
-    assert s0 == s1 and x0 == x1  # the same stopping sweep and iterate on both ranks
+    s0, x0 = res[0][1], res[0][2]
+    for _, s, x in res[1:]:
+        assert s == s0 and x == x0  # the same stopping sweep and iterate on every rank
     n, src, tgt, w = _graph()
     og = O.Graph(n, src, tgt, w, True)
     ref = og.pagerank(directed=True, weighted=True, tol=1e-12)
