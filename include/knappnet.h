@@ -496,8 +496,9 @@ NET_API int32_t net_pagerank_csr_static(int64_t n, const uint32_t *d_offsets,
  * the current iterate (n doubles) to host or device memory;
  * net_shard_restart returns the shard to the uniform iterate. The shard
  * lives on the current device and reads the graph's arrays, so the graph
- * must outlive it; its calls run on `stream` (NULL: the default stream) and
- * one shard must not be used by two threads at once.
+ * must outlive it; its calls run on `stream` (NULL: the default stream),
+ * which must order them (the sweep reads what the previous finish wrote),
+ * and one shard must not be used by two threads at once.
  * The boundaries must not decrease and parts is at most 1024. */
 typedef struct NetShard NetShard;
 NET_API int32_t net_shard_bounds(const GraphHandle *h, int32_t directed,

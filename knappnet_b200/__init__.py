@@ -488,8 +488,17 @@ def _stream_ptr(t):
     return None
 
 
-def _dev_ptr(t):
-    return ctypes.c_void_p(t if isinstance(t, int) else t.data_ptr())
+def _dev_ptr(t, count=None):
+    """A device pointer from a raw address or a CUDA tensor; a tensor must
+    be contiguous float64 on a GPU and hold at least `count` values."""
+    if isinstance(t, int):
+        return ctypes.c_void_p(t)
+    import torch
+    if not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+        raise ValueError("the buffer must be a contiguous float64 CUDA tensor")
+    if count is not None and t.numel() < count:
+        raise ValueError(f"the buffer holds {t.numel()} values; {count} are needed")
+    return ctypes.c_void_p(t.data_ptr())
 
 
 class Shard:
@@ -519,14 +528,15 @@ class Shard:
 
     def sweep(self, payload):
         err = ctypes.create_string_buffer(ERR_LEN)
-        _check(lib().net_shard_sweep(self.h, _dev_ptr(payload), _stream_ptr(payload), err,
-                                     ERR_LEN), err)
+        _check(lib().net_shard_sweep(self.h, _dev_ptr(payload, self.payload_len),
+                                     _stream_ptr(payload), err, ERR_LEN), err)
 
     def finish(self, gathered) -> float:
         change = ctypes.c_double()
         err = ctypes.create_string_buffer(ERR_LEN)
-        _check(lib().net_shard_finish(self.h, _dev_ptr(gathered), ctypes.byref(change),
-                                      _stream_ptr(gathered), err, ERR_LEN), err)
+        _check(lib().net_shard_finish(self.h, _dev_ptr(gathered, self.parts * self.payload_len),
+                                      ctypes.byref(change), _stream_ptr(gathered), err,
+                                      ERR_LEN), err)
         return change.value
 
     def restart(self, like=None):
@@ -543,8 +553,8 @@ class Shard:
 
     def scores_device(self, out):
         err = ctypes.create_string_buffer(ERR_LEN)
-        _check(lib().net_shard_scores(self.h, _dev_ptr(out), 1, _stream_ptr(out), err, ERR_LEN),
-               err)
+        _check(lib().net_shard_scores(self.h, _dev_ptr(out, self.n), 1, _stream_ptr(out), err,
+                                      ERR_LEN), err)
 
     def close(self):
         if getattr(self, "h", None) is not None and _lib is not None:

@@ -143,3 +143,13 @@ def test_bounds_balance_rows_plus_arcs(parts):
     indeg = np.bincount(tgt, minlength=n)
     load = [int(b[k + 1] - b[k] + indeg[b[k]:b[k + 1]].sum()) for k in range(parts)]
     assert max(load) - min(load) <= 2 * (indeg.max() + 1)
+
+
+def test_shard_buffers_are_checked_before_any_device_call():
+    torch = pytest.importorskip("torch")
+    import knappnet_b200 as K
+    with pytest.raises(ValueError, match="contiguous float64 CUDA tensor"):
+        K._dev_ptr(torch.zeros(4, dtype=torch.float64), 4)
+    with pytest.raises(ValueError, match="contiguous float64 CUDA tensor"):
+        K._dev_ptr(torch.zeros(4, dtype=torch.float32), 4)
+    assert K._dev_ptr(1 << 20).value == 1 << 20  # a raw device address passes through
